@@ -1,0 +1,222 @@
+/*
+ * pm7_b200.h — C ABI of the B200 PM7/NDDO molecular SCF engine.
+ *
+ * This boundary replaces the Rust entry point of pm7-rs
+ *
+ *     pub fn run_pm7(molecule: &Molecule, params: &Pm7Parameters,
+ *                    options: &Pm7Options) -> Result<Pm7Result>        (src/scf.rs:512-522)
+ *
+ * with plain pointers and sizes: no Rust or torch types cross it. A Rust
+ * host binds it with a small `extern "C"` block (cgo/JNI/ctypes work the
+ * same way). All compute behind `pm7_run` runs on one CUDA device; the
+ * library has no CPU fallback and returns PM7_ERR_CUDA when no device is
+ * usable.
+ *
+ * Units follow the reference: positions in Bohr, energies in eV, heat of
+ * formation in kcal/mol, dipoles in Debye. Dense matrices are row-major
+ * nao x nao doubles. MO coefficients are stored with orbitals as COLUMNS,
+ * exactly like the reference's `mo_coeff` Matrix (A = V diag(e) V^T).
+ */
+#ifndef PM7_B200_H
+#define PM7_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes. One per `Pm7Error` variant (src/error.rs:8-30) plus the two
+ * device-side failures this engine adds. */
+typedef enum pm7_status {
+  PM7_OK = 0,
+  PM7_ERR_INVALID_INPUT = 1,      /* Pm7Error::InvalidInput / Parse      */
+  PM7_ERR_MISSING_ELEMENT = 2,    /* Pm7Error::MissingElement(z)         */
+  PM7_ERR_MISSING_PARAMETER = 3,  /* Pm7Error::MissingParameter          */
+  PM7_ERR_UNSUPPORTED = 4,        /* Pm7Error::UnsupportedFeature        */
+  PM7_ERR_LINEAR_ALGEBRA = 5,     /* Pm7Error::LinearAlgebra             */
+  PM7_ERR_SCF_NOT_CONVERGED = 6,  /* Pm7Error::ScfNotConverged           */
+  PM7_ERR_RESPONSE_FAILED = 7,    /* Pm7Error::ResponseFailed            */
+  PM7_ERR_INSUFFICIENT_MEMORY = 8,/* Pm7Error::InsufficientMemory        */
+  PM7_ERR_CUDA = 9,               /* CUDA runtime / library failure      */
+  PM7_ERR_TIMEOUT = 10            /* a bounded device wait gave up       */
+} pm7_status;
+
+/* PM7 family (src/method.rs:8-15). */
+typedef enum pm7_method {
+  PM7_METHOD_PM7 = 0,
+  PM7_METHOD_PM7_TS = 1,
+  PM7_METHOD_PM7_SPARKLE = 2,
+  PM7_METHOD_PM7_MINUS = 3,
+  PM7_METHOD_PM7_HH = 4
+} pm7_method;
+
+/* SCF accelerator (src/scf.rs:25-34). */
+typedef enum pm7_accelerator {
+  PM7_ACCEL_NONE = 0,
+  PM7_ACCEL_CDIIS = 1,
+  PM7_ACCEL_ADIIS_CDIIS = 2
+} pm7_accelerator;
+
+/* Spin treatment (src/scf.rs:38-47). */
+typedef enum pm7_reference {
+  PM7_REF_AUTO = 0,
+  PM7_REF_RESTRICTED = 1,
+  PM7_REF_UNRESTRICTED = 2
+} pm7_reference;
+
+/* Dipole origin for charged molecules (src/dipole.rs DipoleOrigin). */
+typedef enum pm7_dipole_origin {
+  PM7_DIPOLE_COORDINATES = 0,
+  PM7_DIPOLE_CENTRE_OF_MASS = 1,
+  PM7_DIPOLE_CENTRE_OF_CHARGE = 2
+} pm7_dipole_origin;
+
+/* Arithmetic of the SCF cycles. FP64 is the plain path; MIXED runs the early
+ * cycles in FP32 (Fock build and density on tensor cores with FP32
+ * accumulation) and re-converges in FP64 (engine knob; no reference analogue). */
+typedef enum pm7_precision {
+  PM7_PRECISION_FP64 = 0,
+  PM7_PRECISION_MIXED = 1
+} pm7_precision;
+
+/* `Molecule` (src/system.rs:21-39): atomic numbers and positions in Bohr.
+ * The net charge is NOT read from here: like the reference, `run_pm7` takes
+ * charge and multiplicity from the options (src/scf.rs:588-607). */
+typedef struct pm7_molecule {
+  int32_t n_atoms;
+  const uint8_t *z;        /* n_atoms atomic numbers                */
+  const double *xyz_bohr;  /* 3*n_atoms, x0 y0 z0 x1 ...            */
+} pm7_molecule;
+
+/* `Pm7Options` molecular fields (src/scf.rs:73-188), defaults at
+ * src/scf.rs:207-233 via pm7_options_default(). Periodic, field and
+ * stability options of the reference are outside this engine's scope. */
+typedef struct pm7_options {
+  int32_t method;             /* pm7_method, must equal the parameter set's */
+  double charge;
+  int32_t multiplicity;
+  int32_t max_scf;            /* 200    */
+  double e_tol;               /* 1e-8 eV */
+  double p_tol;               /* 1e-7   */
+  int32_t use_diis;           /* 1      */
+  int32_t accelerator;        /* pm7_accelerator, ADIIS_CDIIS */
+  double adiis_switch;        /* 0.1    */
+  double level_shift;         /* 0.0 eV */
+  int32_t reference;          /* pm7_reference, AUTO */
+  int32_t force_dpath;        /* 0      */
+  int32_t smooth_dispersion;  /* 0      */
+  int64_t max_memory_mb;      /* <0: no explicit budget (PM7_MEM_BUDGET_MB, then device memory) */
+  int32_t dipole_origin;      /* pm7_dipole_origin, CENTRE_OF_MASS */
+  const double *initial_density;      /* NULL or nao*nao */
+  const double *initial_spin_density; /* NULL or nao*nao (UHF only) */
+  /* engine knobs (no reference analogue) */
+  int32_t precision;          /* pm7_precision, FP64 */
+  int32_t device;             /* CUDA device ordinal, 0 */
+  int32_t want_matrices;      /* 1: fill density/mo arrays in the result */
+} pm7_options;
+
+/* `Pm7Result` molecular fields (src/scf.rs:261-342). Arrays are owned by the
+ * library and released by pm7_result_free(). Absent optionals are NaN
+ * (scalars) or NULL (arrays). */
+typedef struct pm7_result {
+  int32_t n_atoms;
+  int32_t nao;
+  int32_t n_occ;
+  int32_t n_occ_beta;        /* -1 for RHF */
+  int32_t unrestricted;
+  int32_t iterations;
+  int32_t converged;
+  double density_error;
+  double electronic_ev;
+  double core_ev;
+  double total_ev;
+  double heat_of_formation_kcal;
+  double correction_kcal;    /* dispersion + H-bond + MM terms inside total/dHf */
+  double homo_ev, lumo_ev, homo_ev_beta, lumo_ev_beta;
+  double dipole_debye[3];
+  double dipole_magnitude;
+  double dipole_point_charge[3];
+  double dipole_sp_hybrid[3];
+  double dipole_pd_hybrid[3];
+  double *charges;            /* n_atoms Mulliken net charges */
+  double *density;            /* nao*nao total density           (want_matrices) */
+  double *spin_density;       /* nao*nao P_alpha - P_beta, UHF   (want_matrices) */
+  double *mo_energies;        /* nao, alpha (or spatial) set, ascending */
+  double *mo_coeff;           /* nao*nao, columns are orbitals   (want_matrices) */
+  double *mo_energies_beta;   /* nao, UHF */
+  double *mo_coeff_beta;      /* nao*nao, UHF                    (want_matrices) */
+  /* engine diagnostics */
+  double device_ms;           /* wall time of the device SCF, ms */
+  int32_t fp32_iterations;    /* cycles run in FP32 (MIXED) */
+} pm7_result;
+
+/* Opaque parameter set (`Pm7Parameters`, src/params.rs:104-111), parsed and
+ * derived once per method and cached for the process like the reference's
+ * OnceLock (src/params.rs:139-155). */
+typedef struct pm7_params pm7_params;
+
+/* Replaces `Pm7Parameters::method` (src/params.rs:127-129). The returned
+ * pointer is process-global and must not be freed. */
+pm7_status pm7_params_load(int32_t method, const pm7_params **out);
+
+/* Fill `Pm7Options::default()` (src/scf.rs:207-233). */
+void pm7_options_default(pm7_options *options);
+
+/* Replaces `run_pm7` (src/scf.rs:512-522). On PM7_OK `*result` is filled and
+ * must be released with pm7_result_free(). A non-converged SCF returns
+ * PM7_ERR_SCF_NOT_CONVERGED with only `iterations` and `density_error` set,
+ * mirroring the reference's error-with-no-result (src/scf.rs:770-775). */
+pm7_status pm7_run(const pm7_molecule *molecule, const pm7_params *params,
+                   const pm7_options *options, pm7_result *result);
+
+/* Release the arrays of a result filled by pm7_run (or the engine). */
+void pm7_result_free(pm7_result *result);
+
+/* Message of the last error on the calling thread (`Pm7Error` Display,
+ * src/error.rs:32-60). Never NULL. */
+const char *pm7_last_error_message(void);
+
+/* Number of CUDA devices the library can see (0 when none). */
+int32_t pm7_device_count(void);
+
+/* ---------------------------------------------------------------------
+ * Stage entry points: each runs one stage of the device pipeline for one
+ * molecule and copies the result to host memory. They exist so the stages
+ * can be checked one by one against the reference's own functions.
+ * ------------------------------------------------------------------- */
+
+/* The core Hamiltonian H_core (`build_core_generic`, src/hamiltonian.rs:310-638),
+ * nao*nao row-major into h_out. *nao_out receives nao. */
+pm7_status pm7_stage_core_hamiltonian(const pm7_molecule *molecule, const pm7_params *params,
+                                      int32_t force_dpath, double *h_out, int32_t *nao_out);
+
+/* The spin Fock matrix F = H + J(P_tot) - K(P_spin)
+ * (`build_fock_spin_x` with no exchange cutoff, src/fock.rs:149-418). */
+pm7_status pm7_stage_fock(const pm7_molecule *molecule, const pm7_params *params,
+                          int32_t force_dpath, const double *p_tot, const double *p_spin,
+                          double *f_out);
+
+/* Per-pair two-centre blocks for atoms (i, j) at displacement d = R_j - R_i
+ * (Bohr): w (npair_i x npair_j), e1b/e2a (9x9) and the overlap (9x9), all in
+ * the i-first orientation (`pair_two_electron_g`, src/integrals.rs:186-271, and
+ * `diatom_overlap`, src/overlap.rs:16-40, or their MNDO/d forms). */
+pm7_status pm7_stage_pair(const pm7_params *params, int32_t z_i, int32_t z_j, const double d[3],
+                          int32_t force_dpath, double *w_out, double *e1b_out, double *e2a_out,
+                          double *s_out, int32_t *npair_i, int32_t *npair_j);
+
+/* Core-core repulsion energy in eV (`core_core_energy`, src/repulsion.rs:16-36). */
+pm7_status pm7_stage_core_core(const pm7_molecule *molecule, const pm7_params *params,
+                               double *energy_ev);
+
+/* Post-SCF corrections in kcal/mol (`correction_energy`, src/scf.rs:907-932):
+ * out[0] dispersion, out[1] H-bond, out[2] C#C, out[3] Si-O-H, out[4] PM7-HH. */
+pm7_status pm7_stage_corrections(const pm7_molecule *molecule, int32_t method,
+                                 int32_t smooth_dispersion, double out[5]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PM7_B200_H */
