@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""PM7 SCF solves/s on one B200 (and N replicas on N GPUs).
+
+Workload (default): plain FP64 RHF single point of a 1,002-atom water cluster (334 H2O on a
+3.1 A cubic grid, seeded random orientations, +-0.1 A centre jitter, 2,004 basis functions),
+synthetic inputs from pm7b200.geometry with seed 0. A step is one complete solve: core
+Hamiltonian, SCF to the reference's default tolerances (e_tol 1e-8 eV, p_tol 1e-7), core-core
+and post-SCF corrections, charges and dipole.
+
+  value  solves/s from the engine's CUDA events over each solve (device time, inputs resident
+         when the first kernel starts)
+  e2e    solves/s from the wall clock around the public C-ABI call `pm7_run` with host input
+         buffers and host result buffers (host<->device copies inside)
+
+One JSON line on rank 0. `--impl reference` times the CPU restatement of the reference's
+`run_pm7` (oracle/, C++ with OpenMP + OpenBLAS) on all host cores instead.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "pm7-rs_b200"))
+
+import numpy as np  # noqa: E402
+
+A0 = 0.529177210903
+
+
+def workload(name):
+    from pm7b200 import geometry as G
+
+    if name == "water334":
+        z, x = G.water_cluster(334, seed=0)
+        desc = "1002-atom water cluster (334 H2O), 2004 basis functions, RHF FP64"
+    elif name == "water1000":
+        z, x = G.water_cluster(1000, seed=0)
+        desc = "3000-atom water cluster (1000 H2O), 6000 basis functions, RHF FP64"
+    elif name == "decane":
+        z, x = G.decane(0)
+        desc = "n-decane C10H22 (32 atoms, 62 basis functions), RHF FP64"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return z, x, desc
+
+
+def nao_of(z):
+    return int(sum(1 if int(v) == 1 else 4 for v in z))
+
+
+def near_w_doubles(z, x):
+    """Sum of npair(u)*npair(v) over atom pairs closer than 7 Angstrom (the stored blocks)."""
+    npair = np.array([1 if int(v) == 1 else 10 for v in z], dtype=np.int64)
+    tot = 0
+    for i in range(len(z)):
+        d = np.linalg.norm(x[i + 1:] - x[i], axis=1) * A0
+        tot += int(np.sum(npair[i] * npair[i + 1:][d < 7.0]))
+    return tot
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, max, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for name, val in zip(names, r[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+def fp64_dgemm_peak(device):
+    """FP64 tensor-core peak measured here: best cuBLAS DGEMM (torch.matmul, float64)."""
+    import torch
+
+    torch.cuda.set_device(device)
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ b
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def read_traffic(kernel):
+    """Per-launch DRAM bytes of `kernel` from a committed ncu summary, scaled to the bench size."""
+    p = ROOT / "profiles" / "traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_sample_full(z, x):
+    """One full oracle solve on all host cores: (seconds, iterations)."""
+    from oracle import harness
+
+    harness.set_threads(os.cpu_count() or 1)
+    t = time.perf_counter()
+    r = harness.run(z, x, want_matrices=0)
+    return time.perf_counter() - t, r["iterations"]
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def allreduce_max(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def run_reference(args, world, rank):
+    """CPU restatement of the reference (oracle/) on the host cores; rank 0 only."""
+    if rank != 0:
+        return
+    from oracle import harness
+
+    z, x, desc = workload(args.workload)
+    cores = os.cpu_count() or 1
+    harness.set_threads(cores)
+    # untimed probe: the iteration count of the complete solve (deterministic for this input)
+    probe_t, n_full = cpu_sample_full(z, x)
+    n_sample = min(3, n_full)
+    for _ in range(args.warmup):
+        harness.sample(z, x, n_sample, want_matrices=0)
+    totals = []
+    for _ in range(args.steps):
+        tb, ti, tp, it = harness.sample(z, x, n_sample, want_matrices=0)
+        per_iter = ti / max(it, 1)
+        totals.append(tb + tp + per_iter * n_full)
+    solve_s = sum(totals) / len(totals)
+    value = 1.0 / solve_s
+    sample = (f"per step: core build + {n_sample} of the {n_full} SCF iterations + post-SCF terms of the {desc}, "
+              f"scaled to one complete solve (untimed full-solve probe: {probe_t:.1f} s)")
+    line = {
+        "impl": "reference", "metric": "PM7 SCF solves/s (RHF single point)", "value": value, "unit": "solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": solve_s * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "description": desc, "seed": 0, "scf_iterations": n_full},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, world, rank, local):
+    from pm7b200 import api
+
+    if api.device_count() < 1:
+        raise SystemExit("no CUDA device visible: the engine has no CPU fallback")
+    z, x, desc = workload(args.workload)
+    n_atoms, nao = len(z), nao_of(z)
+    opts = dict(device=local, want_matrices=0)
+    for _ in range(args.warmup):
+        api.run_pm7(z, x, **opts)
+    peaks = measured_peaks()
+    dgemm = fp64_dgemm_peak(local) if rank == 0 and not args.no_fp64_peak else None
+    barrier(world)
+    sampler = ClockSampler(local)
+    sampler.start()
+    api.profile_enable(True)
+    launches0 = api.launch_count()
+    dev_ms = 0.0
+    results = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r = api.run_pm7(z, x, **opts)
+        dev_ms += r["device_ms"]
+        results.append(r)
+    wall = time.perf_counter() - t0
+    launches = api.launch_count() - launches0
+    prof = api.profile_read()
+    api.profile_enable(False)
+    clocks = sampler.stop()
+    barrier(world)
+    dev_s = allreduce_max(dev_ms * 1e-3, world)
+    wall = allreduce_max(wall, world)
+    if rank != 0:
+        return
+    total = args.steps * world
+    value = total / dev_s
+    e2e = total / wall
+    r0 = results[-1]
+    # dominant kernel of ours and its roofline
+    own = {k: v for k, v in prof.items() if k != "eigensolve"}
+    stages = {k: {"ms_total": round(v[0], 3), "calls": v[1], "ms_avg": round(v[0] / max(v[1], 1), 4)}
+              for k, v in prof.items()}
+    dom = max(own, key=lambda k: own[k][0]) if own else None
+    roofline = None
+    if dom == "commutator_gemm" or dom == "density_gemm":
+        ms, calls = own[dom]
+        avg = ms / calls * 1e-3
+        flops = 2.0 * nao ** 3 if dom == "commutator_gemm" else 1.0 * nao * nao * r0["n_occ"] * 2.0
+        achieved = flops / avg / 1e12
+        roofline = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": dgemm, "unit": "TFLOP/s",
+                    "frac": (achieved / dgemm) if dgemm else None, "traffic": read_traffic(dom),
+                    "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
+                    "algorithmic_per_launch": f"{flops:.4g} flop"}
+    fock_ms, fock_calls = prof.get("fock", (0.0, 0))
+    fock_roof = None
+    if fock_calls:
+        w_near = near_w_doubles(z, x)
+        nbytes = 8.0 * (w_near + 3.0 * nao * nao)
+        achieved_gbs = nbytes / (fock_ms / fock_calls * 1e-3) / 1e9
+        fock_roof = {"kernel": "fock", "bound": "hbm", "achieved": achieved_gbs, "peak": peaks.get("hbm_gbs"),
+                     "unit": "GB/s", "frac": achieved_gbs / peaks.get("hbm_gbs", 6650.0),
+                     "traffic": read_traffic("fock"), "algorithmic_per_launch": f"{nbytes:.4g} B",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+    if roofline is None and dom == "fock":
+        roofline = fock_roof
+    if roofline is None and dom is not None:
+        roofline = {"kernel": dom, "bound": "hbm", "achieved": None, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                    "frac": None, "traffic": None}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        t_cpu, it_cpu = cpu_sample_full(z, x)
+        cpu = {"value": 1.0 / t_cpu, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"one complete oracle solve of the same {desc} ({it_cpu} iterations, {t_cpu:.1f} s)"}
+    h2d = n_atoms * (1 + 24)
+    d2h = 8 * n_atoms + 8 * nao + 8 * 30
+    line = {
+        "metric": "PM7 SCF solves/s (RHF single point)", "value": value, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "description": desc, "seed": 0, "n_atoms": n_atoms, "nao": nao,
+                   "scf_iterations": r0["iterations"], "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (H, F, P and DIIS history are 32 MB each at nao=2004)"},
+        "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "roofline_fock": fock_roof,
+        "stages": stages,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+        "result": {"heat_of_formation_kcal": r0["heat_of_formation_kcal"], "total_ev": r0["total_ev"]},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="water334", choices=["water334", "water1000", "decane"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-peak", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        # CPU only: rank 0 runs, the other ranks exit without joining a process group
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_b200(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

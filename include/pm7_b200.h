@@ -215,6 +215,21 @@ pm7_status pm7_stage_core_core(const pm7_molecule *molecule, const pm7_params *p
 pm7_status pm7_stage_corrections(const pm7_molecule *molecule, int32_t method,
                                  int32_t smooth_dispersion, double out[5]);
 
+/* ---------------------------------------------------------------------
+ * Engine diagnostics (no reference analogue).
+ * ------------------------------------------------------------------- */
+
+/* Number of CUDA kernels this library has launched since the process started. */
+int64_t pm7_launch_count(void);
+
+/* Per-stage device timing with CUDA events on the engine's stream: enable (1) resets
+ * and starts recording, 0 stops. Stages: "build", "fock", "commutator_gemm",
+ * "density_gemm", "eigensolve", "diis_dots", "combine", "corrections". */
+void pm7_profile_enable(int32_t on);
+int32_t pm7_profile_count(void);
+/* Entry i: name, total device milliseconds and number of timed calls. */
+pm7_status pm7_profile_entry(int32_t i, const char **name, double *total_ms, int64_t *calls);
+
 #ifdef __cplusplus
 }
 #endif

@@ -137,6 +137,17 @@ def run(z, xyz_bohr, **options):
         lib().pm7_oracle_result_free(C.byref(r))
 
 
+def sample(z, xyz_bohr, n_iter, **options):
+    """Timed bounded sample: (build s, seconds of n_iter iterations, post-SCF s, iterations)."""
+    L = lib()
+    L.pm7_oracle_sample.argtypes = [C.POINTER(abi.Molecule), C.POINTER(abi.Options), C.c_int, abi.DP]
+    m = _Mol(z, xyz_bohr)
+    o = abi.default_options(**options)
+    out = np.zeros(4)
+    _check(L.pm7_oracle_sample(C.byref(m.s), C.byref(o), int(n_iter), out.ctypes.data_as(abi.DP)))
+    return tuple(out)
+
+
 def core_hamiltonian(z, xyz_bohr, method=0, force_dpath=False):
     m = _Mol(z, xyz_bohr)
     nao = C.c_int()

@@ -1083,6 +1083,36 @@ pm7_status pm7_oracle_pair(int method, int zi, int zj, const double d[3], int fo
   });
 }
 
+// Timed bounded sample of a solve, for the CPU baseline: the core-Hamiltonian build,
+// `n_iter` RHF iterations (no convergence required) and the post-SCF terms.
+// out = {build seconds, seconds of the n_iter iterations, post-SCF seconds, iterations run}.
+pm7_status pm7_oracle_sample(const pm7_molecule *m, const pm7_options *o, int n_iter, double out[4]) {
+  return guarded([&] {
+    Molecule mol = to_molecule(m);
+    const Params &p = params_for(o->method);
+    auto now = [] { return omp_get_wtime(); };
+    double t0 = now();
+    Basis basis = build_basis(mol, p);
+    CoreHamiltonian core = build_core(mol, basis, p, o->force_dpath != 0);
+    double t1 = now();
+    double n_elec = -o->charge;
+    for (int z : mol.z) n_elec += p.element(z).core_charge;
+    int n_occ = (int)std::llround(n_elec) / 2;
+    pm7_options oo = *o;
+    oo.max_scf = n_iter;
+    ScfState st = rhf_loop(mol, basis, p, core, n_occ, oo);
+    double t2 = now();
+    double parts[5];
+    volatile double sink = core_core_energy(mol, p) + correction_energy(mol, oo, parts) + st.electronic_ev;
+    (void)sink;
+    double t3 = now();
+    out[0] = t1 - t0;
+    out[1] = t2 - t1;
+    out[2] = t3 - t2;
+    out[3] = st.iterations;
+  });
+}
+
 pm7_status pm7_oracle_core_core(const pm7_molecule *m, int method, double *e) {
   return guarded([&] { *e = core_core_energy(to_molecule(m), params_for(method)); });
 }

@@ -1,0 +1,47 @@
+// Per-element constants as the kernels read them: one flat record per atomic number,
+// built once per PM7 method on the host (params.cpp) and copied to device memory.
+#pragma once
+
+#include <cstdint>
+
+namespace pm7 {
+
+constexpr double kEv = 27.211386245988;         // eV per Hartree (CODATA 2018)
+constexpr double kA0 = 0.529177210903;          // Bohr radius in Angstrom
+constexpr double kEvToKcal = 23.06054783061903;
+constexpr double kKcalToEv = 1.0 / kEvToKcal;
+constexpr double kAuDipoleToDebye = 2.541746473;
+constexpr int kMaxZ = 110;
+
+struct ElementRec {
+  int32_t present;     // 1 when the method parameterises this element
+  int32_t z, n, n_orb;  // n: principal quantum number of the valence shell
+  int32_t is_sparkle, n_gauss, ios, iop;
+  double core;          // core charge (tore)
+  double u_ss, u_pp, u_dd;
+  double beta_s, beta_p, beta_d;
+  double zeta_s, zeta_p, zeta_d;
+  double g_ss, g_sp, g_pp, g_p2, h_sp;
+  double dd, qq, rho0, rho1, rho2;  // sp multipole separations and additive terms (Bohr)
+  double po[10];        // MNDO/d additive terms, slots 1..9
+  double ddp[7];        // MNDO/d charge separations, slots 2..6
+  double gauss[4][3];   // core Gaussians (K, L, M)
+  double e_isol, eheat_ev, poc;
+  double repd[53];      // MNDO/d one-centre integrals, slots 1..52
+  int32_t onecenter_slot;  // index into the 45x45 one-centre table array, -1 if none
+  int32_t pad_;
+};
+
+struct PairParamRec {
+  double alpb, xfac;
+};
+
+// Everything a kernel needs about the parameter set, in device memory.
+struct DeviceParams {
+  const ElementRec *elements;   // kMaxZ entries
+  const PairParamRec *pairs;    // kMaxZ*kMaxZ, already completed with the diagonal-average rule
+  const double *onecenter;      // n_onecenter * 2025
+  double vpar[61];              // 1-based
+};
+
+}  // namespace pm7

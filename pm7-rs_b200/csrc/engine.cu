@@ -1,0 +1,1362 @@
+// Host runtime of the engine and the C ABI of include/pm7_b200.h.
+//
+// `pm7_run` restates pm7-rs `run_pm7_once` (src/scf.rs:524-867) for molecules: input
+// validation, electron counting, the memory guard, the core Hamiltonian, the RHF/UHF
+// SCF loops (src/scf.rs:1189-1532) with A-DIIS/CDIIS and the stall guard
+// (src/scf.rs:1534-1916), and the reported quantities. All O(n^2) and O(n^3) work runs
+// on the device; the host keeps only the <= 9x9 extrapolation solves and the control flow.
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "kernels.hpp"
+#include "params.hpp"
+#include "pm7_b200.h"
+#include "scf_host.hpp"
+
+namespace pm7 {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+struct Failure {
+  pm7_status code;
+  std::string msg;
+};
+static thread_local std::string g_last_error = "";
+
+#define CUDA_OK(expr)                                                                            \
+  do {                                                                                           \
+    cudaError_t e_ = (expr);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      throw Failure{PM7_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " + \
+                                      __FILE__ + ":" + std::to_string(__LINE__)};                \
+  } while (0)
+#define SOLVER_OK(expr)                                                                           \
+  do {                                                                                            \
+    cusolverStatus_t s_ = (expr);                                                                 \
+    if (s_ != CUSOLVER_STATUS_SUCCESS)                                                            \
+      throw Failure{PM7_ERR_LINEAR_ALGEBRA, "cuSOLVER status " + std::to_string((int)s_) + " at " + \
+                                                std::to_string(__LINE__)};                        \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// diagnostics: launch counter and per-stage CUDA-event timing
+// ---------------------------------------------------------------------------
+static std::atomic<long long> g_launches{0};
+void note_launch(int kernels) { g_launches.fetch_add(kernels, std::memory_order_relaxed); }
+
+struct StageProfiler {
+  std::mutex mu;
+  bool on = false;
+  struct Open {
+    int stage;
+    cudaEvent_t a, b;
+  };
+  std::vector<Open> pending;
+  std::vector<std::string> names;
+  std::vector<double> total_ms;
+  std::vector<long long> calls;
+  int index(const char *name) {
+    for (size_t i = 0; i < names.size(); ++i)
+      if (names[i] == name) return (int)i;
+    names.push_back(name);
+    total_ms.push_back(0.0);
+    calls.push_back(0);
+    return (int)names.size() - 1;
+  }
+  // Returns a token for end(); -1 when profiling is off.
+  int begin(cudaStream_t st, const char *name) {
+    std::lock_guard<std::mutex> g(mu);
+    if (!on) return -1;
+    Open o;
+    o.stage = index(name);
+    cudaEventCreate(&o.a);
+    cudaEventCreate(&o.b);
+    cudaEventRecord(o.a, st);
+    pending.push_back(o);
+    return (int)pending.size() - 1;
+  }
+  void end(cudaStream_t st, int token) {
+    if (token < 0) return;
+    std::lock_guard<std::mutex> g(mu);
+    if (token < (int)pending.size()) cudaEventRecord(pending[token].b, st);
+  }
+  void flush() {
+    std::lock_guard<std::mutex> g(mu);
+    for (Open &o : pending) {
+      cudaEventSynchronize(o.b);
+      float ms = 0.0f;
+      if (cudaEventElapsedTime(&ms, o.a, o.b) == cudaSuccess) {
+        total_ms[o.stage] += ms;
+        calls[o.stage] += 1;
+      }
+      cudaEventDestroy(o.a);
+      cudaEventDestroy(o.b);
+    }
+    pending.clear();
+  }
+  void reset(bool enable) {
+    flush();
+    std::lock_guard<std::mutex> g(mu);
+    on = enable;
+    names.clear();
+    total_ms.clear();
+    calls.clear();
+  }
+};
+static StageProfiler g_prof;
+
+// RAII stage timer on a stream.
+struct Stage {
+  cudaStream_t st;
+  int token;
+  Stage(cudaStream_t s, const char *name) : st(s), token(g_prof.begin(s, name)) {}
+  ~Stage() { g_prof.end(st, token); }
+};
+
+// ---------------------------------------------------------------------------
+// per-device context: stream, solver handle, parameter tables
+// ---------------------------------------------------------------------------
+struct DeviceContext {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  std::mutex run_mutex;
+  DeviceParams params[5];
+  bool params_ready[5] = {false, false, false, false, false};
+};
+
+static std::mutex g_ctx_mutex;
+static std::unordered_map<int, DeviceContext *> g_contexts;
+
+static DeviceContext &context_for(int device) {
+  std::lock_guard<std::mutex> lock(g_ctx_mutex);
+  auto it = g_contexts.find(device);
+  if (it != g_contexts.end()) return *it->second;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    throw Failure{PM7_ERR_CUDA, "no CUDA device is available; this engine has no CPU fallback"};
+  if (device < 0 || device >= count) throw Failure{PM7_ERR_CUDA, "invalid CUDA device ordinal"};
+  CUDA_OK(cudaSetDevice(device));
+  auto *ctx = new DeviceContext();
+  ctx->device = device;
+  CUDA_OK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  SOLVER_OK(cusolverDnCreate(&ctx->solver));
+  SOLVER_OK(cusolverDnSetStream(ctx->solver, ctx->stream));
+  g_contexts[device] = ctx;
+  return *ctx;
+}
+
+static const DeviceParams &device_params(DeviceContext &ctx, int method) {
+  if (ctx.params_ready[method]) return ctx.params[method];
+  const ParamSet &ps = param_set(method);
+  DeviceParams &d = ctx.params[method];
+  ElementRec *el = nullptr;
+  PairParamRec *pr = nullptr;
+  double *oc = nullptr;
+  CUDA_OK(cudaMalloc(&el, sizeof(ElementRec) * kMaxZ));
+  CUDA_OK(cudaMemcpy(el, ps.elements().data(), sizeof(ElementRec) * kMaxZ, cudaMemcpyHostToDevice));
+  CUDA_OK(cudaMalloc(&pr, sizeof(PairParamRec) * kMaxZ * kMaxZ));
+  CUDA_OK(cudaMemcpy(pr, ps.pairs().data(), sizeof(PairParamRec) * kMaxZ * kMaxZ, cudaMemcpyHostToDevice));
+  const size_t noc = std::max<size_t>(ps.onecenter().size(), 1);
+  CUDA_OK(cudaMalloc(&oc, sizeof(double) * noc));
+  if (!ps.onecenter().empty())
+    CUDA_OK(cudaMemcpy(oc, ps.onecenter().data(), sizeof(double) * ps.onecenter().size(), cudaMemcpyHostToDevice));
+  d.elements = el;
+  d.pairs = pr;
+  d.onecenter = oc;
+  for (int i = 0; i <= 60; ++i) d.vpar[i] = ps.vpar()[i];
+  ctx.params_ready[method] = true;
+  return d;
+}
+
+// ---------------------------------------------------------------------------
+// device buffers with stream-ordered allocation
+// ---------------------------------------------------------------------------
+template <class T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  cudaStream_t st = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  void alloc(size_t count, cudaStream_t s) {
+    release();
+    st = s;
+    n = count;
+    CUDA_OK(cudaMallocAsync((void **)&p, sizeof(T) * std::max<size_t>(count, 1), s));
+  }
+  void release() {
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+  }
+  ~DevBuf() { release(); }
+};
+
+// ---------------------------------------------------------------------------
+// the molecule on the device
+// ---------------------------------------------------------------------------
+struct Molecule {
+  int n = 0;
+  std::vector<int> z;
+  std::vector<double> xyz;  // Bohr
+};
+
+struct Layout {
+  int nao = 0;
+  std::vector<int> aoff, norb, ao_atom, ao_orb;
+  std::vector<NearPair> near;
+  std::vector<int> csr_start;
+  std::vector<int2> csr;
+  int64_t w_len = 0;
+  int32_t e_len = 0;
+  bool has_d = false;
+};
+
+static void validate(const Molecule &m, const pm7_options &o) {  // src/scf.rs:937-1040
+  auto bad = [](const std::string &s) { throw Failure{PM7_ERR_INVALID_INPUT, s}; };
+  if (m.n == 0) bad("a PM7 calculation needs at least one atom");
+  if (!std::isfinite(o.charge)) bad("charge must be finite");
+  if (o.max_scf <= 0) bad("max_scf must be greater than zero");
+  if (!std::isfinite(o.e_tol) || o.e_tol <= 0.0) bad("e_tol must be finite and positive");
+  if (!std::isfinite(o.p_tol) || o.p_tol <= 0.0) bad("p_tol must be finite and positive");
+  if (!std::isfinite(o.level_shift) || o.level_shift < 0.0) bad("level_shift must be finite and non-negative");
+  if (!std::isfinite(o.adiis_switch) || o.adiis_switch < 0.0) bad("adiis_switch must be finite and non-negative");
+  for (int i = 0; i < m.n; ++i)
+    if (!std::isfinite(m.xyz[3 * i]) || !std::isfinite(m.xyz[3 * i + 1]) || !std::isfinite(m.xyz[3 * i + 2]))
+      bad("atom " + std::to_string(i + 1) + " has non-finite coordinates");
+  // Coincident atoms in O(N): buckets much wider than the 1e-10 Bohr threshold.
+  struct K {
+    long long a, b, c;
+    bool operator==(const K &o) const { return a == o.a && b == o.b && c == o.c; }
+  };
+  struct KH {
+    size_t operator()(const K &k) const { return std::hash<long long>()(k.a * 1000003LL ^ k.b * 10007LL ^ k.c); }
+  };
+  std::unordered_map<K, std::vector<int>, KH> cells;
+  const double sp = 1.0e-6;
+  for (int i = 0; i < m.n; ++i) {
+    K k{(long long)std::floor(m.xyz[3 * i] / sp), (long long)std::floor(m.xyz[3 * i + 1] / sp),
+        (long long)std::floor(m.xyz[3 * i + 2] / sp)};
+    for (int dx = -1; dx <= 1; ++dx)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dz = -1; dz <= 1; ++dz) {
+          auto it = cells.find(K{k.a + dx, k.b + dy, k.c + dz});
+          if (it == cells.end()) continue;
+          for (int j : it->second) {
+            const double ex = m.xyz[3 * i] - m.xyz[3 * j], ey = m.xyz[3 * i + 1] - m.xyz[3 * j + 1],
+                         ez = m.xyz[3 * i + 2] - m.xyz[3 * j + 2];
+            if (ex * ex + ey * ey + ez * ez < 1.0e-20)
+              bad("atoms " + std::to_string(std::min(i, j) + 1) + " and " + std::to_string(std::max(i, j) + 1) +
+                  " occupy the same position");
+          }
+        }
+    cells[k].push_back(i);
+  }
+}
+
+// AO layout and the list of atom pairs inside the 7 Angstrom feather range, from a
+// cell list (pairs come out sorted by (u, v), u < v).
+static Layout build_layout(const Molecule &m, const ParamSet &ps) {
+  Layout L;
+  for (int i = 0; i < m.n; ++i) {
+    const ElementRec *e = ps.element(m.z[i]);
+    if (!e) throw Failure{PM7_ERR_MISSING_ELEMENT, "missing PM7 parameter block for Z=" + std::to_string(m.z[i])};
+    L.aoff.push_back(L.nao);
+    L.norb.push_back(e->n_orb);
+    for (int o = 0; o < e->n_orb; ++o) {
+      L.ao_atom.push_back(i);
+      L.ao_orb.push_back(o);
+    }
+    L.nao += e->n_orb;
+    if (e->n_orb == 9) L.has_d = true;
+  }
+  const double cut = 7.0 / kA0;  // Bohr
+  struct K {
+    long long a, b, c;
+    bool operator==(const K &o) const { return a == o.a && b == o.b && c == o.c; }
+  };
+  struct KH {
+    size_t operator()(const K &k) const { return std::hash<long long>()(k.a * 1000003LL ^ k.b * 10007LL ^ k.c); }
+  };
+  std::unordered_map<K, std::vector<int>, KH> cells;
+  std::vector<K> key(m.n);
+  for (int i = 0; i < m.n; ++i) {
+    key[i] = K{(long long)std::floor(m.xyz[3 * i] / cut), (long long)std::floor(m.xyz[3 * i + 1] / cut),
+               (long long)std::floor(m.xyz[3 * i + 2] / cut)};
+    cells[key[i]].push_back(i);
+  }
+  std::vector<int> partners;
+  for (int u = 0; u < m.n; ++u) {
+    partners.clear();
+    for (int dx = -1; dx <= 1; ++dx)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dz = -1; dz <= 1; ++dz) {
+          auto it = cells.find(K{key[u].a + dx, key[u].b + dy, key[u].c + dz});
+          if (it == cells.end()) continue;
+          for (int v : it->second) {
+            if (v <= u) continue;
+            const double ex = m.xyz[3 * v] - m.xyz[3 * u], ey = m.xyz[3 * v + 1] - m.xyz[3 * u + 1],
+                         ez = m.xyz[3 * v + 2] - m.xyz[3 * u + 2];
+            if (std::sqrt(ex * ex + ey * ey + ez * ez) * kA0 < 7.0) partners.push_back(v);
+          }
+        }
+    std::sort(partners.begin(), partners.end());
+    for (int v : partners) {
+      NearPair q;
+      q.u = u;
+      q.v = v;
+      L.near.push_back(q);
+    }
+  }
+  std::vector<std::vector<int2>> lists(m.n);
+  int64_t woff = 0;
+  int32_t eoff = 0;
+  for (size_t p = 0; p < L.near.size(); ++p) {
+    NearPair &q = L.near[p];
+    const int nu = L.norb[q.u], nv = L.norb[q.v];
+    const int pu = nu * (nu + 1) / 2, pv = nv * (nv + 1) / 2;
+    q.woff = woff;
+    woff += (int64_t)pu * pv;
+    q.eoff_u = eoff;
+    eoff += pu;
+    q.eoff_v = eoff;
+    eoff += pv;
+    lists[q.u].push_back(make_int2(q.v, (int)p));
+    lists[q.v].push_back(make_int2(q.u, (int)p));
+  }
+  L.w_len = woff;
+  L.e_len = eoff;
+  L.csr_start.assign(m.n + 1, 0);
+  for (int a = 0; a < m.n; ++a) {
+    std::sort(lists[a].begin(), lists[a].end(), [](const int2 &x, const int2 &y) { return x.x < y.x; });
+    L.csr_start[a + 1] = L.csr_start[a] + (int)lists[a].size();
+  }
+  L.csr.reserve(L.csr_start[m.n]);
+  for (int a = 0; a < m.n; ++a) L.csr.insert(L.csr.end(), lists[a].begin(), lists[a].end());
+  return L;
+}
+
+struct DeviceMolecule {
+  cudaStream_t st;
+  int n = 0, nao = 0, n_near = 0;
+  DevBuf<int> z, aoff, ao_atom, csr_start;
+  DevBuf<double> xyz, H, w, ecore, jbuf, pop, cc_partial, scal;
+  DevBuf<NearPair> near;
+  DevBuf<int2> csr;
+  DevBuf<unsigned char> mask;
+  DevBuf<int> status;
+  double core_core_ev = 0.0;
+
+  FockGeometry geometry() const {
+    FockGeometry g;
+    g.n_atoms = n;
+    g.nao = nao;
+    g.n_near = n_near;
+    g.z = z.p;
+    g.aoff = aoff.p;
+    g.ao_atom = ao_atom.p;
+    g.xyz = xyz.p;
+    g.near_mask = mask.p;
+    g.np = near.p;
+    g.csr_start = csr_start.p;
+    g.csr = csr.p;
+    g.w = w.p;
+    return g;
+  }
+};
+
+__global__ void k_fill_mask(int n_near, int n_atoms, const NearPair *np, unsigned char *mask) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_near) return;
+  mask[(size_t)np[p].u * n_atoms + np[p].v] = 1;
+  mask[(size_t)np[p].v * n_atoms + np[p].u] = 1;
+}
+
+template <class T>
+static void upload(DevBuf<T> &b, const std::vector<T> &v, cudaStream_t st) {
+  b.alloc(v.size(), st);
+  if (!v.empty()) CUDA_OK(cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st));
+}
+
+// Core Hamiltonian and stored pair integrals on the device (hamiltonian.rs:310-638).
+static void build_device_molecule(DeviceMolecule &D, const Molecule &m, const Layout &L, const DeviceParams &P,
+                                  cudaStream_t st) {
+  D.st = st;
+  D.n = m.n;
+  D.nao = L.nao;
+  D.n_near = (int)L.near.size();
+  upload(D.z, m.z, st);
+  upload(D.xyz, m.xyz, st);
+  upload(D.aoff, L.aoff, st);
+  upload(D.ao_atom, L.ao_atom, st);
+  upload(D.csr_start, L.csr_start, st);
+  upload(D.near, L.near, st);
+  upload(D.csr, L.csr, st);
+  D.mask.alloc((size_t)m.n * m.n, st);
+  CUDA_OK(cudaMemsetAsync(D.mask.p, 0, (size_t)m.n * m.n, st));
+  if (D.n_near) k_fill_mask<<<(D.n_near + 255) / 256, 256, 0, st>>>(D.n_near, m.n, D.near.p, D.mask.p);
+  const size_t nao2 = (size_t)L.nao * L.nao;
+  D.H.alloc(nao2, st);
+  CUDA_OK(cudaMemsetAsync(D.H.p, 0, sizeof(double) * nao2, st));
+  D.w.alloc((size_t)L.w_len, st);
+  D.ecore.alloc((size_t)L.e_len, st);
+  D.jbuf.alloc((size_t)L.e_len, st);
+  D.pop.alloc(m.n, st);
+  D.scal.alloc(8, st);
+  D.status.alloc(1, st);
+  CUDA_OK(cudaMemsetAsync(D.status.p, 0, sizeof(int), st));
+  const size_t np = pairs_all_partials(m.n);
+  D.cc_partial.alloc(np, st);
+  launch_pairs_all(st, m.n, D.z.p, D.xyz.p, D.aoff.p, L.nao, P, D.H.p, D.cc_partial.p, D.status.p);
+  launch_near_integrals(st, D.n_near, D.z.p, D.xyz.p, D.near.p, P, D.w.p, D.ecore.p, D.status.p);
+  launch_hcore_diag(st, m.n, D.z.p, D.xyz.p, D.aoff.p, D.csr_start.p, D.csr.p, D.near.p, D.ecore.p, D.mask.p, P,
+                    L.nao, D.H.p);
+  if (m.n >= 2) launch_sum_partials(st, D.cc_partial.p, np, D.scal.p);
+  else CUDA_OK(cudaMemsetAsync(D.scal.p, 0, sizeof(double), st));
+  int status = 0;
+  double cc = 0.0;
+  CUDA_OK(cudaMemcpyAsync(&status, D.status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(&cc, D.scal.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  CUDA_OK(cudaGetLastError());
+  if (status & 1) throw Failure{PM7_ERR_UNSUPPORTED, "Slater overlaps for valence shells with n >= 4 are not implemented on the device"};
+  if (status & 2) throw Failure{PM7_ERR_UNSUPPORTED, "MNDO/d (spd) pair integrals are not implemented on the device"};
+  D.core_core_ev = cc;
+}
+
+// ---------------------------------------------------------------------------
+// SCF on the device
+// ---------------------------------------------------------------------------
+struct Eigen {
+  DeviceContext &ctx;
+  int n;
+  DevBuf<double> work, eps;
+  DevBuf<int> info;
+  int lwork = 0;
+  Eigen(DeviceContext &c, int n_, double *probe) : ctx(c), n(n_) {
+    SOLVER_OK(cusolverDnDsyevd_bufferSize(ctx.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, probe,
+                                          n, nullptr, &lwork));
+    work.alloc((size_t)std::max(lwork, 1), ctx.stream);
+    eps.alloc(n, ctx.stream);
+    info.alloc(1, ctx.stream);
+  }
+  // In place: A (n x n symmetric) becomes the eigenvectors, one per row when read
+  // row-major; eigenvalues ascending in eps.
+  void solve(double *A) {
+    SOLVER_OK(cusolverDnDsyevd(ctx.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A, n, eps.p, work.p,
+                               lwork, info.p));
+  }
+};
+
+// Density from F by SP2 purification: P = w X with X the aufbau projector onto the
+// n_occ lowest eigenvectors of F. Returns false when the iteration does not settle on
+// an idempotent X (degenerate frontier levels), so the caller diagonalises instead.
+struct Purifier {
+  cudaStream_t st;
+  int n;
+  DevBuf<double> X, X2, scratch, bounds, state;
+  int last_iterations = 0;
+  Purifier(cudaStream_t s, int n_) : st(s), n(n_) {
+    X.alloc((size_t)n * n, st);
+    X2.alloc((size_t)n * n, st);
+    scratch.alloc(1024, st);
+    bounds.alloc(2, st);
+    state.alloc(4, st);
+  }
+  bool project(const double *F, int n_occ, double w, double *P) {
+    launch_gershgorin(st, n, F, scratch.p, bounds.p);
+    launch_sp2_init(st, n, F, bounds.p, X.p);
+    std::vector<double> err;
+    bool ok = false;
+    for (int it = 0; it < 100; ++it) {
+      launch_sp2_square(st, n, X.p, X2.p);
+      launch_sp2_trace(st, n, X.p, X2.p, (double)n_occ, state.p);
+      launch_sp2_update(st, n, X.p, X2.p, state.p);
+      double s[4];
+      CUDA_OK(cudaMemcpyAsync(s, state.p, sizeof(s), cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaStreamSynchronize(st));
+      const double e = s[3];
+      err.push_back(e);
+      last_iterations = it + 1;
+      const size_t k = err.size();
+      if (!std::isfinite(e)) break;
+      if (std::fabs(e) <= 1.0e-13 * std::max(1, n_occ)) {
+        ok = true;
+        break;
+      }
+      if (k >= 3 && std::fabs(e) < 1.0e-6 && std::fabs(e) >= std::fabs(err[k - 3])) {
+        ok = true;  // at the rounding floor: no further progress
+        break;
+      }
+    }
+    if (!ok) return false;
+    launch_scale(st, (size_t)n * n, w, X.p, P);
+    return true;
+  }
+};
+
+// Density solver for the SCF loop: SP2 for large systems (tensor-core squarings), the
+// cuSOLVER eigendecomposition for small ones or when SP2 cannot settle. The choice can
+// be forced with PM7_DENSITY_SOLVER=sp2|syevd.
+static bool use_sp2(int n) {
+  const char *env = std::getenv("PM7_DENSITY_SOLVER");
+  if (env && std::strcmp(env, "syevd") == 0) return false;
+  if (env && std::strcmp(env, "sp2") == 0) return true;
+  return n >= 256;
+}
+
+static double host_sum(const DevBuf<double> &partials, size_t count, double *dscal, cudaStream_t st) {
+  launch_sum(st, partials.p, count, dscal);
+  double v = 0.0;
+  CUDA_OK(cudaMemcpyAsync(&v, dscal, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  return v;
+}
+
+struct ScfOut {
+  bool converged = false;
+  int iterations = 0;
+  double density_error = std::numeric_limits<double>::infinity();
+  double electronic_ev = 0.0;
+  std::vector<double> eps_a, eps_b;
+  DevBuf<double> P, Pspin, Va, Vb;  // total density, spin density, eigenvectors (rows)
+  bool unrestricted = false;
+  int n_occ = 0, n_occ_beta = -1;
+};
+
+// SAD guess diagonal (scf.rs:1050-1114).
+static std::vector<double> sad_diag(const Molecule &m, const Layout &L, const ParamSet &ps, double n_electrons) {
+  std::vector<double> d(L.nao, 0.0);
+  double tore = 0.0;
+  for (int zz : m.z) tore += ps.element(zz)->core;
+  const double yy = L.nao > 0 ? (tore - n_electrons) / L.nao : 0.0;
+  for (int a = 0; a < m.n; ++a) {
+    const ElementRec *e = ps.element(m.z[a]);
+    const int off = L.aoff[a], no = L.norb[a], z = m.z[a];
+    const double t = e->core;
+    if (no == 1) {
+      d[off] = t - yy;
+    } else if (no == 4) {
+      for (int k = 0; k < 4; ++k) d[off + k] = t * 0.25 - yy;
+    } else if (no == 9) {
+      const bool mg = z < 21 || (z > 30 && z < 39) || (z > 48 && z < 57);
+      if (mg) {
+        for (int k = 0; k < 4; ++k) d[off + k] = t * 0.25 - yy;
+        for (int k = 4; k < 9; ++k) d[off + k] = -yy;
+      } else {
+        double sum = t - 9.0 * yy;
+        d[off] = std::min(std::max(sum, 0.0), 2.0);
+        sum -= 2.0;
+        if (sum > 0.0) {
+          for (int k = 4; k < 9; ++k) d[off + k] = std::min(std::max(sum * 0.2, 0.0), 2.0);
+          sum -= 10.0;
+          if (sum > 0.0)
+            for (int k = 1; k < 4; ++k) d[off + k] = sum / 3.0;
+        }
+      }
+    }
+  }
+  return d;
+}
+
+static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D, const Molecule &m,
+                    const Layout &L, const ParamSet &ps, int n_occ, const pm7_options &o, ScfOut &out) {
+  cudaStream_t st = ctx.stream;
+  const int n = L.nao;
+  const size_t nn = (size_t)n * n;
+  const FockGeometry g = D.geometry();
+  out.P.alloc(nn, st);
+  DevBuf<double> Pnew, F, Fuse, X, partials, dscal, coef, dots;
+  Pnew.alloc(nn, st);
+  F.alloc(nn, st);
+  Fuse.alloc(nn, st);
+  X.alloc(nn, st);
+  const int kmax = 8;
+  std::vector<DevBuf<double>> hF(kmax), hE(kmax), hD(kmax);
+  const bool accel_on = o.use_diis && o.accelerator != PM7_ACCEL_NONE;
+  partials.alloc(std::max<size_t>(((size_t)(n + 31) / 32) * ((n + 31) / 32), 4096), st);
+  dscal.alloc(8, st);
+  coef.alloc(kmax + 1, st);
+  const int dot_blocks = 296;
+  dots.alloc((size_t)dot_blocks * 32, st);
+  DevBuf<double> dotout;
+  dotout.alloc(64, st);
+  DevBuf<const double *> ptrs;
+  ptrs.alloc(64, st);
+
+  if (o.initial_density) {
+    CUDA_OK(cudaMemcpyAsync(out.P.p, o.initial_density, sizeof(double) * nn, cudaMemcpyHostToDevice, st));
+  } else {
+    std::vector<double> diag = sad_diag(m, L, ps, 2.0 * n_occ);
+    DevBuf<double> dd;
+    upload(dd, diag, st);
+    launch_set_diag(st, n, dd.p, out.P.p);
+    CUDA_OK(cudaStreamSynchronize(st));
+  }
+  Eigen eig(ctx, n, Fuse.p);
+  const bool sp2 = use_sp2(n);
+  Purifier pur(st, sp2 ? n : 1);
+  bool diagonalised = false;  // whether Fuse holds the eigenvectors of the last iteration
+  HistoryHost hist(kmax);
+  StallGuardHost guard(o.level_shift);
+  const bool trace = std::getenv("PM7_SCF_TRACE") != nullptr;
+  double e_old = 0.0;
+  for (int iter = 0; iter < o.max_scf; ++iter) {
+    out.iterations = iter + 1;
+    const int slot = hist.push();  // chronological bookkeeping of the ring
+    if (!hF[slot].p) {
+      hF[slot].alloc(nn, st);
+      hE[slot].alloc(nn, st);
+      hD[slot].alloc(nn, st);
+    }
+    double *Fk = hF[slot].p;
+    { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, out.P.p, out.P.p, 0.5, Fk, D.pop.p, D.jbuf.p); }
+    size_t ne = launch_energy(st, nn, out.P.p, D.H.p, Fk, partials.p);
+    launch_sum(st, partials.p, ne, dscal.p + 0);
+    CUDA_OK(cudaMemcpyAsync(hD[slot].p, out.P.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+    // DIIS error e = F P - P F = F P - (F P)^T
+    { Stage s_(st, "commutator_gemm"); launch_gemm_tn(st, n, n, n, 1.0, Fk, n, out.P.p, n, X.p, n); }
+    size_t na = launch_antisym(st, n, X.p, hE[slot].p, partials.p);
+    launch_sum(st, partials.p, na, dscal.p + 1);
+    // inner products of the new entry with the history (chronological, newest last)
+    const std::vector<int> older = hist.order();
+    const int k = (int)older.size();
+    std::vector<const double *> hp;
+    for (int i = 0; i < k; ++i) hp.push_back(hE[older[i]].p);
+    hp.push_back(hE[slot].p);
+    for (int i = 0; i < k; ++i) hp.push_back(hF[older[i]].p);
+    hp.push_back(Fk);
+    for (int i = 0; i < k; ++i) hp.push_back(hD[older[i]].p);
+    hp.push_back(hD[slot].p);
+    CUDA_OK(cudaMemcpyAsync(ptrs.p, hp.data(), sizeof(double *) * hp.size(), cudaMemcpyHostToDevice, st));
+    const double *const *dE = ptrs.p, *const *dF = ptrs.p + (k + 1), *const *dD = ptrs.p + 2 * (k + 1);
+    { Stage s_(st, "diis_dots"); launch_dot_many(st, nn, 1, dE + k, k + 1, dE, dots.p, dot_blocks); }  // <e_new, e_i>
+    launch_reduce_rows(st, dots.p, dot_blocks, k + 1, dotout.p);
+    { Stage s_(st, "diis_dots"); launch_dot_many(st, nn, 1, dD + k, k + 1, dF, dots.p, dot_blocks); }  // <D_new, F_j>
+    launch_reduce_rows(st, dots.p, dot_blocks, k + 1, dotout.p + 16);
+    if (k > 0) {
+      { Stage s_(st, "diis_dots"); launch_dot_many(st, nn, 1, dF + k, k, dD, dots.p, dot_blocks); }  // <D_i, F_new>
+      launch_reduce_rows(st, dots.p, dot_blocks, k, dotout.p + 32);
+    }
+    double sc[2], dh[48];
+    CUDA_OK(cudaMemcpyAsync(sc, dscal.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(dh, dotout.p, sizeof(double) * 48, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    const double e_elec = 0.5 * sc[0];
+    const double err_norm = std::sqrt(sc[1]);
+    hist.record(std::vector<double>(dh, dh + k + 1), std::vector<double>(dh + 16, dh + 16 + k + 1),
+                std::vector<double>(dh + 32, dh + 32 + k));
+    // extrapolation weights over the chronological history
+    std::vector<double> w;
+    if (accel_on) {
+      if (o.accelerator == PM7_ACCEL_CDIIS || err_norm <= o.adiis_switch) w = hist.cdiis();
+      else w = hist.adiis();
+    }
+    std::vector<const double *> fp;
+    std::vector<double> cw;
+    if (w.empty()) {
+      fp.push_back(Fk);
+      cw.push_back(1.0);
+    } else {
+      const std::vector<int> &ent = hist.entries();
+      for (size_t i = 0; i < ent.size(); ++i)
+        if (w[i] != 0.0) {  // an exact zero weight adds exactly nothing
+          fp.push_back(hF[ent[i]].p);
+          cw.push_back(w[i]);
+        }
+    }
+    CUDA_OK(cudaMemcpyAsync(ptrs.p + 48, fp.data(), sizeof(double *) * fp.size(), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(coef.p, cw.data(), sizeof(double) * cw.size(), cudaMemcpyHostToDevice, st));
+    { Stage s_(st, "combine"); launch_combine(st, n, (int)fp.size(), ptrs.p + 48, coef.p, out.P.p, 2.0, guard.shift, Fuse.p); }
+    bool purified = false;
+    if (sp2) {
+      Stage s_(st, "sp2_purify");
+      purified = pur.project(Fuse.p, n_occ, 2.0, Pnew.p);
+    }
+    diagonalised = !purified;
+    if (!purified) {
+      { Stage s_(st, "eigensolve"); eig.solve(Fuse.p); }
+      { Stage s_(st, "density_gemm"); launch_density(st, n, n_occ, 2.0, Fuse.p, n, Pnew.p); }
+    }
+    size_t nd = launch_sqdiff(st, nn, Pnew.p, out.P.p, partials.p);
+    const double dp = std::sqrt(host_sum(partials, nd, dscal.p + 2, st) / (double)std::max<size_t>(nn, 1));
+    out.density_error = dp;
+    const double de = std::fabs(e_elec - e_old);
+    std::swap(out.P.p, Pnew.p);
+    e_old = e_elec;
+    const bool residual_ok = guard.shift == 0.0 && err_norm < 1.0e-7;
+    if (iter > 0 && de < o.e_tol && (dp < o.p_tol || residual_ok)) {
+      out.converged = true;
+      break;
+    }
+    guard.update(dp, e_elec);
+    if (trace)
+      std::fprintf(stderr, "scf %4d E %.10f dp %.3e err %.3e shift %.2f\n", out.iterations, e_elec, dp, err_norm,
+                   guard.shift);
+  }
+  // final Fock and energy at the converged density
+  { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, out.P.p, out.P.p, 0.5, F.p, D.pop.p, D.jbuf.p); }
+  size_t ne = launch_energy(st, nn, out.P.p, D.H.p, F.p, partials.p);
+  out.electronic_ev = 0.5 * host_sum(partials, ne, dscal.p, st);
+  out.Va.alloc(nn, st);
+  // Reported orbitals: the eigenvectors of the last extrapolated Fock, or of the real
+  // Fock when a level shift was active (scf.rs:1299-1305).
+  if (guard.shift > 0.0) {
+    CUDA_OK(cudaMemcpyAsync(Fuse.p, F.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+    { Stage s_(st, "eigensolve"); eig.solve(Fuse.p); }
+  } else if (!diagonalised) {
+    { Stage s_(st, "eigensolve"); eig.solve(Fuse.p); }
+  }
+  CUDA_OK(cudaMemcpyAsync(out.Va.p, Fuse.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+  out.eps_a.resize(n);
+  CUDA_OK(cudaMemcpyAsync(out.eps_a.data(), eig.eps.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  out.n_occ = n_occ;
+}
+
+static void run_uhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D, const Molecule &m,
+                    const Layout &L, const ParamSet &ps, int n_alpha, int n_beta, const pm7_options &o,
+                    ScfOut &out) {
+  cudaStream_t st = ctx.stream;
+  const int n = L.nao;
+  const size_t nn = (size_t)n * n;
+  const FockGeometry g = D.geometry();
+  DevBuf<double> Pa, Pb, Pt, Fa, Fb, X, E, Ua, Ub, partials, dscal, Pan, Pbn;
+  for (DevBuf<double> *b : {&Pa, &Pb, &Pt, &Fa, &Fb, &X, &E, &Ua, &Ub, &Pan, &Pbn}) b->alloc(nn, st);
+  partials.alloc(std::max<size_t>(((size_t)(n + 31) / 32) * ((n + 31) / 32), 4096), st);
+  dscal.alloc(8, st);
+  const double ntot = std::max(n_alpha + n_beta, 1);
+  {
+    DevBuf<double> total;
+    total.alloc(nn, st);
+    if (o.initial_density) {
+      CUDA_OK(cudaMemcpyAsync(total.p, o.initial_density, sizeof(double) * nn, cudaMemcpyHostToDevice, st));
+    } else {
+      std::vector<double> diag = sad_diag(m, L, ps, (double)(n_alpha + n_beta));
+      DevBuf<double> dd;
+      upload(dd, diag, st);
+      launch_set_diag(st, n, dd.p, total.p);
+      CUDA_OK(cudaStreamSynchronize(st));
+    }
+    launch_scale(st, nn, n_alpha / ntot, total.p, Pa.p);
+    launch_scale(st, nn, n_beta / ntot, total.p, Pb.p);
+    if (o.initial_spin_density) {
+      DevBuf<double> s;
+      s.alloc(nn, st);
+      CUDA_OK(cudaMemcpyAsync(s.p, o.initial_spin_density, sizeof(double) * nn, cudaMemcpyHostToDevice, st));
+      launch_axpby(st, nn, 1.0, Pa.p, 0.5, s.p, Pa.p);
+      launch_axpby(st, nn, 1.0, Pb.p, -0.5, s.p, Pb.p);
+      CUDA_OK(cudaStreamSynchronize(st));
+    }
+    CUDA_OK(cudaStreamSynchronize(st));
+  }
+  Eigen eig(ctx, n, Ua.p);
+  const bool sp2 = use_sp2(n);
+  Purifier pur(st, sp2 ? n : 1);
+  bool diag_a = false;  // whether Ua holds the alpha eigenvectors of the last iteration
+  DevBuf<double> eps_b;
+  eps_b.alloc(n, st);
+  StallGuardHost guard(o.level_shift);
+  const bool trace = std::getenv("PM7_SCF_TRACE") != nullptr;
+  double e_old = 0.0;
+  auto energy = [&](const double *pt, const double *pa, const double *fa, const double *pb, const double *fb) {
+    size_t c1 = launch_dot(st, nn, pt, D.H.p, partials.p);
+    launch_sum(st, partials.p, c1, dscal.p + 0);
+    c1 = launch_dot(st, nn, pa, fa, partials.p);
+    launch_sum(st, partials.p, c1, dscal.p + 1);
+    c1 = launch_dot(st, nn, pb, fb, partials.p);
+    launch_sum(st, partials.p, c1, dscal.p + 2);
+  };
+  for (int iter = 0; iter < o.max_scf; ++iter) {
+    out.iterations = iter + 1;
+    launch_axpby(st, nn, 1.0, Pa.p, 1.0, Pb.p, Pt.p);
+    { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, Pt.p, Pa.p, 1.0, Fa.p, D.pop.p, D.jbuf.p); }
+    { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, Pt.p, Pb.p, 1.0, Fb.p, D.pop.p, D.jbuf.p); }
+    energy(Pt.p, Pa.p, Fa.p, Pb.p, Fb.p);
+    { Stage s_(st, "commutator_gemm"); launch_gemm_tn(st, n, n, n, 1.0, Fa.p, n, Pa.p, n, X.p, n); }
+    size_t c = launch_antisym(st, n, X.p, E.p, partials.p);
+    launch_sum(st, partials.p, c, dscal.p + 3);
+    { Stage s_(st, "commutator_gemm"); launch_gemm_tn(st, n, n, n, 1.0, Fb.p, n, Pb.p, n, X.p, n); }
+    c = launch_antisym(st, n, X.p, E.p, partials.p);
+    launch_sum(st, partials.p, c, dscal.p + 4);
+    double sc[5];
+    CUDA_OK(cudaMemcpyAsync(sc, dscal.p, sizeof(double) * 5, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    const double e_elec = 0.5 * (sc[0] + sc[1] + sc[2]);
+    const double err_norm = std::sqrt(sc[3] + sc[4]);
+    const double one = 1.0;
+    double *dcoef = dscal.p + 6;
+    CUDA_OK(cudaMemcpyAsync(dcoef, &one, sizeof(double), cudaMemcpyHostToDevice, st));
+    DevBuf<const double *> ptr;
+    ptr.alloc(2, st);
+    const double *pp[2] = {Fa.p, Fb.p};
+    CUDA_OK(cudaMemcpyAsync(ptr.p, pp, sizeof(pp), cudaMemcpyHostToDevice, st));
+    { Stage s_(st, "combine"); launch_combine(st, n, 1, ptr.p, dcoef, Pa.p, 1.0, guard.shift, Ua.p); }
+    { Stage s_(st, "combine"); launch_combine(st, n, 1, ptr.p + 1, dcoef, Pb.p, 1.0, guard.shift, Ub.p); }
+    std::vector<double> ea(n, 0.0);
+    bool pa_ok = false, pb_ok = false;
+    if (sp2) {
+      Stage s_(st, "sp2_purify");
+      pa_ok = pur.project(Ua.p, n_alpha, 1.0, Pan.p);
+      pb_ok = pur.project(Ub.p, n_beta, 1.0, Pbn.p);
+    }
+    diag_a = !pa_ok;
+    if (!pa_ok) {
+      { Stage s_(st, "eigensolve"); eig.solve(Ua.p); }
+      { Stage s_(st, "density_gemm"); launch_density(st, n, n_alpha, 1.0, Ua.p, n, Pan.p); }
+      CUDA_OK(cudaMemcpyAsync(ea.data(), eig.eps.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    }
+    if (!pb_ok) {
+      { Stage s_(st, "eigensolve"); eig.solve(Ub.p); }
+      { Stage s_(st, "density_gemm"); launch_density(st, n, n_beta, 1.0, Ub.p, n, Pbn.p); }
+    }
+    size_t c2 = launch_sqdiff(st, nn, Pan.p, Pa.p, partials.p);
+    const double dpa = std::sqrt(host_sum(partials, c2, dscal.p + 5, st) / (double)nn);
+    c2 = launch_sqdiff(st, nn, Pbn.p, Pb.p, partials.p);
+    const double dpb = std::sqrt(host_sum(partials, c2, dscal.p + 5, st) / (double)nn);
+    const double dp = dpa + dpb;
+    out.density_error = dp;
+    out.eps_a = ea;
+    const double de = std::fabs(e_elec - e_old);
+    std::swap(Pa.p, Pan.p);
+    std::swap(Pb.p, Pbn.p);
+    e_old = e_elec;
+    const bool residual_ok = guard.shift == 0.0 && err_norm < 1.0e-7;
+    if (iter > 0 && de < o.e_tol && (dp < o.p_tol || residual_ok)) {
+      out.converged = true;
+      break;
+    }
+    guard.update(dp, e_elec);
+    if (trace)
+      std::fprintf(stderr, "scf %4d E %.10f dp %.3e err %.3e shift %.2f (uhf)\n", out.iterations, e_elec, dp,
+                   err_norm, guard.shift);
+  }
+  out.P.alloc(nn, st);
+  out.Pspin.alloc(nn, st);
+  launch_axpby(st, nn, 1.0, Pa.p, 1.0, Pb.p, out.P.p);
+  launch_axpby(st, nn, 1.0, Pa.p, -1.0, Pb.p, out.Pspin.p);
+  { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, out.P.p, Pa.p, 1.0, Fa.p, D.pop.p, D.jbuf.p); }
+  { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, out.P.p, Pb.p, 1.0, Fb.p, D.pop.p, D.jbuf.p); }
+  energy(out.P.p, Pa.p, Fa.p, Pb.p, Fb.p);
+  double sc[3];
+  CUDA_OK(cudaMemcpyAsync(sc, dscal.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  out.electronic_ev = 0.5 * (sc[0] + sc[1] + sc[2]);
+  out.Va.alloc(nn, st);
+  out.Vb.alloc(nn, st);
+  if (guard.shift > 0.0) {
+    CUDA_OK(cudaMemcpyAsync(Ua.p, Fa.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+    { Stage s_(st, "eigensolve"); eig.solve(Ua.p); }
+    out.eps_a.resize(n);
+    CUDA_OK(cudaMemcpyAsync(out.eps_a.data(), eig.eps.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  } else if (!diag_a) {
+    { Stage s_(st, "eigensolve"); eig.solve(Ua.p); }
+    out.eps_a.resize(n);
+    CUDA_OK(cudaMemcpyAsync(out.eps_a.data(), eig.eps.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  }
+  CUDA_OK(cudaMemcpyAsync(out.Va.p, Ua.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+  CUDA_OK(cudaMemcpyAsync(Ub.p, Fb.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+  { Stage s_(st, "eigensolve"); eig.solve(Ub.p); }
+  CUDA_OK(cudaMemcpyAsync(out.Vb.p, Ub.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+  out.eps_b.resize(n);
+  CUDA_OK(cudaMemcpyAsync(out.eps_b.data(), eig.eps.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  out.unrestricted = true;
+  out.n_occ = n_alpha;
+  out.n_occ_beta = n_beta;
+}
+
+// ---------------------------------------------------------------------------
+// run_pm7
+// ---------------------------------------------------------------------------
+static double *host_copy(const double *src_dev, size_t count, cudaStream_t st) {
+  double *h = (double *)std::malloc(sizeof(double) * std::max<size_t>(count, 1));
+  if (count) CUDA_OK(cudaMemcpyAsync(h, src_dev, sizeof(double) * count, cudaMemcpyDeviceToHost, st));
+  return h;
+}
+
+static double *host_vec(const std::vector<double> &v) {
+  double *h = (double *)std::malloc(sizeof(double) * std::max<size_t>(v.size(), 1));
+  std::memcpy(h, v.data(), sizeof(double) * v.size());
+  return h;
+}
+
+static uint64_t device_budget(int64_t explicit_mb) {
+  if (explicit_mb >= 0) return (uint64_t)explicit_mb << 20;
+  if (const char *s = std::getenv("PM7_MEM_BUDGET_MB")) {
+    char *end = nullptr;
+    unsigned long long mb = std::strtoull(s, &end, 10);
+    if (end != s) return (uint64_t)mb << 20;
+  }
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 0;
+  return free_b / 5 * 4;
+}
+
+static Molecule to_molecule(const pm7_molecule *mol) {
+  if (!mol || mol->n_atoms < 0 || (mol->n_atoms > 0 && (!mol->z || !mol->xyz_bohr)))
+    throw Failure{PM7_ERR_INVALID_INPUT, "null molecule"};
+  Molecule m;
+  m.n = mol->n_atoms;
+  m.z.assign(mol->z, mol->z + m.n);
+  m.xyz.assign(mol->xyz_bohr, mol->xyz_bohr + 3 * (size_t)m.n);
+  return m;
+}
+
+static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm7_options *opt, pm7_result *res) {
+  if (!opt || !res || !params) throw Failure{PM7_ERR_INVALID_INPUT, "null argument"};
+  const pm7_options &o = *opt;
+  Molecule m = to_molecule(mol);
+  validate(m, o);
+  const int pmethod = *reinterpret_cast<const int *>(params);
+  if (o.method != pmethod)
+    throw Failure{PM7_ERR_INVALID_INPUT, "options method does not match parameter method"};
+  if (o.multiplicity < 1) throw Failure{PM7_ERR_INVALID_INPUT, "multiplicity must be >= 1"};
+  if (o.precision != PM7_PRECISION_FP64 && o.precision != PM7_PRECISION_MIXED)
+    throw Failure{PM7_ERR_INVALID_INPUT, "unknown precision mode"};
+  const ParamSet &ps = param_set(o.method);
+  Layout L = build_layout(m, ps);
+  DeviceContext &ctx = context_for(o.device);
+  std::lock_guard<std::mutex> lock(ctx.run_mutex);
+  CUDA_OK(cudaSetDevice(ctx.device));
+  {
+    // Pre-flight memory guard (memory.rs:95-118) against the device's HBM.
+    const bool has_d = o.force_dpath || L.has_d;
+    const uint64_t mat = (uint64_t)L.nao * L.nao * 8;
+    const uint64_t pairs = (uint64_t)m.n * (m.n > 0 ? m.n - 1 : 0) / 2;
+    const uint64_t need = mat * 30 + pairs * (has_d ? 18000 : 2400);
+    const uint64_t budget = device_budget(o.max_memory_mb);
+    if (budget > 0 && need > budget)
+      throw Failure{PM7_ERR_INSUFFICIENT_MEMORY, "estimated SCF memory ~" + std::to_string((need + (1 << 20) - 1) >> 20) +
+                                                     " MB exceeds the " + std::to_string(budget >> 20) + " MB budget"};
+  }
+  if (o.force_dpath || L.has_d)
+    throw Failure{PM7_ERR_UNSUPPORTED, "MNDO/d (spd) pair integrals are not implemented on the device"};
+  const DeviceParams &P = device_params(ctx, o.method);
+  cudaStream_t st = ctx.stream;
+  cudaEvent_t t0, t1;
+  CUDA_OK(cudaEventCreate(&t0));
+  CUDA_OK(cudaEventCreate(&t1));
+  CUDA_OK(cudaEventRecord(t0, st));
+  DeviceMolecule D;
+  { Stage s_(st, "build"); build_device_molecule(D, m, L, P, st); }
+  // electron count and spin (scf.rs:588-627)
+  double n_elec = 0.0;
+  for (int zz : m.z) n_elec += ps.element(zz)->core;
+  n_elec -= o.charge;
+  const long long ni = std::llround(n_elec);
+  if (std::fabs(n_elec - (double)ni) > 1.0e-6 || ni < 0)
+    throw Failure{PM7_ERR_INVALID_INPUT, "invalid electron count " + std::to_string(n_elec)};
+  const long long unp = o.multiplicity - 1;
+  if (ni - unp < 0 || (ni - unp) % 2 != 0)
+    throw Failure{PM7_ERR_INVALID_INPUT, "electron count " + std::to_string(ni) + " is incompatible with multiplicity " +
+                                             std::to_string(o.multiplicity) + " (need same parity)"};
+  const int n_alpha = (int)((ni + unp) / 2), n_beta = (int)((ni - unp) / 2);
+  bool uhf;
+  if (o.reference == PM7_REF_AUTO) uhf = n_alpha != n_beta;
+  else if (o.reference == PM7_REF_UNRESTRICTED) uhf = true;
+  else {
+    if (n_alpha != n_beta)
+      throw Failure{PM7_ERR_INVALID_INPUT, "restricted (RHF) needs a closed shell, but multiplicity " +
+                                               std::to_string(o.multiplicity) + " gives " + std::to_string(n_alpha) +
+                                               "a/" + std::to_string(n_beta) + "b; use UHF"};
+    uhf = false;
+  }
+  ScfOut S;
+  if (uhf) run_uhf(ctx, P, D, m, L, ps, n_alpha, n_beta, o, S);
+  else run_rhf(ctx, P, D, m, L, ps, n_alpha, o, S);
+  // post-SCF corrections on the device (scf.rs:907-932)
+  DevBuf<double> cscratch, cout;
+  cscratch.alloc(corrections_scratch(m.n), st);
+  cout.alloc(5, st);
+  { Stage s_(st, "corrections"); launch_corrections(st, m.n, D.z.p, D.xyz.p, o.method, o.smooth_dispersion, cscratch.p, cscratch.n, cout.p); }
+  double parts[5];
+  CUDA_OK(cudaMemcpyAsync(parts, cout.p, sizeof(parts), cudaMemcpyDeviceToHost, st));
+  // per-atom populations and the hybrid-dipole density elements
+  std::vector<double> diag_blocks;
+  {
+    DevBuf<double> pop;
+    pop.alloc(m.n, st);
+    launch_atom_pop(st, m.n, D.aoff.p, D.z.p, P, L.nao, S.P.p, pop.p);
+    diag_blocks.resize(m.n);
+    CUDA_OK(cudaMemcpyAsync(diag_blocks.data(), pop.p, sizeof(double) * m.n, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+  }
+  CUDA_OK(cudaEventRecord(t1, st));
+  CUDA_OK(cudaEventSynchronize(t1));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, t0, t1);
+  g_prof.flush();
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+
+  double corr = parts[0];
+  corr += parts[1];
+  corr += parts[4];
+  corr += parts[2];
+  corr += parts[3];
+  const double core_ev = D.core_core_ev;
+  const double total = S.electronic_ev + core_ev + corr * kKcalToEv;
+  double e_isol = 0.0, eheat = 0.0;
+  for (int zz : m.z) {
+    e_isol += ps.element(zz)->e_isol;
+    eheat += ps.element(zz)->eheat_ev;
+  }
+  const double dhf = (S.electronic_ev + core_ev - e_isol + eheat) * kEvToKcal + corr;
+  std::memset(res, 0, sizeof(*res));
+  res->iterations = S.iterations;
+  res->density_error = S.density_error;
+  if (!S.converged) {
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "PM7 SCF did not converge after %d iterations (error=%.3e)", S.iterations,
+                  S.density_error);
+    throw Failure{PM7_ERR_SCF_NOT_CONVERGED, buf};
+  }
+  const int nao = L.nao;
+  const size_t nn = (size_t)nao * nao;
+  std::vector<double> Ph(nn);
+  CUDA_OK(cudaMemcpyAsync(Ph.data(), S.P.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  std::vector<double> q(m.n);
+  for (int a = 0; a < m.n; ++a) q[a] = ps.element(m.z[a])->core - diag_blocks[a];
+  res->n_atoms = m.n;
+  res->nao = nao;
+  res->n_occ = S.n_occ;
+  res->n_occ_beta = S.n_occ_beta;
+  res->unrestricted = S.unrestricted;
+  res->converged = 1;
+  res->electronic_ev = S.electronic_ev;
+  res->core_ev = core_ev;
+  res->total_ev = total;
+  res->heat_of_formation_kcal = dhf;
+  res->correction_kcal = corr;
+  res->device_ms = ms;
+  // dipole breakdown (dipole.rs:282-350)
+  {
+    double ox = 0, oy = 0, oz = 0, net = 0;
+    for (double v : q) net += v;
+    if (std::fabs(net) > 0.5 && o.dipole_origin != PM7_DIPOLE_COORDINATES) {
+      double tx = 0, ty = 0, tz = 0, tot = 0;
+      for (int a = 0; a < m.n; ++a) {
+        extern const double *pm7_mass_table();
+        const double wgt = o.dipole_origin == PM7_DIPOLE_CENTRE_OF_MASS ? (m.z[a] < 87 ? pm7_mass_table()[m.z[a]] : 0.0)
+                                                                        : ps.element(m.z[a])->core;
+        tx += m.xyz[3 * a] * wgt;
+        ty += m.xyz[3 * a + 1] * wgt;
+        tz += m.xyz[3 * a + 2] * wgt;
+        tot += wgt;
+      }
+      if (tot > 0.0) {
+        ox = tx / tot;
+        oy = ty / tot;
+        oz = tz / tot;
+      }
+    }
+    double pc[3] = {0, 0, 0}, sp[3] = {0, 0, 0}, pd[3] = {0, 0, 0};
+    const double inv3 = 0.5773502691896258;
+    for (int a = 0; a < m.n; ++a) {
+      pc[0] += (m.xyz[3 * a] - ox) * q[a];
+      pc[1] += (m.xyz[3 * a + 1] - oy) * q[a];
+      pc[2] += (m.xyz[3 * a + 2] - oz) * q[a];
+      const ElementRec *e = ps.element(m.z[a]);
+      const int off = L.aoff[a];
+      auto Pm = [&](int i, int j) { return Ph[(size_t)(off + i) * nao + off + j]; };
+      if (e->n_orb >= 4) {
+        const double hyb = -2.0 * e->dd;
+        for (int k = 0; k < 3; ++k) sp[k] += hyb * Pm(0, 1 + k);
+      }
+      if (e->n_orb == 9) {
+        const double hyb = -2.0 * e->ddp[5];
+        pd[0] += hyb * (Pm(5, 3) + Pm(4, 1) + Pm(8, 2) - inv3 * Pm(6, 1));
+        pd[1] += hyb * (Pm(7, 3) - Pm(4, 2) + Pm(8, 1) - inv3 * Pm(6, 2));
+        pd[2] += hyb * (Pm(5, 1) + Pm(7, 2) + 2.0 * inv3 * Pm(6, 3));
+      }
+    }
+    double mag = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      res->dipole_point_charge[k] = pc[k] * kAuDipoleToDebye;
+      res->dipole_sp_hybrid[k] = sp[k] * kAuDipoleToDebye;
+      res->dipole_pd_hybrid[k] = pd[k] * kAuDipoleToDebye;
+      res->dipole_debye[k] = res->dipole_point_charge[k] + res->dipole_sp_hybrid[k] + res->dipole_pd_hybrid[k];
+      mag += res->dipole_debye[k] * res->dipole_debye[k];
+    }
+    res->dipole_magnitude = std::sqrt(mag);
+  }
+  const double nan = std::numeric_limits<double>::quiet_NaN();
+  res->homo_ev = S.n_occ >= 1 ? S.eps_a[S.n_occ - 1] : nan;
+  res->lumo_ev = S.n_occ < nao ? S.eps_a[S.n_occ] : nan;
+  res->homo_ev_beta = res->lumo_ev_beta = nan;
+  if (S.unrestricted) {
+    res->homo_ev_beta = S.n_occ_beta >= 1 ? S.eps_b[S.n_occ_beta - 1] : nan;
+    res->lumo_ev_beta = S.n_occ_beta < nao ? S.eps_b[S.n_occ_beta] : nan;
+  }
+  res->charges = host_vec(q);
+  res->mo_energies = host_vec(S.eps_a);
+  if (S.unrestricted) res->mo_energies_beta = host_vec(S.eps_b);
+  if (o.want_matrices) {
+    res->density = host_vec(Ph);
+    if (S.unrestricted) res->spin_density = host_copy(S.Pspin.p, nn, st);
+    DevBuf<double> T;
+    T.alloc(nn, st);
+    launch_transpose(st, nao, S.Va.p, T.p);
+    res->mo_coeff = host_copy(T.p, nn, st);
+    if (S.unrestricted) {
+      launch_transpose(st, nao, S.Vb.p, T.p);
+      res->mo_coeff_beta = host_copy(T.p, nn, st);
+    }
+    CUDA_OK(cudaStreamSynchronize(st));
+  }
+}
+
+template <class Fn>
+static pm7_status guarded(Fn fn) {
+  try {
+    fn();
+    g_last_error.clear();
+    return PM7_OK;
+  } catch (const Failure &f) {
+    g_last_error = f.msg;
+    return f.code;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return PM7_ERR_INVALID_INPUT;
+  }
+}
+
+// ---- stage entry points ----------------------------------------------------
+
+static void stage_core(const pm7_molecule *mol, const pm7_params *params, int force_dpath, double *h_out,
+                       int32_t *nao_out, const double *p_tot, const double *p_spin, double *f_out) {
+  Molecule m = to_molecule(mol);
+  const int method = *reinterpret_cast<const int *>(params);
+  const ParamSet &ps = param_set(method);
+  Layout L = build_layout(m, ps);
+  if (nao_out) *nao_out = L.nao;
+  if (!h_out && !f_out) return;
+  if (force_dpath || L.has_d)
+    throw Failure{PM7_ERR_UNSUPPORTED, "MNDO/d (spd) pair integrals are not implemented on the device"};
+  DeviceContext &ctx = context_for(0);
+  std::lock_guard<std::mutex> lock(ctx.run_mutex);
+  CUDA_OK(cudaSetDevice(ctx.device));
+  const DeviceParams &P = device_params(ctx, method);
+  cudaStream_t st = ctx.stream;
+  DeviceMolecule D;
+  build_device_molecule(D, m, L, P, st);
+  const size_t nn = (size_t)L.nao * L.nao;
+  if (h_out) CUDA_OK(cudaMemcpyAsync(h_out, D.H.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+  if (f_out) {
+    DevBuf<double> Pt, Ps, F;
+    upload(Pt, std::vector<double>(p_tot, p_tot + nn), st);
+    upload(Ps, std::vector<double>(p_spin, p_spin + nn), st);
+    F.alloc(nn, st);
+    launch_fock(st, D.geometry(), P, D.H.p, Pt.p, Ps.p, 1.0, F.p, D.pop.p, D.jbuf.p);
+    CUDA_OK(cudaMemcpyAsync(f_out, F.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+  }
+  CUDA_OK(cudaStreamSynchronize(st));
+}
+
+}  // namespace pm7
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+using namespace pm7;
+
+#include "pm7_param_data.h"
+namespace pm7 {
+const double *pm7_mass_table() { return PM7_MASS; }
+}
+
+struct pm7_params {
+  int method;
+};
+
+extern "C" {
+
+pm7_status pm7_params_load(int32_t method, const pm7_params **out) {
+  static pm7_params sets[5] = {{0}, {1}, {2}, {3}, {4}};
+  if (!out) return PM7_ERR_INVALID_INPUT;
+  if (method < 0 || method > 4) {
+    g_last_error = "unknown PM7 method";
+    return PM7_ERR_INVALID_INPUT;
+  }
+  return guarded([&] {
+    param_set(method);
+    *out = &sets[method];
+  });
+}
+
+void pm7_options_default(pm7_options *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->method = PM7_METHOD_PM7;
+  o->charge = 0.0;
+  o->multiplicity = 1;
+  o->max_scf = 200;
+  o->e_tol = 1.0e-8;
+  o->p_tol = 1.0e-7;
+  o->use_diis = 1;
+  o->accelerator = PM7_ACCEL_ADIIS_CDIIS;
+  o->adiis_switch = 0.1;
+  o->level_shift = 0.0;
+  o->reference = PM7_REF_AUTO;
+  o->force_dpath = 0;
+  o->smooth_dispersion = 0;
+  o->max_memory_mb = -1;
+  o->dipole_origin = PM7_DIPOLE_CENTRE_OF_MASS;
+  o->initial_density = nullptr;
+  o->initial_spin_density = nullptr;
+  o->precision = PM7_PRECISION_FP64;
+  o->device = 0;
+  o->want_matrices = 1;
+}
+
+pm7_status pm7_run(const pm7_molecule *molecule, const pm7_params *params, const pm7_options *options,
+                   pm7_result *result) {
+  return guarded([&] { run_impl(molecule, params, options, result); });
+}
+
+void pm7_result_free(pm7_result *r) {
+  if (!r) return;
+  double **arrs[] = {&r->charges, &r->density, &r->spin_density, &r->mo_energies, &r->mo_coeff,
+                     &r->mo_energies_beta, &r->mo_coeff_beta};
+  for (double **a : arrs) {
+    std::free(*a);
+    *a = nullptr;
+  }
+}
+
+const char *pm7_last_error_message(void) { return g_last_error.c_str(); }
+
+int32_t pm7_device_count(void) {
+  int c = 0;
+  if (cudaGetDeviceCount(&c) != cudaSuccess) return 0;
+  return c;
+}
+
+pm7_status pm7_stage_core_hamiltonian(const pm7_molecule *molecule, const pm7_params *params, int32_t force_dpath,
+                                      double *h_out, int32_t *nao_out) {
+  return guarded([&] { stage_core(molecule, params, force_dpath, h_out, nao_out, nullptr, nullptr, nullptr); });
+}
+
+pm7_status pm7_stage_fock(const pm7_molecule *molecule, const pm7_params *params, int32_t force_dpath,
+                          const double *p_tot, const double *p_spin, double *f_out) {
+  return guarded([&] { stage_core(molecule, params, force_dpath, nullptr, nullptr, p_tot, p_spin, f_out); });
+}
+
+pm7_status pm7_stage_pair(const pm7_params *params, int32_t z_i, int32_t z_j, const double d[3], int32_t force_dpath,
+                          double *w_out, double *e1b_out, double *e2a_out, double *s_out, int32_t *npair_i,
+                          int32_t *npair_j) {
+  return guarded([&] {
+    const int method = *reinterpret_cast<const int *>(params);
+    const ParamSet &ps = param_set(method);
+    const ElementRec *ei = ps.element(z_i), *ej = ps.element(z_j);
+    if (!ei) throw Failure{PM7_ERR_MISSING_ELEMENT, "missing PM7 parameter block for Z=" + std::to_string(z_i)};
+    if (!ej) throw Failure{PM7_ERR_MISSING_ELEMENT, "missing PM7 parameter block for Z=" + std::to_string(z_j)};
+    if (ei->n_orb < ej->n_orb) throw Failure{PM7_ERR_INVALID_INPUT, "the first atom must carry at least as many orbitals"};
+    if (force_dpath || ei->n_orb == 9 || ej->n_orb == 9)
+      throw Failure{PM7_ERR_UNSUPPORTED, "MNDO/d (spd) pair integrals are not implemented on the device"};
+    DeviceContext &ctx = context_for(0);
+    std::lock_guard<std::mutex> lock(ctx.run_mutex);
+    CUDA_OK(cudaSetDevice(ctx.device));
+    const DeviceParams &P = device_params(ctx, method);
+    cudaStream_t st = ctx.stream;
+    DevBuf<double> buf;
+    buf.alloc(2025 + 3 * 81, st);
+    DevBuf<int> ib;
+    ib.alloc(3, st);
+    CUDA_OK(cudaMemsetAsync(ib.p, 0, 3 * sizeof(int), st));
+    launch_stage_pair(st, P, z_i, z_j, d, buf.p, buf.p + 2025, buf.p + 2025 + 81, buf.p + 2025 + 162, ib.p, ib.p + 2);
+    int h[3];
+    std::vector<double> hb(2025 + 3 * 81);
+    CUDA_OK(cudaMemcpyAsync(hb.data(), buf.p, sizeof(double) * hb.size(), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(h, ib.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    if (h[2]) throw Failure{PM7_ERR_UNSUPPORTED, "Slater overlaps for valence shells with n >= 4 are not implemented on the device"};
+    *npair_i = h[0];
+    *npair_j = h[1];
+    std::memcpy(w_out, hb.data(), sizeof(double) * h[0] * h[1]);
+    std::memcpy(e1b_out, hb.data() + 2025, sizeof(double) * 81);
+    std::memcpy(e2a_out, hb.data() + 2025 + 81, sizeof(double) * 81);
+    std::memcpy(s_out, hb.data() + 2025 + 162, sizeof(double) * 81);
+  });
+}
+
+pm7_status pm7_stage_core_core(const pm7_molecule *molecule, const pm7_params *params, double *energy_ev) {
+  return guarded([&] {
+    Molecule m = to_molecule(molecule);
+    const int method = *reinterpret_cast<const int *>(params);
+    const ParamSet &ps = param_set(method);
+    Layout L = build_layout(m, ps);
+    DeviceContext &ctx = context_for(0);
+    std::lock_guard<std::mutex> lock(ctx.run_mutex);
+    CUDA_OK(cudaSetDevice(ctx.device));
+    const DeviceParams &P = device_params(ctx, method);
+    DeviceMolecule D;
+    build_device_molecule(D, m, L, P, ctx.stream);
+    *energy_ev = D.core_core_ev;
+  });
+}
+
+pm7_status pm7_stage_corrections(const pm7_molecule *molecule, int32_t method, int32_t smooth_dispersion,
+                                 double out[5]) {
+  return guarded([&] {
+    Molecule m = to_molecule(molecule);
+    DeviceContext &ctx = context_for(0);
+    std::lock_guard<std::mutex> lock(ctx.run_mutex);
+    CUDA_OK(cudaSetDevice(ctx.device));
+    cudaStream_t st = ctx.stream;
+    DevBuf<int> z;
+    DevBuf<double> xyz, scratch, res;
+    upload(z, m.z, st);
+    upload(xyz, m.xyz, st);
+    scratch.alloc(corrections_scratch(m.n), st);
+    res.alloc(5, st);
+    launch_corrections(st, m.n, z.p, xyz.p, method, smooth_dispersion, scratch.p, scratch.n, res.p);
+    CUDA_OK(cudaMemcpyAsync(out, res.p, sizeof(double) * 5, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+int64_t pm7_launch_count(void) { return g_launches.load(); }
+
+void pm7_profile_enable(int32_t on) { g_prof.reset(on != 0); }
+
+int32_t pm7_profile_count(void) {
+  g_prof.flush();
+  return (int32_t)g_prof.names.size();
+}
+
+pm7_status pm7_profile_entry(int32_t i, const char **name, double *total_ms, int64_t *calls) {
+  if (i < 0 || i >= (int32_t)g_prof.names.size()) return PM7_ERR_INVALID_INPUT;
+  if (name) *name = g_prof.names[i].c_str();
+  if (total_ms) *total_ms = g_prof.total_ms[i];
+  if (calls) *calls = g_prof.calls[i];
+  return PM7_OK;
+}
+
+// sizeof of the ABI structs, for the ctypes mirror's self-check.
+void pm7_abi_sizes(int64_t out[3]) {
+  out[0] = (int64_t)sizeof(pm7_molecule);
+  out[1] = (int64_t)sizeof(pm7_options);
+  out[2] = (int64_t)sizeof(pm7_result);
+}
+
+}  // extern "C"

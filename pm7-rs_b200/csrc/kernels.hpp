@@ -1,0 +1,102 @@
+// Host-callable launchers of the engine's CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "device_params.hpp"
+
+namespace pm7 {
+
+// Counts kernels launched by this library (read through pm7_launch_count()).
+void note_launch(int kernels = 1);
+
+// An atom pair closer than the 7 Angstrom feather range, whose two-electron block is
+// stored. u < v; w is npair(u) x npair(v) row-major at `woff`; the packed per-atom
+// blocks (electron-core attraction, then the Coulomb scratch of the Fock build) of
+// u and v start at eoff_u / eoff_v.
+struct NearPair {
+  int32_t u, v;
+  int64_t woff;
+  int32_t eoff_u, eoff_v;
+};
+
+// ---- build (kernels_build.cu) ----
+void launch_pairs_all(cudaStream_t st, int n_atoms, const int *z, const double *xyz, const int *aoff, int nao,
+                      const DeviceParams &P, double *H, double *cc_partial, int *status);
+size_t pairs_all_partials(int n_atoms);
+void launch_near_integrals(cudaStream_t st, int n_near, const int *z, const double *xyz, const NearPair *np,
+                           const DeviceParams &P, double *w, double *ecore, int *status);
+void launch_hcore_diag(cudaStream_t st, int n_atoms, const int *z, const double *xyz, const int *aoff,
+                       const int *csr_start, const int2 *csr, const NearPair *np, const double *ecore,
+                       const unsigned char *near_mask, const DeviceParams &P, int nao, double *H);
+void launch_sum_partials(cudaStream_t st, const double *in, size_t n, double *out);
+
+// ---- Fock build (kernels_fock.cu) ----
+struct FockGeometry {
+  int n_atoms, nao, n_near;
+  const int *z, *aoff, *ao_atom;
+  const double *xyz;
+  const unsigned char *near_mask;  // n_atoms^2
+  const NearPair *np;
+  const int *csr_start;
+  const int2 *csr;  // (partner atom, near-pair index), sorted by partner
+  const double *w;
+};
+// F = H + J(Pt) - K(s * Ps). `pop` (n_atoms) and `jbuf` (packed, like ecore) are scratch.
+void launch_fock(cudaStream_t st, const FockGeometry &g, const DeviceParams &P, const double *H, const double *Pt,
+                 const double *Ps, double s_scale, double *F, double *pop, double *jbuf);
+
+// ---- dense algebra (kernels_dense.cu) ----
+// C[M x N] = alpha * A^T B, A: K x M row-major (lda), B: K x N row-major (ldb), C row-major (ldc). FP64 DMMA.
+void launch_gemm_tn(cudaStream_t st, int M, int N, int K, double alpha, const double *A, int lda, const double *B,
+                    int ldb, double *C, int ldc);
+// P = w * V^T V for the first k rows of V (n columns, row stride ldv); symmetric output.
+void launch_density(cudaStream_t st, int n, int k, double w, const double *V, int ldv, double *P);
+// E = X - X^T, partial sums of E*E into `partials` (returns the partial count).
+size_t launch_antisym(cudaStream_t st, int n, const double *X, double *E, double *partials);
+// partials of sum(a*b) (returns the count).
+size_t launch_dot(cudaStream_t st, size_t len, const double *a, const double *b, double *partials);
+// partials of sum(P*(H+F)).
+size_t launch_energy(cudaStream_t st, size_t len, const double *P, const double *H, const double *F,
+                     double *partials);
+// partials of sum((a-b)^2).
+size_t launch_sqdiff(cudaStream_t st, size_t len, const double *a, const double *b, double *partials);
+// out = sum_i c[i] * X[i] (+ shift*(I - Pd/occ)); coefficients in device memory.
+void launch_combine(cudaStream_t st, int n, int k, const double *const *X, const double *c, const double *Pd,
+                    double occ, double shift, double *out);
+// Many dot products <X_i, Y_j> in one pass: out[i*ny + j] partials; see kernels_dense.cu.
+void launch_dot_many(cudaStream_t st, size_t len, int nx, const double *const *X, int ny, const double *const *Y,
+                     double *out_partials, int n_blocks);
+void launch_reduce_rows(cudaStream_t st, const double *partials, int n_rows, int n_cols, double *out);
+void launch_sum(cudaStream_t st, const double *partials, size_t n, double *out);
+void launch_transpose(cudaStream_t st, int n, const double *in, double *out);
+void launch_scale(cudaStream_t st, size_t len, double s, const double *in, double *out);
+void launch_axpby(cudaStream_t st, size_t len, double a, const double *x, double b, const double *y, double *out);
+void launch_set_diag(cudaStream_t st, int n, const double *diag, double *M);
+void launch_atom_pop(cudaStream_t st, int n_atoms, const int *aoff, const int *z, const DeviceParams &P,
+                     int nao, const double *Pm, double *pop);
+
+// ---- corrections (kernels_corr.cu) ----
+// out[0] dispersion, out[1] H-bond, out[2] C#C, out[3] Si-O-H, out[4] PM7-HH (kcal/mol).
+void launch_corrections(cudaStream_t st, int n_atoms, const int *z, const double *xyz, int method, int smooth,
+                        double *scratch, size_t scratch_len, double *out);
+size_t corrections_scratch(int n_atoms);
+
+}  // namespace pm7
+
+namespace pm7 {
+void launch_stage_pair(cudaStream_t st, const DeviceParams &P, int zi, int zj, const double d[3], double *w,
+                       double *e1b, double *e2a, double *s, int *np_out, int *status);
+}
+
+namespace pm7 {
+// SP2 purification building blocks (kernels_dense.cu).
+void launch_gershgorin(cudaStream_t st, int n, const double *F, double *scratch, double *bounds);
+void launch_sp2_init(cudaStream_t st, int n, const double *F, const double *bounds, double *X);
+void launch_sp2_square(cudaStream_t st, int n, const double *X, double *X2);
+void launch_sp2_trace(cudaStream_t st, int n, const double *X, const double *X2, double n_occ, double *state);
+void launch_sp2_update(cudaStream_t st, int n, double *X, const double *X2, const double *state);
+}

@@ -1,0 +1,347 @@
+// One-time device build of a molecule: resonance (beta*S) blocks and core-core
+// energies over all atom pairs, the stored two-electron blocks of the near pairs
+// (r < 7 Angstrom), and the diagonal blocks of the core Hamiltonian.
+//
+// Follows pm7-rs src/hamiltonian.rs:310-638 (build_core_generic, molecular path)
+// and src/repulsion.rs:16-36,164-263 (core_core_energy).
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "kernels.hpp"
+#include "nddo_sp.cuh"
+
+namespace pm7 {
+
+__device__ __forceinline__ double beta_of(const ElementRec &e, int orb) {
+  return orb == 0 ? e.beta_s : (orb <= 3 ? e.beta_p : e.beta_d);
+}
+
+// Core Gaussian of element `src` for slot `s` (repulsion.rs:250-263).
+__device__ __forceinline__ double core_gaussian(const ElementRec &src, double zz, double ra, int s) {
+  if (s >= src.n_gauss) return 0.0;
+  const double k = src.gauss[s][0], l = src.gauss[s][1], m = src.gauss[s][2];
+  const double ax = (ra - m) * (ra - m) * l;
+  if (ax >= 25.0) return 0.0;
+  return exp(-ax) * (zz * k) / ra;
+}
+
+// PM7 ccrep for one pair at distance r (Bohr), eV (repulsion.rs:164-248).
+__device__ double pair_core_energy(const DeviceParams &P, const ElementRec &ei, const ElementRec &ej, double r) {
+  const int zi = ei.z, zj = ej.z;
+  const double ra = r * kA0;
+  const double zz = ei.core * ej.core;
+  const double po9i = ei.poc > 1.0e-5 ? ei.poc : ei.rho0;
+  const double po9j = ej.poc > 1.0e-5 ? ej.poc : ej.rho0;
+  const double gnddo = (1.0 / sqrt(r * r + (po9i + po9j) * (po9i + po9j))) * kEv;
+  double cf, pt;
+  d_feather(r, cf, pt);
+  double enuc = (gnddo * cf + pt * (1.0 - cf)) * zz;
+  const PairParamRec pp = P.pairs[zi * kMaxZ + zj];
+  const bool defined = fabs(pp.xfac) > 1.0e-5;
+  if (defined) {
+    const double alpb = pp.alpb < 1.0e-6 ? 1.2 : pp.alpb;
+    const double ra6 = ra * ra * ra * ra * ra * ra;
+    double scale = 1.0 + exp(-(ra + ra6 * 0.0003) * alpb) * (2.0 * pp.xfac);
+    const int hi = zi > zj ? zi : zj, lo = zi > zj ? zj : zi;
+    if (lo == 1 && (hi == 6 || hi == 7)) {
+      scale = 1.0 + exp(-(ra * ra) * alpb) * (2.0 * pp.xfac);
+    } else if (lo == 1 && hi == 8) {
+      scale = 1.0 + exp(-(ra * ra) * alpb) * (2.0 * pp.xfac) - exp(ra * (-2.0 * P.vpar[4])) * P.vpar[3];
+    } else if (lo == 6 && hi == 6) {
+      scale = scale + exp(ra * (-P.vpar[2])) * P.vpar[1];
+    } else if (lo == 8 && hi == 14) {
+      scale = scale - exp(-(ra - 2.9) * (ra - 2.9)) * 0.0007;
+    }
+    enuc *= scale;
+  } else {
+    const bool ln = (zi >= 57 && zi <= 71) || (zj >= 57 && zj <= 71);
+    enuc *= 1.0 + exp(ra * (ln ? -3.0 : -2.18)) * 10.0;
+  }
+  double corr = core_gaussian(ei, zz, ra, 0) + core_gaussian(ej, zz, ra, 0);
+  if (!defined)
+    for (int s = 0; s < 4; ++s) corr += core_gaussian(ei, zz, ra, s) + core_gaussian(ej, zz, ra, s);
+  const double red = ra / (pow((double)zi, 0.3333) + pow((double)zj, 0.3333));
+  if (red < 3.0) {
+    const double r2 = red * red, r4 = r2 * r2, r12 = r4 * r4 * r4;
+    const double guard = (1.0 / r12) * 1.0e-8;
+    corr += guard < 1.0e5 ? guard : 1.0e5;
+  }
+  return enuc + corr;
+}
+
+// All pairs u < v: beta*S off-diagonal blocks of H and the core-core energy.
+// Grid: (ceil(N/128), N), block 128; blockIdx.y = u. Energies are reduced per
+// block into `cc_partial[blockIdx.y * gridDim.x + blockIdx.x]`.
+__global__ void k_pairs_all(int n_atoms, const int *__restrict__ z, const double *__restrict__ xyz,
+                            const int *__restrict__ aoff, int nao, DeviceParams P, double *__restrict__ H,
+                            double *__restrict__ cc_partial, int *__restrict__ status) {
+  const int u = blockIdx.y;
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  double ecc = 0.0;
+  if (v > u && v < n_atoms) {
+    const ElementRec &eu = P.elements[z[u]];
+    const ElementRec &ev = P.elements[z[v]];
+    // heavier-first ordering (hamiltonian.rs:388-392)
+    const bool keep = eu.n_orb >= ev.n_orb;
+    const int a = keep ? u : v, b = keep ? v : u;
+    const ElementRec &ea = keep ? eu : ev;
+    const ElementRec &eb = keep ? ev : eu;
+    const double dx = xyz[3 * b] - xyz[3 * a], dy = xyz[3 * b + 1] - xyz[3 * a + 1], dz = xyz[3 * b + 2] - xyz[3 * a + 2];
+    double S[4][4];
+    if (!d_overlap_sp(ea, eb, dx, dy, dz, S)) {
+      atomicOr(status, 1);
+    } else {
+      const int oa = aoff[a], ob = aoff[b];
+      for (int i = 0; i < ea.n_orb && i < 4; ++i) {
+        const double bi = beta_of(ea, i);
+        for (int j = 0; j < eb.n_orb && j < 4; ++j) {
+          const double val = 0.5 * (bi + beta_of(eb, j)) * S[i][j];
+          H[(size_t)(oa + i) * nao + ob + j] = val;
+          H[(size_t)(ob + j) * nao + oa + i] = val;
+        }
+      }
+    }
+    ecc = pair_core_energy(P, eu, ev, sqrt((xyz[3 * v] - xyz[3 * u]) * (xyz[3 * v] - xyz[3 * u]) +
+                                           (xyz[3 * v + 1] - xyz[3 * u + 1]) * (xyz[3 * v + 1] - xyz[3 * u + 1]) +
+                                           (xyz[3 * v + 2] - xyz[3 * u + 2]) * (xyz[3 * v + 2] - xyz[3 * u + 2])));
+  }
+  const double s = block_sum<128>(ecc);
+  if (threadIdx.x == 0) cc_partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+
+// Near pairs: store w in (u,v) orientation and the packed electron-core blocks of
+// both atoms (integrals.rs:186-271 for the sp kernel). One thread per pair.
+__global__ void k_near_integrals(int n_near, const int *__restrict__ z, const double *__restrict__ xyz,
+                                 const NearPair *__restrict__ np, DeviceParams P, double *__restrict__ w,
+                                 double *__restrict__ ecore, int *__restrict__ status) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_near) return;
+  const NearPair q = np[p];
+  const ElementRec &eu = P.elements[z[q.u]];
+  const ElementRec &ev = P.elements[z[q.v]];
+  if (eu.n_orb == 9 || ev.n_orb == 9) {
+    atomicOr(status, 2);
+    return;
+  }
+  const bool keep = eu.n_orb >= ev.n_orb;
+  const int a = keep ? q.u : q.v, b = keep ? q.v : q.u;
+  const ElementRec &ea = keep ? eu : ev;
+  const ElementRec &eb = keep ? ev : eu;
+  const double dx = xyz[3 * b] - xyz[3 * a], dy = xyz[3 * b + 1] - xyz[3 * a + 1], dz = xyz[3 * b + 2] - xyz[3 * a + 2];
+  const double r = sqrt(dx * dx + dy * dy + dz * dz);
+  const double inv = 1.0 / r;
+  double rot[3][3];
+  d_rotation_to_x(-(dx * inv), -(dy * inv), -(dz * inv), rot);
+  const bool ha = ea.n_orb >= 4, hb = eb.n_orb >= 4;
+  double *wp = w + q.woff;
+  double *e_a = ecore + (keep ? q.eoff_u : q.eoff_v);
+  double *e_b = ecore + (keep ? q.eoff_v : q.eoff_u);
+  if (!ha && !hb) {
+    const double aee = (ea.rho0 + eb.rho0) * (ea.rho0 + eb.rho0);
+    double cf, pt;
+    d_feather(r, cf, pt);
+    const double ee = (1.0 / sqrt(r * r + aee)) * kEv * cf + pt * (1.0 - cf);
+    wp[0] = ee;
+    e_a[0] = ee * (-eb.core);
+    e_b[0] = ee * (-ea.core);
+    return;
+  }
+  if (ha && !hb) {
+    double ri[4];
+    d_local_xh(ea, eb, r, ri);
+    double wxh[10];
+    wxh[0] = ri[0];
+    for (int k = 0; k < 3; ++k) wxh[dpack(k + 1, 0)] = ri[1] * rot[0][k];
+    for (int k = 0; k < 3; ++k)
+      for (int l = 0; l <= k; ++l)
+        wxh[dpack(k + 1, l + 1)] =
+            ri[2] * (rot[0][k] * rot[0][l]) + ri[3] * (rot[1][k] * rot[1][l] + rot[2][k] * rot[2][l]);
+    // (u,v) orientation: heavy atom a is u when kept, otherwise v -- a 10x1 or 1x10 block,
+    // stored identically because one dimension is 1.
+    for (int k = 0; k < 10; ++k) {
+      wp[k] = wxh[k];
+      e_a[k] = wxh[k] * (-eb.core);
+    }
+    e_b[0] = wxh[0] * (-ea.core);
+    return;
+  }
+  double ri[22];
+  d_local_xx(ea, eb, r, ri);
+  int pi = 0;
+  for (int kk = 0; kk < 4; ++kk)
+    for (int ll = 0; ll <= kk; ++ll, ++pi) {
+      int pj = 0;
+      for (int mm = 0; mm < 4; ++mm)
+        for (int nn = 0; nn <= mm; ++nn, ++pj) {
+          const double val = d_rotate_xx_elem(ri, rot, kk, ll, mm, nn);
+          if (keep) wp[pi * 10 + pj] = val;
+          else wp[pj * 10 + pi] = val;
+          if (pj == 0) e_a[pi] = val * (-eb.core);
+          if (pi == 0) e_b[pj] = val * (-ea.core);
+        }
+    }
+}
+
+// Diagonal atom blocks of H_core: U on the diagonal plus the electron-core
+// attraction of every other atom. Near partners contribute their stored packed
+// blocks (summed in partner order); every other atom is beyond the 7 Angstrom
+// feather range, where the attraction is exactly the point charge -Z_B * EV / r on
+// the diagonal (integrals.rs:540-574). One block per atom.
+constexpr int HDIAG_THREADS = 128;
+__global__ void __launch_bounds__(HDIAG_THREADS) k_hcore_diag(int n_atoms, const int *__restrict__ z,
+                                                              const double *__restrict__ xyz,
+                                                              const int *__restrict__ aoff,
+                                                              const int *__restrict__ csr_start,
+                                                              const int2 *__restrict__ csr,
+                                                              const NearPair *__restrict__ np,
+                                                              const double *__restrict__ ecore,
+                                                              const unsigned char *__restrict__ near_mask,
+                                                              DeviceParams P, int nao, double *__restrict__ H) {
+  const int A = blockIdx.x;
+  const ElementRec &e = P.elements[z[A]];
+  const int no = e.n_orb, off = aoff[A];
+  if (no == 0) return;
+  const int npk = no * (no + 1) / 2;
+  __shared__ double s_far;
+  __shared__ double acc[45];
+  const double xa = xyz[3 * A], ya = xyz[3 * A + 1], za = xyz[3 * A + 2];
+  const unsigned char *mask = near_mask + (size_t)A * n_atoms;
+  double far = 0.0;
+  for (int B = threadIdx.x; B < n_atoms; B += HDIAG_THREADS) {
+    if (B == A || mask[B]) continue;
+    const double dx = xyz[3 * B] - xa, dy = xyz[3 * B + 1] - ya, dz = xyz[3 * B + 2] - za;
+    far += -P.elements[z[B]].core * ((1.0 / sqrt(dx * dx + dy * dy + dz * dz)) * kEv);
+  }
+  far = block_sum<HDIAG_THREADS>(far);
+  if (threadIdx.x == 0) s_far = far;
+  const int c0 = csr_start[A], c1 = csr_start[A + 1];
+  for (int k = threadIdx.x; k < npk; k += HDIAG_THREADS) {
+    double a = 0.0;
+    for (int c = c0; c < c1; ++c) {
+      const NearPair q = np[csr[c].y];
+      a += ecore[(q.u == A ? q.eoff_u : q.eoff_v) + k];
+    }
+    acc[k] = a;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < npk; idx += HDIAG_THREADS) {
+    int mu = 0;
+    while ((mu + 1) * (mu + 2) / 2 <= idx) ++mu;
+    const int nu = idx - mu * (mu + 1) / 2;
+    double v = acc[idx];
+    if (mu == nu) v += (mu == 0 ? e.u_ss : (mu <= 3 ? e.u_pp : e.u_dd)) + s_far;
+    H[(size_t)(off + mu) * nao + off + nu] = v;
+    H[(size_t)(off + nu) * nao + off + mu] = v;
+  }
+}
+
+__global__ void k_sum_partials(const double *__restrict__ in, size_t n, double *__restrict__ out) {
+  double s = 0.0;
+  for (size_t i = threadIdx.x; i < n; i += blockDim.x) s += in[i];
+  s = block_sum<256>(s);
+  if (threadIdx.x == 0) *out = s;
+}
+
+// ---- host launchers ------------------------------------------------------
+
+void launch_pairs_all(cudaStream_t st, int n_atoms, const int *z, const double *xyz, const int *aoff, int nao,
+                      const DeviceParams &P, double *H, double *cc_partial, int *status) {
+  if (n_atoms < 2) return;
+  dim3 grid((n_atoms + 127) / 128, n_atoms);
+  k_pairs_all<<<grid, 128, 0, st>>>(n_atoms, z, xyz, aoff, nao, P, H, cc_partial, status);
+  note_launch();
+}
+
+size_t pairs_all_partials(int n_atoms) { return (size_t)((n_atoms + 127) / 128) * (size_t)n_atoms; }
+
+void launch_near_integrals(cudaStream_t st, int n_near, const int *z, const double *xyz, const NearPair *np,
+                           const DeviceParams &P, double *w, double *ecore, int *status) {
+  if (n_near == 0) return;
+  k_near_integrals<<<(n_near + 127) / 128, 128, 0, st>>>(n_near, z, xyz, np, P, w, ecore, status);
+  note_launch();
+}
+
+void launch_hcore_diag(cudaStream_t st, int n_atoms, const int *z, const double *xyz, const int *aoff,
+                       const int *csr_start, const int2 *csr, const NearPair *np, const double *ecore,
+                       const unsigned char *near_mask, const DeviceParams &P, int nao, double *H) {
+  k_hcore_diag<<<n_atoms, HDIAG_THREADS, 0, st>>>(n_atoms, z, xyz, aoff, csr_start, csr, np, ecore, near_mask, P,
+                                                  nao, H);
+  note_launch();
+}
+
+void launch_sum_partials(cudaStream_t st, const double *in, size_t n, double *out) {
+  k_sum_partials<<<1, 256, 0, st>>>(in, n, out);
+  note_launch();
+}
+
+}  // namespace pm7
+
+namespace pm7 {
+
+// One pair's blocks in the (i, j) orientation with n_orb(i) >= n_orb(j), for the
+// stage entry point: w (npair_i x npair_j), e1b/e2a (9x9) and the overlap (9x9).
+__global__ void k_stage_pair(DeviceParams P, int zi, int zj, double dx, double dy, double dz, double *w,
+                             double *e1b, double *e2a, double *s, int *np_out, int *status) {
+  const ElementRec &ea = P.elements[zi];
+  const ElementRec &eb = P.elements[zj];
+  for (int k = 0; k < 81; ++k) e1b[k] = e2a[k] = s[k] = 0.0;
+  double S[4][4];
+  if (!d_overlap_sp(ea, eb, dx, dy, dz, S)) {
+    *status = 1;
+    return;
+  }
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) s[i * 9 + j] = (i < ea.n_orb && j < eb.n_orb) ? S[i][j] : S[i][j];
+  const double r = sqrt(dx * dx + dy * dy + dz * dz), inv = 1.0 / r;
+  double rot[3][3];
+  d_rotation_to_x(-(dx * inv), -(dy * inv), -(dz * inv), rot);
+  const bool ha = ea.n_orb >= 4, hb = eb.n_orb >= 4;
+  if (!ha && !hb) {
+    double cf, pt;
+    d_feather(r, cf, pt);
+    const double ee = (1.0 / sqrt(r * r + (ea.rho0 + eb.rho0) * (ea.rho0 + eb.rho0))) * kEv * cf + pt * (1.0 - cf);
+    w[0] = ee;
+    e1b[0] = ee * (-eb.core);
+    e2a[0] = ee * (-ea.core);
+    np_out[0] = np_out[1] = 1;
+    return;
+  }
+  if (ha && !hb) {
+    double ri[4];
+    d_local_xh(ea, eb, r, ri);
+    w[0] = ri[0];
+    for (int k = 0; k < 3; ++k) w[dpack(k + 1, 0)] = ri[1] * rot[0][k];
+    for (int k = 0; k < 3; ++k)
+      for (int l = 0; l <= k; ++l)
+        w[dpack(k + 1, l + 1)] = ri[2] * (rot[0][k] * rot[0][l]) + ri[3] * (rot[1][k] * rot[1][l] + rot[2][k] * rot[2][l]);
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) e1b[a * 9 + b] = w[dpack(a, b)] * (-eb.core);
+    e2a[0] = w[0] * (-ea.core);
+    np_out[0] = 10;
+    np_out[1] = 1;
+    return;
+  }
+  double ri[22];
+  d_local_xx(ea, eb, r, ri);
+  int pi = 0;
+  for (int kk = 0; kk < 4; ++kk)
+    for (int ll = 0; ll <= kk; ++ll, ++pi) {
+      int pj = 0;
+      for (int mm = 0; mm < 4; ++mm)
+        for (int nn = 0; nn <= mm; ++nn, ++pj) w[pi * 10 + pj] = d_rotate_xx_elem(ri, rot, kk, ll, mm, nn);
+    }
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) {
+      e1b[a * 9 + b] = w[dpack(a, b) * 10] * (-eb.core);
+      e2a[a * 9 + b] = w[dpack(a, b)] * (-ea.core);
+    }
+  np_out[0] = np_out[1] = 10;
+}
+
+void launch_stage_pair(cudaStream_t st, const DeviceParams &P, int zi, int zj, const double d[3], double *w,
+                       double *e1b, double *e2a, double *s, int *np_out, int *status) {
+  k_stage_pair<<<1, 1, 0, st>>>(P, zi, zj, d[0], d[1], d[2], w, e1b, e2a, s, np_out, status);
+  note_launch();
+}
+
+}  // namespace pm7

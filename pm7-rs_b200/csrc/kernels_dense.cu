@@ -1,0 +1,468 @@
+// Dense FP64 algebra of the SCF loop: the tensor-core contractions (density
+// P = w V_occ^T V_occ and the DIIS commutator F P) and the HBM-bound reductions
+// around them. All reductions write fixed per-block partials that are summed in a
+// fixed order, so results are bitwise reproducible.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "kernels.hpp"
+
+namespace pm7 {
+
+// ---------------------------------------------------------------------------
+// FP64 tensor-core GEMM, C = alpha * A^T * B (A: K x M, B: K x N, both row-major).
+// mma.sync m8n8k4 (DMMA) is the FP64 tensor-core instruction on sm_100a; tcgen05
+// has no FP64 kind. 64x64x16 block tiles, 4 warps of 32x32, two-stage cp.async.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int BM = 64, BN = 64, BK = 16, PADW = 8;
+
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  const int bytes = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+}  // namespace
+
+// sym != 0: only tiles with bm >= bn are computed; the lower triangle is written and
+// mirrored, so the output is exactly symmetric (used for P = w V^T V).
+__global__ void __launch_bounds__(128) k_gemm_tn(int M, int N, int K, double alpha, const double *__restrict__ A,
+                                                 int lda, const double *__restrict__ B, int ldb,
+                                                 double *__restrict__ C, int ldc, int sym) {
+  const int bn = blockIdx.x, bm = blockIdx.y;
+  if (sym && bm < bn) return;
+  __shared__ __align__(16) double As[2][BK][BM + PADW];
+  __shared__ __align__(16) double Bs[2][BK][BN + PADW];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int g = lane >> 2, t = lane & 3;
+  const int m0 = bm * BM, n0 = bn * BN;
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  auto load_tile = [&](int stage, int k0) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int e = tid + 128 * i, row = e >> 6, col = e & 63;
+      const int kr = k0 + row;
+      const bool pa = kr < K && (m0 + col) < M;
+      const bool pb = kr < K && (n0 + col) < N;
+      cp_async8(&As[stage][row][col], pa ? A + (size_t)kr * lda + m0 + col : A, pa);
+      cp_async8(&Bs[stage][row][col], pb ? B + (size_t)kr * ldb + n0 + col : B, pb);
+    }
+    cp_async_commit();
+  };
+
+  const int ktiles = (K + BK - 1) / BK;
+  if (ktiles > 0) load_tile(0, 0);
+  for (int kt = 0; kt < ktiles; ++kt) {
+    const int stage = kt & 1;
+    if (kt + 1 < ktiles) {
+      load_tile(stage ^ 1, (kt + 1) * BK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[stage][kk + t][wm * 32 + i * 8 + g];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[stage][kk + t][wn * 32 + j * 8 + g];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int m = m0 + wm * 32 + i * 8 + g;
+        const int n = n0 + wn * 32 + j * 8 + 2 * t + h;
+        if (m >= M || n >= N) continue;
+        const double v = alpha * acc[i][j][h];
+        if (!sym) {
+          C[(size_t)m * ldc + n] = v;
+        } else if (m >= n) {
+          C[(size_t)m * ldc + n] = v;
+          C[(size_t)n * ldc + m] = v;
+        }
+      }
+}
+
+void launch_gemm_tn(cudaStream_t st, int M, int N, int K, double alpha, const double *A, int lda, const double *B,
+                    int ldb, double *C, int ldc) {
+  dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+  k_gemm_tn<<<grid, 128, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc, 0);
+  note_launch();
+}
+
+void launch_density(cudaStream_t st, int n, int k, double w, const double *V, int ldv, double *P) {
+  if (k == 0) {
+    cudaMemsetAsync(P, 0, sizeof(double) * (size_t)n * n, st);
+    return;
+  }
+  dim3 grid((n + BN - 1) / BN, (n + BM - 1) / BM);
+  k_gemm_tn<<<grid, 128, 0, st>>>(n, n, k, w, V, ldv, V, ldv, P, n, 1);
+  note_launch();
+}
+
+// ---------------------------------------------------------------------------
+// Reductions with fixed partial layouts.
+// ---------------------------------------------------------------------------
+constexpr int RED_BLOCKS = 592;  // 4 x 148 SMs
+constexpr int RED_THREADS = 256;
+
+__global__ void __launch_bounds__(RED_THREADS) k_dot(size_t len, const double *__restrict__ a,
+                                                     const double *__restrict__ b, double *__restrict__ partials) {
+  double s = 0.0;
+  for (size_t i = (size_t)blockIdx.x * RED_THREADS + threadIdx.x; i < len; i += (size_t)gridDim.x * RED_THREADS)
+    s += a[i] * b[i];
+  s = block_sum<RED_THREADS>(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_energy(size_t len, const double *__restrict__ P,
+                                                        const double *__restrict__ H, const double *__restrict__ F,
+                                                        double *__restrict__ partials) {
+  double s = 0.0;
+  for (size_t i = (size_t)blockIdx.x * RED_THREADS + threadIdx.x; i < len; i += (size_t)gridDim.x * RED_THREADS)
+    s += P[i] * (H[i] + F[i]);
+  s = block_sum<RED_THREADS>(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_sqdiff(size_t len, const double *__restrict__ a,
+                                                        const double *__restrict__ b, double *__restrict__ partials) {
+  double s = 0.0;
+  for (size_t i = (size_t)blockIdx.x * RED_THREADS + threadIdx.x; i < len; i += (size_t)gridDim.x * RED_THREADS) {
+    const double d = a[i] - b[i];
+    s += d * d;
+  }
+  s = block_sum<RED_THREADS>(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+size_t launch_dot(cudaStream_t st, size_t len, const double *a, const double *b, double *partials) {
+  k_dot<<<RED_BLOCKS, RED_THREADS, 0, st>>>(len, a, b, partials);
+  note_launch();
+  return RED_BLOCKS;
+}
+size_t launch_energy(cudaStream_t st, size_t len, const double *P, const double *H, const double *F,
+                     double *partials) {
+  k_energy<<<RED_BLOCKS, RED_THREADS, 0, st>>>(len, P, H, F, partials);
+  note_launch();
+  return RED_BLOCKS;
+}
+size_t launch_sqdiff(cudaStream_t st, size_t len, const double *a, const double *b, double *partials) {
+  k_sqdiff<<<RED_BLOCKS, RED_THREADS, 0, st>>>(len, a, b, partials);
+  note_launch();
+  return RED_BLOCKS;
+}
+
+__global__ void k_sum(const double *__restrict__ in, size_t n, double *__restrict__ out) {
+  double s = 0.0;
+  for (size_t i = threadIdx.x; i < n; i += blockDim.x) s += in[i];
+  s = block_sum<256>(s);
+  if (threadIdx.x == 0) *out = s;
+}
+void launch_sum(cudaStream_t st, const double *partials, size_t n, double *out) {
+  k_sum<<<1, 256, 0, st>>>(partials, n, out);
+  note_launch();
+}
+
+// E = X - X^T via 32x32 shared tiles; partial sums of E^2 per block.
+__global__ void k_antisym(int n, const double *__restrict__ X, double *__restrict__ E, double *__restrict__ partials) {
+  __shared__ double tile[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int r = ty; r < 32; r += 8) {
+    const int i = bx + r, j = by + tx;  // transposed tile source
+    tile[r][tx] = (i < n && j < n) ? X[(size_t)i * n + j] : 0.0;
+  }
+  __syncthreads();
+  double s = 0.0;
+  for (int r = ty; r < 32; r += 8) {
+    const int i = by + r, j = bx + tx;
+    if (i < n && j < n) {
+      const double e = X[(size_t)i * n + j] - tile[tx][r];
+      E[(size_t)i * n + j] = e;
+      s += e * e;
+    }
+  }
+  // block of 256 threads
+  s = block_sum<256>(s);
+  if (tx == 0 && ty == 0) partials[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+size_t launch_antisym(cudaStream_t st, int n, const double *X, double *E, double *partials) {
+  dim3 grid((n + 31) / 32, (n + 31) / 32), blk(32, 8);
+  k_antisym<<<grid, blk, 0, st>>>(n, X, E, partials);
+  note_launch();
+  return (size_t)grid.x * grid.y;
+}
+
+__global__ void k_transpose(int n, const double *__restrict__ in, double *__restrict__ out) {
+  __shared__ double tile[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int i = by + r, j = bx + threadIdx.x;
+    if (i < n && j < n) tile[r][threadIdx.x] = in[(size_t)i * n + j];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int i = bx + r, j = by + threadIdx.x;
+    if (i < n && j < n) out[(size_t)i * n + j] = tile[threadIdx.x][r];
+  }
+}
+void launch_transpose(cudaStream_t st, int n, const double *in, double *out) {
+  dim3 grid((n + 31) / 32, (n + 31) / 32), blk(32, 8);
+  k_transpose<<<grid, blk, 0, st>>>(n, in, out);
+  note_launch();
+}
+
+// out = sum_i c_i X_i + shift * (delta_ij - Pd_ij / occ)
+__global__ void k_combine(int n, int k, const double *const *__restrict__ X, const double *__restrict__ c,
+                          const double *__restrict__ Pd, double inv_occ, double shift, double *__restrict__ out) {
+  const size_t len = (size_t)n * n;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    for (int i = 0; i < k; ++i) v += c[i] * X[i][e];
+    if (shift > 0.0) {
+      const size_t row = e / n, col = e - row * n;
+      const double q = Pd[e] * inv_occ;
+      v += shift * ((row == col) ? 1.0 - q : -q);
+    }
+    out[e] = v;
+  }
+}
+void launch_combine(cudaStream_t st, int n, int k, const double *const *X, const double *c, const double *Pd,
+                    double occ, double shift, double *out) {
+  k_combine<<<RED_BLOCKS * 2, 256, 0, st>>>(n, k, X, c, Pd, 1.0 / occ, shift, out);
+  note_launch();
+}
+
+// Dot products of one X with NY vectors Y_j in one sweep, accumulators in registers;
+// partials laid out [block][j].
+template <int NY>
+__global__ void __launch_bounds__(256) k_dot_row(size_t len, const double *const *__restrict__ Xp,
+                                                 const double *const *__restrict__ Yp, double *__restrict__ out) {
+  const double *x = Xp[0];
+  const double *y[NY];
+#pragma unroll
+  for (int j = 0; j < NY; ++j) y[j] = Yp[j];
+  double acc[NY];
+#pragma unroll
+  for (int j = 0; j < NY; ++j) acc[j] = 0.0;
+  for (size_t e = (size_t)blockIdx.x * 256 + threadIdx.x; e < len; e += (size_t)gridDim.x * 256) {
+    const double xv = x[e];
+#pragma unroll
+    for (int j = 0; j < NY; ++j) acc[j] += xv * y[j][e];
+  }
+#pragma unroll
+  for (int j = 0; j < NY; ++j) {
+    const double s = block_sum<256>(acc[j]);
+    if (threadIdx.x == 0) out[(size_t)blockIdx.x * NY + j] = s;
+  }
+}
+
+void launch_dot_many(cudaStream_t st, size_t len, int nx, const double *const *X, int ny, const double *const *Y,
+                     double *out_partials, int n_blocks) {
+  (void)nx;  // one X per sweep
+  switch (ny) {
+#define DOT_CASE(k) \
+  case k: k_dot_row<k><<<n_blocks, 256, 0, st>>>(len, X, Y, out_partials); break;
+    DOT_CASE(1) DOT_CASE(2) DOT_CASE(3) DOT_CASE(4) DOT_CASE(5) DOT_CASE(6) DOT_CASE(7) DOT_CASE(8) DOT_CASE(9)
+#undef DOT_CASE
+    default: return;
+  }
+  note_launch();
+}
+
+// out[c] = sum over rows of partials[row * n_cols + c]
+__global__ void k_reduce_rows(const double *__restrict__ partials, int n_rows, int n_cols, double *__restrict__ out) {
+  const int c = blockIdx.x;
+  double s = 0.0;
+  for (int r = threadIdx.x; r < n_rows; r += 256) s += partials[(size_t)r * n_cols + c];
+  s = block_sum<256>(s);
+  if (threadIdx.x == 0) out[c] = s;
+}
+void launch_reduce_rows(cudaStream_t st, const double *partials, int n_rows, int n_cols, double *out) {
+  k_reduce_rows<<<n_cols, 256, 0, st>>>(partials, n_rows, n_cols, out);
+  note_launch();
+}
+
+__global__ void k_scale(size_t len, double s, const double *__restrict__ in, double *__restrict__ out) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x)
+    out[e] = s * in[e];
+}
+void launch_scale(cudaStream_t st, size_t len, double s, const double *in, double *out) {
+  k_scale<<<RED_BLOCKS * 2, 256, 0, st>>>(len, s, in, out);
+  note_launch();
+}
+
+__global__ void k_axpby(size_t len, double a, const double *__restrict__ x, double b, const double *__restrict__ y,
+                        double *__restrict__ out) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x)
+    out[e] = a * x[e] + b * y[e];
+}
+void launch_axpby(cudaStream_t st, size_t len, double a, const double *x, double b, const double *y, double *out) {
+  k_axpby<<<RED_BLOCKS * 2, 256, 0, st>>>(len, a, x, b, y, out);
+  note_launch();
+}
+
+__global__ void k_set_diag(int n, const double *__restrict__ d, double *__restrict__ M) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) M[(size_t)i * n + i] = d[i];
+}
+void launch_set_diag(cudaStream_t st, int n, const double *diag, double *M) {
+  cudaMemsetAsync(M, 0, sizeof(double) * (size_t)n * n, st);
+  k_set_diag<<<(n + 255) / 256, 256, 0, st>>>(n, diag, M);
+  note_launch();
+}
+
+}  // namespace pm7
+
+namespace pm7 {
+
+// ---------------------------------------------------------------------------
+// SP2 density-matrix purification (second-order spectral projection): the aufbau
+// projector onto the n_occ lowest eigenvectors of a symmetric F from matrix squarings
+// on the FP64 tensor cores, without an eigendecomposition.
+// ---------------------------------------------------------------------------
+
+// Gershgorin bounds of each row: lo = F_ii - sum_j!=i |F_ij|, hi = F_ii + sum_j!=i |F_ij|;
+// block-reduced into partial min / max.
+__global__ void k_gershgorin(int n, const double *__restrict__ F, double *__restrict__ part_lo,
+                             double *__restrict__ part_hi) {
+  __shared__ double slo[8], shi[8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double lo = 1.0e300, hi = -1.0e300;
+  for (int row = blockIdx.x * 8 + warp; row < n; row += gridDim.x * 8) {
+    double off = 0.0;
+    const double *r = F + (size_t)row * n;
+    for (int j = lane; j < n; j += 32)
+      if (j != row) off += fabs(r[j]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) off += __shfl_down_sync(0xffffffffu, off, o);
+    if (lane == 0) {
+      lo = fmin(lo, r[row] - off);
+      hi = fmax(hi, r[row] + off);
+    }
+  }
+  if (lane == 0) {
+    slo[warp] = lo;
+    shi[warp] = hi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < 8; ++w) {
+      lo = fmin(lo, slo[w]);
+      hi = fmax(hi, shi[w]);
+    }
+    part_lo[blockIdx.x] = lo;
+    part_hi[blockIdx.x] = hi;
+  }
+}
+
+// bounds[0] = min, bounds[1] = max over the partials.
+__global__ void k_minmax(int m, const double *__restrict__ lo, const double *__restrict__ hi, double *bounds) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double a = 1.0e300, b = -1.0e300;
+  for (int i = 0; i < m; ++i) {
+    a = fmin(a, lo[i]);
+    b = fmax(b, hi[i]);
+  }
+  bounds[0] = a;
+  bounds[1] = b;
+}
+
+// X = (emax I - F) / (emax - emin): spectrum mapped into [0, 1], occupied levels near 1.
+__global__ void k_sp2_init(int n, const double *__restrict__ F, const double *__restrict__ bounds,
+                           double *__restrict__ X) {
+  const double emin = bounds[0], emax = bounds[1];
+  const double inv = 1.0 / (emax - emin);
+  const size_t len = (size_t)n * n;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = e / n, j = e - i * n;
+    X[e] = ((i == j ? emax : 0.0) - F[e]) * inv;
+  }
+}
+
+// Traces of X and X^2 and the SP2 branch: state[0] = tr X, state[1] = tr X^2,
+// state[2] = 1 when squaring brings the trace closer to n_occ, state[3] = tr X - tr X^2.
+__global__ void k_sp2_trace(int n, const double *__restrict__ X, const double *__restrict__ X2, double n_occ,
+                            double *__restrict__ state) {
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    a += X[(size_t)i * n + i];
+    b += X2[(size_t)i * n + i];
+  }
+  a = block_sum<256>(a);
+  b = block_sum<256>(b);
+  if (threadIdx.x == 0) {
+    state[0] = a;
+    state[1] = b;
+    state[2] = fabs(b - n_occ) < fabs(2.0 * a - b - n_occ) ? 1.0 : 0.0;
+    state[3] = a - b;
+  }
+}
+
+// X <- X^2 or 2X - X^2 according to state[2].
+__global__ void k_sp2_update(size_t len, double *__restrict__ X, const double *__restrict__ X2,
+                             const double *__restrict__ state) {
+  const bool square = state[2] != 0.0;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x)
+    X[e] = square ? X2[e] : 2.0 * X[e] - X2[e];
+}
+
+void launch_gershgorin(cudaStream_t st, int n, const double *F, double *scratch, double *bounds) {
+  const int blocks = 296;
+  k_gershgorin<<<blocks, 256, 0, st>>>(n, F, scratch, scratch + blocks);
+  note_launch();
+  k_minmax<<<1, 32, 0, st>>>(blocks, scratch, scratch + blocks, bounds);
+  note_launch();
+}
+
+void launch_sp2_init(cudaStream_t st, int n, const double *F, const double *bounds, double *X) {
+  k_sp2_init<<<RED_BLOCKS * 2, 256, 0, st>>>(n, F, bounds, X);
+  note_launch();
+}
+
+void launch_sp2_square(cudaStream_t st, int n, const double *X, double *X2) {
+  dim3 grid((n + BN - 1) / BN, (n + BM - 1) / BM);
+  k_gemm_tn<<<grid, 128, 0, st>>>(n, n, n, 1.0, X, n, X, n, X2, n, 1);
+  note_launch();
+}
+
+void launch_sp2_trace(cudaStream_t st, int n, const double *X, const double *X2, double n_occ, double *state) {
+  k_sp2_trace<<<1, 256, 0, st>>>(n, X, X2, n_occ, state);
+  note_launch();
+}
+
+void launch_sp2_update(cudaStream_t st, int n, double *X, const double *X2, const double *state) {
+  k_sp2_update<<<RED_BLOCKS * 2, 256, 0, st>>>((size_t)n * n, X, X2, state);
+  note_launch();
+}
+
+}  // namespace pm7

@@ -1,0 +1,183 @@
+// Device Fock build F = H + J(P_tot) - K(P_spin), molecular path.
+//
+// Follows pm7-rs src/fock.rs:149-418 (build_fock_spin_x, no exchange cutoff). Every
+// element of F is written by exactly one kernel, so the three kernels need no atomics
+// and give the same bits on every run:
+//   * k_fock_far   - off-diagonal atom blocks of pairs beyond the 7 Angstrom feather
+//                    range, where (mu nu|la si) = delta_mu,nu delta_la,si EV/r and the
+//                    exchange block is -P_spin * EV/r (integrals.rs:540-574);
+//   * k_fock_near  - off-diagonal blocks of the near pairs from their stored integrals,
+//                    plus each pair's packed Coulomb contributions to both atoms;
+//   * k_fock_atom  - diagonal atom blocks: one-centre terms, the near Coulomb
+//                    contributions in partner order, and the far point-charge Coulomb.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "kernels.hpp"
+#include "nddo_sp.cuh"
+
+namespace pm7 {
+
+__global__ void k_atom_pop(int n_atoms, const int *__restrict__ aoff, const int *__restrict__ z, DeviceParams P,
+                           int nao, const double *__restrict__ Pm, double *__restrict__ pop) {
+  const int A = blockIdx.x * blockDim.x + threadIdx.x;
+  if (A >= n_atoms) return;
+  const int off = aoff[A], no = P.elements[z[A]].n_orb;
+  double s = 0.0;
+  for (int k = 0; k < no; ++k) s += Pm[(size_t)(off + k) * nao + off + k];
+  pop[A] = s;
+}
+
+__global__ void k_fock_far(FockGeometry g, const double *__restrict__ H, const double *__restrict__ Ps,
+                           double s_scale, double *__restrict__ F) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.nao || j >= g.nao) return;
+  const int A = g.ao_atom[i], B = g.ao_atom[j];
+  if (A == B || g.near_mask[(size_t)A * g.n_atoms + B]) return;
+  const double dx = g.xyz[3 * B] - g.xyz[3 * A], dy = g.xyz[3 * B + 1] - g.xyz[3 * A + 1],
+               dz = g.xyz[3 * B + 2] - g.xyz[3 * A + 2];
+  const double v = (1.0 / sqrt(dx * dx + dy * dy + dz * dz)) * kEv;
+  const size_t ij = (size_t)i * g.nao + j;
+  F[ij] = H[ij] - s_scale * Ps[ij] * v;
+}
+
+__global__ void k_fock_near(FockGeometry g, DeviceParams P, const double *__restrict__ H,
+                            const double *__restrict__ Pt, const double *__restrict__ Ps, double s_scale,
+                            double *__restrict__ F, double *__restrict__ jbuf) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= g.n_near) return;
+  const NearPair q = g.np[p];
+  const int nu_ = P.elements[g.z[q.u]].n_orb, nv = P.elements[g.z[q.v]].n_orb;
+  const int ou = g.aoff[q.u], ov = g.aoff[q.v], nao = g.nao;
+  const int npv = nv * (nv + 1) / 2, npu = nu_ * (nu_ + 1) / 2;
+  const double *w = g.w + q.woff;
+  // exchange block
+  for (int mu = 0; mu < nu_; ++mu)
+    for (int la = 0; la < nv; ++la) {
+      double acc = 0.0;
+      for (int nu = 0; nu < nu_; ++nu) {
+        const double *row = w + dpack(mu, nu) * npv;
+        for (int si = 0; si < nv; ++si) acc += Ps[(size_t)(ou + nu) * nao + ov + si] * row[dpack(la, si)];
+      }
+      const double kv = -acc * s_scale;
+      const size_t e1 = (size_t)(ou + mu) * nao + ov + la, e2 = (size_t)(ov + la) * nao + ou + mu;
+      F[e1] = H[e1] + kv;
+      F[e2] = H[e2] + kv;
+    }
+  // Coulomb on u from P_vv
+  double *ju = jbuf + q.eoff_u;
+  for (int mu = 0; mu < nu_; ++mu)
+    for (int nu = 0; nu <= mu; ++nu) {
+      const double *row = w + dpack(mu, nu) * npv;
+      double acc = 0.0;
+      for (int la = 0; la < nv; ++la)
+        for (int si = 0; si < nv; ++si) acc += Pt[(size_t)(ov + la) * nao + ov + si] * row[dpack(la, si)];
+      ju[dpack(mu, nu)] = acc;
+    }
+  // Coulomb on v from P_uu
+  double *jv = jbuf + q.eoff_v;
+  for (int la = 0; la < nv; ++la)
+    for (int si = 0; si <= la; ++si) {
+      const int col = dpack(la, si);
+      double acc = 0.0;
+      for (int mu = 0; mu < nu_; ++mu)
+        for (int nu = 0; nu < nu_; ++nu) acc += Pt[(size_t)(ou + mu) * nao + ou + nu] * w[dpack(mu, nu) * npv + col];
+      jv[col] = acc;
+    }
+  (void)npu;
+}
+
+// One-centre two-electron integral (a b | c d) of an sp atom (fock.rs:69-107).
+__device__ __forceinline__ double oc_sp(int a, int b, int c, int d, const ElementRec &e) {
+  if (a == b && c == d) {
+    if (a == 0 && c == 0) return e.g_ss;
+    if (a == 0 || c == 0) return e.g_sp;
+    return a == c ? e.g_pp : e.g_p2;
+  }
+  const int ba = a < b ? a : b, bb = a < b ? b : a, kc = c < d ? c : d, kd = c < d ? d : c;
+  if (ba == 0 && bb != 0 && kc == 0 && kd != 0 && bb == kd) return e.h_sp;
+  if (ba != 0 && bb != 0 && ba != bb && ba == kc && bb == kd) return 0.5 * (e.g_pp - e.g_p2);
+  return 0.0;
+}
+
+// One block per atom: the far point-charge Coulomb (threads over partner atoms, fixed
+// block reduction), the near Coulomb contributions summed in partner order (threads
+// over packed elements), then the one-centre terms (threads over block elements).
+constexpr int ATOM_THREADS = 128;
+__global__ void __launch_bounds__(ATOM_THREADS) k_fock_atom(FockGeometry g, DeviceParams P,
+                                                            const double *__restrict__ H,
+                                                            const double *__restrict__ Pt,
+                                                            const double *__restrict__ Ps, double s_scale,
+                                                            const double *__restrict__ pop,
+                                                            const double *__restrict__ jbuf,
+                                                            double *__restrict__ F) {
+  const int A = blockIdx.x;
+  const ElementRec &e = P.elements[g.z[A]];
+  const int no = e.n_orb, off = g.aoff[A], nao = g.nao;
+  if (no == 0) return;
+  const int npk = no * (no + 1) / 2;
+  __shared__ double s_far;
+  __shared__ double jacc[45];
+  const double xa = g.xyz[3 * A], ya = g.xyz[3 * A + 1], za = g.xyz[3 * A + 2];
+  const unsigned char *mask = g.near_mask + (size_t)A * g.n_atoms;
+  double far = 0.0;
+  for (int B = threadIdx.x; B < g.n_atoms; B += ATOM_THREADS) {
+    if (B == A || mask[B]) continue;
+    const double dx = g.xyz[3 * B] - xa, dy = g.xyz[3 * B + 1] - ya, dz = g.xyz[3 * B + 2] - za;
+    far += ((1.0 / sqrt(dx * dx + dy * dy + dz * dz)) * kEv) * pop[B];
+  }
+  far = block_sum<ATOM_THREADS>(far);
+  if (threadIdx.x == 0) s_far = far;
+  const int c0 = g.csr_start[A], c1 = g.csr_start[A + 1];
+  for (int k = threadIdx.x; k < npk; k += ATOM_THREADS) {
+    double acc = 0.0;
+    for (int c = c0; c < c1; ++c) {
+      const NearPair q = g.np[g.csr[c].y];
+      acc += jbuf[(q.u == A ? q.eoff_u : q.eoff_v) + k];
+    }
+    jacc[k] = acc;
+  }
+  __syncthreads();
+  const double *oc = (no == 9 && e.onecenter_slot >= 0) ? P.onecenter + (size_t)e.onecenter_slot * 2025 : nullptr;
+  for (int idx = threadIdx.x; idx < no * no; idx += ATOM_THREADS) {
+    const int mu = idx / no, nu = idx - mu * no;
+    double acc = 0.0;
+    for (int la = 0; la < no; ++la)
+      for (int si = 0; si < no; ++si) {
+        const double pt = Pt[(size_t)(off + la) * nao + off + si];
+        const double ps = s_scale * Ps[(size_t)(off + la) * nao + off + si];
+        if (oc) {
+          acc += pt * oc[dpack(mu, nu) * 45 + dpack(la, si)];
+          acc -= ps * oc[dpack(mu, la) * 45 + dpack(nu, si)];
+        } else {
+          acc += pt * oc_sp(mu, nu, la, si, e);
+          acc -= ps * oc_sp(mu, la, nu, si, e);
+        }
+      }
+    double v = acc + jacc[dpack(mu, nu)];
+    if (mu == nu) v += s_far;
+    const size_t ij = (size_t)(off + mu) * nao + off + nu;
+    F[ij] = H[ij] + v;
+  }
+}
+
+void launch_atom_pop(cudaStream_t st, int n_atoms, const int *aoff, const int *z, const DeviceParams &P, int nao,
+                     const double *Pm, double *pop) {
+  k_atom_pop<<<(n_atoms + 127) / 128, 128, 0, st>>>(n_atoms, aoff, z, P, nao, Pm, pop);
+  note_launch();
+}
+
+void launch_fock(cudaStream_t st, const FockGeometry &g, const DeviceParams &P, const double *H, const double *Pt,
+                 const double *Ps, double s_scale, double *F, double *pop, double *jbuf) {
+  launch_atom_pop(st, g.n_atoms, g.aoff, g.z, P, g.nao, Pt, pop);
+  dim3 blk(32, 8), grd((g.nao + 31) / 32, (g.nao + 7) / 8);
+  k_fock_far<<<grd, blk, 0, st>>>(g, H, Ps, s_scale, F);
+  note_launch();
+  if (g.n_near > 0) k_fock_near<<<(g.n_near + 127) / 128, 128, 0, st>>>(g, P, H, Pt, Ps, s_scale, F, jbuf);
+  note_launch();
+  k_fock_atom<<<g.n_atoms, ATOM_THREADS, 0, st>>>(g, P, H, Pt, Ps, s_scale, pop, jbuf, F);
+  note_launch();
+}
+
+}  // namespace pm7

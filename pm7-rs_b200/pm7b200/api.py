@@ -1,0 +1,208 @@
+"""Python host API of the engine: `run_pm7` and the stage functions over the C ABI.
+
+Mirrors the reference's public surface for the molecular single point
+(pm7-rs src/scf.rs:512-522 `run_pm7`, `Pm7Options` defaults :207-233, `Pm7Result`
+fields :261-342): positions in Bohr, energies in eV, heat of formation in kcal/mol.
+Errors raise `Pm7Error` carrying the C status code. There is no CPU fallback: when the
+shared library or a CUDA device is missing the calls fail loudly.
+"""
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import abi
+
+LIB_PATH = Path(__file__).resolve().parent / "libpm7b200.so"
+
+_lib = None
+
+EXPORTED = [
+    "pm7_params_load", "pm7_options_default", "pm7_run", "pm7_result_free", "pm7_last_error_message",
+    "pm7_device_count", "pm7_stage_core_hamiltonian", "pm7_stage_fock", "pm7_stage_pair", "pm7_stage_core_core",
+    "pm7_stage_corrections",
+]
+
+
+class Pm7Error(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"{abi.STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+def lib():
+    """Load the engine's shared library (built in-tree by `make -C pm7-rs_b200`)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise FileNotFoundError(f"{LIB_PATH} is not built; run `make -C pm7-rs_b200`")
+    L = C.CDLL(str(LIB_PATH))
+    L.pm7_params_load.argtypes = [C.c_int32, C.POINTER(C.c_void_p)]
+    L.pm7_options_default.argtypes = [C.POINTER(abi.Options)]
+    L.pm7_run.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, C.POINTER(abi.Options), C.POINTER(abi.Result)]
+    L.pm7_result_free.argtypes = [C.POINTER(abi.Result)]
+    L.pm7_last_error_message.restype = C.c_char_p
+    L.pm7_device_count.restype = C.c_int32
+    L.pm7_stage_core_hamiltonian.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, C.c_int32, abi.DP,
+                                             C.POINTER(C.c_int32)]
+    L.pm7_stage_fock.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, C.c_int32, abi.DP, abi.DP, abi.DP]
+    L.pm7_stage_pair.argtypes = [C.c_void_p, C.c_int32, C.c_int32, abi.DP, C.c_int32, abi.DP, abi.DP, abi.DP, abi.DP,
+                                 C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.pm7_stage_core_core.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, abi.DP]
+    L.pm7_stage_corrections.argtypes = [C.POINTER(abi.Molecule), C.c_int32, C.c_int32, abi.DP]
+    L.pm7_abi_sizes.argtypes = [C.POINTER(C.c_int64)]
+    _lib = L
+    return L
+
+
+def device_count():
+    return int(lib().pm7_device_count())
+
+
+def _check(code):
+    if code != 0:
+        raise Pm7Error(code, lib().pm7_last_error_message().decode())
+
+
+def params(method=0):
+    """`Pm7Parameters::method` (src/params.rs:127-129): the cached parameter handle."""
+    if isinstance(method, str):
+        method = abi.METHODS[method]
+    h = C.c_void_p()
+    _check(lib().pm7_params_load(int(method), C.byref(h)))
+    return h
+
+
+class _Mol:
+    def __init__(self, z, xyz_bohr):
+        self.z = np.ascontiguousarray(z, dtype=np.uint8)
+        self.xyz = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(-1)
+        if self.xyz.size != 3 * self.z.size:
+            raise ValueError("xyz must hold 3 coordinates per atom")
+        self.s = abi.Molecule(len(self.z), self.z.ctypes.data_as(C.POINTER(C.c_uint8)),
+                              self.xyz.ctypes.data_as(abi.DP))
+
+
+def _arr(ptr, n):
+    if not ptr:
+        return None
+    return np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+
+
+def result_to_dict(r):
+    n, nao = r.n_atoms, r.nao
+    d = {k: getattr(r, k) for k in ("n_atoms", "nao", "n_occ", "n_occ_beta", "unrestricted", "iterations",
+                                     "converged", "density_error", "electronic_ev", "core_ev", "total_ev",
+                                     "heat_of_formation_kcal", "correction_kcal", "homo_ev", "lumo_ev",
+                                     "homo_ev_beta", "lumo_ev_beta", "dipole_magnitude", "device_ms",
+                                     "fp32_iterations")}
+    for k in ("dipole_debye", "dipole_point_charge", "dipole_sp_hybrid", "dipole_pd_hybrid"):
+        d[k] = np.array(list(getattr(r, k)))
+    d["charges"] = _arr(r.charges, n)
+    d["mo_energies"] = _arr(r.mo_energies, nao)
+    d["mo_energies_beta"] = _arr(r.mo_energies_beta, nao)
+    for k in ("density", "spin_density", "mo_coeff", "mo_coeff_beta"):
+        a = _arr(getattr(r, k), nao * nao)
+        d[k] = None if a is None else a.reshape(nao, nao)
+    return d
+
+
+def run_pm7(z, xyz_bohr, **options):
+    """`run_pm7` (src/scf.rs:512-522) on the device. Options take the `Pm7Options`
+    field names; the method may be given as a string ("pm7", "pm7-ts", ...)."""
+    m = _Mol(z, xyz_bohr)
+    keep = []
+    for k in ("initial_density", "initial_spin_density"):
+        if options.get(k) is not None:
+            a = np.ascontiguousarray(options[k], dtype=np.float64)
+            keep.append(a)
+            options[k] = a.ctypes.data_as(abi.DP)
+    o = abi.default_options(**options)
+    h = params(o.method)
+    r = abi.Result()
+    code = lib().pm7_run(C.byref(m.s), h, C.byref(o), C.byref(r))
+    if code != 0:
+        raise Pm7Error(code, lib().pm7_last_error_message().decode())
+    try:
+        return result_to_dict(r)
+    finally:
+        lib().pm7_result_free(C.byref(r))
+
+
+def core_hamiltonian(z, xyz_bohr, method=0, force_dpath=False):
+    m = _Mol(z, xyz_bohr)
+    h = params(method)
+    nao = C.c_int32()
+    _check(lib().pm7_stage_core_hamiltonian(C.byref(m.s), h, int(force_dpath), None, C.byref(nao)))
+    out = np.zeros((nao.value, nao.value))
+    _check(lib().pm7_stage_core_hamiltonian(C.byref(m.s), h, int(force_dpath), out.ctypes.data_as(abi.DP),
+                                            C.byref(nao)))
+    return out
+
+
+def fock(z, xyz_bohr, p_tot, p_spin, method=0, force_dpath=False):
+    m = _Mol(z, xyz_bohr)
+    pt = np.ascontiguousarray(p_tot, dtype=np.float64)
+    ps = np.ascontiguousarray(p_spin, dtype=np.float64)
+    f = np.zeros_like(pt)
+    _check(lib().pm7_stage_fock(C.byref(m.s), params(method), int(force_dpath), pt.ctypes.data_as(abi.DP),
+                                ps.ctypes.data_as(abi.DP), f.ctypes.data_as(abi.DP)))
+    return f
+
+
+def pair(zi, zj, d, method=0, force_dpath=False):
+    dd = np.ascontiguousarray(d, dtype=np.float64)
+    w = np.zeros(45 * 45)
+    e1b, e2a, s = np.zeros(81), np.zeros(81), np.zeros(81)
+    npi, npj = C.c_int32(), C.c_int32()
+    _check(lib().pm7_stage_pair(params(method), int(zi), int(zj), dd.ctypes.data_as(abi.DP), int(force_dpath),
+                                w.ctypes.data_as(abi.DP), e1b.ctypes.data_as(abi.DP), e2a.ctypes.data_as(abi.DP),
+                                s.ctypes.data_as(abi.DP), C.byref(npi), C.byref(npj)))
+    return (w[: npi.value * npj.value].reshape(npi.value, npj.value), e1b.reshape(9, 9), e2a.reshape(9, 9),
+            s.reshape(9, 9))
+
+
+def core_core(z, xyz_bohr, method=0):
+    m = _Mol(z, xyz_bohr)
+    e = C.c_double()
+    _check(lib().pm7_stage_core_core(C.byref(m.s), params(method), C.byref(e)))
+    return e.value
+
+
+def corrections(z, xyz_bohr, method=0, smooth=False):
+    m = _Mol(z, xyz_bohr)
+    out = np.zeros(5)
+    _check(lib().pm7_stage_corrections(C.byref(m.s), int(method), int(smooth), out.ctypes.data_as(abi.DP)))
+    return out
+
+
+def abi_sizes():
+    out = (C.c_int64 * 3)()
+    lib().pm7_abi_sizes(out)
+    return tuple(out)
+
+
+def launch_count():
+    """Kernels launched by the engine since process start."""
+    lib().pm7_launch_count.restype = C.c_int64
+    return int(lib().pm7_launch_count())
+
+
+def profile_enable(on=True):
+    lib().pm7_profile_enable.argtypes = [C.c_int32]
+    lib().pm7_profile_enable(1 if on else 0)
+
+
+def profile_read():
+    """{stage: (total_ms, calls)} recorded since profile_enable(True)."""
+    L = lib()
+    L.pm7_profile_count.restype = C.c_int32
+    L.pm7_profile_entry.argtypes = [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    out = {}
+    for i in range(L.pm7_profile_count()):
+        name, ms, calls = C.c_char_p(), C.c_double(), C.c_int64()
+        _check(L.pm7_profile_entry(i, C.byref(name), C.byref(ms), C.byref(calls)))
+        out[name.value.decode()] = (ms.value, calls.value)
+    return out

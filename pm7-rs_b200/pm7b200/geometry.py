@@ -1,0 +1,140 @@
+"""Seeded synthetic molecules of the benchmark workloads (positions returned in Bohr).
+
+* `decane(seed)` - n-decane C10H22 in the all-staggered zig-zag (C-C 1.54 A, C-H
+  1.09 A, tetrahedral angles), every coordinate jittered by U(-0.02, 0.02) A.
+* `alkane(n, seed, jitter)` - the same builder for C_nH_(2n+2).
+* `water_cluster(k, seed)` - k H2O (O-H 0.96 A, H-O-H 104.5 deg) on the first k sites
+  of a cubic grid of spacing 3.1 A, uniformly random orientation (normalised Gaussian
+  quaternion), U(-0.1, 0.1) A centre jitter.
+* `batch(count, seed)` - half alkanes C_nH_2n+2 with n ~ U{1..40}, half water clusters
+  of 2..64 molecules, jitter 0.02 A.
+All draws use numpy.random.default_rng(seed).
+"""
+import math
+
+import numpy as np
+
+A0 = 0.529177210903
+ANG = 1.0 / A0
+
+
+def _tetra_hydrogens(c, prev, nxt, r):
+    """Two hydrogens on an sp3 carbon with backbone neighbours prev/nxt (Angstrom)."""
+    b1 = prev - c
+    b2 = nxt - c
+    b1 /= np.linalg.norm(b1)
+    b2 /= np.linalg.norm(b2)
+    bis = -(b1 + b2)
+    bis /= np.linalg.norm(bis)
+    perp = np.cross(b1, b2)
+    perp /= np.linalg.norm(perp)
+    half = math.radians(109.471) / 2.0
+    return [c + r * (math.cos(half) * bis + math.sin(half) * perp),
+            c + r * (math.cos(half) * bis - math.sin(half) * perp)]
+
+
+def alkane_angstrom(n):
+    """Ideal all-staggered C_nH_(2n+2): list of (Z, xyz Angstrom)."""
+    cc, ch = 1.54, 1.09
+    theta = math.radians(109.471)
+    dx = cc * math.sin(theta / 2.0)
+    dz = cc * math.cos(theta / 2.0)
+    carbons = [np.array([i * dx, 0.0, (i % 2) * dz]) for i in range(n)]
+    atoms = [(6, c) for c in carbons]
+    hyd = []
+    for i, c in enumerate(carbons):
+        if n == 1:
+            # methane
+            s = ch / math.sqrt(3.0)
+            for v in ((1, 1, 1), (1, -1, -1), (-1, 1, -1), (-1, -1, 1)):
+                hyd.append(c + s * np.array(v, dtype=float))
+            continue
+        prev = carbons[i - 1] if i > 0 else None
+        nxt = carbons[i + 1] if i + 1 < n else None
+        if prev is None:
+            prev = c + (c - nxt) * 1.0 + np.array([0.0, 0.0, 0.0])
+            prev = c - (nxt - c)
+            # mirror of the next bond through the carbon, rotated into the zig-zag
+            ang = np.array([-dx, 0.0, dz if i % 2 == 0 else -dz])
+            prev = c + ang
+        if nxt is None:
+            ang = np.array([dx, 0.0, -dz if i % 2 == 1 else dz])
+            nxt = c + ang
+        hyd.extend(_tetra_hydrogens(c, prev, nxt, ch))
+        if i == 0:
+            d = (prev - c)
+            hyd.append(c + ch * d / np.linalg.norm(d))
+        if i == n - 1:
+            d = (nxt - c)
+            hyd.append(c + ch * d / np.linalg.norm(d))
+    atoms += [(1, h) for h in hyd]
+    return atoms
+
+
+def _finish(atoms, rng, jitter):
+    z = np.array([a[0] for a in atoms], dtype=np.uint8)
+    xyz = np.array([a[1] for a in atoms], dtype=np.float64)
+    if jitter:
+        xyz = xyz + rng.uniform(-jitter, jitter, size=xyz.shape)
+    return z, xyz * ANG
+
+
+def alkane(n, seed=0, jitter=0.02, rng=None):
+    rng = rng if rng is not None else np.random.default_rng(seed)
+    return _finish(alkane_angstrom(n), rng, jitter)
+
+
+def decane(seed=0):
+    return alkane(10, seed=seed, jitter=0.02)
+
+
+def _random_rotation(rng):
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    w, x, y, z = q
+    return np.array([
+        [1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+        [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+        [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)],
+    ])
+
+
+def water_cluster(k, seed=0, spacing=3.1, centre_jitter=0.1, rng=None):
+    """k waters on the first k sites of the smallest cube grid holding them (Bohr out)."""
+    rng = rng if rng is not None else np.random.default_rng(seed)
+    side = 1
+    while side ** 3 < k:
+        side += 1
+    r, half = 0.96, math.radians(104.5) / 2.0
+    mono = np.array([[0.0, 0.0, 0.0], [r * math.sin(half), 0.0, r * math.cos(half)],
+                     [-r * math.sin(half), 0.0, r * math.cos(half)]])
+    z, xyz = [], []
+    count = 0
+    for i in range(side):
+        for j in range(side):
+            for l in range(side):
+                if count == k:
+                    break
+                centre = np.array([i, j, l], dtype=float) * spacing
+                centre = centre + rng.uniform(-centre_jitter, centre_jitter, size=3)
+                rot = _random_rotation(rng)
+                for zz, p in zip((8, 1, 1), mono):
+                    z.append(zz)
+                    xyz.append(centre + rot @ p)
+                count += 1
+    return np.array(z, dtype=np.uint8), np.array(xyz) * ANG
+
+
+def batch(count, seed=0):
+    """The mixed-size batch: alternating alkanes C_nH_2n+2 (n ~ U{1..40}) and water
+    clusters (k ~ U{2..64}) with 0.02 A jitter."""
+    rng = np.random.default_rng(seed)
+    mols = []
+    for i in range(count):
+        if i % 2 == 0:
+            n = int(rng.integers(1, 41))
+            mols.append(alkane(n, jitter=0.02, rng=rng))
+        else:
+            k = int(rng.integers(2, 65))
+            mols.append(water_cluster(k, centre_jitter=0.02, rng=rng))
+    return mols

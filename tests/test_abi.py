@@ -1,0 +1,66 @@
+"""The C-ABI library loads and exports every symbol include/pm7_b200.h declares (CPU)."""
+import re
+from pathlib import Path
+
+import pytest
+
+from pm7b200 import abi, api
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_functions():
+    text = (ROOT / "include" / "pm7_b200.h").read_text()
+    return sorted(set(re.findall(r"\b(pm7_[a-z_]+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    names = declared_functions()
+    for required in ("pm7_run", "pm7_params_load", "pm7_options_default", "pm7_result_free",
+                     "pm7_last_error_message"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = api.lib()
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_struct_layouts_match_the_header():
+    import ctypes as C
+
+    sizes = api.abi_sizes()
+    assert sizes == (C.sizeof(abi.Molecule), C.sizeof(abi.Options), C.sizeof(abi.Result))
+
+
+def test_options_default_matches_reference_defaults():
+    import ctypes as C
+
+    o = abi.Options()
+    api.lib().pm7_options_default(C.byref(o))
+    ref = abi.default_options()
+    for name, _ in abi.Options._fields_:
+        a, b = getattr(o, name), getattr(ref, name)
+        if name.startswith("initial"):
+            assert not a and not b
+        else:
+            assert a == b, name
+
+
+def test_params_load_rejects_unknown_method():
+    with pytest.raises(api.Pm7Error) as info:
+        api.params(7)
+    assert info.value.code == 1
+
+
+def test_invalid_molecule_is_rejected_before_any_device_work():
+    import numpy as np
+
+    with pytest.raises(api.Pm7Error) as info:
+        api.run_pm7(np.array([], dtype=np.uint8), np.zeros((0, 3)))
+    assert info.value.code == 1
+    with pytest.raises(api.Pm7Error) as info:
+        api.run_pm7(np.array([1, 1], dtype=np.uint8), np.zeros((2, 3)))
+    assert info.value.code == 1
+    assert "same position" in api.lib().pm7_last_error_message().decode()
