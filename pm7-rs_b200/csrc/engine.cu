@@ -137,7 +137,11 @@ struct DeviceContext {
   std::mutex run_mutex;
   DeviceParams params[5];
   bool params_ready[5] = {false, false, false, false, false};
+  // Pinned staging area for the small per-iteration transfers (pointer lists,
+  // extrapolation weights, scalars), so they never go through pageable memory.
+  unsigned char *pinned = nullptr;
 };
+static constexpr size_t kPinnedBytes = 1 << 16;
 
 static std::mutex g_ctx_mutex;
 static std::unordered_map<int, DeviceContext *> g_contexts;
@@ -154,6 +158,15 @@ static DeviceContext &context_for(int device) {
   auto *ctx = new DeviceContext();
   ctx->device = device;
   CUDA_OK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  {
+    // Keep freed stream-ordered allocations in the pool across synchronisations, so the
+    // per-solve buffers are recycled instead of being remapped on every call.
+    cudaMemPool_t pool;
+    CUDA_OK(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = UINT64_MAX;
+    CUDA_OK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
+  CUDA_OK(cudaMallocHost((void **)&ctx->pinned, kPinnedBytes));
   SOLVER_OK(cusolverDnCreate(&ctx->solver));
   SOLVER_OK(cusolverDnSetStream(ctx->solver, ctx->stream));
   g_contexts[device] = ctx;
@@ -471,7 +484,8 @@ struct Purifier {
   int n;
   DevBuf<double> X, X2, scratch, bounds, state;
   int last_iterations = 0;
-  Purifier(cudaStream_t s, int n_) : st(s), n(n_) {
+  double *pin = nullptr;  // 4 pinned doubles for the per-step state
+  Purifier(cudaStream_t s, int n_, double *pinned_state) : st(s), n(n_), pin(pinned_state) {
     X.alloc((size_t)n * n, st);
     X2.alloc((size_t)n * n, st);
     scratch.alloc(1024, st);
@@ -487,8 +501,8 @@ struct Purifier {
       launch_sp2_square(st, n, X.p, X2.p);
       launch_sp2_trace(st, n, X.p, X2.p, (double)n_occ, state.p);
       launch_sp2_update(st, n, X.p, X2.p, state.p);
-      double s[4];
-      CUDA_OK(cudaMemcpyAsync(s, state.p, sizeof(s), cudaMemcpyDeviceToHost, st));
+      double *s = pin;
+      CUDA_OK(cudaMemcpyAsync(s, state.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
       CUDA_OK(cudaStreamSynchronize(st));
       const double e = s[3];
       err.push_back(e);
@@ -520,12 +534,15 @@ static bool use_sp2(int n) {
   return n >= 256;
 }
 
+static thread_local double *t_pinned_scalar = nullptr;  // set per solve from the context
+
 static double host_sum(const DevBuf<double> &partials, size_t count, double *dscal, cudaStream_t st) {
   launch_sum(st, partials.p, count, dscal);
-  double v = 0.0;
-  CUDA_OK(cudaMemcpyAsync(&v, dscal, sizeof(double), cudaMemcpyDeviceToHost, st));
+  double local = 0.0;
+  double *v = t_pinned_scalar ? t_pinned_scalar : &local;
+  CUDA_OK(cudaMemcpyAsync(v, dscal, sizeof(double), cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaStreamSynchronize(st));
-  return v;
+  return *v;
 }
 
 struct ScfOut {
@@ -610,7 +627,7 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   }
   Eigen eig(ctx, n, Fuse.p);
   const bool sp2 = use_sp2(n);
-  Purifier pur(st, sp2 ? n : 1);
+  Purifier pur(st, sp2 ? n : 1, reinterpret_cast<double *>(ctx.pinned + 4096));
   bool diagonalised = false;  // whether Fuse holds the eigenvectors of the last iteration
   HistoryHost hist(kmax);
   StallGuardHost guard(o.level_shift);
@@ -643,7 +660,9 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     hp.push_back(Fk);
     for (int i = 0; i < k; ++i) hp.push_back(hD[older[i]].p);
     hp.push_back(hD[slot].p);
-    CUDA_OK(cudaMemcpyAsync(ptrs.p, hp.data(), sizeof(double *) * hp.size(), cudaMemcpyHostToDevice, st));
+    const double **pin_ptrs = reinterpret_cast<const double **>(ctx.pinned + 1024);
+    std::copy(hp.begin(), hp.end(), pin_ptrs);
+    CUDA_OK(cudaMemcpyAsync(ptrs.p, pin_ptrs, sizeof(double *) * hp.size(), cudaMemcpyHostToDevice, st));
     const double *const *dE = ptrs.p, *const *dF = ptrs.p + (k + 1), *const *dD = ptrs.p + 2 * (k + 1);
     { Stage s_(st, "diis_dots"); launch_dot_many(st, nn, 1, dE + k, k + 1, dE, dots.p, dot_blocks); }  // <e_new, e_i>
     launch_reduce_rows(st, dots.p, dot_blocks, k + 1, dotout.p);
@@ -653,7 +672,7 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
       { Stage s_(st, "diis_dots"); launch_dot_many(st, nn, 1, dF + k, k, dD, dots.p, dot_blocks); }  // <D_i, F_new>
       launch_reduce_rows(st, dots.p, dot_blocks, k, dotout.p + 32);
     }
-    double sc[2], dh[48];
+    double *sc = reinterpret_cast<double *>(ctx.pinned), *dh = sc + 8;
     CUDA_OK(cudaMemcpyAsync(sc, dscal.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaMemcpyAsync(dh, dotout.p, sizeof(double) * 48, cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
@@ -680,8 +699,12 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
           cw.push_back(w[i]);
         }
     }
-    CUDA_OK(cudaMemcpyAsync(ptrs.p + 48, fp.data(), sizeof(double *) * fp.size(), cudaMemcpyHostToDevice, st));
-    CUDA_OK(cudaMemcpyAsync(coef.p, cw.data(), sizeof(double) * cw.size(), cudaMemcpyHostToDevice, st));
+    const double **pin_fp = reinterpret_cast<const double **>(ctx.pinned + 2048);
+    double *pin_cw = reinterpret_cast<double *>(ctx.pinned + 3072);
+    std::copy(fp.begin(), fp.end(), pin_fp);
+    std::copy(cw.begin(), cw.end(), pin_cw);
+    CUDA_OK(cudaMemcpyAsync(ptrs.p + 48, pin_fp, sizeof(double *) * fp.size(), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(coef.p, pin_cw, sizeof(double) * cw.size(), cudaMemcpyHostToDevice, st));
     { Stage s_(st, "combine"); launch_combine(st, n, (int)fp.size(), ptrs.p + 48, coef.p, out.P.p, 2.0, guard.shift, Fuse.p); }
     bool purified = false;
     if (sp2) {
@@ -767,7 +790,7 @@ static void run_uhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   }
   Eigen eig(ctx, n, Ua.p);
   const bool sp2 = use_sp2(n);
-  Purifier pur(st, sp2 ? n : 1);
+  Purifier pur(st, sp2 ? n : 1, reinterpret_cast<double *>(ctx.pinned + 4096));
   bool diag_a = false;  // whether Ua holds the alpha eigenvectors of the last iteration
   DevBuf<double> eps_b;
   eps_b.alloc(n, st);
@@ -949,6 +972,7 @@ static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm
     throw Failure{PM7_ERR_UNSUPPORTED, "MNDO/d (spd) pair integrals are not implemented on the device"};
   const DeviceParams &P = device_params(ctx, o.method);
   cudaStream_t st = ctx.stream;
+  t_pinned_scalar = reinterpret_cast<double *>(ctx.pinned + 4608);
   cudaEvent_t t0, t1;
   CUDA_OK(cudaEventCreate(&t0));
   CUDA_OK(cudaEventCreate(&t1));
