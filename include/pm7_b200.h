@@ -230,6 +230,35 @@ int32_t pm7_profile_count(void);
 /* Entry i: name, total device milliseconds and number of timed calls. */
 pm7_status pm7_profile_entry(int32_t i, const char **name, double *total_ms, int64_t *calls);
 
+/* ---------------------------------------------------------------------
+ * Allocation-free post-SCF corrections. This entry point has no counterpart in
+ * the reference; it exists for callers that cannot call cudaMalloc: a host that
+ * owns all device memory through its own pool (a framework's caching allocator,
+ * a serving process with a fixed HBM budget), or a loop that must not take the
+ * implicit synchronisation a device allocation can cause.
+ *
+ * Same result as pm7_stage_corrections(), but every pointer is a DEVICE pointer
+ * supplied by the caller: z_dev (n_atoms int32 atomic numbers), xyz_bohr_dev
+ * (3*n_atoms doubles, Bohr) and out_dev (5 doubles, kcal/mol: dispersion, H-bond,
+ * C#C, Si-O-H, PM7-HH). Work is queued on `stream` (a cudaStream_t, NULL for the
+ * default stream) and the call returns without waiting for it.
+ *
+ * The kernels' scratch is one static device array sized for at most
+ * pm7_corrections_noalloc_max_atoms() atoms (2048, about 1 MB), held by every GPU
+ * that loads the library until the process exits; larger molecules are rejected
+ * with PM7_ERR_INVALID_INPUT. The first call on each device looks up that array's
+ * device address (with the device current), so make that first call before any
+ * stream capture. All calls on a device share the one array: calls whose work
+ * overlaps on the GPU (different streams, or different host threads) race and must
+ * be serialised by the caller. The call allocates nothing: no cudaMalloc, no
+ * cudaFree, no library allocator. */
+pm7_status pm7_corrections_noalloc(int32_t n_atoms, const int32_t *z_dev, const double *xyz_bohr_dev,
+                                   int32_t method, int32_t smooth_dispersion, double *out_dev, void *stream);
+/* Message of the last pm7_corrections_noalloc failure on the calling thread. */
+const char *pm7_corrections_noalloc_error(void);
+/* Largest n_atoms pm7_corrections_noalloc accepts. */
+int32_t pm7_corrections_noalloc_max_atoms(void);
+
 #ifdef __cplusplus
 }
 #endif
