@@ -498,7 +498,10 @@ struct Purifier {
     std::vector<double> err;
     bool ok = false;
     for (int it = 0; it < 100; ++it) {
-      launch_sp2_square(st, n, X.p, X2.p);
+      {
+        Stage g_(st, "sp2_square_gemm");
+        launch_sp2_square(st, n, X.p, X2.p);
+      }
       launch_sp2_trace(st, n, X.p, X2.p, (double)n_occ, state.p);
       launch_sp2_update(st, n, X.p, X2.p, state.p);
       double *s = pin;
