@@ -3,7 +3,7 @@
 // TEST INFRASTRUCTURE ONLY. This code is the correctness oracle and the timed
 // CPU baseline; the product (pm7-rs_b200/) never links or calls it. Every
 // function cites the pm7-rs file:line it restates. Parity is pinned by
-// tests/test_oracle_golden.py against the 176 recorded pm7-rs results of
+// tests/test_oracle_golden.py against the 175 recorded pm7-rs results of
 // tools/oracle/baselines/reference.json.
 #pragma once
 

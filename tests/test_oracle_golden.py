@@ -23,17 +23,11 @@ def _cases(golden):
 
 
 def test_golden_cases(golden):
-    checked, unsupported, failures = 0, [], []
+    checked, failures = 0, []
     for name in _cases(golden):
         case = golden[name]
         z, xyz = harness.parse_lines(case["atoms"])
-        try:
-            r = harness.run(z, xyz, charge=float(case["charge"]), multiplicity=case["multiplicity"])
-        except harness.OracleError as e:
-            if e.code == 4:  # PM7_ERR_UNSUPPORTED: restatement not yet covering this path
-                unsupported.append(name)
-                continue
-            raise
+        r = harness.run(z, xyz, charge=float(case["charge"]), multiplicity=case["multiplicity"])
         ref = case["pm7_rs"]
         n = len(z)
         checks = [
@@ -48,7 +42,8 @@ def test_golden_cases(golden):
                 failures.append(f"{name}: {label} {got!r} vs {want!r}")
         checked += 1
     assert not failures, "\n".join(failures)
-    assert checked >= 80, (checked, unsupported)
+    # Every recorded case, sp and MNDO/d elements alike (s, p, d shells; H..No).
+    assert checked == len(golden) >= 175, checked
 
 
 def test_water_known_answer():
