@@ -29,11 +29,22 @@ struct ElementRec {
   double e_isol, eheat_ev, poc;
   double repd[53];      // MNDO/d one-centre integrals, slots 1..52
   int32_t onecenter_slot;  // index into the 45x45 one-centre table array, -1 if none
-  int32_t pad_;
+  int32_t iod;             // ground-state d occupation (PM7 d-balance switch)
 };
 
 struct PairParamRec {
   double alpb, xfac;
+};
+
+// Index tables of the MNDO/d two-centre integrals (MOPAC fordd: 1-based values) and the
+// Gauss-Legendre rules of the numerical Slater overlaps, one copy per device.
+struct DTables {
+  uint16_t ind2[2025];   // (ij, kl) -> local integral number, 0 = none
+  int16_t isym[492];     // 0: evaluate; +-n (n >= 35): copy (negated) integral n
+  uint8_t indpp[9], inddp[15], inddd[25], pad_[7];
+  double ch[675];        // multipole coefficients ch(ij, l, m)
+  double gl48_t[48], gl48_w[48];  // 48-point rule on [-1, 1]
+  double gl40_t[40], gl40_w[40];  // 40-point rule on [-1, 1]
 };
 
 // Everything a kernel needs about the parameter set, in device memory.
@@ -41,6 +52,7 @@ struct DeviceParams {
   const ElementRec *elements;   // kMaxZ entries
   const PairParamRec *pairs;    // kMaxZ*kMaxZ, already completed with the diagonal-average rule
   const double *onecenter;      // n_onecenter * 2025
+  const DTables *tab;           // MNDO/d index tables and quadrature rules
   double vpar[61];              // 1-based
 };
 

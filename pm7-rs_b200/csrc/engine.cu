@@ -188,9 +188,13 @@ static const DeviceParams &device_params(DeviceContext &ctx, int method) {
   CUDA_OK(cudaMalloc(&oc, sizeof(double) * noc));
   if (!ps.onecenter().empty())
     CUDA_OK(cudaMemcpy(oc, ps.onecenter().data(), sizeof(double) * ps.onecenter().size(), cudaMemcpyHostToDevice));
+  DTables *tab = nullptr;
+  CUDA_OK(cudaMalloc(&tab, sizeof(DTables)));
+  CUDA_OK(cudaMemcpy(tab, &mndod_tables(), sizeof(DTables), cudaMemcpyHostToDevice));
   d.elements = el;
   d.pairs = pr;
   d.onecenter = oc;
+  d.tab = tab;
   for (int i = 0; i <= 60; ++i) d.vpar[i] = ps.vpar()[i];
   ctx.params_ready[method] = true;
   return d;
@@ -407,8 +411,10 @@ static void upload(DevBuf<T> &b, const std::vector<T> &v, cudaStream_t st) {
 }
 
 // Core Hamiltonian and stored pair integrals on the device (hamiltonian.rs:310-638).
+// `dpath`: the molecule has a d-shell atom (or the caller forced it), so every pair is
+// evaluated in the MNDO/d frame (hamiltonian.rs:346-355).
 static void build_device_molecule(DeviceMolecule &D, const Molecule &m, const Layout &L, const DeviceParams &P,
-                                  cudaStream_t st) {
+                                  bool dpath, cudaStream_t st) {
   D.st = st;
   D.n = m.n;
   D.nao = L.nao;
@@ -435,8 +441,13 @@ static void build_device_molecule(DeviceMolecule &D, const Molecule &m, const La
   CUDA_OK(cudaMemsetAsync(D.status.p, 0, sizeof(int), st));
   const size_t np = pairs_all_partials(m.n);
   D.cc_partial.alloc(np, st);
-  launch_pairs_all(st, m.n, D.z.p, D.xyz.p, D.aoff.p, L.nao, P, D.H.p, D.cc_partial.p, D.status.p);
-  launch_near_integrals(st, D.n_near, D.z.p, D.xyz.p, D.near.p, P, D.w.p, D.ecore.p, D.status.p);
+  if (dpath) {
+    launch_pairs_all_d(st, m.n, D.z.p, D.xyz.p, D.aoff.p, L.nao, P, D.H.p, D.cc_partial.p);
+    launch_near_integrals_d(st, D.n_near, D.z.p, D.xyz.p, D.near.p, P, D.w.p, D.ecore.p);
+  } else {
+    launch_pairs_all(st, m.n, D.z.p, D.xyz.p, D.aoff.p, L.nao, P, D.H.p, D.cc_partial.p, D.status.p);
+    launch_near_integrals(st, D.n_near, D.z.p, D.xyz.p, D.near.p, P, D.w.p, D.ecore.p, D.status.p);
+  }
   launch_hcore_diag(st, m.n, D.z.p, D.xyz.p, D.aoff.p, D.csr_start.p, D.csr.p, D.near.p, D.ecore.p, D.mask.p, P,
                     L.nao, D.H.p);
   if (m.n >= 2) launch_sum_partials(st, D.cc_partial.p, np, D.scal.p);
@@ -447,8 +458,7 @@ static void build_device_molecule(DeviceMolecule &D, const Molecule &m, const La
   CUDA_OK(cudaMemcpyAsync(&cc, D.scal.p, sizeof(double), cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaStreamSynchronize(st));
   CUDA_OK(cudaGetLastError());
-  if (status & 1) throw Failure{PM7_ERR_UNSUPPORTED, "Slater overlaps for valence shells with n >= 4 are not implemented on the device"};
-  if (status & 2) throw Failure{PM7_ERR_UNSUPPORTED, "MNDO/d (spd) pair integrals are not implemented on the device"};
+  if (status != 0) throw Failure{PM7_ERR_UNSUPPORTED, "a pair's shells are outside the sp-frame integral kernels"};
   D.core_core_ev = cc;
 }
 
@@ -971,8 +981,6 @@ static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm
       throw Failure{PM7_ERR_INSUFFICIENT_MEMORY, "estimated SCF memory ~" + std::to_string((need + (1 << 20) - 1) >> 20) +
                                                      " MB exceeds the " + std::to_string(budget >> 20) + " MB budget"};
   }
-  if (o.force_dpath || L.has_d)
-    throw Failure{PM7_ERR_UNSUPPORTED, "MNDO/d (spd) pair integrals are not implemented on the device"};
   const DeviceParams &P = device_params(ctx, o.method);
   cudaStream_t st = ctx.stream;
   t_pinned_scalar = reinterpret_cast<double *>(ctx.pinned + 4608);
@@ -981,7 +989,7 @@ static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm
   CUDA_OK(cudaEventCreate(&t1));
   CUDA_OK(cudaEventRecord(t0, st));
   DeviceMolecule D;
-  { Stage s_(st, "build"); build_device_molecule(D, m, L, P, st); }
+  { Stage s_(st, "build"); build_device_molecule(D, m, L, P, o.force_dpath || L.has_d, st); }
   // electron count and spin (scf.rs:588-627)
   double n_elec = 0.0;
   for (int zz : m.z) n_elec += ps.element(zz)->core;
@@ -1175,15 +1183,13 @@ static void stage_core(const pm7_molecule *mol, const pm7_params *params, int fo
   Layout L = build_layout(m, ps);
   if (nao_out) *nao_out = L.nao;
   if (!h_out && !f_out) return;
-  if (force_dpath || L.has_d)
-    throw Failure{PM7_ERR_UNSUPPORTED, "MNDO/d (spd) pair integrals are not implemented on the device"};
   DeviceContext &ctx = context_for(0);
   std::lock_guard<std::mutex> lock(ctx.run_mutex);
   CUDA_OK(cudaSetDevice(ctx.device));
   const DeviceParams &P = device_params(ctx, method);
   cudaStream_t st = ctx.stream;
   DeviceMolecule D;
-  build_device_molecule(D, m, L, P, st);
+  build_device_molecule(D, m, L, P, force_dpath || L.has_d, st);
   const size_t nn = (size_t)L.nao * L.nao;
   if (h_out) CUDA_OK(cudaMemcpyAsync(h_out, D.H.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
   if (f_out) {
@@ -1297,8 +1303,7 @@ pm7_status pm7_stage_pair(const pm7_params *params, int32_t z_i, int32_t z_j, co
     if (!ei) throw Failure{PM7_ERR_MISSING_ELEMENT, "missing PM7 parameter block for Z=" + std::to_string(z_i)};
     if (!ej) throw Failure{PM7_ERR_MISSING_ELEMENT, "missing PM7 parameter block for Z=" + std::to_string(z_j)};
     if (ei->n_orb < ej->n_orb) throw Failure{PM7_ERR_INVALID_INPUT, "the first atom must carry at least as many orbitals"};
-    if (force_dpath || ei->n_orb == 9 || ej->n_orb == 9)
-      throw Failure{PM7_ERR_UNSUPPORTED, "MNDO/d (spd) pair integrals are not implemented on the device"};
+    const bool dpath = force_dpath || ei->n_orb == 9 || ej->n_orb == 9;
     DeviceContext &ctx = context_for(0);
     std::lock_guard<std::mutex> lock(ctx.run_mutex);
     CUDA_OK(cudaSetDevice(ctx.device));
@@ -1309,13 +1314,17 @@ pm7_status pm7_stage_pair(const pm7_params *params, int32_t z_i, int32_t z_j, co
     DevBuf<int> ib;
     ib.alloc(3, st);
     CUDA_OK(cudaMemsetAsync(ib.p, 0, 3 * sizeof(int), st));
-    launch_stage_pair(st, P, z_i, z_j, d, buf.p, buf.p + 2025, buf.p + 2025 + 81, buf.p + 2025 + 162, ib.p, ib.p + 2);
+    if (dpath)
+      launch_stage_pair_d(st, P, z_i, z_j, d, buf.p, buf.p + 2025, buf.p + 2025 + 81, buf.p + 2025 + 162, ib.p);
+    else
+      launch_stage_pair(st, P, z_i, z_j, d, buf.p, buf.p + 2025, buf.p + 2025 + 81, buf.p + 2025 + 162, ib.p,
+                        ib.p + 2);
     int h[3];
     std::vector<double> hb(2025 + 3 * 81);
     CUDA_OK(cudaMemcpyAsync(hb.data(), buf.p, sizeof(double) * hb.size(), cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaMemcpyAsync(h, ib.p, sizeof(h), cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
-    if (h[2]) throw Failure{PM7_ERR_UNSUPPORTED, "Slater overlaps for valence shells with n >= 4 are not implemented on the device"};
+    if (h[2]) throw Failure{PM7_ERR_UNSUPPORTED, "a pair's shells are outside the sp-frame integral kernels"};
     *npair_i = h[0];
     *npair_j = h[1];
     std::memcpy(w_out, hb.data(), sizeof(double) * h[0] * h[1]);
@@ -1336,7 +1345,7 @@ pm7_status pm7_stage_core_core(const pm7_molecule *molecule, const pm7_params *p
     CUDA_OK(cudaSetDevice(ctx.device));
     const DeviceParams &P = device_params(ctx, method);
     DeviceMolecule D;
-    build_device_molecule(D, m, L, P, ctx.stream);
+    build_device_molecule(D, m, L, P, L.has_d, ctx.stream);
     *energy_ev = D.core_core_ev;
   });
 }

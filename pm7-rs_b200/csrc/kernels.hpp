@@ -34,6 +34,17 @@ void launch_hcore_diag(cudaStream_t st, int n_atoms, const int *z, const double 
                        const unsigned char *near_mask, const DeviceParams &P, int nao, double *H);
 void launch_sum_partials(cudaStream_t st, const double *in, size_t n, double *out);
 
+// ---- MNDO/d frame (kernels_d.cu): used for every pair of a molecule with a d-shell atom ----
+// beta*S blocks from the general Slater overlaps, plus core-core partials (as launch_pairs_all).
+void launch_pairs_all_d(cudaStream_t st, int n_atoms, const int *z, const double *xyz, const int *aoff, int nao,
+                        const DeviceParams &P, double *H, double *cc_partial);
+// Near-pair w blocks and packed electron-core blocks (as launch_near_integrals), one warp per pair.
+void launch_near_integrals_d(cudaStream_t st, int n_near, const int *z, const double *xyz, const NearPair *np,
+                             const DeviceParams &P, double *w, double *ecore);
+// One pair in the (i, j) orientation, n_orb(i) >= n_orb(j): w, e1b, e2a, S (9x9), np_out[2].
+void launch_stage_pair_d(cudaStream_t st, const DeviceParams &P, int zi, int zj, const double d[3], double *w,
+                         double *e1b, double *e2a, double *s, int *np_out);
+
 // ---- Fock build (kernels_fock.cu) ----
 struct FockGeometry {
   int n_atoms, nao, n_near;

@@ -234,13 +234,75 @@ __device__ __forceinline__ void d_bint(double x, double b[13]) {
   }
 }
 
-// Local overlaps (s111, s211, s121, s221, s222) with ea.n >= eb.n >= 1, ea.n <= 3
-// (overlap.rs:120-296). Returns false for shells the closed form does not cover.
-__device__ inline bool d_overlap_locals(const ElementRec &ea, const ElementRec &eb, double r, double s[5]) {
+// a^b for integer b by binary exponentiation (the evaluation Rust's f64::powi lowers to).
+__device__ __forceinline__ double d_powi(double a, int b) {
+  const bool recip = b < 0;
+  double r = 1.0;
+  while (true) {
+    if (b & 1) r *= a;
+    b /= 2;
+    if (b == 0) break;
+    a *= a;
+  }
+  return recip ? 1.0 / r : r;
+}
+
+// Radial normalisation (2 zeta)^(n+1/2) / sqrt((2n)!) of a Slater orbital.
+__device__ __forceinline__ double d_slater_norm(int n, double zeta) {
+  double f = 1.0;
+  for (int k = 1; k <= 2 * n; ++k) f *= (double)k;
+  return pow(2.0 * zeta, n + 0.5) / sqrt(fmax(f, 1.0));
+}
+
+// <chi(na, la, m) on a | chi(nb, lb, m) on b> for Slater orbitals in the local frame, by
+// Gauss-Legendre quadrature in prolate spheroidal coordinates: 48 points in xi on
+// [1, 1 + 60/max(p, 0.05)] and 40 in eta on [-1, 1] (overlap_numeric.rs:48-113).
+__device__ inline double d_overlap_sto(const DTables *T, int na, double za, int la, int ma, int nb, double zb, int lb,
+                                       double r) {
+  double c;
+  if (la == 0 && lb == 0) c = 0.5;
+  else if ((la == 1 && lb == 0 && ma == 0) || (la == 0 && lb == 1 && ma == 0)) c = 0.8660254037844386;
+  else if (la == 1 && lb == 1 && ma == 0) c = 1.5;
+  else if (la == 1 && lb == 1 && ma == 1) c = 0.75;
+  else return 0.0;
+  const double norm = d_slater_norm(na, za) * d_slater_norm(nb, zb);
+  const double half_r = r * 0.5;
+  const double p = (za + zb) * half_r;
+  const double xi_max = 1.0 + 60.0 / fmax(p, 0.05);
+  const double mid = 0.5 * (1.0 + xi_max), half = 0.5 * (xi_max - 1.0);
+  double sum = 0.0;
+  for (int i = 0; i < 48; ++i) {
+    const double xi = mid + half * T->gl48_t[i], wx = half * T->gl48_w[i];
+    for (int j = 0; j < 40; ++j) {
+      const double eta = T->gl40_t[j];
+      const double ra = half_r * (xi + eta), rb = half_r * (xi - eta);
+      if (ra <= 0.0 || rb <= 0.0) continue;
+      const double cos_a = (1.0 + xi * eta) / (xi + eta), cos_b = (xi * eta - 1.0) / (xi - eta);
+      const double ang_a = la == 0 ? 1.0 : (ma == 0 ? cos_a : sqrt(fmax(1.0 - cos_a * cos_a, 0.0)));
+      const double ang_b = lb == 0 ? 1.0 : (ma == 0 ? cos_b : sqrt(fmax(1.0 - cos_b * cos_b, 0.0)));
+      const double radial = d_powi(ra, na - 1) * d_powi(rb, nb - 1) * exp(ra * (-za) - rb * zb);
+      sum = sum + radial * (wx * T->gl40_w[j] * ang_a * ang_b * (xi * xi - eta * eta));
+    }
+  }
+  return d_powi(half_r, 3) * sum * (norm * c);
+}
+
+// Local overlaps (s111, s211, s121, s221, s222) with ea.n >= eb.n >= 1 (overlap.rs:120-296):
+// the closed forms for valence shells n <= 3 and the numerical quadrature of
+// overlap_numeric.rs:25-43 above (Zn, Ge, As, Se, ... as sp elements).
+__device__ inline bool d_overlap_locals(const ElementRec &ea, const ElementRec &eb, double r, double s[5],
+                                        const DTables *T) {
   const double za0 = ea.zeta_s, za1 = ea.zeta_p, zb0 = eb.zeta_s, zb1 = eb.zeta_p;
   s[0] = s[1] = s[2] = s[3] = s[4] = 0.0;
   const int na = ea.n, nb = eb.n;
-  if (na > 3) return false;
+  if (na > 3) {
+    s[0] = d_overlap_sto(T, na, za0, 0, 0, nb, zb0, 0, r);
+    s[1] = d_overlap_sto(T, na, za1, 1, 0, nb, zb0, 0, r);
+    s[2] = -d_overlap_sto(T, na, za0, 0, 0, nb, zb1, 1, r);
+    s[3] = -d_overlap_sto(T, na, za1, 1, 0, nb, zb1, 1, r);
+    s[4] = d_overlap_sto(T, na, za1, 1, 1, nb, zb1, 1, r);
+    return true;
+  }
   double A[13], B[13];
   const double sq3 = 1.7320508075688772;
   // s111 (s-s)
@@ -340,9 +402,9 @@ __device__ inline bool d_overlap_locals(const ElementRec &ea, const ElementRec &
 }
 
 // 4x4 overlap block S[a_i][b_j] for atoms i, j with displacement d = R_j - R_i
-// (overlap.rs:16-40,301-328). Returns false when a shell needs the numerical path.
+// (overlap.rs:16-40,301-328). Returns false for a shell pair no formula covers.
 __device__ inline bool d_overlap_sp(const ElementRec &ei, const ElementRec &ej, double dx, double dy, double dz,
-                                    double S[4][4]) {
+                                    double S[4][4], const DTables *T) {
   const double r = sqrt(dx * dx + dy * dy + dz * dz);
   for (int a = 0; a < 4; ++a)
     for (int b = 0; b < 4; ++b) S[a][b] = 0.0;
@@ -354,7 +416,7 @@ __device__ inline bool d_overlap_sp(const ElementRec &ei, const ElementRec &ej, 
   const ElementRec &ea = swap ? ej : ei;
   const ElementRec &eb = swap ? ei : ej;
   double loc[5];
-  if (!d_overlap_locals(ea, eb, r, loc)) return false;
+  if (!d_overlap_locals(ea, eb, r, loc, T)) return false;
   const double sgn = swap ? -1.0 : 1.0;
   double rr[3][3];
   d_rotation_to_x(sgn * dx / r, sgn * dy / r, sgn * dz / r, rr);

@@ -288,6 +288,7 @@ ElementRec element_from_row(const double *row, const Radial &R, std::vector<doub
   e.ios = (int)row[Cols::ios];
   e.iop = (int)row[Cols::iop];
   const int iod = (int)row[Cols::iod];
+  e.iod = iod;
   e.core = row[Cols::core];
   e.u_ss = row[Cols::uss];
   e.u_pp = row[Cols::upp];
@@ -428,6 +429,61 @@ ParamSet::ParamSet(int method) : method_(method) {
 const ElementRec *ParamSet::element(int z) const {
   if (z <= 0 || z >= kMaxZ || !elements_[z].present) return nullptr;
   return &elements_[z];
+}
+
+namespace {
+
+// Legendre polynomial P_n and its derivative by the three-term recurrence.
+void legendre(int n, double x, double &p, double &dp) {
+  double p0 = 1.0, p1 = x;
+  for (int k = 2; k <= n; ++k) {
+    const double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+    p0 = p1;
+    p1 = p2;
+  }
+  p = p1;
+  dp = n * (x * p1 - p0) / (x * x - 1.0);
+}
+
+// n-point Gauss-Legendre rule on [-1, 1]: Newton iteration from the Chebyshev guess
+// (the rule pm7-rs src/overlap_numeric.rs:134-159 uses for the heavy-shell overlaps).
+void gauss_legendre(int n, double *t, double *w) {
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    double x = std::cos(M_PI * (i + 0.75) / (n + 0.5));
+    for (int it = 0; it < 100; ++it) {
+      double p, dp;
+      legendre(n, x, p, dp);
+      const double dx = -p / dp;
+      x += dx;
+      if (std::fabs(dx) < 1.0e-15) break;
+    }
+    double p, dp;
+    legendre(n, x, p, dp);
+    const double wt = 2.0 / ((1.0 - x * x) * dp * dp);
+    t[i] = -x;
+    t[n - 1 - i] = x;
+    w[i] = wt;
+    w[n - 1 - i] = wt;
+  }
+}
+
+}  // namespace
+
+const DTables &mndod_tables() {
+  static const DTables *tab = [] {
+    auto *t = new DTables;
+    std::memset(t, 0, sizeof *t);
+    for (int i = 0; i < 2025; ++i) t->ind2[i] = MNDOD_IND2[i];
+    for (int i = 0; i < 492; ++i) t->isym[i] = MNDOD_ISYM[i];
+    for (int i = 0; i < 9; ++i) t->indpp[i] = MNDOD_INDPP[i];
+    for (int i = 0; i < 15; ++i) t->inddp[i] = MNDOD_INDDP[i];
+    for (int i = 0; i < 25; ++i) t->inddd[i] = MNDOD_INDDD[i];
+    for (int i = 0; i < 675; ++i) t->ch[i] = MNDOD_CH[i];
+    gauss_legendre(48, t->gl48_t, t->gl48_w);
+    gauss_legendre(40, t->gl40_t, t->gl40_w);
+    return t;
+  }();
+  return *tab;
 }
 
 const ParamSet &param_set(int method) {

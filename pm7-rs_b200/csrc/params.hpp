@@ -31,4 +31,7 @@ class ParamSet {
 // Process-global, thread-safe cache (method 0..4).
 const ParamSet &param_set(int method);
 
+// MNDO/d index tables and the Gauss-Legendre rules (built once, method independent).
+const DTables &mndod_tables();
+
 }  // namespace pm7
