@@ -259,6 +259,46 @@ const char *pm7_corrections_noalloc_error(void);
 /* Largest n_atoms pm7_corrections_noalloc accepts. */
 int32_t pm7_corrections_noalloc_max_atoms(void);
 
+/* ---- batched and served solves ------------------------------------------------
+ * No counterpart in pm7-rs: its callers (src/python.rs:437, src/bin/pm7_rs.rs:176,
+ * src/optimizer.rs:318) loop over run_pm7 one molecule at a time. These entry points
+ * give the same per-molecule results (closed-shell RHF in the batch; other requests
+ * take the pm7_run path) while many molecules share each SCF-phase launch. */
+
+/* Solves n_molecules independent molecules with options[i] each (options[0].device
+ * selects the GPU and options[0].max_memory_mb, when >= 0, caps the HBM the batch
+ * holds at once). results[i] / statuses[i] receive what pm7_run would return for
+ * molecule i; release each result with pm7_result_free. Returns PM7_OK when the batch
+ * ran (per-molecule failures are in statuses), or the error that stopped it. */
+pm7_status pm7_run_batch(int32_t n_molecules, const pm7_molecule *molecules, const pm7_params *params,
+                         const pm7_options *options, pm7_result *results, pm7_status *statuses);
+
+/* A serving engine: a worker thread on one GPU admits submitted closed-shell RHF
+ * requests as HBM (their device footprint against hbm_budget_mb, or 80% of free
+ * memory when -1) and max_active (0 = unlimited) allow, advances all admitted
+ * requests together one SCF iteration per step, and retires each as it converges. */
+typedef struct pm7_engine pm7_engine;
+typedef struct pm7_engine_config {
+  int32_t device;
+  int32_t method;        /* pm7_method of every request */
+  int64_t hbm_budget_mb; /* -1: 80% of the device's free memory at creation */
+  int32_t max_active;    /* 0: no limit besides memory */
+} pm7_engine_config;
+
+void pm7_engine_config_default(pm7_engine_config *config);
+pm7_status pm7_engine_create(const pm7_engine_config *config, pm7_engine **out);
+/* Queues one request; *ticket identifies it. Invalid input is reported by poll. */
+pm7_status pm7_engine_submit(pm7_engine *engine, const pm7_molecule *molecule, const pm7_options *options,
+                             uint64_t *ticket);
+/* *done = 1 when the request finished; the return value is then its pm7_run status,
+ * *result is filled (caller frees) and *latency_ms is submit-to-finish time. With
+ * wait != 0 the call blocks until the request finishes. A finished ticket is
+ * forgotten after it is polled. */
+pm7_status pm7_engine_poll(pm7_engine *engine, uint64_t ticket, int32_t wait, int32_t *done, pm7_result *result,
+                           double *latency_ms);
+/* Finishes every submitted request, then stops the worker. */
+pm7_status pm7_engine_destroy(pm7_engine *engine);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <mutex>
 #include <string>
@@ -25,32 +26,14 @@
 #include "params.hpp"
 #include "pm7_b200.h"
 #include "scf_host.hpp"
+#include "engine_internal.hpp"
 
 namespace pm7 {
 
 // ---------------------------------------------------------------------------
 // errors
 // ---------------------------------------------------------------------------
-struct Failure {
-  pm7_status code;
-  std::string msg;
-};
-static thread_local std::string g_last_error = "";
-
-#define CUDA_OK(expr)                                                                            \
-  do {                                                                                           \
-    cudaError_t e_ = (expr);                                                                     \
-    if (e_ != cudaSuccess)                                                                       \
-      throw Failure{PM7_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " + \
-                                      __FILE__ + ":" + std::to_string(__LINE__)};                \
-  } while (0)
-#define SOLVER_OK(expr)                                                                           \
-  do {                                                                                            \
-    cusolverStatus_t s_ = (expr);                                                                 \
-    if (s_ != CUSOLVER_STATUS_SUCCESS)                                                            \
-      throw Failure{PM7_ERR_LINEAR_ALGEBRA, "cuSOLVER status " + std::to_string((int)s_) + " at " + \
-                                                std::to_string(__LINE__)};                        \
-  } while (0)
+thread_local std::string g_last_error = "";
 
 // ---------------------------------------------------------------------------
 // diagnostics: launch counter and per-stage CUDA-event timing
@@ -58,95 +41,15 @@ static thread_local std::string g_last_error = "";
 static std::atomic<long long> g_launches{0};
 void note_launch(int kernels) { g_launches.fetch_add(kernels, std::memory_order_relaxed); }
 
-struct StageProfiler {
-  std::mutex mu;
-  bool on = false;
-  struct Open {
-    int stage;
-    cudaEvent_t a, b;
-  };
-  std::vector<Open> pending;
-  std::vector<std::string> names;
-  std::vector<double> total_ms;
-  std::vector<long long> calls;
-  int index(const char *name) {
-    for (size_t i = 0; i < names.size(); ++i)
-      if (names[i] == name) return (int)i;
-    names.push_back(name);
-    total_ms.push_back(0.0);
-    calls.push_back(0);
-    return (int)names.size() - 1;
-  }
-  // Returns a token for end(); -1 when profiling is off.
-  int begin(cudaStream_t st, const char *name) {
-    std::lock_guard<std::mutex> g(mu);
-    if (!on) return -1;
-    Open o;
-    o.stage = index(name);
-    cudaEventCreate(&o.a);
-    cudaEventCreate(&o.b);
-    cudaEventRecord(o.a, st);
-    pending.push_back(o);
-    return (int)pending.size() - 1;
-  }
-  void end(cudaStream_t st, int token) {
-    if (token < 0) return;
-    std::lock_guard<std::mutex> g(mu);
-    if (token < (int)pending.size()) cudaEventRecord(pending[token].b, st);
-  }
-  void flush() {
-    std::lock_guard<std::mutex> g(mu);
-    for (Open &o : pending) {
-      cudaEventSynchronize(o.b);
-      float ms = 0.0f;
-      if (cudaEventElapsedTime(&ms, o.a, o.b) == cudaSuccess) {
-        total_ms[o.stage] += ms;
-        calls[o.stage] += 1;
-      }
-      cudaEventDestroy(o.a);
-      cudaEventDestroy(o.b);
-    }
-    pending.clear();
-  }
-  void reset(bool enable) {
-    flush();
-    std::lock_guard<std::mutex> g(mu);
-    on = enable;
-    names.clear();
-    total_ms.clear();
-    calls.clear();
-  }
-};
-static StageProfiler g_prof;
-
-// RAII stage timer on a stream.
-struct Stage {
-  cudaStream_t st;
-  int token;
-  Stage(cudaStream_t s, const char *name) : st(s), token(g_prof.begin(s, name)) {}
-  ~Stage() { g_prof.end(st, token); }
-};
+StageProfiler g_prof;
 
 // ---------------------------------------------------------------------------
 // per-device context: stream, solver handle, parameter tables
 // ---------------------------------------------------------------------------
-struct DeviceContext {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  cusolverDnHandle_t solver = nullptr;
-  std::mutex run_mutex;
-  DeviceParams params[5];
-  bool params_ready[5] = {false, false, false, false, false};
-  // Pinned staging area for the small per-iteration transfers (pointer lists,
-  // extrapolation weights, scalars), so they never go through pageable memory.
-  unsigned char *pinned = nullptr;
-};
-static constexpr size_t kPinnedBytes = 1 << 16;
-
 static std::mutex g_ctx_mutex;
 static std::unordered_map<int, DeviceContext *> g_contexts;
 
-static DeviceContext &context_for(int device) {
+DeviceContext &context_for(int device) {
   std::lock_guard<std::mutex> lock(g_ctx_mutex);
   auto it = g_contexts.find(device);
   if (it != g_contexts.end()) return *it->second;
@@ -173,7 +76,7 @@ static DeviceContext &context_for(int device) {
   return *ctx;
 }
 
-static const DeviceParams &device_params(DeviceContext &ctx, int method) {
+const DeviceParams &device_params(DeviceContext &ctx, int method) {
   if (ctx.params_ready[method]) return ctx.params[method];
   const ParamSet &ps = param_set(method);
   DeviceParams &d = ctx.params[method];
@@ -203,48 +106,10 @@ static const DeviceParams &device_params(DeviceContext &ctx, int method) {
 // ---------------------------------------------------------------------------
 // device buffers with stream-ordered allocation
 // ---------------------------------------------------------------------------
-template <class T>
-struct DevBuf {
-  T *p = nullptr;
-  size_t n = 0;
-  cudaStream_t st = nullptr;
-  DevBuf() = default;
-  DevBuf(const DevBuf &) = delete;
-  DevBuf &operator=(const DevBuf &) = delete;
-  void alloc(size_t count, cudaStream_t s) {
-    release();
-    st = s;
-    n = count;
-    CUDA_OK(cudaMallocAsync((void **)&p, sizeof(T) * std::max<size_t>(count, 1), s));
-  }
-  void release() {
-    if (p) cudaFreeAsync(p, st);
-    p = nullptr;
-  }
-  ~DevBuf() { release(); }
-};
-
 // ---------------------------------------------------------------------------
 // the molecule on the device
 // ---------------------------------------------------------------------------
-struct Molecule {
-  int n = 0;
-  std::vector<int> z;
-  std::vector<double> xyz;  // Bohr
-};
-
-struct Layout {
-  int nao = 0;
-  std::vector<int> aoff, norb, ao_atom, ao_orb;
-  std::vector<NearPair> near;
-  std::vector<int> csr_start;
-  std::vector<int2> csr;
-  int64_t w_len = 0;
-  int32_t e_len = 0;
-  bool has_d = false;
-};
-
-static void validate(const Molecule &m, const pm7_options &o) {  // src/scf.rs:937-1040
+void validate(const Molecule &m, const pm7_options &o) {  // src/scf.rs:937-1040
   auto bad = [](const std::string &s) { throw Failure{PM7_ERR_INVALID_INPUT, s}; };
   if (m.n == 0) bad("a PM7 calculation needs at least one atom");
   if (!std::isfinite(o.charge)) bad("charge must be finite");
@@ -288,7 +153,7 @@ static void validate(const Molecule &m, const pm7_options &o) {  // src/scf.rs:9
 
 // AO layout and the list of atom pairs inside the 7 Angstrom feather range, from a
 // cell list (pairs come out sorted by (u, v), u < v).
-static Layout build_layout(const Molecule &m, const ParamSet &ps) {
+Layout build_layout(const Molecule &m, const ParamSet &ps) {
   Layout L;
   for (int i = 0; i < m.n; ++i) {
     const ElementRec *e = ps.element(m.z[i]);
@@ -404,13 +269,6 @@ __global__ void k_fill_mask(int n_near, int n_atoms, const NearPair *np, unsigne
   mask[(size_t)np[p].v * n_atoms + np[p].u] = 1;
 }
 
-template <class T>
-static void upload(DevBuf<T> &b, const std::vector<T> &v, cudaStream_t st) {
-  b.alloc(v.size(), st);
-  if (!v.empty()) CUDA_OK(cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st));
-}
-
-// Core Hamiltonian and stored pair integrals on the device (hamiltonian.rs:310-638).
 // `dpath`: the molecule has a d-shell atom (or the caller forced it), so every pair is
 // evaluated in the MNDO/d frame (hamiltonian.rs:346-355).
 static void build_device_molecule(DeviceMolecule &D, const Molecule &m, const Layout &L, const DeviceParams &P,
@@ -570,7 +428,7 @@ struct ScfOut {
 };
 
 // SAD guess diagonal (scf.rs:1050-1114).
-static std::vector<double> sad_diag(const Molecule &m, const Layout &L, const ParamSet &ps, double n_electrons) {
+std::vector<double> sad_diag(const Molecule &m, const Layout &L, const ParamSet &ps, double n_electrons) {
   std::vector<double> d(L.nao, 0.0);
   double tore = 0.0;
   for (int zz : m.z) tore += ps.element(zz)->core;
@@ -920,19 +778,19 @@ static void run_uhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
 // ---------------------------------------------------------------------------
 // run_pm7
 // ---------------------------------------------------------------------------
-static double *host_copy(const double *src_dev, size_t count, cudaStream_t st) {
+double *host_copy(const double *src_dev, size_t count, cudaStream_t st) {
   double *h = (double *)std::malloc(sizeof(double) * std::max<size_t>(count, 1));
   if (count) CUDA_OK(cudaMemcpyAsync(h, src_dev, sizeof(double) * count, cudaMemcpyDeviceToHost, st));
   return h;
 }
 
-static double *host_vec(const std::vector<double> &v) {
+double *host_vec(const std::vector<double> &v) {
   double *h = (double *)std::malloc(sizeof(double) * std::max<size_t>(v.size(), 1));
   std::memcpy(h, v.data(), sizeof(double) * v.size());
   return h;
 }
 
-static uint64_t device_budget(int64_t explicit_mb) {
+uint64_t device_budget(int64_t explicit_mb) {
   if (explicit_mb >= 0) return (uint64_t)explicit_mb << 20;
   if (const char *s = std::getenv("PM7_MEM_BUDGET_MB")) {
     char *end = nullptr;
@@ -944,7 +802,7 @@ static uint64_t device_budget(int64_t explicit_mb) {
   return free_b / 5 * 4;
 }
 
-static Molecule to_molecule(const pm7_molecule *mol) {
+Molecule to_molecule(const pm7_molecule *mol) {
   if (!mol || mol->n_atoms < 0 || (mol->n_atoms > 0 && (!mol->z || !mol->xyz_bohr)))
     throw Failure{PM7_ERR_INVALID_INPUT, "null molecule"};
   Molecule m;
@@ -952,6 +810,108 @@ static Molecule to_molecule(const pm7_molecule *mol) {
   m.z.assign(mol->z, mol->z + m.n);
   m.xyz.assign(mol->xyz_bohr, mol->xyz_bohr + 3 * (size_t)m.n);
   return m;
+}
+
+void fill_result(pm7_result *res, const Molecule &m, const Layout &L, const ParamSet &ps, const pm7_options &o,
+                 const ResultParts &S, const std::vector<double> &pops,
+                 const std::function<double(int, int, int)> &Pm) {
+  // correction sum in the reference's order (scf.rs:907-932)
+  double corr = S.corr[0];
+  corr += S.corr[1];
+  corr += S.corr[4];
+  corr += S.corr[2];
+  corr += S.corr[3];
+  const double total = S.electronic_ev + S.core_ev + corr * kKcalToEv;
+  double e_isol = 0.0, eheat = 0.0;
+  for (int zz : m.z) {
+    e_isol += ps.element(zz)->e_isol;
+    eheat += ps.element(zz)->eheat_ev;
+  }
+  const double dhf = (S.electronic_ev + S.core_ev - e_isol + eheat) * kEvToKcal + corr;
+  std::memset(res, 0, sizeof(*res));
+  res->iterations = S.iterations;
+  res->density_error = S.density_error;
+  res->fp32_iterations = S.fp32_iterations;
+  if (!S.converged) {
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "PM7 SCF did not converge after %d iterations (error=%.3e)", S.iterations,
+                  S.density_error);
+    throw Failure{PM7_ERR_SCF_NOT_CONVERGED, buf};
+  }
+  const int nao = L.nao;
+  std::vector<double> q(m.n);
+  for (int a = 0; a < m.n; ++a) q[a] = ps.element(m.z[a])->core - pops[a];
+  res->n_atoms = m.n;
+  res->nao = nao;
+  res->n_occ = S.n_occ;
+  res->n_occ_beta = S.n_occ_beta;
+  res->unrestricted = S.unrestricted;
+  res->converged = 1;
+  res->electronic_ev = S.electronic_ev;
+  res->core_ev = S.core_ev;
+  res->total_ev = total;
+  res->heat_of_formation_kcal = dhf;
+  res->correction_kcal = corr;
+  res->device_ms = S.device_ms;
+  // dipole breakdown (dipole.rs:282-350)
+  {
+    double ox = 0, oy = 0, oz = 0, net = 0;
+    for (double v : q) net += v;
+    if (std::fabs(net) > 0.5 && o.dipole_origin != PM7_DIPOLE_COORDINATES) {
+      double tx = 0, ty = 0, tz = 0, tot = 0;
+      for (int a = 0; a < m.n; ++a) {
+        const double wgt = o.dipole_origin == PM7_DIPOLE_CENTRE_OF_MASS ? (m.z[a] < 87 ? pm7_mass_table()[m.z[a]] : 0.0)
+                                                                        : ps.element(m.z[a])->core;
+        tx += m.xyz[3 * a] * wgt;
+        ty += m.xyz[3 * a + 1] * wgt;
+        tz += m.xyz[3 * a + 2] * wgt;
+        tot += wgt;
+      }
+      if (tot > 0.0) {
+        ox = tx / tot;
+        oy = ty / tot;
+        oz = tz / tot;
+      }
+    }
+    double pc[3] = {0, 0, 0}, sp[3] = {0, 0, 0}, pd[3] = {0, 0, 0};
+    const double inv3 = 0.5773502691896258;
+    for (int a = 0; a < m.n; ++a) {
+      pc[0] += (m.xyz[3 * a] - ox) * q[a];
+      pc[1] += (m.xyz[3 * a + 1] - oy) * q[a];
+      pc[2] += (m.xyz[3 * a + 2] - oz) * q[a];
+      const ElementRec *e = ps.element(m.z[a]);
+      if (e->n_orb >= 4) {
+        const double hyb = -2.0 * e->dd;
+        for (int k = 0; k < 3; ++k) sp[k] += hyb * Pm(a, 0, 1 + k);
+      }
+      if (e->n_orb == 9) {
+        const double hyb = -2.0 * e->ddp[5];
+        pd[0] += hyb * (Pm(a, 5, 3) + Pm(a, 4, 1) + Pm(a, 8, 2) - inv3 * Pm(a, 6, 1));
+        pd[1] += hyb * (Pm(a, 7, 3) - Pm(a, 4, 2) + Pm(a, 8, 1) - inv3 * Pm(a, 6, 2));
+        pd[2] += hyb * (Pm(a, 5, 1) + Pm(a, 7, 2) + 2.0 * inv3 * Pm(a, 6, 3));
+      }
+    }
+    double mag = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      res->dipole_point_charge[k] = pc[k] * kAuDipoleToDebye;
+      res->dipole_sp_hybrid[k] = sp[k] * kAuDipoleToDebye;
+      res->dipole_pd_hybrid[k] = pd[k] * kAuDipoleToDebye;
+      res->dipole_debye[k] = res->dipole_point_charge[k] + res->dipole_sp_hybrid[k] + res->dipole_pd_hybrid[k];
+      mag += res->dipole_debye[k] * res->dipole_debye[k];
+    }
+    res->dipole_magnitude = std::sqrt(mag);
+  }
+  const double nan = std::numeric_limits<double>::quiet_NaN();
+  res->homo_ev = S.n_occ >= 1 ? S.eps_a[S.n_occ - 1] : nan;
+  res->lumo_ev = S.n_occ < nao ? S.eps_a[S.n_occ] : nan;
+  res->homo_ev_beta = res->lumo_ev_beta = nan;
+  if (S.unrestricted) {
+    res->homo_ev_beta = S.n_occ_beta >= 1 ? S.eps_b[S.n_occ_beta - 1] : nan;
+    res->lumo_ev_beta = S.n_occ_beta < nao ? S.eps_b[S.n_occ_beta] : nan;
+  }
+  res->charges = host_vec(q);
+  res->mo_energies = host_vec(S.eps_a);
+  if (S.unrestricted) res->mo_energies_beta = host_vec(S.eps_b);
 }
 
 static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm7_options *opt, pm7_result *res) {
@@ -1040,109 +1000,29 @@ static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
 
-  double corr = parts[0];
-  corr += parts[1];
-  corr += parts[4];
-  corr += parts[2];
-  corr += parts[3];
-  const double core_ev = D.core_core_ev;
-  const double total = S.electronic_ev + core_ev + corr * kKcalToEv;
-  double e_isol = 0.0, eheat = 0.0;
-  for (int zz : m.z) {
-    e_isol += ps.element(zz)->e_isol;
-    eheat += ps.element(zz)->eheat_ev;
-  }
-  const double dhf = (S.electronic_ev + core_ev - e_isol + eheat) * kEvToKcal + corr;
-  std::memset(res, 0, sizeof(*res));
-  res->iterations = S.iterations;
-  res->density_error = S.density_error;
-  if (!S.converged) {
-    char buf[160];
-    std::snprintf(buf, sizeof buf, "PM7 SCF did not converge after %d iterations (error=%.3e)", S.iterations,
-                  S.density_error);
-    throw Failure{PM7_ERR_SCF_NOT_CONVERGED, buf};
-  }
+  ResultParts R;
+  R.iterations = S.iterations;
+  R.density_error = S.density_error;
+  R.converged = S.converged;
+  R.electronic_ev = S.electronic_ev;
+  R.core_ev = D.core_core_ev;
+  for (int k = 0; k < 5; ++k) R.corr[k] = parts[k];
+  R.n_occ = S.n_occ;
+  R.n_occ_beta = S.n_occ_beta;
+  R.unrestricted = S.unrestricted;
+  R.eps_a = S.eps_a;
+  R.eps_b = S.eps_b;
+  R.device_ms = ms;
   const int nao = L.nao;
   const size_t nn = (size_t)nao * nao;
-  std::vector<double> Ph(nn);
-  CUDA_OK(cudaMemcpyAsync(Ph.data(), S.P.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
-  CUDA_OK(cudaStreamSynchronize(st));
-  std::vector<double> q(m.n);
-  for (int a = 0; a < m.n; ++a) q[a] = ps.element(m.z[a])->core - diag_blocks[a];
-  res->n_atoms = m.n;
-  res->nao = nao;
-  res->n_occ = S.n_occ;
-  res->n_occ_beta = S.n_occ_beta;
-  res->unrestricted = S.unrestricted;
-  res->converged = 1;
-  res->electronic_ev = S.electronic_ev;
-  res->core_ev = core_ev;
-  res->total_ev = total;
-  res->heat_of_formation_kcal = dhf;
-  res->correction_kcal = corr;
-  res->device_ms = ms;
-  // dipole breakdown (dipole.rs:282-350)
-  {
-    double ox = 0, oy = 0, oz = 0, net = 0;
-    for (double v : q) net += v;
-    if (std::fabs(net) > 0.5 && o.dipole_origin != PM7_DIPOLE_COORDINATES) {
-      double tx = 0, ty = 0, tz = 0, tot = 0;
-      for (int a = 0; a < m.n; ++a) {
-        extern const double *pm7_mass_table();
-        const double wgt = o.dipole_origin == PM7_DIPOLE_CENTRE_OF_MASS ? (m.z[a] < 87 ? pm7_mass_table()[m.z[a]] : 0.0)
-                                                                        : ps.element(m.z[a])->core;
-        tx += m.xyz[3 * a] * wgt;
-        ty += m.xyz[3 * a + 1] * wgt;
-        tz += m.xyz[3 * a + 2] * wgt;
-        tot += wgt;
-      }
-      if (tot > 0.0) {
-        ox = tx / tot;
-        oy = ty / tot;
-        oz = tz / tot;
-      }
-    }
-    double pc[3] = {0, 0, 0}, sp[3] = {0, 0, 0}, pd[3] = {0, 0, 0};
-    const double inv3 = 0.5773502691896258;
-    for (int a = 0; a < m.n; ++a) {
-      pc[0] += (m.xyz[3 * a] - ox) * q[a];
-      pc[1] += (m.xyz[3 * a + 1] - oy) * q[a];
-      pc[2] += (m.xyz[3 * a + 2] - oz) * q[a];
-      const ElementRec *e = ps.element(m.z[a]);
-      const int off = L.aoff[a];
-      auto Pm = [&](int i, int j) { return Ph[(size_t)(off + i) * nao + off + j]; };
-      if (e->n_orb >= 4) {
-        const double hyb = -2.0 * e->dd;
-        for (int k = 0; k < 3; ++k) sp[k] += hyb * Pm(0, 1 + k);
-      }
-      if (e->n_orb == 9) {
-        const double hyb = -2.0 * e->ddp[5];
-        pd[0] += hyb * (Pm(5, 3) + Pm(4, 1) + Pm(8, 2) - inv3 * Pm(6, 1));
-        pd[1] += hyb * (Pm(7, 3) - Pm(4, 2) + Pm(8, 1) - inv3 * Pm(6, 2));
-        pd[2] += hyb * (Pm(5, 1) + Pm(7, 2) + 2.0 * inv3 * Pm(6, 3));
-      }
-    }
-    double mag = 0.0;
-    for (int k = 0; k < 3; ++k) {
-      res->dipole_point_charge[k] = pc[k] * kAuDipoleToDebye;
-      res->dipole_sp_hybrid[k] = sp[k] * kAuDipoleToDebye;
-      res->dipole_pd_hybrid[k] = pd[k] * kAuDipoleToDebye;
-      res->dipole_debye[k] = res->dipole_point_charge[k] + res->dipole_sp_hybrid[k] + res->dipole_pd_hybrid[k];
-      mag += res->dipole_debye[k] * res->dipole_debye[k];
-    }
-    res->dipole_magnitude = std::sqrt(mag);
+  std::vector<double> Ph;
+  if (S.converged) {
+    Ph.resize(nn);
+    CUDA_OK(cudaMemcpyAsync(Ph.data(), S.P.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
   }
-  const double nan = std::numeric_limits<double>::quiet_NaN();
-  res->homo_ev = S.n_occ >= 1 ? S.eps_a[S.n_occ - 1] : nan;
-  res->lumo_ev = S.n_occ < nao ? S.eps_a[S.n_occ] : nan;
-  res->homo_ev_beta = res->lumo_ev_beta = nan;
-  if (S.unrestricted) {
-    res->homo_ev_beta = S.n_occ_beta >= 1 ? S.eps_b[S.n_occ_beta - 1] : nan;
-    res->lumo_ev_beta = S.n_occ_beta < nao ? S.eps_b[S.n_occ_beta] : nan;
-  }
-  res->charges = host_vec(q);
-  res->mo_energies = host_vec(S.eps_a);
-  if (S.unrestricted) res->mo_energies_beta = host_vec(S.eps_b);
+  fill_result(res, m, L, ps, o, R, diag_blocks,
+              [&](int a, int i, int j) { return Ph[(size_t)(L.aoff[a] + i) * nao + L.aoff[a] + j]; });
   if (o.want_matrices) {
     res->density = host_vec(Ph);
     if (S.unrestricted) res->spin_density = host_copy(S.Pspin.p, nn, st);

@@ -10,6 +10,7 @@
 #include "kernels.hpp"
 #include "core_repulsion.cuh"
 #include "nddo_sp.cuh"
+#include "batch.hpp"
 
 namespace pm7 {
 
@@ -17,14 +18,11 @@ __device__ __forceinline__ double beta_of(const ElementRec &e, int orb) {
   return orb == 0 ? e.beta_s : (orb <= 3 ? e.beta_p : e.beta_d);
 }
 
-// All pairs u < v: beta*S off-diagonal blocks of H and the core-core energy.
-// Grid: (ceil(N/128), N), block 128; blockIdx.y = u. Energies are reduced per
-// block into `cc_partial[blockIdx.y * gridDim.x + blockIdx.x]`.
-__global__ void k_pairs_all(int n_atoms, const int *__restrict__ z, const double *__restrict__ xyz,
-                            const int *__restrict__ aoff, int nao, DeviceParams P, double *__restrict__ H,
-                            double *__restrict__ cc_partial, int *__restrict__ status) {
-  const int u = blockIdx.y;
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+// One pair u < v (v may be out of range): beta*S off-diagonal blocks of H; returns the
+// core-core energy of the pair (0 when v is not a partner).
+__device__ __forceinline__ double pair_sp_elem(int n_atoms, const int *__restrict__ z, const double *__restrict__ xyz,
+                                               const int *__restrict__ aoff, int nao, const DeviceParams &P,
+                                               double *__restrict__ H, int *status, int u, int v) {
   double ecc = 0.0;
   if (v > u && v < n_atoms) {
     const ElementRec &eu = P.elements[z[u]];
@@ -37,7 +35,7 @@ __global__ void k_pairs_all(int n_atoms, const int *__restrict__ z, const double
     const double dx = xyz[3 * b] - xyz[3 * a], dy = xyz[3 * b + 1] - xyz[3 * a + 1], dz = xyz[3 * b + 2] - xyz[3 * a + 2];
     double S[4][4];
     if (!d_overlap_sp(ea, eb, dx, dy, dz, S, P.tab)) {
-      atomicOr(status, 1);
+      if (status) atomicOr(status, 1);
     } else {
       const int oa = aoff[a], ob = aoff[b];
       for (int i = 0; i < ea.n_orb && i < 4; ++i) {
@@ -53,22 +51,43 @@ __global__ void k_pairs_all(int n_atoms, const int *__restrict__ z, const double
                                            (xyz[3 * v + 1] - xyz[3 * u + 1]) * (xyz[3 * v + 1] - xyz[3 * u + 1]) +
                                            (xyz[3 * v + 2] - xyz[3 * u + 2]) * (xyz[3 * v + 2] - xyz[3 * u + 2])));
   }
+  return ecc;
+}
+
+// All pairs u < v: beta*S off-diagonal blocks of H and the core-core energy.
+// Grid: (ceil(N/128), N), block 128; blockIdx.y = u. Energies are reduced per
+// block into `cc_partial[blockIdx.y * gridDim.x + blockIdx.x]`.
+__global__ void k_pairs_all(int n_atoms, const int *__restrict__ z, const double *__restrict__ xyz,
+                            const int *__restrict__ aoff, int nao, DeviceParams P, double *__restrict__ H,
+                            double *__restrict__ cc_partial, int *__restrict__ status) {
+  const double ecc = pair_sp_elem(n_atoms, z, xyz, aoff, nao, P, H, status, blockIdx.y,
+                                  blockIdx.x * blockDim.x + threadIdx.x);
   const double s = block_sum<128>(ecc);
   if (threadIdx.x == 0) cc_partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
 }
 
+// Batched: item = (atom u, column block) of one molecule; partial u * cc_nx + block.
+__global__ void k_b_pairs_all(BatchList L, const MolDesc *__restrict__ D, DeviceParams P) {
+  const int item = blockIdx.x;
+  const int m = batch_find(L, item);
+  const MolDesc &d = D[L.slot[m]];
+  const int local = item - L.prefix[m];
+  const int u = local / d.cc_nx, bx = local - u * d.cc_nx;
+  const double ecc = pair_sp_elem(d.g.n_atoms, d.g.z, d.g.xyz, d.g.aoff, d.g.nao, P, d.H, nullptr, u,
+                                  bx * blockDim.x + threadIdx.x);
+  const double s = block_sum<128>(ecc);
+  if (threadIdx.x == 0) d.cc_partial[(size_t)u * d.cc_nx + bx] = s;
+}
+
 // Near pairs: store w in (u,v) orientation and the packed electron-core blocks of
 // both atoms (integrals.rs:186-271 for the sp kernel). One thread per pair.
-__global__ void k_near_integrals(int n_near, const int *__restrict__ z, const double *__restrict__ xyz,
-                                 const NearPair *__restrict__ np, DeviceParams P, double *__restrict__ w,
-                                 double *__restrict__ ecore, int *__restrict__ status) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n_near) return;
-  const NearPair q = np[p];
+__device__ __forceinline__ void near_sp_pair(const int *__restrict__ z, const double *__restrict__ xyz,
+                                             const NearPair q, const DeviceParams &P, double *__restrict__ w,
+                                             double *__restrict__ ecore, int *status) {
   const ElementRec &eu = P.elements[z[q.u]];
   const ElementRec &ev = P.elements[z[q.v]];
   if (eu.n_orb == 9 || ev.n_orb == 9) {
-    atomicOr(status, 2);
+    if (status) atomicOr(status, 2);
     return;
   }
   const bool keep = eu.n_orb >= ev.n_orb;
@@ -130,22 +149,36 @@ __global__ void k_near_integrals(int n_near, const int *__restrict__ z, const do
     }
 }
 
+__global__ void k_near_integrals(int n_near, const int *__restrict__ z, const double *__restrict__ xyz,
+                                 const NearPair *__restrict__ np, DeviceParams P, double *__restrict__ w,
+                                 double *__restrict__ ecore, int *__restrict__ status) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_near) return;
+  near_sp_pair(z, xyz, np[p], P, w, ecore, status);
+}
+
+// Batched: item = a chunk of 128 near pairs of one molecule.
+__global__ void k_b_near_integrals(BatchList L, const MolDesc *__restrict__ D, DeviceParams P) {
+  const int item = blockIdx.x;
+  const int m = batch_find(L, item);
+  const MolDesc &d = D[L.slot[m]];
+  const int p = (item - L.prefix[m]) * 128 + threadIdx.x;
+  if (p >= d.g.n_near) return;
+  near_sp_pair(d.g.z, d.g.xyz, d.g.np[p], P, d.w, d.ecore, nullptr);
+}
+
 // Diagonal atom blocks of H_core: U on the diagonal plus the electron-core
 // attraction of every other atom. Near partners contribute their stored packed
 // blocks (summed in partner order); every other atom is beyond the 7 Angstrom
 // feather range, where the attraction is exactly the point charge -Z_B * EV / r on
 // the diagonal (integrals.rs:540-574). One block per atom.
 constexpr int HDIAG_THREADS = 128;
-__global__ void __launch_bounds__(HDIAG_THREADS) k_hcore_diag(int n_atoms, const int *__restrict__ z,
-                                                              const double *__restrict__ xyz,
-                                                              const int *__restrict__ aoff,
-                                                              const int *__restrict__ csr_start,
-                                                              const int2 *__restrict__ csr,
-                                                              const NearPair *__restrict__ np,
-                                                              const double *__restrict__ ecore,
-                                                              const unsigned char *__restrict__ near_mask,
-                                                              DeviceParams P, int nao, double *__restrict__ H) {
-  const int A = blockIdx.x;
+__device__ __forceinline__ void hcore_diag_block(int A, int n_atoms, const int *__restrict__ z,
+                                                 const double *__restrict__ xyz, const int *__restrict__ aoff,
+                                                 const int *__restrict__ csr_start, const int2 *__restrict__ csr,
+                                                 const NearPair *__restrict__ np, const double *__restrict__ ecore,
+                                                 const unsigned char *__restrict__ near_mask, const DeviceParams &P,
+                                                 int nao, double *__restrict__ H) {
   const ElementRec &e = P.elements[z[A]];
   const int no = e.n_orb, off = aoff[A];
   if (no == 0) return;
@@ -183,6 +216,28 @@ __global__ void __launch_bounds__(HDIAG_THREADS) k_hcore_diag(int n_atoms, const
   }
 }
 
+__global__ void __launch_bounds__(HDIAG_THREADS) k_hcore_diag(int n_atoms, const int *__restrict__ z,
+                                                              const double *__restrict__ xyz,
+                                                              const int *__restrict__ aoff,
+                                                              const int *__restrict__ csr_start,
+                                                              const int2 *__restrict__ csr,
+                                                              const NearPair *__restrict__ np,
+                                                              const double *__restrict__ ecore,
+                                                              const unsigned char *__restrict__ near_mask,
+                                                              DeviceParams P, int nao, double *__restrict__ H) {
+  hcore_diag_block(blockIdx.x, n_atoms, z, xyz, aoff, csr_start, csr, np, ecore, near_mask, P, nao, H);
+}
+
+// Batched: item = an atom of one molecule.
+__global__ void __launch_bounds__(HDIAG_THREADS) k_b_hcore_diag(BatchList L, const MolDesc *__restrict__ D,
+                                                                DeviceParams P) {
+  const int item = blockIdx.x;
+  const int m = batch_find(L, item);
+  const MolDesc &d = D[L.slot[m]];
+  hcore_diag_block(item - L.prefix[m], d.g.n_atoms, d.g.z, d.g.xyz, d.g.aoff, d.g.csr_start, d.g.csr, d.g.np,
+                   d.ecore, d.g.near_mask, P, d.g.nao, d.H);
+}
+
 __global__ void k_sum_partials(const double *__restrict__ in, size_t n, double *__restrict__ out) {
   double s = 0.0;
   for (size_t i = threadIdx.x; i < n; i += blockDim.x) s += in[i];
@@ -214,6 +269,24 @@ void launch_hcore_diag(cudaStream_t st, int n_atoms, const int *z, const double 
                        const unsigned char *near_mask, const DeviceParams &P, int nao, double *H) {
   k_hcore_diag<<<n_atoms, HDIAG_THREADS, 0, st>>>(n_atoms, z, xyz, aoff, csr_start, csr, np, ecore, near_mask, P,
                                                   nao, H);
+  note_launch();
+}
+
+void launch_b_pairs_all(cudaStream_t st, const BatchList &L, const MolDesc *D, const DeviceParams &P) {
+  if (L.total <= 0) return;
+  k_b_pairs_all<<<L.total, 128, 0, st>>>(L, D, P);
+  note_launch();
+}
+
+void launch_b_near_integrals(cudaStream_t st, const BatchList &L, const MolDesc *D, const DeviceParams &P) {
+  if (L.total <= 0) return;
+  k_b_near_integrals<<<L.total, 128, 0, st>>>(L, D, P);
+  note_launch();
+}
+
+void launch_b_hcore_diag(cudaStream_t st, const BatchList &L, const MolDesc *D, const DeviceParams &P) {
+  if (L.total <= 0) return;
+  k_b_hcore_diag<<<L.total, HDIAG_THREADS, 0, st>>>(L, D, P);
   note_launch();
 }
 

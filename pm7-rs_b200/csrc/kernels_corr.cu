@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "batch.hpp"
 #include "kernels.hpp"
 
 namespace pm7 {
@@ -87,9 +88,8 @@ __device__ double pair_dispersion(int zi, int zj, double c6i, double c6j, double
 }
 
 // Per-atom effective C6: discrete neighbour count (MOPAC nbonds) or the smooth one.
-__global__ void k_c6(int n, const int *__restrict__ z, const double *__restrict__ xyz, int smooth,
-                     double *__restrict__ c6) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void c6_atom(int n, const int *__restrict__ z, const double *__restrict__ xyz, int smooth,
+                                        double *__restrict__ c6, int i) {
   if (i >= n) return;
   int cnt = 0;
   double scnt = 0.0;
@@ -117,11 +117,12 @@ __global__ void k_c6(int n, const int *__restrict__ z, const double *__restrict_
 }
 
 // Pair terms of every u < v: dispersion, C#C and PM7-HH. Grid (ceil(N/128), N).
-__global__ void k_pair_corr(int n, const int *__restrict__ z, const double *__restrict__ xyz,
-                            const double *__restrict__ c6, int hh, double *__restrict__ part_disp,
-                            double *__restrict__ part_yne, double *__restrict__ part_hh) {
-  const int u = blockIdx.y, v = blockIdx.x * blockDim.x + threadIdx.x;
-  double ed = 0.0, ey = 0.0, eh = 0.0;
+__device__ __forceinline__ void pair_corr_elem(int n, const int *__restrict__ z, const double *__restrict__ xyz,
+                                               const double *__restrict__ c6, int hh, int u, int v, double &ed,
+                                               double &ey, double &eh) {
+  ed = 0.0;
+  ey = 0.0;
+  eh = 0.0;
   if (v > u && v < n) {
     const double dx = xyz[3 * v] - xyz[3 * u], dy = xyz[3 * v + 1] - xyz[3 * u + 1], dz = xyz[3 * v + 2] - xyz[3 * u + 2];
     const double r = sqrt(dx * dx + dy * dy + dz * dz);
@@ -147,7 +148,15 @@ __global__ void k_pair_corr(int n, const int *__restrict__ z, const double *__re
       }
     }
   }
-  const size_t slot = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+}
+
+// Block sums of one (u, column block) of the pair sweep into partial `slot`.
+__device__ __forceinline__ void pair_corr_block(int n, const int *__restrict__ z, const double *__restrict__ xyz,
+                                                const double *__restrict__ c6, int hh, int u, int bx, size_t slot,
+                                                double *__restrict__ part_disp, double *__restrict__ part_yne,
+                                                double *__restrict__ part_hh) {
+  double ed, ey, eh;
+  pair_corr_elem(n, z, xyz, c6, hh, u, bx * blockDim.x + threadIdx.x, ed, ey, eh);
   const double sd = block_sum<128>(ed);
   const double sy = block_sum<128>(ey);
   const double sh = block_sum<128>(eh);
@@ -159,8 +168,8 @@ __global__ void k_pair_corr(int n, const int *__restrict__ z, const double *__re
 }
 
 // Si-O-H bending penalty, one thread per oxygen (mm_corrections.rs:154-224).
-__global__ void k_sioh(int n, const int *__restrict__ z, const double *__restrict__ xyz, double *__restrict__ e_out) {
-  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void sioh_atom(int n, const int *__restrict__ z, const double *__restrict__ xyz,
+                                          double *__restrict__ e_out, int o) {
   if (o >= n) return;
   double e = 0.0;
   if (z[o] == 8) {
@@ -248,9 +257,8 @@ __device__ double dihed(const double *xyz, int i, int j, int k, int l) {
 __device__ __forceinline__ double bonding(const int *z, int x, int y) { return covrad43(z[x]) + covrad43(z[y]); }
 
 // Covalent neighbours (ascending scan, at most 4: a fifth evicts the longest).
-__global__ void k_hb_neighbours(int n, const int *__restrict__ z, const double *__restrict__ xyz,
-                                int *__restrict__ nbr, int *__restrict__ nbc) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void hb_neighbours_atom(int n, const int *__restrict__ z, const double *__restrict__ xyz,
+                                                   int *__restrict__ nbr, int *__restrict__ nbc, int a) {
   if (a >= n) return;
   int list[5];
   int cnt = 0;
@@ -442,10 +450,10 @@ __device__ __forceinline__ bool is_acceptor(int z) { return z == 7 || z == 8; }
 // acceptor k (N/O within 7 A of i, D-H...A angle above 90 degrees, lanes over k), each
 // unordered {i,k} once with the lower-index donor taking the bond as in the reference's
 // scan; lane sums are combined in a fixed shuffle order.
-__global__ void k_hbonds(int n, const int *__restrict__ z, const double *__restrict__ xyz, const int *__restrict__ nbr,
-                         const int *__restrict__ nbc, double *__restrict__ e_out) {
+__device__ __forceinline__ void hbonds_warp(int n, const int *__restrict__ z, const double *__restrict__ xyz,
+                                            const int *__restrict__ nbr, const int *__restrict__ nbc,
+                                            double *__restrict__ e_out, int j) {
   const int lane = threadIdx.x & 31;
-  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (j >= n) return;
   double e = 0.0;
   if (z[j] == 1) {
@@ -472,9 +480,10 @@ __global__ void k_hbonds(int n, const int *__restrict__ z, const double *__restr
   if (lane == 0) e_out[j] = e;
 }
 
-__global__ void k_finish(int n_pairs_part, const double *__restrict__ pd, const double *__restrict__ py,
-                         const double *__restrict__ ph, int n, const double *__restrict__ ehb,
-                         const double *__restrict__ esioh, double *__restrict__ out) {
+__device__ __forceinline__ void finish_block(int n_pairs_part, const double *__restrict__ pd,
+                                             const double *__restrict__ py, const double *__restrict__ ph, int n,
+                                             const double *__restrict__ ehb, const double *__restrict__ esioh,
+                                             double *__restrict__ out) {
   double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
   for (int i = threadIdx.x; i < n_pairs_part; i += 256) {
     s0 += pd[i];
@@ -499,11 +508,122 @@ __global__ void k_finish(int n_pairs_part, const double *__restrict__ pd, const 
   }
 }
 
+// Scratch of one molecule's corrections (corrections_scratch floats of layout below).
+struct CorrView {
+  int n, gx;
+  size_t parts;
+  double *pd, *py, *ph, *c6, *ehb, *esioh;
+  int *nbr, *nbc;
+};
+__host__ __device__ inline CorrView corr_view(int n, double *scratch) {
+  CorrView v;
+  v.n = n;
+  v.gx = (n + 127) / 128;
+  v.parts = (size_t)v.gx * n;
+  v.pd = scratch;
+  v.py = v.pd + v.parts;
+  v.ph = v.py + v.parts;
+  v.c6 = v.ph + v.parts;
+  v.ehb = v.c6 + n;
+  v.esioh = v.ehb + n;
+  v.nbr = reinterpret_cast<int *>(v.esioh + n);
+  v.nbc = v.nbr + 4 * n;
+  return v;
+}
+
+// ---- one molecule ----
+__global__ void k_c6(int n, const int *__restrict__ z, const double *__restrict__ xyz, int smooth,
+                     double *__restrict__ c6) {
+  c6_atom(n, z, xyz, smooth, c6, blockIdx.x * blockDim.x + threadIdx.x);
+}
+__global__ void k_pair_corr(int n, const int *__restrict__ z, const double *__restrict__ xyz,
+                            const double *__restrict__ c6, int hh, double *__restrict__ part_disp,
+                            double *__restrict__ part_yne, double *__restrict__ part_hh) {
+  pair_corr_block(n, z, xyz, c6, hh, blockIdx.y, blockIdx.x, (size_t)blockIdx.y * gridDim.x + blockIdx.x, part_disp,
+                  part_yne, part_hh);
+}
+__global__ void k_sioh(int n, const int *__restrict__ z, const double *__restrict__ xyz, double *__restrict__ e_out) {
+  sioh_atom(n, z, xyz, e_out, blockIdx.x * blockDim.x + threadIdx.x);
+}
+__global__ void k_hb_neighbours(int n, const int *__restrict__ z, const double *__restrict__ xyz,
+                                int *__restrict__ nbr, int *__restrict__ nbc) {
+  hb_neighbours_atom(n, z, xyz, nbr, nbc, blockIdx.x * blockDim.x + threadIdx.x);
+}
+__global__ void k_hbonds(int n, const int *__restrict__ z, const double *__restrict__ xyz, const int *__restrict__ nbr,
+                         const int *__restrict__ nbc, double *__restrict__ e_out) {
+  hbonds_warp(n, z, xyz, nbr, nbc, e_out, blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+}
+__global__ void k_finish(int n_pairs_part, const double *__restrict__ pd, const double *__restrict__ py,
+                         const double *__restrict__ ph, int n, const double *__restrict__ ehb,
+                         const double *__restrict__ esioh, double *__restrict__ out) {
+  finish_block(n_pairs_part, pd, py, ph, n, ehb, esioh, out);
+}
+
+// ---- batched: molecule = L.slot[blockIdx.z] (per-atom kernels) or a prefix item ----
+__global__ void k_b_c6(BatchList L, const MolDesc *__restrict__ D) {
+  const MolDesc &d = D[L.slot[blockIdx.z]];
+  const CorrView v = corr_view(d.g.n_atoms, d.corr_scratch);
+  c6_atom(v.n, d.g.z, d.g.xyz, d.smooth_dispersion, v.c6, blockIdx.x * blockDim.x + threadIdx.x);
+}
+__global__ void k_b_hb_neighbours(BatchList L, const MolDesc *__restrict__ D) {
+  const MolDesc &d = D[L.slot[blockIdx.z]];
+  const CorrView v = corr_view(d.g.n_atoms, d.corr_scratch);
+  hb_neighbours_atom(v.n, d.g.z, d.g.xyz, v.nbr, v.nbc, blockIdx.x * blockDim.x + threadIdx.x);
+}
+__global__ void k_b_sioh(BatchList L, const MolDesc *__restrict__ D) {
+  const MolDesc &d = D[L.slot[blockIdx.z]];
+  const CorrView v = corr_view(d.g.n_atoms, d.corr_scratch);
+  sioh_atom(v.n, d.g.z, d.g.xyz, v.esioh, blockIdx.x * blockDim.x + threadIdx.x);
+}
+__global__ void k_b_hbonds(BatchList L, const MolDesc *__restrict__ D) {
+  const MolDesc &d = D[L.slot[blockIdx.z]];
+  const CorrView v = corr_view(d.g.n_atoms, d.corr_scratch);
+  hbonds_warp(v.n, d.g.z, d.g.xyz, v.nbr, v.nbc, v.ehb, blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+}
+// item = (atom u, column block) of one molecule, as in the core-core sweep
+__global__ void k_b_pair_corr(BatchList L, const MolDesc *__restrict__ D, int hh) {
+  const int item = blockIdx.x;
+  const int m = batch_find(L, item);
+  const MolDesc &d = D[L.slot[m]];
+  const CorrView v = corr_view(d.g.n_atoms, d.corr_scratch);
+  const int local = item - L.prefix[m];
+  const int u = local / v.gx, bx = local - u * v.gx;
+  pair_corr_block(v.n, d.g.z, d.g.xyz, v.c6, hh, u, bx, (size_t)u * v.gx + bx, v.pd, v.py, v.ph);
+}
+__global__ void k_b_finish(BatchList L, const MolDesc *__restrict__ D, MolCtl *__restrict__ C, int zero) {
+  const int slot = L.slot[blockIdx.x];
+  const MolDesc &d = D[slot];
+  if (zero) {
+    if (threadIdx.x < 5) C[slot].corr[threadIdx.x] = 0.0;
+    return;
+  }
+  const CorrView v = corr_view(d.g.n_atoms, d.corr_scratch);
+  finish_block((int)v.parts, v.pd, v.py, v.ph, v.n, v.ehb, v.esioh, C[slot].corr);
+}
+
 }  // namespace
 
 size_t corrections_scratch(int n_atoms) {
   const size_t parts = (size_t)((n_atoms + 127) / 128) * (size_t)(n_atoms > 0 ? n_atoms : 1);
   return 3 * parts + 3 * (size_t)n_atoms + 8 * (size_t)n_atoms;
+}
+
+void launch_b_corrections(cudaStream_t st, const BatchList &Lmol, const BatchList &Lpairs, const MolDesc *D, MolCtl *C,
+                          int method, int max_atoms) {
+  if (Lmol.n <= 0) return;
+  if (method == 3 || max_atoms == 0) {  // PM7-minus carries no post-SCF corrections
+    k_b_finish<<<Lmol.n, 256, 0, st>>>(Lmol, D, C, 1);
+    note_launch();
+    return;
+  }
+  const int ga = (max_atoms + 127) / 128;
+  k_b_c6<<<dim3(ga, 1, Lmol.n), 128, 0, st>>>(Lmol, D);
+  if (Lpairs.total > 0) k_b_pair_corr<<<Lpairs.total, 128, 0, st>>>(Lpairs, D, method == 4);
+  k_b_hb_neighbours<<<dim3(ga, 1, Lmol.n), 128, 0, st>>>(Lmol, D);
+  k_b_hbonds<<<dim3((max_atoms + 3) / 4, 1, Lmol.n), 128, 0, st>>>(Lmol, D);
+  k_b_sioh<<<dim3(ga, 1, Lmol.n), 128, 0, st>>>(Lmol, D);
+  k_b_finish<<<Lmol.n, 256, 0, st>>>(Lmol, D, C, 0);
+  note_launch(6);
 }
 
 void launch_corrections(cudaStream_t st, int n, const int *z, const double *xyz, int method, int smooth,

@@ -16,6 +16,7 @@
 
 #include "common.cuh"
 #include "core_repulsion.cuh"
+#include "batch.hpp"
 #include "kernels.hpp"
 #include "nddo_sp.cuh"
 
@@ -724,20 +725,13 @@ __device__ __forceinline__ void unpack(int k, int &mu, int &nu) {
   nu = k - m * (m + 1) / 2;
 }
 
-constexpr int kDWarps = 2;  // pairs per block
+constexpr int kDWarps = kDPairsPerBlock;  // pairs (warps) per block
 
-// Near pairs in the MNDO/d frame: w in (u, v) orientation and the packed electron-core
-// blocks of both atoms. One warp per pair.
-__global__ void __launch_bounds__(32 * kDWarps) k_near_integrals_d(int n_near, const int *__restrict__ z,
-                                                                   const double *__restrict__ xyz,
-                                                                   const NearPair *__restrict__ np, DeviceParams P,
-                                                                   double *__restrict__ w, double *__restrict__ ecore) {
-  extern __shared__ double smem_d[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int p = blockIdx.x * kDWarps + warp;
-  if (p >= n_near) return;
-  DPairShared &S = reinterpret_cast<DPairShared *>(smem_d)[warp];
-  const NearPair q = np[p];
+// One near pair in the MNDO/d frame by one warp: w in (u, v) orientation and the packed
+// electron-core blocks of both atoms.
+__device__ __forceinline__ void near_d_pair(DPairShared &S, const DeviceParams &P, const int *__restrict__ z,
+                                            const double *__restrict__ xyz, const NearPair q,
+                                            double *__restrict__ w, double *__restrict__ ecore, int lane) {
   const ElementRec &eu = P.elements[z[q.u]];
   const ElementRec &ev = P.elements[z[q.v]];
   const bool keep = eu.n_orb >= ev.n_orb;  // heavier-first ordering (hamiltonian.rs:388-392)
@@ -764,6 +758,32 @@ __global__ void __launch_bounds__(32 * kDWarps) k_near_integrals_d(int n_near, c
       e_b[t - limij] = elenuc(S, P.tab, 2, mu + 1, nu + 1);
     }
   }
+  __syncwarp();
+}
+
+// Near pairs in the MNDO/d frame, one warp per pair.
+__global__ void __launch_bounds__(32 * kDWarps) k_near_integrals_d(int n_near, const int *__restrict__ z,
+                                                                   const double *__restrict__ xyz,
+                                                                   const NearPair *__restrict__ np, DeviceParams P,
+                                                                   double *__restrict__ w, double *__restrict__ ecore) {
+  extern __shared__ double smem_d[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = blockIdx.x * kDWarps + warp;
+  if (p >= n_near) return;
+  near_d_pair(reinterpret_cast<DPairShared *>(smem_d)[warp], P, z, xyz, np[p], w, ecore, lane);
+}
+
+// Batched: item = kDWarps consecutive near pairs of one molecule.
+__global__ void __launch_bounds__(32 * kDWarps) k_b_near_integrals_d(BatchList L, const MolDesc *__restrict__ D,
+                                                                     DeviceParams P) {
+  extern __shared__ double smem_d[];
+  const int item = blockIdx.x;
+  const int m = batch_find(L, item);
+  const MolDesc &d = D[L.slot[m]];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = (item - L.prefix[m]) * kDWarps + warp;
+  if (p >= d.g.n_near) return;
+  near_d_pair(reinterpret_cast<DPairShared *>(smem_d)[warp], P, d.g.z, d.g.xyz, d.g.np[p], d.w, d.ecore, lane);
 }
 
 // ---- general Slater overlaps (src/overlap_d.rs) -------------------------------------
@@ -988,33 +1008,49 @@ __device__ __forceinline__ double beta_of(const ElementRec &e, int orb) {
   return orb == 0 ? e.beta_s : (orb <= 3 ? e.beta_p : e.beta_d);
 }
 
-// All pairs u < v in the MNDO/d frame: beta*S blocks of H (d-frame overlap) and the
-// core-core energy partials. Grid (ceil(N/128), N), block 128, blockIdx.y = u.
+// One pair u < v in the MNDO/d frame (v may be out of range): beta*S blocks of H from the
+// d-frame overlap; returns the pair's core-core energy.
+__device__ __forceinline__ double pair_d_elem(int n_atoms, const int *__restrict__ z, const double *__restrict__ xyz,
+                                              const int *__restrict__ aoff, int nao, const DeviceParams &P,
+                                              double *__restrict__ H, int u, int v) {
+  if (!(v > u && v < n_atoms)) return 0.0;
+  const ElementRec &eu = P.elements[z[u]];
+  const ElementRec &ev = P.elements[z[v]];
+  const bool keep = eu.n_orb >= ev.n_orb;
+  const int a = keep ? u : v, b = keep ? v : u;
+  const ElementRec &ea = keep ? eu : ev;
+  const ElementRec &eb = keep ? ev : eu;
+  const double dx = xyz[3 * b] - xyz[3 * a], dy = xyz[3 * b + 1] - xyz[3 * a + 1], dz = xyz[3 * b + 2] - xyz[3 * a + 2];
+  const int oa = aoff[a], ob = aoff[b];
+  diat_overlap(ea, eb, dx, dy, dz, [&](int i, int j, double s) {
+    const double val = 0.5 * (beta_of(ea, i - 1) + beta_of(eb, j - 1)) * s;
+    H[(size_t)(oa + i - 1) * nao + ob + j - 1] = val;
+    H[(size_t)(ob + j - 1) * nao + oa + i - 1] = val;
+  });
+  const double ex = xyz[3 * v] - xyz[3 * u], ey = xyz[3 * v + 1] - xyz[3 * u + 1], ez = xyz[3 * v + 2] - xyz[3 * u + 2];
+  return pair_core_energy(P, eu, ev, sqrt(ex * ex + ey * ey + ez * ez));
+}
+
+// All pairs u < v in the MNDO/d frame: beta*S blocks of H and the core-core energy
+// partials. Grid (ceil(N/128), N), block 128, blockIdx.y = u.
 __global__ void k_pairs_all_d(int n_atoms, const int *__restrict__ z, const double *__restrict__ xyz,
                               const int *__restrict__ aoff, int nao, DeviceParams P, double *__restrict__ H,
                               double *__restrict__ cc_partial) {
-  const int u = blockIdx.y;
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  double ecc = 0.0;
-  if (v > u && v < n_atoms) {
-    const ElementRec &eu = P.elements[z[u]];
-    const ElementRec &ev = P.elements[z[v]];
-    const bool keep = eu.n_orb >= ev.n_orb;
-    const int a = keep ? u : v, b = keep ? v : u;
-    const ElementRec &ea = keep ? eu : ev;
-    const ElementRec &eb = keep ? ev : eu;
-    const double dx = xyz[3 * b] - xyz[3 * a], dy = xyz[3 * b + 1] - xyz[3 * a + 1], dz = xyz[3 * b + 2] - xyz[3 * a + 2];
-    const int oa = aoff[a], ob = aoff[b];
-    diat_overlap(ea, eb, dx, dy, dz, [&](int i, int j, double s) {
-      const double val = 0.5 * (beta_of(ea, i - 1) + beta_of(eb, j - 1)) * s;
-      H[(size_t)(oa + i - 1) * nao + ob + j - 1] = val;
-      H[(size_t)(ob + j - 1) * nao + oa + i - 1] = val;
-    });
-    const double ex = xyz[3 * v] - xyz[3 * u], ey = xyz[3 * v + 1] - xyz[3 * u + 1], ez = xyz[3 * v + 2] - xyz[3 * u + 2];
-    ecc = pair_core_energy(P, eu, ev, sqrt(ex * ex + ey * ey + ez * ez));
-  }
+  const double ecc = pair_d_elem(n_atoms, z, xyz, aoff, nao, P, H, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
   const double s = block_sum<128>(ecc);
   if (threadIdx.x == 0) cc_partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+
+// Batched: item = (atom u, column block) of one molecule.
+__global__ void k_b_pairs_all_d(BatchList L, const MolDesc *__restrict__ D, DeviceParams P) {
+  const int item = blockIdx.x;
+  const int m = batch_find(L, item);
+  const MolDesc &d = D[L.slot[m]];
+  const int local = item - L.prefix[m];
+  const int u = local / d.cc_nx, bx = local - u * d.cc_nx;
+  const double ecc = pair_d_elem(d.g.n_atoms, d.g.z, d.g.xyz, d.g.aoff, d.g.nao, P, d.H, u, bx * blockDim.x + threadIdx.x);
+  const double s = block_sum<128>(ecc);
+  if (threadIdx.x == 0) d.cc_partial[(size_t)u * d.cc_nx + bx] = s;
 }
 
 // One pair for the stage entry point: w (npair_a x npair_b), e1b/e2a and S (9x9 each).
@@ -1064,6 +1100,24 @@ void launch_near_integrals_d(cudaStream_t st, int n_near, const int *z, const do
     attr = true;
   }
   k_near_integrals_d<<<(n_near + kDWarps - 1) / kDWarps, 32 * kDWarps, smem, st>>>(n_near, z, xyz, np, P, w, ecore);
+  note_launch();
+}
+
+void launch_b_pairs_all_d(cudaStream_t st, const BatchList &L, const MolDesc *D, const DeviceParams &P) {
+  if (L.total <= 0) return;
+  k_b_pairs_all_d<<<L.total, 128, 0, st>>>(L, D, P);
+  note_launch();
+}
+
+void launch_b_near_integrals_d(cudaStream_t st, const BatchList &L, const MolDesc *D, const DeviceParams &P) {
+  if (L.total <= 0) return;
+  const size_t smem = sizeof(DPairShared) * kDWarps;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_b_near_integrals_d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  k_b_near_integrals_d<<<L.total, 32 * kDWarps, smem, st>>>(L, D, P);
   note_launch();
 }
 

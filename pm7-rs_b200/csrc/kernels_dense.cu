@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "batch.hpp"
 #include "kernels.hpp"
 
 namespace pm7 {
@@ -37,11 +38,9 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
 
 // sym != 0: only tiles with bm >= bn are computed; the lower triangle is written and
 // mirrored, so the output is exactly symmetric (used for P = w V^T V).
-__global__ void __launch_bounds__(128) k_gemm_tn(int M, int N, int K, double alpha, const double *__restrict__ A,
-                                                 int lda, const double *__restrict__ B, int ldb,
-                                                 double *__restrict__ C, int ldc, int sym) {
-  const int bn = blockIdx.x, bm = blockIdx.y;
-  if (sym && bm < bn) return;
+__device__ __forceinline__ void gemm_tile(int bm, int bn, int M, int N, int K, double alpha,
+                                          const double *__restrict__ A, int lda, const double *__restrict__ B, int ldb,
+                                          double *__restrict__ C, int ldc, int sym) {
   __shared__ __align__(16) double As[2][BK][BM + PADW];
   __shared__ __align__(16) double Bs[2][BK][BN + PADW];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -109,6 +108,42 @@ __global__ void __launch_bounds__(128) k_gemm_tn(int M, int N, int K, double alp
           C[(size_t)n * ldc + m] = v;
         }
       }
+}
+
+__global__ void __launch_bounds__(128) k_gemm_tn(int M, int N, int K, double alpha, const double *__restrict__ A,
+                                                 int lda, const double *__restrict__ B, int ldb,
+                                                 double *__restrict__ C, int ldc, int sym) {
+  const int bn = blockIdx.x, bm = blockIdx.y;
+  if (sym && bm < bn) return;
+  gemm_tile(bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym);
+}
+
+// Grouped over molecules: item = one 64x64 tile of one molecule's product.
+// op 0: X = F_slot P (F symmetric, so F^T P = F P), all tiles.
+// op 1: Pn = 2 V_occ^T V_occ from this iteration's eigenvectors, lower tiles mirrored.
+__global__ void __launch_bounds__(128) k_b_gemm(BatchList L, const MolDesc *__restrict__ D,
+                                                const MolCtl *__restrict__ Cc, const EigSlot *__restrict__ E, int op) {
+  const int item = blockIdx.x;
+  const int m = batch_find(L, item);
+  const int slot = L.slot[m];
+  const MolDesc &d = D[slot];
+  const int n = d.g.nao, tiles = (n + BM - 1) / BM;
+  const int local = item - L.prefix[m];
+  if (op == 0) {
+    const int bm = local / tiles, bn = local - bm * tiles;
+    gemm_tile(bm, bn, n, n, n, 1.0, hist_F(d, Cc[slot].slot), n, d.P, n, d.X, n, 0);
+  } else {
+    int bm = 0;
+    while ((bm + 1) * (bm + 2) / 2 <= local) ++bm;
+    const int bn = local - bm * (bm + 1) / 2;
+    gemm_tile(bm, bn, n, n, d.n_occ, 2.0, E[m].in, E[m].ldv, E[m].in, E[m].ldv, d.Pn, n, 1);
+  }
+}
+
+void launch_b_gemm(cudaStream_t st, const BatchList &L, const MolDesc *D, const MolCtl *C, const EigSlot *E, int op) {
+  if (L.total <= 0) return;
+  k_b_gemm<<<L.total, 128, 0, st>>>(L, D, C, E, op);
+  note_launch();
 }
 
 void launch_gemm_tn(cudaStream_t st, int M, int N, int K, double alpha, const double *A, int lda, const double *B,

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "batch.hpp"
 #include "kernels.hpp"
 #include "nddo_sp.cuh"
 
@@ -28,11 +29,9 @@ __global__ void k_atom_pop(int n_atoms, const int *__restrict__ aoff, const int 
   pop[A] = s;
 }
 
-__global__ void k_fock_far(FockGeometry g, const double *__restrict__ H, const double *__restrict__ Ps,
-                           double s_scale, double *__restrict__ F) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= g.nao || j >= g.nao) return;
+__device__ __forceinline__ void fock_far_elem(const FockGeometry &g, const double *__restrict__ H,
+                                              const double *__restrict__ Ps, double s_scale, double *__restrict__ F,
+                                              int i, int j) {
   const int A = g.ao_atom[i], B = g.ao_atom[j];
   if (A == B || g.near_mask[(size_t)A * g.n_atoms + B]) return;
   const double dx = g.xyz[3 * B] - g.xyz[3 * A], dy = g.xyz[3 * B + 1] - g.xyz[3 * A + 1],
@@ -42,11 +41,18 @@ __global__ void k_fock_far(FockGeometry g, const double *__restrict__ H, const d
   F[ij] = H[ij] - s_scale * Ps[ij] * v;
 }
 
-__global__ void k_fock_near(FockGeometry g, DeviceParams P, const double *__restrict__ H,
-                            const double *__restrict__ Pt, const double *__restrict__ Ps, double s_scale,
-                            double *__restrict__ F, double *__restrict__ jbuf) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= g.n_near) return;
+__global__ void k_fock_far(FockGeometry g, const double *__restrict__ H, const double *__restrict__ Ps,
+                           double s_scale, double *__restrict__ F) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.nao || j >= g.nao) return;
+  fock_far_elem(g, H, Ps, s_scale, F, i, j);
+}
+
+__device__ __forceinline__ void fock_near_pair(const FockGeometry &g, const DeviceParams &P,
+                                               const double *__restrict__ H, const double *__restrict__ Pt,
+                                               const double *__restrict__ Ps, double s_scale,
+                                               double *__restrict__ F, double *__restrict__ jbuf, int p) {
   const NearPair q = g.np[p];
   const int nu_ = P.elements[g.z[q.u]].n_orb, nv = P.elements[g.z[q.v]].n_orb;
   const int ou = g.aoff[q.u], ov = g.aoff[q.v], nao = g.nao;
@@ -88,6 +94,14 @@ __global__ void k_fock_near(FockGeometry g, DeviceParams P, const double *__rest
   (void)npu;
 }
 
+__global__ void k_fock_near(FockGeometry g, DeviceParams P, const double *__restrict__ H,
+                            const double *__restrict__ Pt, const double *__restrict__ Ps, double s_scale,
+                            double *__restrict__ F, double *__restrict__ jbuf) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= g.n_near) return;
+  fock_near_pair(g, P, H, Pt, Ps, s_scale, F, jbuf, p);
+}
+
 // One-centre two-electron integral (a b | c d) of an sp atom (fock.rs:69-107).
 __device__ __forceinline__ double oc_sp(int a, int b, int c, int d, const ElementRec &e) {
   if (a == b && c == d) {
@@ -105,14 +119,11 @@ __device__ __forceinline__ double oc_sp(int a, int b, int c, int d, const Elemen
 // block reduction), the near Coulomb contributions summed in partner order (threads
 // over packed elements), then the one-centre terms (threads over block elements).
 constexpr int ATOM_THREADS = 128;
-__global__ void __launch_bounds__(ATOM_THREADS) k_fock_atom(FockGeometry g, DeviceParams P,
-                                                            const double *__restrict__ H,
-                                                            const double *__restrict__ Pt,
-                                                            const double *__restrict__ Ps, double s_scale,
-                                                            const double *__restrict__ pop,
-                                                            const double *__restrict__ jbuf,
-                                                            double *__restrict__ F) {
-  const int A = blockIdx.x;
+__device__ __forceinline__ void fock_atom_block(const FockGeometry &g, const DeviceParams &P,
+                                                const double *__restrict__ H, const double *__restrict__ Pt,
+                                                const double *__restrict__ Ps, double s_scale,
+                                                const double *__restrict__ pop, const double *__restrict__ jbuf,
+                                                double *__restrict__ F, int A) {
   const ElementRec &e = P.elements[g.z[A]];
   const int no = e.n_orb, off = g.aoff[A], nao = g.nao;
   if (no == 0) return;
@@ -160,6 +171,82 @@ __global__ void __launch_bounds__(ATOM_THREADS) k_fock_atom(FockGeometry g, Devi
     const size_t ij = (size_t)(off + mu) * nao + off + nu;
     F[ij] = H[ij] + v;
   }
+}
+
+__global__ void __launch_bounds__(ATOM_THREADS) k_fock_atom(FockGeometry g, DeviceParams P,
+                                                            const double *__restrict__ H,
+                                                            const double *__restrict__ Pt,
+                                                            const double *__restrict__ Ps, double s_scale,
+                                                            const double *__restrict__ pop,
+                                                            const double *__restrict__ jbuf,
+                                                            double *__restrict__ F) {
+  fock_atom_block(g, P, H, Pt, Ps, s_scale, pop, jbuf, F, blockIdx.x);
+}
+
+// ---- batched Fock (RHF: P_spin = P/2) ----------------------------------------------
+
+__device__ __forceinline__ double *fock_target(const MolDesc &d, const MolCtl &c, int final_pass) {
+  return final_pass ? d.X : hist_F(d, c.slot);
+}
+
+// Per molecule: atom populations of P.
+__global__ void k_b_atom_pop(BatchList L, const MolDesc *__restrict__ D, DeviceParams P) {
+  const MolDesc &d = D[L.slot[blockIdx.x]];
+  for (int A = threadIdx.x; A < d.g.n_atoms; A += blockDim.x) {
+    const int off = d.g.aoff[A], no = P.elements[d.g.z[A]].n_orb;
+    double s = 0.0;
+    for (int k = 0; k < no; ++k) s += d.P[(size_t)(off + k) * d.g.nao + off + k];
+    d.pop[A] = s;
+  }
+}
+
+// Item = 8 rows of one molecule's matrix (warp per row, lanes over columns).
+__global__ void __launch_bounds__(256) k_b_fock_far(BatchList L, const MolDesc *__restrict__ D,
+                                                    const MolCtl *__restrict__ C, int final_pass) {
+  const int item = blockIdx.x;
+  const int m = batch_find(L, item);
+  const int slot = L.slot[m];
+  const MolDesc &d = D[slot];
+  const int i = (item - L.prefix[m]) * 8 + (threadIdx.x >> 5);
+  if (i >= d.g.nao) return;
+  double *F = fock_target(d, C[slot], final_pass);
+  for (int j = threadIdx.x & 31; j < d.g.nao; j += 32) fock_far_elem(d.g, d.H, d.P, 0.5, F, i, j);
+}
+
+// Item = 128 near pairs of one molecule (thread per pair).
+__global__ void k_b_fock_near(BatchList L, const MolDesc *__restrict__ D, const MolCtl *__restrict__ C,
+                              DeviceParams P, int final_pass) {
+  const int item = blockIdx.x;
+  const int m = batch_find(L, item);
+  const int slot = L.slot[m];
+  const MolDesc &d = D[slot];
+  const int p = (item - L.prefix[m]) * 128 + threadIdx.x;
+  if (p >= d.g.n_near) return;
+  fock_near_pair(d.g, P, d.H, d.P, d.P, 0.5, fock_target(d, C[slot], final_pass), d.jbuf, p);
+}
+
+// Item = an atom of one molecule (block per atom).
+__global__ void __launch_bounds__(ATOM_THREADS) k_b_fock_atom(BatchList L, const MolDesc *__restrict__ D,
+                                                              const MolCtl *__restrict__ C, DeviceParams P,
+                                                              int final_pass) {
+  const int item = blockIdx.x;
+  const int m = batch_find(L, item);
+  const int slot = L.slot[m];
+  const MolDesc &d = D[slot];
+  fock_atom_block(d.g, P, d.H, d.P, d.P, 0.5, d.pop, d.jbuf, fock_target(d, C[slot], final_pass), item - L.prefix[m]);
+}
+
+void launch_b_fock(cudaStream_t st, const BatchList &Lmol, const BatchList &Lrows, const BatchList &Lnear,
+                   const BatchList &Latoms, const MolDesc *D, const MolCtl *C, const DeviceParams &P, int final_pass) {
+  if (Lmol.n <= 0) return;
+  k_b_atom_pop<<<Lmol.n, 128, 0, st>>>(Lmol, D, P);
+  note_launch();
+  if (Lrows.total > 0) k_b_fock_far<<<Lrows.total, 256, 0, st>>>(Lrows, D, C, final_pass);
+  note_launch();
+  if (Lnear.total > 0) k_b_fock_near<<<Lnear.total, 128, 0, st>>>(Lnear, D, C, P, final_pass);
+  note_launch();
+  if (Latoms.total > 0) k_b_fock_atom<<<Latoms.total, ATOM_THREADS, 0, st>>>(Latoms, D, C, P, final_pass);
+  note_launch();
 }
 
 void launch_atom_pop(cudaStream_t st, int n_atoms, const int *aoff, const int *z, const DeviceParams &P, int nao,

@@ -37,6 +37,15 @@ class Molecule(C.Structure):
     ]
 
 
+class EngineConfig(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32),
+        ("method", C.c_int32),
+        ("hbm_budget_mb", C.c_int64),
+        ("max_active", C.c_int32),
+    ]
+
+
 class Options(C.Structure):
     _fields_ = [
         ("method", C.c_int32),

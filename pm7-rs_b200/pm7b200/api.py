@@ -21,7 +21,8 @@ _lib = None
 EXPORTED = [
     "pm7_params_load", "pm7_options_default", "pm7_run", "pm7_result_free", "pm7_last_error_message",
     "pm7_device_count", "pm7_stage_core_hamiltonian", "pm7_stage_fock", "pm7_stage_pair", "pm7_stage_core_core",
-    "pm7_stage_corrections",
+    "pm7_stage_corrections", "pm7_run_batch", "pm7_engine_config_default", "pm7_engine_create", "pm7_engine_submit",
+    "pm7_engine_poll", "pm7_engine_destroy",
 ]
 
 
@@ -53,6 +54,15 @@ def lib():
     L.pm7_stage_core_core.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, abi.DP]
     L.pm7_stage_corrections.argtypes = [C.POINTER(abi.Molecule), C.c_int32, C.c_int32, abi.DP]
     L.pm7_abi_sizes.argtypes = [C.POINTER(C.c_int64)]
+    L.pm7_run_batch.argtypes = [C.c_int32, C.POINTER(abi.Molecule), C.c_void_p, C.POINTER(abi.Options),
+                                C.POINTER(abi.Result), C.POINTER(C.c_int32)]
+    L.pm7_engine_config_default.argtypes = [C.POINTER(abi.EngineConfig)]
+    L.pm7_engine_create.argtypes = [C.POINTER(abi.EngineConfig), C.POINTER(C.c_void_p)]
+    L.pm7_engine_submit.argtypes = [C.c_void_p, C.POINTER(abi.Molecule), C.POINTER(abi.Options),
+                                    C.POINTER(C.c_uint64)]
+    L.pm7_engine_poll.argtypes = [C.c_void_p, C.c_uint64, C.c_int32, C.POINTER(C.c_int32), C.POINTER(abi.Result),
+                                  C.POINTER(C.c_double)]
+    L.pm7_engine_destroy.argtypes = [C.c_void_p]
     _lib = L
     return L
 
@@ -206,3 +216,113 @@ def profile_read():
         _check(L.pm7_profile_entry(i, C.byref(name), C.byref(ms), C.byref(calls)))
         out[name.value.decode()] = (ms.value, calls.value)
     return out
+
+
+def _options_with_arrays(options, keep):
+    options = dict(options)
+    for k in ("initial_density", "initial_spin_density"):
+        if options.get(k) is not None:
+            a = np.ascontiguousarray(options[k], dtype=np.float64)
+            keep.append(a)
+            options[k] = a.ctypes.data_as(abi.DP)
+    return abi.default_options(**options)
+
+
+def run_batch(molecules, options=None, **common):
+    """Solve many molecules in one batched device run (`pm7_run_batch`).
+
+    `molecules` is a list of (z, xyz_bohr); `options` an optional list of per-molecule
+    option dicts merged over `common`. Returns one entry per molecule: the result dict
+    of `run_pm7`, or the `Pm7Error` that `run_pm7` would have raised for it.
+    """
+    n = len(molecules)
+    mols = [_Mol(z, x) for z, x in molecules]
+    keep = []
+    opts = (abi.Options * max(n, 1))()
+    for i in range(n):
+        o = dict(common)
+        if options is not None:
+            o.update(options[i])
+        opts[i] = _options_with_arrays(o, keep)
+    ms = (abi.Molecule * max(n, 1))(*[m.s for m in mols])
+    res = (abi.Result * max(n, 1))()
+    st = (C.c_int32 * max(n, 1))()
+    h = params(opts[0].method if n else 0)
+    code = lib().pm7_run_batch(n, ms, h, opts, res, st)
+    if code != 0:
+        raise Pm7Error(code, lib().pm7_last_error_message().decode())
+    out = []
+    for i in range(n):
+        if st[i] == 0:
+            out.append(result_to_dict(res[i]))
+        else:
+            out.append(Pm7Error(st[i], "batched solve failed"))
+        lib().pm7_result_free(C.byref(res[i]))
+    return out
+
+
+class Engine:
+    """The serving engine (`pm7_engine_*`): submit requests as they arrive, poll results.
+
+    Requests are admitted by their HBM footprint and advanced together one SCF iteration
+    per step on the device; each finished request reports its submit-to-finish latency.
+    """
+
+    def __init__(self, method=0, device=0, hbm_budget_mb=-1, max_active=0):
+        if isinstance(method, str):
+            method = abi.METHODS[method]
+        cfg = abi.EngineConfig()
+        lib().pm7_engine_config_default(C.byref(cfg))
+        cfg.device, cfg.method, cfg.hbm_budget_mb, cfg.max_active = device, method, hbm_budget_mb, max_active
+        self._h = C.c_void_p()
+        _check(lib().pm7_engine_create(C.byref(cfg), C.byref(self._h)))
+        self.method = method
+        self._keep = {}
+
+    def submit(self, z, xyz_bohr, **options):
+        m = _Mol(z, xyz_bohr)
+        keep = [m]
+        options.setdefault("method", self.method)
+        o = _options_with_arrays(options, keep)
+        t = C.c_uint64()
+        _check(lib().pm7_engine_submit(self._h, C.byref(m.s), C.byref(o), C.byref(t)))
+        self._keep[t.value] = keep
+        return t.value
+
+    def poll(self, ticket, wait=False):
+        """(done, result): result is the run_pm7 dict plus "latency_ms", or a Pm7Error."""
+        done = C.c_int32()
+        r = abi.Result()
+        lat = C.c_double()
+        code = lib().pm7_engine_poll(self._h, ticket, int(bool(wait)), C.byref(done), C.byref(r), C.byref(lat))
+        if not done.value:
+            if code != 0:
+                raise Pm7Error(code, lib().pm7_last_error_message().decode())
+            return False, None
+        self._keep.pop(ticket, None)
+        if code != 0:
+            lib().pm7_result_free(C.byref(r))
+            return True, Pm7Error(code, lib().pm7_last_error_message().decode())
+        try:
+            d = result_to_dict(r)
+        finally:
+            lib().pm7_result_free(C.byref(r))
+        d["latency_ms"] = lat.value
+        return True, d
+
+    def close(self):
+        if self._h:
+            lib().pm7_engine_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,133 @@
+"""The batched and served device SCF against the single-molecule path and the oracle.
+
+`pm7_run_batch` and the `pm7_engine_*` serving loop advance many closed-shell RHF
+molecules together (one launch per SCF phase over all of them, per-molecule DIIS and
+convergence control on the device). Each molecule's result must be the one `run_pm7`
+gives for it: 1e-5 kcal/mol in the heat of formation against the oracle, and the same
+result alone and in a mixed batch.
+"""
+import numpy as np
+import pytest
+
+from oracle import harness
+from pm7b200 import api
+from pm7b200 import geometry as G
+
+pytestmark = pytest.mark.gpu
+
+DHF_TOL = 1.0e-5
+Q_TOL = 1.0e-6
+
+
+def _closed_shell_golden(golden, limit=None):
+    out = []
+    for name, case in sorted(golden.items()):
+        if case["multiplicity"] != 1:
+            continue
+        z, x = harness.parse_lines(case["atoms"])
+        out.append((name, z, x, float(case["charge"])))
+    return out[:limit] if limit else out
+
+
+def _mixed_set(golden):
+    mols = [(n, z, x, q) for n, z, x, q in _closed_shell_golden(golden)]
+    for k in (3, 9, 17):
+        z, x = G.water_cluster(k, seed=k)
+        mols.append((f"water{k}", z, x, 0.0))
+    for n in (1, 5, 12, 23):
+        z, x = G.alkane(n, seed=n)
+        mols.append((f"alkane{n}", z, x, 0.0))
+    return mols
+
+
+def test_batch_matches_oracle_and_single_path(golden):
+    mols = _mixed_set(golden)
+    res = api.run_batch([(z, x) for _, z, x, _ in mols], options=[{"charge": q} for *_, q in mols])
+    bad = []
+    for (name, z, x, q), r in zip(mols, res):
+        if isinstance(r, Exception):
+            bad.append(f"{name}: {r}")
+            continue
+        o = harness.run(z, x, charge=q)
+        if abs(r["heat_of_formation_kcal"] - o["heat_of_formation_kcal"]) > DHF_TOL:
+            bad.append(f"{name}: dHf {r['heat_of_formation_kcal']} vs oracle {o['heat_of_formation_kcal']}")
+        if np.max(np.abs(r["charges"] - o["charges"])) > Q_TOL:
+            bad.append(f"{name}: charges")
+        if abs(r["homo_ev"] - o["homo_ev"]) > 1e-5:
+            bad.append(f"{name}: homo {r['homo_ev']} vs {o['homo_ev']}")
+        np.testing.assert_allclose(r["dipole_debye"], o["dipole_debye"], rtol=0, atol=1e-5)
+    assert not bad, "\n".join(bad)
+    # the golden values themselves
+    for (name, z, x, q), r in zip(mols, res):
+        if name in golden:
+            assert abs(r["heat_of_formation_kcal"] - golden[name]["pm7_rs"]["heat_of_formation_kcal"]) < DHF_TOL, name
+
+
+def test_batch_statuses_mirror_run_pm7(golden):
+    z_ok, x_ok = G.decane(1)
+    z_rad, x_rad = harness.parse_lines(golden["methyl_radical"]["atoms"])
+    mols = [(z_ok, x_ok), (np.array([1, 1], np.uint8), np.zeros((2, 3))), (z_rad, x_rad), (z_ok, x_ok)]
+    opts = [{}, {}, {"multiplicity": 2}, {"max_scf": 2}]
+    res = api.run_batch(mols, options=opts)
+    assert not isinstance(res[0], Exception)
+    assert isinstance(res[1], api.Pm7Error) and res[1].code == 1          # coincident atoms
+    assert not isinstance(res[2], Exception) and res[2]["unrestricted"] == 1  # open shell: pm7_run path
+    o = harness.run(z_rad, x_rad, multiplicity=2)
+    assert abs(res[2]["heat_of_formation_kcal"] - o["heat_of_formation_kcal"]) < DHF_TOL
+    assert isinstance(res[3], api.Pm7Error) and res[3].code == 6          # not converged in 2 cycles
+    single = api.run_pm7(z_ok, x_ok)
+    assert abs(res[0]["heat_of_formation_kcal"] - single["heat_of_formation_kcal"]) < 1e-7
+
+
+def test_batch_matrices_are_consistent():
+    z, x = G.water_cluster(6, seed=4)
+    (r,) = api.run_batch([(z, x)], want_matrices=1)
+    c = r["mo_coeff"]
+    n_occ = r["n_occ"]
+    p = 2.0 * c[:, :n_occ] @ c[:, :n_occ].T
+    assert np.max(np.abs(p - r["density"])) < 1e-6
+    s = api.run_pm7(z, x, want_matrices=1)
+    assert np.max(np.abs(s["density"] - r["density"])) < 1e-6
+    np.testing.assert_allclose(r["mo_energies"], s["mo_energies"], rtol=0, atol=1e-5)
+
+
+def test_batch_options_level_shift_and_accelerators():
+    z, x = G.alkane(4, seed=3)
+    for kw in ({"accelerator": 0}, {"accelerator": 1}, {"level_shift": 0.5}):
+        (r,) = api.run_batch([(z, x)], **kw)
+        o = harness.run(z, x, **kw)
+        assert abs(r["heat_of_formation_kcal"] - o["heat_of_formation_kcal"]) < DHF_TOL, kw
+
+
+def test_engine_serves_and_alone_equals_mixed(golden):
+    target = G.water_cluster(12, seed=21)
+    others = [G.alkane(n, seed=n) for n in (2, 7, 15, 30)] + [G.water_cluster(k, seed=k) for k in (4, 20, 33)]
+    with api.Engine() as eng:
+        t = eng.submit(*target)
+        done, alone = eng.poll(t, wait=True)
+        assert done and not isinstance(alone, Exception)
+        tickets = [eng.submit(*m) for m in others[:3]]
+        t2 = eng.submit(*target)
+        tickets += [eng.submit(*m) for m in others[3:]]
+        done, mixed = eng.poll(t2, wait=True)
+        assert done
+        rest = [eng.poll(tk, wait=True)[1] for tk in tickets]
+    assert all(not isinstance(r, Exception) for r in rest)
+    assert mixed["latency_ms"] > 0
+    # the same molecule alone and among others: identical to SCF precision
+    assert abs(alone["heat_of_formation_kcal"] - mixed["heat_of_formation_kcal"]) < 1e-9
+    assert alone["iterations"] == mixed["iterations"]
+    assert np.max(np.abs(alone["charges"] - mixed["charges"])) < 1e-10
+    o = harness.run(*target)
+    assert abs(mixed["heat_of_formation_kcal"] - o["heat_of_formation_kcal"]) < DHF_TOL
+
+
+def test_engine_rejects_open_shell_and_bad_input():
+    with api.Engine() as eng:
+        t = eng.submit(np.array([6, 1, 1, 1], np.uint8),
+                       np.array([[0, 0, 0], [2.0, 0, 0], [-1.0, 1.7, 0], [-1.0, -1.7, 0]]), multiplicity=2)
+        done, r = eng.poll(t, wait=True)
+        assert done and isinstance(r, api.Pm7Error) and r.code == 4
+        t = eng.submit(np.array([1, 1], np.uint8), np.zeros((2, 3)))
+        done, r = eng.poll(t, wait=True)
+        assert done and isinstance(r, api.Pm7Error) and r.code == 1
