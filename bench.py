@@ -14,6 +14,17 @@ and post-SCF corrections, charges and dipole.
 
 One JSON line on rank 0. `--impl reference` times the CPU restatement of the reference's
 `run_pm7` (oracle/, C++ with OpenMP + OpenBLAS) on all host cores instead.
+
+Other workloads (`--workload`):
+  batch4096  the mixed batch of 4,096 molecules (half alkanes C_nH_2n+2, n ~ U{1..40}, half
+             water clusters of 2..64 H2O, 0.02 A jitter, seed 0) through `pm7_run_batch`; a
+             step is one complete batch; value = molecules solved per second of wall time
+             around the call (host inputs, uploads and results inside); beside it the plain
+             single-molecule path on a fixed sample of the same molecules.
+  stream     the served stream: molecules of log-uniform size in 3..500 atoms (substituted
+             C/S chains with Cl, and water clusters, seed 0) submitted to `pm7_engine` with
+             Poisson arrivals at 80% of the engine's measured burst capacity; reports
+             solves/s and p50/p99 submit-to-finish latency, and the plain path on a sample.
 """
 import argparse
 import json
@@ -256,9 +267,12 @@ def run_b200(args, world, rank, local):
     launches0 = api.launch_count()
     dev_ms = 0.0
     results = []
+    lat = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
+        ts = time.perf_counter()
         r = api.run_pm7(z, x, **opts)
+        lat.append((time.perf_counter() - ts) * 1e3)
         dev_ms += r["device_ms"]
         results.append(r)
     wall = time.perf_counter() - t0
@@ -322,6 +336,8 @@ def run_b200(args, world, rank, local):
                    "l2": "inputs larger than L2 (H, F, P and DIIS history are 32 MB each at nao=2004)"},
         "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "device_p50": float(np.percentile([q["device_ms"] for q in results], 50))},
         "roofline": roofline,
         "roofline_fock": fock_roof,
         "stages": stages,
@@ -332,13 +348,166 @@ def run_b200(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def _percentiles(v):
+    return {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99)), "max": float(np.max(v))}
+
+
+def _plain_sample(api, mols, idx, device):
+    """The plain single-molecule path on a sample: (solves/s, results by index)."""
+    out = {}
+    t = time.perf_counter()
+    for i in idx:
+        z, x = mols[i]
+        out[i] = api.run_pm7(z, x, device=device, want_matrices=0)
+    return len(idx) / (time.perf_counter() - t), out
+
+
+def _oracle_sample(mols, idx):
+    from oracle import harness
+
+    harness.set_threads(os.cpu_count() or 1)
+    t = time.perf_counter()
+    res = {}
+    for i in idx:
+        res[i] = harness.run(*mols[i], want_matrices=0)
+    return len(idx) / (time.perf_counter() - t), res
+
+
+def run_batch_bench(args, world, rank, local):
+    """Configuration: 4,096 molecules of uneven size in one batched device run."""
+    from pm7b200 import api
+    from pm7b200 import geometry as G
+
+    mols = G.batch(4096, seed=rank)
+    opts = dict(device=local, want_matrices=0)
+    for _ in range(args.warmup):
+        api.run_batch(mols[:128], **opts)
+    barrier(world)
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = api.launch_count()
+    api.profile_enable(True)
+    walls = []
+    res = None
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        res = api.run_batch(mols, **opts)
+        walls.append(time.perf_counter() - t)
+    launches = api.launch_count() - launches0
+    prof = api.profile_read()
+    api.profile_enable(False)
+    clocks = sampler.stop()
+    barrier(world)
+    wall = allreduce_max(sum(walls), world)
+    if rank != 0:
+        return
+    failed = sum(1 for r in res if isinstance(r, Exception))
+    value = 4096 * args.steps * world / wall
+    rng = np.random.default_rng(7)
+    idx = sorted(rng.choice(len(mols), size=48, replace=False).tolist())
+    plain, plain_res = _plain_sample(api, mols, idx, local)
+    dhf = max(abs(res[i]["heat_of_formation_kcal"] - plain_res[i]["heat_of_formation_kcal"]) for i in idx)
+    cpu = None
+    if not args.no_cpu_baseline:
+        cidx = idx[:12]
+        cpu_rate, cres = _oracle_sample(mols, cidx)
+        dhf_oracle = max(abs(res[i]["heat_of_formation_kcal"] - cres[i]["heat_of_formation_kcal"]) for i in cidx)
+        cpu = {"value": cpu_rate, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"12 molecules of the batch solved one by one by the oracle (max |dHf| vs batch "
+                         f"{dhf_oracle:.2e} kcal/mol)"}
+    natoms = [len(z) for z, _ in mols]
+    line = {
+        "metric": "PM7 SCF solves/s (batched RHF single points)", "value": value, "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batch4096", "molecules": 4096, "seed": rank, "atoms_min": min(natoms),
+                   "atoms_max": max(natoms), "atoms_mean": float(np.mean(natoms)), "failed": failed,
+                   "parallelism": f"replicas{world}"},
+        "e2e": {"value": value, "unit": "solves/s", "note": "wall clock around pm7_run_batch with host buffers"},
+        "plain_path": {"value": plain, "unit": "solves/s", "sample": "48 molecules of the batch through pm7_run",
+                       "batched_over_plain": value / plain, "max_dhf_diff_kcal": dhf},
+        "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
+        "stages": {k: {"ms_total": round(v[0], 3), "calls": v[1]} for k, v in prof.items()},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_stream_bench(args, world, rank, local):
+    """Configuration: a served stream with Poisson arrivals at ~80% of capacity."""
+    from pm7b200 import api
+    from pm7b200 import geometry as G
+
+    count = args.stream_count
+    mols = G.stream(count, seed=rank)
+    with api.Engine(device=local) as eng:
+        # warm-up and capacity: a burst of the first molecules submitted at once
+        burst = mols[: min(count, 120)]
+        t = time.perf_counter()
+        tk = [eng.submit(z, x, want_matrices=0) for z, x in burst]
+        for k in tk:
+            eng.poll(k, wait=True)
+        capacity = len(burst) / (time.perf_counter() - t)
+        rate = 0.8 * capacity
+        rng = np.random.default_rng(11)
+        gaps = rng.exponential(1.0 / rate, size=count)
+        barrier(world)
+        sampler = ClockSampler(local)
+        sampler.start()
+        launches0 = api.launch_count()
+        api.profile_enable(True)
+        tickets = [None] * count
+        t0 = time.perf_counter()
+        due = t0
+        for i, (z, x) in enumerate(mols):
+            due += gaps[i]
+            now = time.perf_counter()
+            if due > now:
+                time.sleep(due - now)
+            tickets[i] = eng.submit(z, x, want_matrices=0)
+        res = [eng.poll(tk, wait=True)[1] for tk in tickets]
+        wall = time.perf_counter() - t0
+        launches = api.launch_count() - launches0
+        prof = api.profile_read()
+        api.profile_enable(False)
+        clocks = sampler.stop()
+    barrier(world)
+    wall = allreduce_max(wall, world)
+    if rank != 0:
+        return
+    ok = [r for r in res if not isinstance(r, Exception)]
+    lat = [r["latency_ms"] for r in ok]
+    value = len(ok) * world / wall
+    idx = list(range(0, count, max(1, count // 24)))[:24]
+    plain, plain_res = _plain_sample(api, mols, idx, local)
+    dhf = max(abs(res[i]["heat_of_formation_kcal"] - plain_res[i]["heat_of_formation_kcal"])
+              for i in idx if not isinstance(res[i], Exception))
+    natoms = [len(z) for z, _ in mols]
+    line = {
+        "metric": "PM7 SCF solves/s and p50/p99 latency (served stream)", "value": value, "unit": "solves/s",
+        "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": wall * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "stream", "requests": count, "seed": rank, "arrival": "Poisson",
+                   "rate_per_s": rate, "burst_capacity_per_s": capacity, "atoms_min": min(natoms),
+                   "atoms_max": max(natoms), "failed": count - len(ok), "parallelism": f"replicas{world}"},
+        "latency_ms": _percentiles(lat),
+        "e2e": {"value": value, "unit": "solves/s", "note": "submit to finish through pm7_engine, host buffers"},
+        "plain_path": {"value": plain, "unit": "solves/s", "sample": f"{len(idx)} molecules of the stream via pm7_run",
+                       "served_over_plain": value / plain, "max_dhf_diff_kcal": dhf},
+        "gpu_launches": launches, "clocks": clocks,
+        "stages": {k: {"ms_total": round(v[0], 3), "calls": v[1]} for k, v in prof.items()},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="water334", choices=["water334", "water1000", "decane"])
+    ap.add_argument("--workload", default="water334",
+                    choices=["water334", "water1000", "decane", "batch4096", "stream"])
+    ap.add_argument("--stream-count", type=int, default=600)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-peak", action="store_true")
     args = ap.parse_args()
@@ -350,6 +519,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload == "batch4096":
+            run_batch_bench(args, world, rank, local)
+        elif args.workload == "stream":
+            run_stream_bench(args, world, rank, local)
         else:
             run_b200(args, world, rank, local)
     finally:

@@ -18,6 +18,8 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -104,55 +106,67 @@ __global__ void k_b_push(int n, const int *__restrict__ slots, MolCtl *__restric
   }
 }
 
-// E_el = 1/2 sum P (H + F) (scf.rs:1237); in the SCF loop also D_slot = P.
-__global__ void __launch_bounds__(RB) k_b_energy(BatchList L, const MolDesc *__restrict__ D, MolCtl *__restrict__ C,
-                                                 int final_pass) {
-  const int slot = L.slot[blockIdx.x];
-  const MolDesc &d = D[slot];
-  MolCtl &c = C[slot];
-  const size_t nn = mol_nn(d);
+// Chunk `item` of a chunk list: list position, slot and element range [e0, e1).
+struct ChunkRef {
+  int m, slot, q;
+  size_t e0, e1;
+};
+__device__ __forceinline__ ChunkRef chunk_ref(const BatchList &L, const MolDesc *D, int item) {
+  ChunkRef r;
+  r.m = batch_find(L, item);
+  r.slot = L.slot[r.m];
+  r.q = item - L.prefix[r.m];
+  const size_t nn = mol_nn(D[r.slot]);
+  r.e0 = (size_t)r.q * kChunk;
+  r.e1 = r.e0 + kChunk < nn ? r.e0 + kChunk : nn;
+  return r;
+}
+
+// Partial of E_el = 1/2 sum P (H + F) (scf.rs:1237) into part[0]; in the SCF loop also
+// D_slot = P. Item = a chunk.
+__global__ void __launch_bounds__(RB) k_b_energy_c(BatchList L, const MolDesc *__restrict__ D,
+                                                   const MolCtl *__restrict__ C, int final_pass) {
+  const ChunkRef r = chunk_ref(L, D, blockIdx.x);
+  const MolDesc &d = D[r.slot];
+  const MolCtl &c = C[r.slot];
   const double *F = final_pass ? d.X : hist_F(d, c.slot);
   double *Dc = final_pass ? nullptr : hist_D(d, c.slot);
   double v[1] = {0.0};
-  for (size_t i = threadIdx.x; i < nn; i += RB) {
+  for (size_t i = r.e0 + threadIdx.x; i < r.e1; i += RB) {
     const double p = d.P[i];
     v[0] += p * (d.H[i] + F[i]);
     if (Dc) Dc[i] = p;
   }
   block_sum_n<1>(v);
-  if (threadIdx.x == 0) {
-    if (final_pass) c.e_final = 0.5 * v[0];
-    else c.e_elec = 0.5 * v[0];
-  }
+  if (threadIdx.x == 0) d.part[(size_t)r.q * kPart + 0] = v[0];
 }
 
-// E_slot = X - X^T with X = F P, and |E|^2 (scf.rs:1148-1156).
-__global__ void __launch_bounds__(RB) k_b_antisym(BatchList L, const MolDesc *__restrict__ D, MolCtl *__restrict__ C) {
-  const int slot = L.slot[blockIdx.x];
-  const MolDesc &d = D[slot];
-  MolCtl &c = C[slot];
+// E_slot = X - X^T with X = F P (scf.rs:1148-1156), partial |E|^2 into part[1].
+__global__ void __launch_bounds__(RB) k_b_antisym_c(BatchList L, const MolDesc *__restrict__ D,
+                                                    const MolCtl *__restrict__ C) {
+  const ChunkRef r = chunk_ref(L, D, blockIdx.x);
+  const MolDesc &d = D[r.slot];
   const int n = d.g.nao;
-  const size_t nn = (size_t)n * n;
-  double *E = hist_E(d, c.slot);
+  double *E = hist_E(d, C[r.slot].slot);
   double v[1] = {0.0};
-  for (size_t i = threadIdx.x; i < nn; i += RB) {
-    const size_t r = i / n, col = i - r * n;
-    const double e = d.X[i] - d.X[col * n + r];
+  for (size_t i = r.e0 + threadIdx.x; i < r.e1; i += RB) {
+    const size_t row = i / n, col = i - row * n;
+    const double e = d.X[i] - d.X[col * n + row];
     E[i] = e;
     v[0] += e * e;
   }
   block_sum_n<1>(v);
-  if (threadIdx.x == 0) c.err2 = v[0];
+  if (threadIdx.x == 0) d.part[(size_t)r.q * kPart + 1] = v[0];
 }
 
-// Inner products of the new history entry with the older ones (chronological):
-// ee[i] = <E_i, E_new>, ee[k] = <E_new, E_new>; df_row[j] = <D_new, F_j>, df_row[k] =
-// <D_new, F_new>; df_col[i] = <D_i, F_new>.
-__global__ void __launch_bounds__(RB) k_b_dots(BatchList L, const MolDesc *__restrict__ D, MolCtl *__restrict__ C) {
-  const int slot = L.slot[blockIdx.x];
-  const MolDesc &d = D[slot];
-  MolCtl &c = C[slot];
-  const size_t nn = mol_nn(d);
+// Partials of the inner products of the new history entry with the older ones
+// (chronological) into part[2..27]: <E_i, E_new> (i < k) and <E_new, E_new>; <D_new, F_j>
+// and <D_new, F_new>; <D_i, F_new>.
+__global__ void __launch_bounds__(RB) k_b_dots_c(BatchList L, const MolDesc *__restrict__ D,
+                                                 const MolCtl *__restrict__ C) {
+  const ChunkRef r = chunk_ref(L, D, blockIdx.x);
+  const MolDesc &d = D[r.slot];
+  const MolCtl &c = C[r.slot];
   const int k = c.n_ord;
   const double *En = hist_E(d, c.slot), *Fn = hist_F(d, c.slot), *Dn = hist_D(d, c.slot);
   const double *Eo[kHist], *Fo[kHist], *Do[kHist];
@@ -166,7 +180,7 @@ __global__ void __launch_bounds__(RB) k_b_dots(BatchList L, const MolDesc *__res
   double v[3 * kHist + 2];
 #pragma unroll
   for (int i = 0; i < 3 * kHist + 2; ++i) v[i] = 0.0;
-  for (size_t e = threadIdx.x; e < nn; e += RB) {
+  for (size_t e = r.e0 + threadIdx.x; e < r.e1; e += RB) {
     const double en = En[e], dn = Dn[e], fn = Fn[e];
 #pragma unroll
     for (int i = 0; i < kHist; ++i) {
@@ -180,14 +194,41 @@ __global__ void __launch_bounds__(RB) k_b_dots(BatchList L, const MolDesc *__res
     v[2 * kHist + 1] += dn * fn;
   }
   block_sum_n<3 * kHist + 2>(v);
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < k; ++i) {
-      c.ee[i] = v[i];
-      c.df_row[i] = v[kHist + 1 + i];
-      c.df_col[i] = v[2 * kHist + 2 + i];
-    }
-    c.ee[k] = v[kHist];
-    c.df_row[k] = v[2 * kHist + 1];
+  if (threadIdx.x == 0)
+    for (int i = 0; i < 3 * kHist + 2; ++i) d.part[(size_t)r.q * kPart + 2 + i] = v[i];
+}
+
+// Per molecule: the chunk partials summed in chunk order. what 0: E_el, |E|^2 and the
+// DIIS inner products; what 1: the final E_el.
+__global__ void k_b_reduce(int n, const int *__restrict__ slots, const MolDesc *__restrict__ D,
+                           MolCtl *__restrict__ C, int what) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  const MolDesc &d = D[slots[m]];
+  MolCtl &c = C[slots[m]];
+  const int nc = items_chunks(d.g.nao);
+  double e = 0.0;
+  for (int q = 0; q < nc; ++q) e += d.part[(size_t)q * kPart + 0];
+  if (what == 1) {
+    c.e_final = 0.5 * e;
+    return;
+  }
+  c.e_elec = 0.5 * e;
+  double err2 = 0.0;
+  for (int q = 0; q < nc; ++q) err2 += d.part[(size_t)q * kPart + 1];
+  c.err2 = err2;
+  const int k = c.n_ord;
+  for (int t = 0; t < 3 * kHist + 2; ++t) {
+    const bool used = t < k || t == kHist || (t > kHist && t < kHist + 1 + k) || t == 2 * kHist + 1 ||
+                      (t >= 2 * kHist + 2 && t < 2 * kHist + 2 + k);
+    if (!used) continue;
+    double s = 0.0;
+    for (int q = 0; q < nc; ++q) s += d.part[(size_t)q * kPart + 2 + t];
+    if (t < kHist) c.ee[t] = s;
+    else if (t == kHist) c.ee[k] = s;
+    else if (t < 2 * kHist + 1) c.df_row[t - kHist - 1] = s;
+    else if (t == 2 * kHist + 1) c.df_row[k] = s;
+    else c.df_col[t - 2 * kHist - 2] = s;
   }
 }
 
@@ -362,8 +403,23 @@ __global__ void k_b_control(int n, const int *__restrict__ slots, MolCtl *__rest
   }
 }
 
-// Extrapolated Fock sum_i c_i F_i + shift (I - P/2) (src = 0), or the final Fock X
-// (src = 1), written into the molecule's padded bucket matrix.
+// Element (r, col) of this iteration's extrapolated Fock sum_i c_i F_i + shift (I - P/2)
+// (the combine of scf.rs:1169-1176 with the level shift of :1537-1580).
+__device__ __forceinline__ double fuse_elem(const MolDesc &d, const MolCtl &c, const double *const *Fs, int r,
+                                            int col) {
+  const size_t ij = (size_t)r * d.g.nao + col;
+  double v = 0.0;
+  for (int i = 0; i < c.ncoef; ++i) v += c.coef[i] * Fs[i][ij];
+  if (c.shift > 0.0) {
+    const double q = d.P[ij] * 0.5;
+    v += c.shift * ((r == col) ? 1.0 - q : -q);
+  }
+  return v;
+}
+
+// The molecule's padded bucket matrix from: the extrapolated Fock (src 0), the final
+// Fock in X (src 1), or, for reporting orbitals, the final Fock when a level shift was
+// active and the last extrapolated Fock otherwise (src 2, scf.rs:1299-1305).
 __global__ void __launch_bounds__(RB) k_b_to_bucket(BatchList L, const MolDesc *__restrict__ D,
                                                     const MolCtl *__restrict__ C, const EigSlot *__restrict__ E,
                                                     int src) {
@@ -372,6 +428,7 @@ __global__ void __launch_bounds__(RB) k_b_to_bucket(BatchList L, const MolDesc *
   const MolDesc &d = D[slot];
   const MolCtl &c = C[slot];
   const int n = d.g.nao, np = E[m].ldv;
+  if (src == 2) src = c.shift > 0.0 ? 1 : 0;
   double *out = E[m].in;
   const double *Fs[kHist];
   for (int i = 0; i < kHist; ++i) Fs[i] = hist_F(d, i < c.ncoef ? c.csrc[i] : 0);
@@ -379,22 +436,156 @@ __global__ void __launch_bounds__(RB) k_b_to_bucket(BatchList L, const MolDesc *
   for (size_t e = threadIdx.x; e < len; e += RB) {
     const int r = (int)(e / np), col = (int)(e - (size_t)r * np);
     double v;
-    if (r < n && col < n) {
-      const size_t ij = (size_t)r * n + col;
-      if (src == 1) {
-        v = d.X[ij];
-      } else {
-        v = 0.0;
-        for (int i = 0; i < c.ncoef; ++i) v += c.coef[i] * Fs[i][ij];
-        if (c.shift > 0.0) {
-          const double q = d.P[ij] * 0.5;
-          v += c.shift * ((r == col) ? 1.0 - q : -q);
-        }
-      }
-    } else {
-      v = r == col ? kPad : 0.0;
-    }
+    if (r < n && col < n) v = src == 1 ? d.X[(size_t)r * n + col] : fuse_elem(d, c, Fs, r, col);
+    else v = r == col ? kPad : 0.0;
     out[e] = v;
+  }
+}
+
+// SP2 start, item = 8 rows: X = the extrapolated Fock, and the rows' Gershgorin bounds
+// (min of F_ii - sum_j |F_ij|, max of F_ii + sum_j |F_ij|) into part[0..1].
+__global__ void __launch_bounds__(RB) k_b_sp2_fuse(BatchList L, const MolDesc *__restrict__ D,
+                                                   const MolCtl *__restrict__ C) {
+  const int item = blockIdx.x;
+  const int m = batch_find(L, item);
+  const int slot = L.slot[m];
+  const MolDesc &d = D[slot];
+  const MolCtl &c = C[slot];
+  const int n = d.g.nao, q = item - L.prefix[m];
+  const double *Fs[kHist];
+  for (int i = 0; i < kHist; ++i) Fs[i] = hist_F(d, i < c.ncoef ? c.csrc[i] : 0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = q * 8 + warp;
+  double lo = 1.0e300, hi = -1.0e300;
+  if (r < n) {
+    double off = 0.0, diag = 0.0;
+    for (int j = lane; j < n; j += 32) {
+      const double v = fuse_elem(d, c, Fs, r, j);
+      d.X[(size_t)r * n + j] = v;
+      if (j == r) diag = v;
+      else off += fabs(v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_down_sync(0xffffffffu, off, o);
+      diag += __shfl_down_sync(0xffffffffu, diag, o);
+    }
+    lo = diag - off;
+    hi = diag + off;
+  }
+  __shared__ double slo[RB / 32], shi[RB / 32];
+  if (lane == 0) {
+    slo[warp] = lo;
+    shi[warp] = hi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 1.0e300, b = -1.0e300;
+    for (int w = 0; w < RB / 32; ++w) {
+      a = fmin(a, slo[w]);
+      b = fmax(b, shi[w]);
+    }
+    d.part[(size_t)q * kPart + 0] = a;
+    d.part[(size_t)q * kPart + 1] = b;
+  }
+}
+
+// Per molecule: the spectrum interval from the row partials, widened so that no level
+// starts on 0 or 1 (fixed points of both SP2 maps); the purification state is reset.
+__global__ void k_b_sp2_bounds(int n, const int *__restrict__ slots, const MolDesc *__restrict__ D,
+                               MolCtl *__restrict__ C) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  const MolDesc &d = D[slots[m]];
+  MolCtl &c = C[slots[m]];
+  double a = 1.0e300, b = -1.0e300;
+  const int rows = (d.g.nao + 7) / 8;
+  for (int q = 0; q < rows; ++q) {
+    a = fmin(a, d.part[(size_t)q * kPart + 0]);
+    b = fmax(b, d.part[(size_t)q * kPart + 1]);
+  }
+  const double pad = 1.0e-3 * (b - a) + 1.0e-6;
+  c.sp2_emin = a - pad;
+  c.sp2_emax = b + pad;
+  c.sp2_state = 0;
+  c.sp2_steps = 0;
+  c.sp2_apply = 0;
+}
+
+// X <- (emax I - X) / (emax - emin): spectrum in [0, 1], occupied levels near 1. Item = a chunk.
+__global__ void __launch_bounds__(RB) k_b_sp2_x0(BatchList L, const MolDesc *__restrict__ D,
+                                                 const MolCtl *__restrict__ C) {
+  const ChunkRef r = chunk_ref(L, D, blockIdx.x);
+  const MolDesc &d = D[r.slot];
+  const MolCtl &c = C[r.slot];
+  const int n = d.g.nao;
+  const double emax = c.sp2_emax, inv = 1.0 / (c.sp2_emax - c.sp2_emin);
+  for (size_t e = r.e0 + threadIdx.x; e < r.e1; e += RB) {
+    const size_t i = e / n, j = e - i * n;
+    d.X[e] = ((i == j ? emax : 0.0) - d.X[e]) * inv;
+  }
+}
+
+// One SP2 decision after Pn = X X (block per molecule): the trace rule picks X <- X^2 or
+// 2X - X^2 (whichever moves tr X toward n_occ); the purification stops at idempotency
+// (tr X - tr X^2 at the rounding floor) with tr X = n_occ, or gives up (non-finite, 100
+// steps, or an idempotent X of the wrong trace) and leaves the molecule to the
+// eigensolver. flags[m]: 0 running, 1 done, 2 failed.
+__global__ void __launch_bounds__(RB) k_b_sp2_decide(BatchList L, const MolDesc *__restrict__ D,
+                                                     MolCtl *__restrict__ C, unsigned char *__restrict__ flags) {
+  const int m = blockIdx.x;
+  const int slot = L.slot[m];
+  const MolDesc &d = D[slot];
+  MolCtl &c = C[slot];
+  if (c.sp2_state != 0) {
+    if (threadIdx.x == 0) c.sp2_apply = 0;
+    return;
+  }
+  const int n = d.g.nao;
+  double v[2] = {0.0, 0.0};
+  for (int i = threadIdx.x; i < n; i += RB) {
+    v[0] += d.X[(size_t)i * n + i];
+    v[1] += d.Pn[(size_t)i * n + i];
+  }
+  block_sum_n<2>(v);
+  if (threadIdx.x == 0) {
+    const double a = v[0], b = v[1], nocc = (double)d.n_occ;
+    c.sp2_square = fabs(b - nocc) < fabs(2.0 * a - b - nocc) ? 1 : 0;
+    const double e = a - b;
+    const int k = c.sp2_steps;  // errors recorded before this one
+    int state = 0;
+    if (!isfinite(e)) {
+      state = 2;
+    } else if (fabs(e) <= 1.0e-13 * fmax(1.0, nocc)) {
+      state = 1;
+    } else if (k >= 2 && fabs(e) < 1.0e-6 && fabs(e) >= fabs(c.sp2_err[(k + 1) % 3])) {
+      state = 1;  // at the rounding floor: no further progress
+    } else if (k + 1 >= 100) {
+      state = 2;
+    }
+    if (state == 1 && fabs(a - nocc) > 1.0e-3) state = 2;
+    c.sp2_err[k % 3] = e;
+    c.sp2_steps = k + 1;
+    c.sp2_state = state;
+    c.sp2_apply = 1;
+    flags[m] = (unsigned char)state;
+  }
+}
+
+// X <- X^2 or 2X - X^2 for the molecules decided this step; Pn = 2 X for those that
+// converged. Item = a chunk.
+__global__ void __launch_bounds__(RB) k_b_sp2_apply(BatchList L, const MolDesc *__restrict__ D,
+                                                    const MolCtl *__restrict__ C) {
+  const ChunkRef r = chunk_ref(L, D, blockIdx.x);
+  const MolDesc &d = D[r.slot];
+  const MolCtl &c = C[r.slot];
+  if (!c.sp2_apply) return;
+  const bool sq = c.sp2_square != 0, fin = c.sp2_state == 1;
+  for (size_t e = r.e0 + threadIdx.x; e < r.e1; e += RB) {
+    const double x2 = d.Pn[e];
+    const double x = sq ? x2 : 2.0 * d.X[e] - x2;
+    d.X[e] = x;
+    if (fin) d.Pn[e] = 2.0 * x;
   }
 }
 
@@ -437,56 +628,50 @@ __device__ void guard_update(MolCtl &c, double step, double energy) {
   }
 }
 
-// Density step, convergence test (scf.rs:1274-1287), stall guard, P <- P'; a molecule
-// that converged with no level shift keeps this iteration's orbitals.
-__global__ void __launch_bounds__(RB) k_b_converge(BatchList L, MolDesc *__restrict__ D, MolCtl *__restrict__ C,
-                                                   const EigSlot *__restrict__ E, unsigned char *__restrict__ flags) {
-  const int m = blockIdx.x;
-  const int slot = L.slot[m];
-  MolDesc &d = D[slot];
-  MolCtl &c = C[slot];
-  const int n = d.g.nao;
-  const size_t nn = (size_t)n * n;
+// Partial of sum (P' - P)^2 into part[28]. Item = a chunk.
+__global__ void __launch_bounds__(RB) k_b_sqdiff_c(BatchList L, const MolDesc *__restrict__ D) {
+  const ChunkRef r = chunk_ref(L, D, blockIdx.x);
+  const MolDesc &d = D[r.slot];
   double v[1] = {0.0};
-  for (size_t i = threadIdx.x; i < nn; i += RB) {
+  for (size_t i = r.e0 + threadIdx.x; i < r.e1; i += RB) {
     const double t = d.Pn[i] - d.P[i];
     v[0] += t * t;
   }
   block_sum_n<1>(v);
-  __shared__ int s_save;
-  if (threadIdx.x == 0) {
-    const double dp = sqrt(v[0] / (double)(nn > 0 ? nn : 1));
-    c.dp = dp;
-    const double de = fabs(c.e_elec - c.e_old);
-    double *t = d.P;
-    d.P = d.Pn;
-    d.Pn = t;
-    c.e_old = c.e_elec;
-    const bool residual_ok = c.shift == 0.0 && sqrt(c.err2) < 1.0e-7;
-    if (c.iter > 0 && de < c.e_tol && (dp < c.p_tol || residual_ok)) {
-      c.converged = 1;
-      c.done = 1;
-    } else {
-      guard_update(c, dp, c.e_elec);
-    }
-    c.iter += 1;
-    if (!c.done && c.iter >= c.max_scf) c.done = 1;
-    flags[m] = (unsigned char)c.done;
-    s_save = c.converged && c.shift == 0.0;
-  }
-  __syncthreads();
-  if (s_save) {
-    const int ld = E[m].ldv;
-    for (int i = threadIdx.x; i < n; i += RB) d.eps_out[i] = E[m].eps[i];
-    if (d.want_matrices)
-      for (size_t e = threadIdx.x; e < nn; e += RB) {
-        const size_t r = e / n, col = e - r * n;
-        d.V_out[e] = E[m].in[r * ld + col];
-      }
-  }
+  if (threadIdx.x == 0) d.part[(size_t)r.q * kPart + 28] = v[0];
 }
 
-// Orbitals of the final Fock (level-shifted molecules) from the bucket output.
+// Density step, convergence test (scf.rs:1274-1287), stall guard, P <- P' (per molecule).
+__global__ void k_b_converge(int n, const int *__restrict__ slots, MolDesc *__restrict__ D, MolCtl *__restrict__ C,
+                             unsigned char *__restrict__ flags) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  MolDesc &d = D[slots[m]];
+  MolCtl &c = C[slots[m]];
+  const size_t nn = mol_nn(d);
+  const int nc = items_chunks(d.g.nao);
+  double sq = 0.0;
+  for (int q = 0; q < nc; ++q) sq += d.part[(size_t)q * kPart + 28];
+  const double dp = sqrt(sq / (double)(nn > 0 ? nn : 1));
+  c.dp = dp;
+  const double de = fabs(c.e_elec - c.e_old);
+  double *t = d.P;
+  d.P = d.Pn;
+  d.Pn = t;
+  c.e_old = c.e_elec;
+  const bool residual_ok = c.shift == 0.0 && sqrt(c.err2) < 1.0e-7;
+  if (c.iter > 0 && de < c.e_tol && (dp < c.p_tol || residual_ok)) {
+    c.converged = 1;
+    c.done = 1;
+  } else {
+    guard_update(c, dp, c.e_elec);
+  }
+  c.iter += 1;
+  if (!c.done && c.iter >= c.max_scf) c.done = 1;
+  flags[m] = (unsigned char)c.done;
+}
+
+// Reported orbitals (energies, and vectors when asked) from the bucket output.
 __global__ void __launch_bounds__(RB) k_b_save_orbitals(BatchList L, const MolDesc *__restrict__ D,
                                                         const EigSlot *__restrict__ E) {
   const int m = blockIdx.x;
@@ -519,6 +704,30 @@ __global__ void k_b_atom_out(BatchList L, const MolDesc *__restrict__ D, DeviceP
       for (int k = 0; k < 11; ++k) o[4 + k] = pm(ij[k][0], ij[k][1]);
     }
   }
+}
+
+// Packs what the host reports of each listed molecule into out + off[m]: 11 control
+// scalars, the orbital energies (nao) and the per-atom outputs (kAtomOut n).
+constexpr int kOutScalars = 11;
+__global__ void k_b_gather_out(BatchList L, const MolDesc *__restrict__ D, const MolCtl *__restrict__ C,
+                               const long long *__restrict__ off, double *__restrict__ out) {
+  const int m = blockIdx.x;
+  const int slot = L.slot[m];
+  const MolDesc &d = D[slot];
+  const MolCtl &c = C[slot];
+  double *o = out + off[m];
+  if (threadIdx.x == 0) {
+    o[0] = c.iter;
+    o[1] = c.dp;
+    o[2] = c.converged;
+    o[3] = c.e_final;
+    o[4] = c.core_core;
+    for (int k = 0; k < 5; ++k) o[5 + k] = c.corr[k];
+    o[10] = c.shift;
+  }
+  const int nao = d.g.nao, na = kAtomOut * d.g.n_atoms;
+  for (int i = threadIdx.x; i < nao; i += blockDim.x) o[kOutScalars + i] = d.eps_out[i];
+  for (int i = threadIdx.x; i < na; i += blockDim.x) o[kOutScalars + nao + i] = d.atom_out[i];
 }
 
 }  // namespace
@@ -597,6 +806,24 @@ struct BatchMol {
 
 static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
+// fn(i) for i in [0, n) on the host's cores (contiguous chunks; fn must not throw).
+template <class Fn>
+static void parallel_for(int n, Fn fn) {
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int workers = std::min(hw, std::max(1, n / 16));
+  if (workers <= 1) {
+    for (int i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int w = 0; w < workers; ++w)
+    th.emplace_back([&, w] {
+      const int a = (int)((long long)n * w / workers), b = (int)((long long)n * (w + 1) / workers);
+      for (int i = a; i < b; ++i) fn(i);
+    });
+  for (auto &t : th) t.join();
+}
+
 static int bucket_size(int nao) { return nao <= 256 ? ((nao + 15) / 16) * 16 : ((nao + 63) / 64) * 64; }
 
 // Device bytes of one molecule (the footprint admission counts), with the layout filled
@@ -626,6 +853,7 @@ static size_t mol_layout(BatchMol &b, char *base) {
   d.eps_out = (double *)take(8 * (size_t)nao);
   d.V_out = b.o.want_matrices ? (double *)take(8 * nn) : nullptr;
   d.atom_out = (double *)take(8 * (size_t)kAtomOut * n);
+  d.part = (double *)take(8 * (size_t)kPart * std::max(items_chunks(nao), items_rows8(nao)));
   d.corr_scratch = (double *)take(8 * corrections_scratch(n));
   // the uploaded tables, contiguous: xyz | sad | z | aoff | ao_atom | csr_start | csr | near | mask
   const size_t up0 = off;
@@ -706,6 +934,12 @@ class BatchRunner {
     SOLVER_OK(cusolverDnCreate(&solver_));
     SOLVER_OK(cusolverDnSetStream(solver_, st_));
     SOLVER_OK(cusolverDnCreateParams(&sparams_));
+    // density of each SCF iteration: SP2 purification from sp2_min_nao_ basis functions up,
+    // the eigensolver below; PM7_BATCH_DENSITY=eig|sp2 forces one of them for every molecule
+    if (const char *e = std::getenv("PM7_BATCH_DENSITY")) {
+      if (std::strcmp(e, "eig") == 0) sp2_min_nao_ = 1 << 30;
+      if (std::strcmp(e, "sp2") == 0) sp2_min_nao_ = 0;
+    }
   }
   ~BatchRunner() {
     cudaSetDevice(ctx_.device);
@@ -717,6 +951,8 @@ class BatchRunner {
     if (work_) cudaFree(work_);
     if (flags_h_) cudaFreeHost(flags_h_);
     if (flags_d_) cudaFree(flags_d_);
+    if (pin_) cudaFreeHost(pin_);
+    if (out_d_) cudaFree(out_d_);
     cusolverDnDestroyParams(sparams_);
     cusolverDnDestroy(solver_);
     cudaStreamDestroy(st_);
@@ -765,6 +1001,7 @@ class BatchRunner {
   }
 
   size_t bytes_in_use() const { return bytes_in_use_; }
+  long long sp2_fallbacks() const { return sp2_fallbacks_; }
   int active_count() const { return (int)active_.size(); }
 
   // Allocate, upload and build the integrals of the given molecules (one launch per
@@ -772,24 +1009,28 @@ class BatchRunner {
   void admit(std::vector<BatchMol *> &in) {
     if (in.empty()) return;
     CUDA_OK(cudaSetDevice(ctx_.device));
+    const int n = (int)in.size();
     for (BatchMol *b : in) {
       b->slot = take_slot();
       CUDA_OK(cudaMallocAsync((void **)&b->base, b->bytes, st_));
       mol_layout(*b, b->base);
-      std::vector<char> img = upload_image(*b);
-      size_t start, bytes;
-      upload_span(*b, start, bytes);
-      staging_.emplace_back(std::move(img));
-      CUDA_OK(cudaMemcpyAsync(b->base + start, staging_.back().data(), staging_.back().size(),
-                              cudaMemcpyHostToDevice, st_));
-      if (!b->init_density.empty())
-        CUDA_OK(cudaMemcpyAsync(b->d.Pn, b->init_density.data(), 8 * b->init_density.size(), cudaMemcpyHostToDevice,
-                                st_));
       bytes_in_use_ += b->bytes;
     }
-    // descriptors and control records
-    for (BatchMol *b : in) {
-      CUDA_OK(cudaMemcpyAsync(desc_ + b->slot, &b->d, sizeof(MolDesc), cudaMemcpyHostToDevice, st_));
+    // one pinned staging area for the wave: table images, descriptors, control records
+    std::vector<size_t> img_off(n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+      size_t start, bytes;
+      upload_span(*in[i], start, bytes);
+      img_off[i + 1] = img_off[i] + align256(bytes);
+    }
+    const size_t desc_off = img_off[n], ctl_off = desc_off + align256(sizeof(MolDesc) * n);
+    const size_t total = ctl_off + align256(sizeof(MolCtl) * n);
+    char *host = pinned_stage(total);
+    parallel_for(n, [&](int i) {
+      BatchMol *b = in[i];
+      std::vector<char> img = upload_image(*b);
+      std::memcpy(host + img_off[i], img.data(), img.size());
+      std::memcpy(host + desc_off + sizeof(MolDesc) * i, &b->d, sizeof(MolDesc));
       MolCtl c;
       std::memset(&c, 0, sizeof c);
       c.max_scf = b->o.max_scf;
@@ -799,8 +1040,20 @@ class BatchRunner {
       c.adiis_switch = b->o.adiis_switch;
       c.shift_floor = b->o.level_shift;
       c.shift = b->o.level_shift;
-      ctl_stage_.push_back(c);
-      CUDA_OK(cudaMemcpyAsync(ctl_ + b->slot, &ctl_stage_.back(), sizeof(MolCtl), cudaMemcpyHostToDevice, st_));
+      std::memcpy(host + ctl_off + sizeof(MolCtl) * i, &c, sizeof(MolCtl));
+    });
+    for (int i = 0; i < n; ++i) {
+      BatchMol *b = in[i];
+      size_t start, bytes;
+      upload_span(*b, start, bytes);
+      CUDA_OK(cudaMemcpyAsync(b->base + start, host + img_off[i], bytes, cudaMemcpyHostToDevice, st_));
+      CUDA_OK(cudaMemcpyAsync(desc_ + b->slot, host + desc_off + sizeof(MolDesc) * i, sizeof(MolDesc),
+                              cudaMemcpyHostToDevice, st_));
+      CUDA_OK(cudaMemcpyAsync(ctl_ + b->slot, host + ctl_off + sizeof(MolCtl) * i, sizeof(MolCtl),
+                              cudaMemcpyHostToDevice, st_));
+      if (!b->init_density.empty())
+        CUDA_OK(cudaMemcpyAsync(b->d.Pn, b->init_density.data(), 8 * b->init_density.size(), cudaMemcpyHostToDevice,
+                                st_));
     }
     // build phase, batched over the newcomers
     Lists A = lists(in, false);
@@ -821,8 +1074,6 @@ class BatchRunner {
     }
     CUDA_OK(cudaStreamSynchronize(st_));
     CUDA_OK(cudaGetLastError());
-    staging_.clear();
-    ctl_stage_.clear();
     for (BatchMol *b : in) active_.push_back(b);
   }
 
@@ -832,38 +1083,75 @@ class BatchRunner {
     std::vector<BatchMol *> finished;
     if (active_.empty()) return finished;
     CUDA_OK(cudaSetDevice(ctx_.device));
-    Lists A = lists(active_, true);
+    Lists A = lists(active_, false);
     const int n = A.mol.n;
+    const int nb = (n + 127) / 128;
     {
       Stage s_(st_, "batch_fock");
-      k_b_push<<<(n + 127) / 128, 128, 0, st_>>>(n, A.mol.slot, ctl_);
+      k_b_push<<<nb, 128, 0, st_>>>(n, A.mol.slot, ctl_);
       note_launch();
       launch_b_fock(st_, A.mol, A.rows, A.near, A.atoms, desc_, ctl_, *P_, 0);
-      k_b_energy<<<n, RB, 0, st_>>>(A.mol, desc_, ctl_, 0);
+      k_b_energy_c<<<A.chunks.total, RB, 0, st_>>>(A.chunks, desc_, ctl_, 0);
       note_launch();
     }
     {
       Stage s_(st_, "batch_commutator");
-      launch_b_gemm(st_, A.gfull, desc_, ctl_, A.eig, 0);
-      k_b_antisym<<<n, RB, 0, st_>>>(A.mol, desc_, ctl_);
+      launch_b_gemm(st_, A.gfull, desc_, ctl_, nullptr, 0);
+      k_b_antisym_c<<<A.chunks.total, RB, 0, st_>>>(A.chunks, desc_, ctl_);
       note_launch();
     }
     {
       Stage s_(st_, "batch_diis");
-      k_b_dots<<<n, RB, 0, st_>>>(A.mol, desc_, ctl_);
+      k_b_dots_c<<<A.chunks.total, RB, 0, st_>>>(A.chunks, desc_, ctl_);
+      k_b_reduce<<<nb, 128, 0, st_>>>(n, A.mol.slot, desc_, ctl_, 0);
       k_b_control<<<(n + 63) / 64, 64, 0, st_>>>(n, A.mol.slot, ctl_);
-      k_b_to_bucket<<<n, RB, 0, st_>>>(A.mol, desc_, ctl_, A.eig, 0);
       note_launch(3);
     }
-    {
+    // density: SP2 purification on the tensor cores for the larger molecules, the batched
+    // eigensolver for the small ones (where it is as fast) and for what SP2 leaves
+    std::vector<BatchMol *> fallback, purify;
+    for (BatchMol *b : active_) (b->L.nao >= sp2_min_nao_ ? purify : fallback).push_back(b);
+    if (!purify.empty()) {
+      Stage s_(st_, "batch_sp2");
+      Lists S = lists(purify, false, &up_sp2_);
+      const int ns = S.mol.n;
+      k_b_sp2_fuse<<<S.rows.total, RB, 0, st_>>>(S.rows, desc_, ctl_);
+      k_b_sp2_bounds<<<(ns + 127) / 128, 128, 0, st_>>>(ns, S.mol.slot, desc_, ctl_);
+      k_b_sp2_x0<<<S.chunks.total, RB, 0, st_>>>(S.chunks, desc_, ctl_);
+      note_launch(3);
+      const int chunk = 8;
+      bool running = true;
+      for (int step = 0; step < 100 && running; step += chunk) {
+        for (int k = 0; k < chunk; ++k) {
+          launch_b_gemm(st_, S.glow, desc_, ctl_, nullptr, 2);
+          k_b_sp2_decide<<<ns, RB, 0, st_>>>(S.mol, desc_, ctl_, flags_d_);
+          k_b_sp2_apply<<<S.chunks.total, RB, 0, st_>>>(S.chunks, desc_, ctl_);
+          note_launch(2);
+        }
+        CUDA_OK(cudaMemcpyAsync(flags_h_, flags_d_, ns, cudaMemcpyDeviceToHost, st_));
+        CUDA_OK(cudaStreamSynchronize(st_));
+        running = false;
+        for (int m = 0; m < ns; ++m) running = running || flags_h_[m] == 0;
+      }
+      for (int m = 0; m < ns; ++m)
+        if (flags_h_[m] != 1) {
+          fallback.push_back(purify[m]);
+          ++sp2_fallbacks_;
+        }
+    }
+    if (!fallback.empty()) {
       Stage s_(st_, "batch_eigensolve");
-      eigensolve(A);
+      Lists B = lists(fallback, true, &up_fallback_);
+      k_b_to_bucket<<<B.mol.n, RB, 0, st_>>>(B.mol, desc_, ctl_, B.eig, 0);
+      note_launch();
+      eigensolve(B);
+      launch_b_gemm(st_, B.glow, desc_, ctl_, B.eig, 1);
     }
     {
-      Stage s_(st_, "batch_density");
-      launch_b_gemm(st_, A.glow, desc_, ctl_, A.eig, 1);
-      k_b_converge<<<n, RB, 0, st_>>>(A.mol, desc_, ctl_, A.eig, flags_d_);
-      note_launch();
+      Stage s_(st_, "batch_converge");
+      k_b_sqdiff_c<<<A.chunks.total, RB, 0, st_>>>(A.chunks, desc_);
+      k_b_converge<<<nb, 128, 0, st_>>>(n, A.mol.slot, desc_, ctl_, flags_d_);
+      note_launch(2);
     }
     CUDA_OK(cudaMemcpyAsync(flags_h_, flags_d_, n, cudaMemcpyDeviceToHost, st_));
     CUDA_OK(cudaStreamSynchronize(st_));
@@ -877,12 +1165,22 @@ class BatchRunner {
 
  private:
   struct Lists {
-    BatchList mol, rows, near, atoms, gfull, glow, sp_pairs, d_pairs, sp_near, d_near, pairs;
+    BatchList mol, rows, chunks, near, atoms, gfull, glow, sp_pairs, d_pairs, sp_near, d_near, pairs;
     const EigSlot *eig = nullptr;
     std::vector<EigSlot> eig_h;
     std::map<int, std::vector<int>> buckets;  // np -> list positions
     int max_atoms = 0;
   };
+
+  // A pinned host buffer of at least `bytes` (reused; the caller syncs before reuse).
+  char *pinned_stage(size_t bytes) {
+    if (bytes > pin_cap_) {
+      if (pin_) CUDA_OK(cudaFreeHost(pin_));
+      pin_cap_ = bytes + bytes / 4 + 4096;
+      CUDA_OK(cudaMallocHost((void **)&pin_, pin_cap_));
+    }
+    return pin_;
+  }
 
   int take_slot() {
     if (free_slots_.empty()) grow(std::max(cap_ * 2, 256));
@@ -930,7 +1228,11 @@ class BatchRunner {
   }
 
   // Work lists of one launch sequence over `mols` (list position = index in mols).
-  Lists lists(const std::vector<BatchMol *> &mols, bool with_eig) {
+  // Each ListUpload backs at most one list set in flight: the host writes its pinned
+  // buffer immediately, so a second set on the same buffer before a stream sync would
+  // overwrite what queued copies have not yet read.
+  Lists lists(const std::vector<BatchMol *> &mols, bool with_eig, ListUpload *upl = nullptr) {
+    ListUpload &up_ = upl ? *upl : this->up_;
     Lists A;
     const int n = (int)mols.size();
     up_.begin();
@@ -943,6 +1245,7 @@ class BatchRunner {
     std::vector<Spec> specs = {
         {&A.mol, [](const BatchMol &) { return 1; }, all},
         {&A.rows, [](const BatchMol &b) { return items_rows8(b.L.nao); }, all},
+        {&A.chunks, [](const BatchMol &b) { return items_chunks(b.L.nao); }, all},
         {&A.near, [](const BatchMol &b) { return items_near_chunks((int)b.L.near.size()); }, all},
         {&A.atoms, [](const BatchMol &b) { return b.m.n; }, all},
         {&A.gfull, [](const BatchMol &b) { return items_gemm_full(b.L.nao); }, all},
@@ -1012,112 +1315,149 @@ class BatchRunner {
     return A;
   }
 
-  // One batched eigensolve per bucket size (eigenvalues ascending, vectors in place).
-  void eigensolve(const Lists &A) {
+  // Eigendecomposition of every bucket matrix (eigenvalues ascending; with `vectors`,
+  // eigenvector k in row k, in place): one batched call per bucket size, or one
+  // divide-and-conquer call per matrix for the large sizes.
+  void eigensolve(const Lists &A, bool vectors = true) {
+    const cusolverEigMode_t jobz = vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
     for (auto &kv : A.buckets) {
       const int np = kv.first, cnt = (int)kv.second.size();
       double *in = A.eig_h[kv.second[0]].in, *w = A.eig_h[kv.second[0]].eps;
+      if ((size_t)cnt > info_cap_) {
+        if (info_) CUDA_OK(cudaFreeAsync(info_, st_));
+        info_cap_ = cnt * 2;
+        CUDA_OK(cudaMallocAsync((void **)&info_, sizeof(int) * info_cap_, st_));
+      }
+      if (np >= 512) {
+        int lwork = 0;
+        SOLVER_OK(cusolverDnDsyevd_bufferSize(solver_, jobz, CUBLAS_FILL_MODE_LOWER, np, in, np, w, &lwork));
+        const size_t wd = sizeof(double) * (size_t)lwork;
+        if (wd > work_cap_) {
+          if (work_) CUDA_OK(cudaFreeAsync(work_, st_));
+          work_cap_ = wd + wd / 4;
+          CUDA_OK(cudaMallocAsync(&work_, work_cap_, st_));
+        }
+        for (int i = 0; i < cnt; ++i) {
+          const EigSlot &e = A.eig_h[kv.second[i]];
+          SOLVER_OK(cusolverDnDsyevd(solver_, jobz, CUBLAS_FILL_MODE_LOWER, np, e.in, np, e.eps, (double *)work_,
+                                     lwork, info_ + i));
+        }
+        continue;
+      }
       size_t wd = 0, wh = 0;
-      SOLVER_OK(cusolverDnXsyevBatched_bufferSize(solver_, sparams_, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
-                                                  np, CUDA_R_64F, in, np, CUDA_R_64F, w, CUDA_R_64F, &wd, &wh, cnt));
+      SOLVER_OK(cusolverDnXsyevBatched_bufferSize(solver_, sparams_, jobz, CUBLAS_FILL_MODE_LOWER, np, CUDA_R_64F, in,
+                                                  np, CUDA_R_64F, w, CUDA_R_64F, &wd, &wh, cnt));
       if (wd > work_cap_) {
         if (work_) CUDA_OK(cudaFreeAsync(work_, st_));
         work_cap_ = wd + wd / 4;
         CUDA_OK(cudaMallocAsync(&work_, work_cap_, st_));
       }
       if (wh > host_work_.size()) host_work_.resize(wh);
-      if ((size_t)cnt > info_cap_) {
-        if (info_) CUDA_OK(cudaFreeAsync(info_, st_));
-        info_cap_ = cnt * 2;
-        CUDA_OK(cudaMallocAsync((void **)&info_, sizeof(int) * info_cap_, st_));
-      }
-      SOLVER_OK(cusolverDnXsyevBatched(solver_, sparams_, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, np,
-                                       CUDA_R_64F, in, np, CUDA_R_64F, w, CUDA_R_64F, work_, work_cap_,
+      SOLVER_OK(cusolverDnXsyevBatched(solver_, sparams_, jobz, CUBLAS_FILL_MODE_LOWER, np, CUDA_R_64F, in, np,
+                                       CUDA_R_64F, w, CUDA_R_64F, work_, work_cap_,
                                        host_work_.empty() ? nullptr : host_work_.data(), wh, info_, cnt));
     }
   }
 
-  // Final Fock and energy, corrections, orbitals of level-shifted solves, the per-atom
-  // outputs, and the results on the host; then the molecules' device memory is freed.
+  // Final Fock and energy, corrections, reported orbitals and per-atom outputs of the
+  // finished molecules, one packed read-back, the results on the host; then the
+  // molecules' device memory is freed.
   void retire(std::vector<BatchMol *> &R) {
-    Lists A = lists(R, false);
+    Lists A = lists(R, true);
     const int n = A.mol.n;
+    bool vectors = false;
+    for (const BatchMol *b : R) vectors = vectors || b->o.want_matrices;
     {
       Stage s_(st_, "batch_finish");
       launch_b_fock(st_, A.mol, A.rows, A.near, A.atoms, desc_, ctl_, *P_, 1);
-      k_b_energy<<<n, RB, 0, st_>>>(A.mol, desc_, ctl_, 1);
-      note_launch();
+      k_b_energy_c<<<A.chunks.total, RB, 0, st_>>>(A.chunks, desc_, ctl_, 1);
+      k_b_reduce<<<(n + 127) / 128, 128, 0, st_>>>(n, A.mol.slot, desc_, ctl_, 1);
+      note_launch(2);
       launch_b_corrections(st_, A.mol, A.pairs, desc_, ctl_, method_, A.max_atoms);
       k_b_atom_out<<<n, 128, 0, st_>>>(A.mol, desc_, *P_);
       note_launch();
     }
-    std::vector<MolCtl> ctl(n);
-    for (int m = 0; m < n; ++m)
-      CUDA_OK(cudaMemcpyAsync(&ctl[m], ctl_ + R[m]->slot, sizeof(MolCtl), cudaMemcpyDeviceToHost, st_));
-    CUDA_OK(cudaStreamSynchronize(st_));
-    // level-shifted solves report the orbitals of the final Fock (scf.rs:1299-1305)
-    std::vector<BatchMol *> shifted;
-    for (int m = 0; m < n; ++m)
-      if (ctl[m].converged && ctl[m].shift > 0.0) shifted.push_back(R[m]);
-    if (!shifted.empty()) {
-      Lists S = lists(shifted, true);
-      k_b_to_bucket<<<S.mol.n, RB, 0, st_>>>(S.mol, desc_, ctl_, S.eig, 1);
-      eigensolve(S);
-      k_b_save_orbitals<<<S.mol.n, RB, 0, st_>>>(S.mol, desc_, S.eig);
+    {
+      // reported orbitals: eigenvectors of the last extrapolated Fock, or of the final
+      // Fock when a level shift was active (scf.rs:1299-1305)
+      Stage s_(st_, "batch_orbitals");
+      k_b_to_bucket<<<n, RB, 0, st_>>>(A.mol, desc_, ctl_, A.eig, 2);
+      eigensolve(A, true);
+      k_b_save_orbitals<<<n, RB, 0, st_>>>(A.mol, desc_, A.eig);
       note_launch(2);
     }
-    std::vector<std::vector<double>> atom(n), eps(n), V(n), Pd(n);
-    for (int m = 0; m < n; ++m) {
-      BatchMol &b = *R[m];
-      const size_t nao = b.L.nao, nn = nao * nao;
-      atom[m].resize((size_t)kAtomOut * b.m.n);
-      eps[m].resize(nao);
-      CUDA_OK(cudaMemcpyAsync(atom[m].data(), b.d.atom_out, 8 * atom[m].size(), cudaMemcpyDeviceToHost, st_));
-      CUDA_OK(cudaMemcpyAsync(eps[m].data(), b.d.eps_out, 8 * nao, cudaMemcpyDeviceToHost, st_));
-      if (b.o.want_matrices && ctl[m].converged) {
+    std::vector<long long> off(n + 1, 0);
+    for (int m = 0; m < n; ++m)
+      off[m + 1] = off[m] + kOutScalars + R[m]->L.nao + (long long)kAtomOut * R[m]->m.n;
+    ptr_up_.begin();
+    size_t oo;
+    void *ho = ptr_up_.add(sizeof(long long) * off.size(), oo);
+    std::memcpy(ho, off.data(), sizeof(long long) * off.size());
+    const long long *doff = (const long long *)(ptr_up_.commit(st_) + oo);
+    const size_t total = (size_t)off[n];
+    if (total > out_cap_) {
+      if (out_d_) CUDA_OK(cudaFreeAsync(out_d_, st_));
+      out_cap_ = total + total / 4;
+      CUDA_OK(cudaMallocAsync((void **)&out_d_, 8 * out_cap_, st_));
+    }
+    k_b_gather_out<<<n, 128, 0, st_>>>(A.mol, desc_, ctl_, doff, out_d_);
+    note_launch();
+    double *host = (double *)pinned_stage(8 * total);
+    CUDA_OK(cudaMemcpyAsync(host, out_d_, 8 * total, cudaMemcpyDeviceToHost, st_));
+    CUDA_OK(cudaStreamSynchronize(st_));
+    std::vector<std::vector<double>> V(n), Pd(n);
+    if (vectors) {
+      for (int m = 0; m < n; ++m) {
+        BatchMol &b = *R[m];
+        const double *o = host + off[m];
+        if (!b.o.want_matrices || o[2] == 0.0) continue;
+        const size_t nn = (size_t)b.L.nao * b.L.nao;
         V[m].resize(nn);
         Pd[m].resize(nn);
         CUDA_OK(cudaMemcpyAsync(V[m].data(), b.d.V_out, 8 * nn, cudaMemcpyDeviceToHost, st_));
-        const double *Pnow = (ctl[m].iter % 2 == 0) ? b.d.P : b.d.Pn;
+        const double *Pnow = ((int)o[0] % 2 == 0) ? b.d.P : b.d.Pn;  // P and P' swap every iteration
         CUDA_OK(cudaMemcpyAsync(Pd[m].data(), Pnow, 8 * nn, cudaMemcpyDeviceToHost, st_));
       }
+      CUDA_OK(cudaStreamSynchronize(st_));
     }
-    CUDA_OK(cudaStreamSynchronize(st_));
-    for (int m = 0; m < n; ++m) {
+    parallel_for(n, [&](int m) {
       BatchMol &b = *R[m];
-      const MolCtl &c = ctl[m];
+      const double *o = host + off[m];
+      const int nao = b.L.nao;
       ResultParts rp;
-      rp.iterations = c.iter;
-      rp.density_error = c.dp;
-      rp.converged = c.converged != 0;
-      rp.electronic_ev = c.e_final;
-      rp.core_ev = c.core_core;
-      for (int k = 0; k < 5; ++k) rp.corr[k] = c.corr[k];
+      rp.iterations = (int)o[0];
+      rp.density_error = o[1];
+      rp.converged = o[2] != 0.0;
+      rp.electronic_ev = o[3];
+      rp.core_ev = o[4];
+      for (int k = 0; k < 5; ++k) rp.corr[k] = o[5 + k];
       rp.n_occ = b.n_occ;
-      rp.eps_a = eps[m];
+      rp.eps_a.assign(o + kOutScalars, o + kOutScalars + nao);
+      const double *ao = o + kOutScalars + nao;
       std::vector<double> pops(b.m.n);
-      for (int a = 0; a < b.m.n; ++a) pops[a] = atom[m][(size_t)kAtomOut * a];
-      const std::vector<double> &ao = atom[m];
+      for (int a = 0; a < b.m.n; ++a) pops[a] = ao[(size_t)kAtomOut * a];
       try {
         fill_result(&b.result, b.m, b.L, *b.ps, b.o, rp, pops, [&](int a, int i, int j) {
           const int k = atom_out_index(i, j);
           return k < 0 ? 0.0 : ao[(size_t)kAtomOut * a + k];
         });
         if (b.o.want_matrices) {
-          const int nao = b.L.nao;
           b.result.density = host_vec(Pd[m]);
-          std::vector<double> C((size_t)nao * nao);
+          std::vector<double> Cm((size_t)nao * nao);
           for (int i = 0; i < nao; ++i)
-            for (int k = 0; k < nao; ++k) C[(size_t)i * nao + k] = V[m][(size_t)k * nao + i];
-          b.result.mo_coeff = host_vec(C);
+            for (int k = 0; k < nao; ++k) Cm[(size_t)i * nao + k] = V[m][(size_t)k * nao + i];
+          b.result.mo_coeff = host_vec(Cm);
         }
         b.status = PM7_OK;
       } catch (const Failure &f) {
         b.status = f.code;
         b.error = f.msg;
+      } catch (const std::exception &e) {
+        b.status = PM7_ERR_INVALID_INPUT;
+        b.error = e.what();
       }
-      release(b);
-    }
+    });
+    for (BatchMol *b : R) release(*b);
   }
 
   DeviceContext &ctx_;
@@ -1133,9 +1473,11 @@ class BatchRunner {
   std::vector<int> free_slots_;
   std::vector<BatchMol *> active_;
   size_t bytes_in_use_ = 0;
-  ListUpload up_, ptr_up_;
-  std::deque<std::vector<char>> staging_;
-  std::deque<MolCtl> ctl_stage_;
+  ListUpload up_, up_fallback_, up_sp2_, ptr_up_;
+  char *pin_ = nullptr;
+  size_t pin_cap_ = 0;
+  double *out_d_ = nullptr;
+  size_t out_cap_ = 0;
   double *arena_ = nullptr;
   size_t arena_cap_ = 0;
   void *work_ = nullptr;
@@ -1144,6 +1486,8 @@ class BatchRunner {
   int *info_ = nullptr;
   size_t info_cap_ = 0;
   unsigned char *flags_h_ = nullptr, *flags_d_ = nullptr;
+  int sp2_min_nao_ = 96;  // SP2 from this many basis functions up
+  long long sp2_fallbacks_ = 0;
 };
 
 // HBM budget for a batch: the caller's max_memory_mb when given, else 80% of free memory.
@@ -1161,29 +1505,39 @@ static void run_batch_impl(int n, const pm7_molecule *mols, const pm7_params *pa
   if (n < 0 || (n > 0 && (!mols || !opts || !results || !status || !params)))
     throw Failure{PM7_ERR_INVALID_INPUT, "null argument"};
   if (n == 0) return;
+  const auto t_start = std::chrono::steady_clock::now();
   const int method = *reinterpret_cast<const int *>(params);
   const int device = opts[0].device;
   BatchRunner runner(device, method);
   std::vector<std::unique_ptr<BatchMol>> items(n);
   std::vector<BatchMol *> pending;
-  for (int i = 0; i < n; ++i) {
-    std::memset(&results[i], 0, sizeof(pm7_result));
-    status[i] = PM7_OK;
+  std::vector<pm7_status> prep(n, PM7_OK);
+  // host preparation (validation, layout, pair lists) on all host cores
+  parallel_for(n, [&](int i) {
     try {
       items[i] = runner.prepare(to_molecule(&mols[i]), opts[i]);
-      if (!BatchRunner::batchable(*items[i])) {
-        status[i] = pm7_run(&mols[i], params, &opts[i], &results[i]);
-        items[i].reset();
-        continue;
-      }
-      pending.push_back(items[i].get());
     } catch (const Failure &f) {
-      status[i] = f.code;
-      items[i].reset();
+      prep[i] = f.code;
+    } catch (const std::exception &) {
+      prep[i] = PM7_ERR_INVALID_INPUT;
     }
+  });
+  for (int i = 0; i < n; ++i) {
+    std::memset(&results[i], 0, sizeof(pm7_result));
+    status[i] = prep[i];
+    if (!items[i]) continue;
+    if (!BatchRunner::batchable(*items[i])) {
+      status[i] = pm7_run(&mols[i], params, &opts[i], &results[i]);
+      items[i].reset();
+      continue;
+    }
+    pending.push_back(items[i].get());
   }
+  const auto t_prep = std::chrono::steady_clock::now();
   const size_t budget = batch_budget(opts[0].max_memory_mb);
   size_t next = 0;
+  double t_admit = 0.0, t_iter = 0.0;
+  int n_iter = 0;
   while (next < pending.size() || runner.active_count() > 0) {
     std::vector<BatchMol *> admit;
     size_t used = runner.bytes_in_use();
@@ -1191,9 +1545,19 @@ static void run_batch_impl(int n, const pm7_molecule *mols, const pm7_params *pa
       used += pending[next]->bytes;
       admit.push_back(pending[next++]);
     }
+    const auto a0 = std::chrono::steady_clock::now();
     runner.admit(admit);
+    const auto a1 = std::chrono::steady_clock::now();
     runner.iterate();
+    const auto a2 = std::chrono::steady_clock::now();
+    t_admit += std::chrono::duration<double>(a1 - a0).count();
+    t_iter += std::chrono::duration<double>(a2 - a1).count();
+    ++n_iter;
   }
+  if (std::getenv("PM7_BATCH_TRACE"))
+    std::fprintf(stderr, "batch: %d molecules, prepare %.3f s, admit %.3f s, %d iterations %.3f s, sp2 fallbacks %lld\n",
+                 n, std::chrono::duration<double>(t_prep - t_start).count(), t_admit, n_iter, t_iter,
+                 runner.sp2_fallbacks());
   for (int i = 0; i < n; ++i)
     if (items[i]) {
       results[i] = items[i]->result;

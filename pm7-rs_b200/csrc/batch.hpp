@@ -28,6 +28,7 @@ struct MolDesc {
   double *hist;              // kHist x {F, E = FP - PF, D} blocks of nao^2
   double *eps_out, *V_out;   // reported orbital energies (nao) and vectors (nao^2, optional)
   double *atom_out;          // per atom: population and the hybrid-dipole density elements
+  double *part;              // per-item partial sums of the chunked reductions (kPart each)
   double *corr_scratch;      // post-SCF corrections scratch
 };
 
@@ -50,6 +51,9 @@ struct MolCtl {
   double coef[kHist];
   // inner products of this iteration (see k_b_dots)
   double ee[kHist + 1], df_row[kHist + 1], df_col[kHist];
+  // SP2 purification of this iteration: state 0 running, 1 converged, 2 failed
+  int sp2_state, sp2_steps, sp2_fallbacks, sp2_square, sp2_apply;
+  double sp2_err[3], sp2_emin, sp2_emax;
   // results
   double core_core, e_final, corr[5];
 };
@@ -92,6 +96,14 @@ inline int items_near_chunks(int n_near) { return (n_near + 127) / 128; }
 inline int items_gemm_full(int nao) { const int t = (nao + 63) / 64; return t * t; }
 inline int items_gemm_lower(int nao) { const int t = (nao + 63) / 64; return t * (t + 1) / 2; }
 inline int items_rows8(int nao) { return (nao + 7) / 8; }
+// Matrix-element chunks of the elementwise and reduction kernels: a large molecule is
+// spread over many blocks; each chunk leaves kPart partial sums that a per-molecule pass
+// adds in chunk order.
+constexpr int kChunk = 32768;
+constexpr int kPart = 32;
+__host__ __device__ inline int items_chunks(int nao) {
+  return (int)(((size_t)nao * nao + kChunk - 1) / kChunk);
+}
 constexpr int kDPairsPerBlock = 2;
 inline int items_near_d(int n_near) { return (n_near + kDPairsPerBlock - 1) / kDPairsPerBlock; }
 
@@ -108,7 +120,8 @@ void launch_b_hcore_diag(cudaStream_t st, const BatchList &L, const MolDesc *D, 
 void launch_b_fock(cudaStream_t st, const BatchList &Lmol, const BatchList &Lrows, const BatchList &Lnear,
                    const BatchList &Latoms, const MolDesc *D, const MolCtl *C, const DeviceParams &P, int final_pass);
 
-// op 0: X = F_slot P (full tiles); op 1: Pn = 2 V_occ^T V_occ (lower tiles, mirrored).
+// op 0: X = F_slot P (full tiles); op 1: Pn = 2 V_occ^T V_occ (lower tiles, mirrored);
+// op 2: Pn = X X for molecules whose SP2 purification is still running (lower tiles).
 void launch_b_gemm(cudaStream_t st, const BatchList &L, const MolDesc *D, const MolCtl *C, const EigSlot *E, int op);
 
 // Post-SCF corrections of the listed molecules into C[slot].corr (dispersion variant per

@@ -389,6 +389,8 @@ struct Purifier {
         break;
       }
     }
+    // an idempotent X whose trace is not n_occ is a wrong projector (degenerate frontier)
+    if (ok && std::fabs(pin[0] - (double)n_occ) > 1.0e-3) ok = false;
     if (!ok) return false;
     launch_scale(st, (size_t)n * n, w, X.p, P);
     return true;

@@ -136,7 +136,8 @@ __global__ void __launch_bounds__(128) k_b_gemm(BatchList L, const MolDesc *__re
     int bm = 0;
     while ((bm + 1) * (bm + 2) / 2 <= local) ++bm;
     const int bn = local - bm * (bm + 1) / 2;
-    gemm_tile(bm, bn, n, n, d.n_occ, 2.0, E[m].in, E[m].ldv, E[m].in, E[m].ldv, d.Pn, n, 1);
+    if (op == 1) gemm_tile(bm, bn, n, n, d.n_occ, 2.0, E[m].in, E[m].ldv, E[m].in, E[m].ldv, d.Pn, n, 1);
+    else if (Cc[slot].sp2_state == 0) gemm_tile(bm, bn, n, n, n, 1.0, d.X, n, d.X, n, d.Pn, n, 1);
   }
 }
 
@@ -428,8 +429,10 @@ __global__ void k_minmax(int m, const double *__restrict__ lo, const double *__r
     a = fmin(a, lo[i]);
     b = fmax(b, hi[i]);
   }
-  bounds[0] = a;
-  bounds[1] = b;
+  // widen the interval so no level starts on 0 or 1 (fixed points of both SP2 maps)
+  const double pad = 1.0e-3 * (b - a) + 1.0e-6;
+  bounds[0] = a - pad;
+  bounds[1] = b + pad;
 }
 
 // X = (emax I - F) / (emax - emin): spectrum mapped into [0, 1], occupied levels near 1.

@@ -8,6 +8,10 @@
   quaternion), U(-0.1, 0.1) A centre jitter.
 * `batch(count, seed)` - half alkanes C_nH_2n+2 with n ~ U{1..40}, half water clusters
   of 2..64 molecules, jitter 0.02 A.
+* `substituted_chain(n, rng)` - a zig-zag chain of n heavy atoms where each interior CH2
+  becomes S with probability 0.1 (C-S 1.82 A) and each H becomes Cl with probability 0.1
+  (C-Cl 1.77 A); `stream(count, seed)` - molecules of log-uniform size in 3..500 atoms,
+  half such chains and half water clusters.
 All draws use numpy.random.default_rng(seed).
 """
 import math
@@ -137,4 +141,61 @@ def batch(count, seed=0):
         else:
             k = int(rng.integers(2, 65))
             mols.append(water_cluster(k, centre_jitter=0.02, rng=rng))
+    return mols
+
+
+def substituted_chain(n, rng, p_s=0.1, p_cl=0.1, jitter=0.02):
+    """Zig-zag C/S chain of n heavy atoms with hydrogens, some H replaced by Cl (Bohr out)."""
+    theta = math.radians(109.471)
+    sx, sz = math.sin(theta / 2.0), math.cos(theta / 2.0)
+    kinds = [6] * n
+    for i in range(1, n - 1):
+        if rng.random() < p_s and kinds[i - 1] != 16:
+            kinds[i] = 16
+    pos = [np.zeros(3)]
+    for i in range(1, n):
+        b = 1.82 if (kinds[i] == 16 or kinds[i - 1] == 16) else 1.54
+        step = np.array([sx, 0.0, sz if i % 2 == 1 else -sz]) * b
+        pos.append(pos[-1] + step)
+    atoms = [(kinds[i], pos[i]) for i in range(n)]
+    hyd = []
+    for i in range(n):
+        if kinds[i] != 6:
+            continue
+        c = pos[i]
+        if n == 1:
+            s = 1.09 / math.sqrt(3.0)
+            hyd += [(c, c + s * np.array(v, dtype=float)) for v in ((1, 1, 1), (1, -1, -1), (-1, 1, -1), (-1, -1, 1))]
+            continue
+        prev = pos[i - 1] if i > 0 else c + np.array([-sx, 0.0, -sz if i % 2 == 1 else sz])
+        nxt = pos[i + 1] if i + 1 < n else c + np.array([sx, 0.0, sz if (i + 1) % 2 == 1 else -sz])
+        hyd += [(c, h) for h in _tetra_hydrogens(c, prev, nxt, 1.09)]
+        if i == 0:
+            d = prev - c
+            hyd.append((c, c + 1.09 * d / np.linalg.norm(d)))
+        if i == n - 1:
+            d = nxt - c
+            hyd.append((c, c + 1.09 * d / np.linalg.norm(d)))
+    for c, h in hyd:
+        if rng.random() < p_cl:
+            d = (h - c) / np.linalg.norm(h - c)
+            atoms.append((17, c + 1.77 * d))
+        else:
+            atoms.append((1, h))
+    return _finish(atoms, rng, jitter)
+
+
+def stream(count, seed=0, lo=3, hi=500):
+    """Molecules of the served stream: sizes log-uniform in lo..hi atoms, alternating
+    substituted chains and water clusters."""
+    rng = np.random.default_rng(seed)
+    mols = []
+    for i in range(count):
+        target = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+        if i % 2 == 0:
+            n = max(1, int(round((target - 2.0) / 3.0)))
+            mols.append(substituted_chain(n, rng))
+        else:
+            k = max(1, int(round(target / 3.0)))
+            mols.append(water_cluster(k, centre_jitter=0.1, rng=rng))
     return mols

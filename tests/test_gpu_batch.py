@@ -131,3 +131,25 @@ def test_engine_rejects_open_shell_and_bad_input():
         t = eng.submit(np.array([1, 1], np.uint8), np.zeros((2, 3)))
         done, r = eng.poll(t, wait=True)
         assert done and isinstance(r, api.Pm7Error) and r.code == 1
+
+
+def test_batch_density_by_sp2_and_by_eigensolver_agree(monkeypatch):
+    # SP2 purification (tensor-core squarings) and the eigensolver give the same SCF
+    mols = [G.water_cluster(k, seed=k) for k in (2, 11, 40)] + [G.alkane(n, seed=n) for n in (3, 18, 40)]
+    monkeypatch.setenv("PM7_BATCH_DENSITY", "sp2")
+    sp2 = api.run_batch(mols)
+    monkeypatch.setenv("PM7_BATCH_DENSITY", "eig")
+    eig = api.run_batch(mols)
+    for a, b in zip(sp2, eig):
+        assert abs(a["heat_of_formation_kcal"] - b["heat_of_formation_kcal"]) < 1e-7
+        assert np.max(np.abs(a["charges"] - b["charges"])) < 1e-8
+        assert abs(a["homo_ev"] - b["homo_ev"]) < 1e-7
+
+
+def test_batch_takes_the_single_path_iterations(golden):
+    # the device-side DIIS of the batch follows the same trajectory as run_pm7
+    for name in ("alkane_c20", "formic_acid_dimer", "benzene"):
+        z, x = harness.parse_lines(golden[name]["atoms"])
+        (r,) = api.run_batch([(z, x)])
+        s = api.run_pm7(z, x)
+        assert abs(r["iterations"] - s["iterations"]) <= 1, (name, r["iterations"], s["iterations"])
