@@ -1319,8 +1319,11 @@ class BatchRunner {
   // eigenvector k in row k, in place): one batched call per bucket size, or one
   // divide-and-conquer call per matrix for the large sizes.
   void eigensolve(const Lists &A, bool vectors = true) {
-    const cusolverEigMode_t jobz = vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
     for (auto &kv : A.buckets) {
+      // the batched routine is faster with vectors than without at these sizes; the
+      // divide-and-conquer one saves its back-transformation when only values are needed
+      const cusolverEigMode_t jobz =
+          (vectors || kv.first < 512) ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
       const int np = kv.first, cnt = (int)kv.second.size();
       double *in = A.eig_h[kv.second[0]].in, *w = A.eig_h[kv.second[0]].eps;
       if ((size_t)cnt > info_cap_) {
@@ -1382,7 +1385,7 @@ class BatchRunner {
       // Fock when a level shift was active (scf.rs:1299-1305)
       Stage s_(st_, "batch_orbitals");
       k_b_to_bucket<<<n, RB, 0, st_>>>(A.mol, desc_, ctl_, A.eig, 2);
-      eigensolve(A, true);
+      eigensolve(A, vectors);
       k_b_save_orbitals<<<n, RB, 0, st_>>>(A.mol, desc_, A.eig);
       note_launch(2);
     }
