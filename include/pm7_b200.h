@@ -206,6 +206,11 @@ pm7_status pm7_stage_pair(const pm7_params *params, int32_t z_i, int32_t z_j, co
                           int32_t force_dpath, double *w_out, double *e1b_out, double *e2a_out,
                           double *s_out, int32_t *npair_i, int32_t *npair_j);
 
+/* The mixed-precision SP2 squaring C = X X of a symmetric n x n matrix on the tcgen05
+ * tensor cores (3xTF32 split, fp32 accumulation), as a stage for accuracy tests; no
+ * counterpart in pm7-rs (its density step diagonalises). */
+pm7_status pm7_stage_square_tf32(int32_t n, const double *x, double *c_out);
+
 /* Core-core repulsion energy in eV (`core_core_energy`, src/repulsion.rs:16-36). */
 pm7_status pm7_stage_core_core(const pm7_molecule *molecule, const pm7_params *params,
                                double *energy_ev);

@@ -360,6 +360,68 @@ struct Purifier {
     bounds.alloc(2, st);
     state.alloc(4, st);
   }
+  // fp32 iterate of the mixed-precision purification: X, its tf32 split, X^2 (ld x ld)
+  int ld = 0;
+  DevBuf<float> X32, hi32, lo32, C32;
+  DevBuf<int> err32;
+  alignas(64) unsigned char map_hi[128], map_lo[128];
+  void ensure32() {
+    if (ld) return;
+    ld = ((n + 31) / 32) * 32;
+    const size_t ll = (size_t)ld * ld;
+    for (DevBuf<float> *b : {&X32, &hi32, &lo32, &C32}) {
+      b->alloc(ll, st);
+      CUDA_OK(cudaMemsetAsync(b->p, 0, sizeof(float) * ll, st));  // the padding stays zero
+    }
+    err32.alloc(1, st);
+    CUDA_OK(cudaMemsetAsync(err32.p, 0, sizeof(int), st));
+    if (!make_square_map(hi32.p, ld, map_hi) || !make_square_map(lo32.p, ld, map_lo))
+      throw Failure{PM7_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
+  }
+  // SP2 with the squarings on the tcgen05 tensor cores (3xTF32, fp32 accumulation). The
+  // fp32 iterate reaches idempotency only to its rounding floor, so the density carries
+  // about 1e-5 relative error: the SCF uses it for its early cycles only.
+  bool project32(const double *F, int n_occ, double w, double *P) {
+    ensure32();
+    launch_gershgorin(st, n, F, scratch.p, bounds.p);
+    launch_sp2_init32(st, n, ld, F, bounds.p, X32.p, hi32.p, lo32.p);
+    std::vector<double> err;
+    bool ok = false;
+    const double scale = std::max(1, n_occ);
+    for (int it = 0; it < 100; ++it) {
+      {
+        Stage g_(st, "sp2_square_tf32");
+        launch_square_tf32x3(st, n, ld, map_hi, map_lo, C32.p, err32.p);
+      }
+      launch_sp2_trace32(st, n, ld, X32.p, C32.p, (double)n_occ, state.p);
+      launch_sp2_update32(st, n, ld, X32.p, C32.p, state.p, hi32.p, lo32.p);
+      double *s = pin;
+      CUDA_OK(cudaMemcpyAsync(s, state.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaStreamSynchronize(st));
+      const double e = s[3];
+      err.push_back(e);
+      last_iterations = it + 1;
+      const size_t k = err.size();
+      if (!std::isfinite(e)) break;
+      if (std::fabs(e) <= 1.0e-6 * scale) {
+        ok = true;
+        break;
+      }
+      if (k >= 3 && std::fabs(e) < 1.0e-2 * scale && std::fabs(e) >= std::fabs(err[k - 3])) {
+        ok = true;  // at the fp32 rounding floor
+        break;
+      }
+    }
+    if (ok && std::fabs(pin[0] - (double)n_occ) > 1.0e-2 * scale) ok = false;
+    int bad = 0;
+    CUDA_OK(cudaMemcpyAsync(&bad, err32.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    if (bad) throw Failure{PM7_ERR_CUDA, "tcgen05 squaring: a pipeline wait expired"};
+    if (!ok) return false;
+    launch_sp2_density32(st, n, ld, X32.p, w, P);
+    return true;
+  }
+
   bool project(const double *F, int n_occ, double w, double *P) {
     launch_gershgorin(st, n, F, scratch.p, bounds.p);
     launch_sp2_init(st, n, F, bounds.p, X.p);
@@ -400,6 +462,9 @@ struct Purifier {
 // Density solver for the SCF loop: SP2 for large systems (tensor-core squarings), the
 // cuSOLVER eigendecomposition for small ones or when SP2 cannot settle. The choice can
 // be forced with PM7_DENSITY_SOLVER=sp2|syevd.
+// DIIS error below which the mixed-precision SCF switches to fp64 densities.
+static constexpr double kMixedSwitch = 1.0e-3;
+
 static bool use_sp2(int n) {
   const char *env = std::getenv("PM7_DENSITY_SOLVER");
   if (env && std::strcmp(env, "syevd") == 0) return false;
@@ -427,6 +492,7 @@ struct ScfOut {
   DevBuf<double> P, Pspin, Va, Vb;  // total density, spin density, eigenvectors (rows)
   bool unrestricted = false;
   int n_occ = 0, n_occ_beta = -1;
+  int fp32_iterations = 0;
 };
 
 // SAD guess diagonal (scf.rs:1050-1114).
@@ -502,6 +568,9 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   const bool sp2 = use_sp2(n);
   Purifier pur(st, sp2 ? n : 1, reinterpret_cast<double *>(ctx.pinned + 4096));
   bool diagonalised = false;  // whether Fuse holds the eigenvectors of the last iteration
+  // Mixed precision: fp32 (tcgen05) densities while the DIIS error is large, then fp64
+  // refinement cycles; only an fp64 cycle may end the SCF.
+  bool phase32 = sp2 && o.precision == PM7_PRECISION_MIXED;
   HistoryHost hist(kmax);
   StallGuardHost guard(o.level_shift);
   const bool trace = std::getenv("PM7_SCF_TRACE") != nullptr;
@@ -580,10 +649,13 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     CUDA_OK(cudaMemcpyAsync(coef.p, pin_cw, sizeof(double) * cw.size(), cudaMemcpyHostToDevice, st));
     { Stage s_(st, "combine"); launch_combine(st, n, (int)fp.size(), ptrs.p + 48, coef.p, out.P.p, 2.0, guard.shift, Fuse.p); }
     bool purified = false;
+    if (phase32 && err_norm < kMixedSwitch) phase32 = false;
+    const bool used32 = phase32;
     if (sp2) {
       Stage s_(st, "sp2_purify");
-      purified = pur.project(Fuse.p, n_occ, 2.0, Pnew.p);
+      purified = used32 ? pur.project32(Fuse.p, n_occ, 2.0, Pnew.p) : pur.project(Fuse.p, n_occ, 2.0, Pnew.p);
     }
+    if (used32) ++out.fp32_iterations;
     diagonalised = !purified;
     if (!purified) {
       { Stage s_(st, "eigensolve"); eig.solve(Fuse.p); }
@@ -596,14 +668,14 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     std::swap(out.P.p, Pnew.p);
     e_old = e_elec;
     const bool residual_ok = guard.shift == 0.0 && err_norm < 1.0e-7;
-    if (iter > 0 && de < o.e_tol && (dp < o.p_tol || residual_ok)) {
+    if (!used32 && iter > 0 && de < o.e_tol && (dp < o.p_tol || residual_ok)) {
       out.converged = true;
       break;
     }
     guard.update(dp, e_elec);
     if (trace)
-      std::fprintf(stderr, "scf %4d E %.10f dp %.3e err %.3e shift %.2f\n", out.iterations, e_elec, dp, err_norm,
-                   guard.shift);
+      std::fprintf(stderr, "scf %4d E %.10f dp %.3e err %.3e shift %.2f%s\n", out.iterations, e_elec, dp, err_norm,
+                   guard.shift, used32 ? " fp32" : "");
   }
   // final Fock and energy at the converged density
   { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, out.P.p, out.P.p, 0.5, F.p, D.pop.p, D.jbuf.p); }
@@ -1015,6 +1087,7 @@ static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm
   R.eps_a = S.eps_a;
   R.eps_b = S.eps_b;
   R.device_ms = ms;
+  R.fp32_iterations = S.fp32_iterations;
   const int nao = L.nao;
   const size_t nn = (size_t)nao * nao;
   std::vector<double> Ph;
@@ -1213,6 +1286,41 @@ pm7_status pm7_stage_pair(const pm7_params *params, int32_t z_i, int32_t z_j, co
     std::memcpy(e1b_out, hb.data() + 2025, sizeof(double) * 81);
     std::memcpy(e2a_out, hb.data() + 2025 + 81, sizeof(double) * 81);
     std::memcpy(s_out, hb.data() + 2025 + 162, sizeof(double) * 81);
+  });
+}
+
+pm7_status pm7_stage_square_tf32(int32_t n, const double *x, double *c_out) {
+  return guarded([&] {
+    if (n < 1 || !x || !c_out) throw Failure{PM7_ERR_INVALID_INPUT, "square_tf32 needs n >= 1 and buffers"};
+    DeviceContext &ctx = context_for(0);
+    std::lock_guard<std::mutex> lock(ctx.run_mutex);
+    CUDA_OK(cudaSetDevice(ctx.device));
+    cudaStream_t st = ctx.stream;
+    const int ld = ((n + 31) / 32) * 32;
+    const size_t nn = (size_t)n * n, ll = (size_t)ld * ld;
+    DevBuf<double> X, C;
+    DevBuf<float> hi, lo, C32;
+    DevBuf<int> err;
+    upload(X, std::vector<double>(x, x + nn), st);
+    hi.alloc(ll, st);
+    lo.alloc(ll, st);
+    C32.alloc(ll, st);
+    C.alloc(nn, st);
+    err.alloc(1, st);
+    CUDA_OK(cudaMemsetAsync(err.p, 0, sizeof(int), st));
+    CUDA_OK(cudaMemsetAsync(C32.p, 0, sizeof(float) * ll, st));
+    launch_split_tf32(st, n, ld, X.p, hi.p, lo.p);
+    alignas(64) unsigned char map_hi[128], map_lo[128];
+    if (!make_square_map(hi.p, ld, map_hi) || !make_square_map(lo.p, ld, map_lo))
+      throw Failure{PM7_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
+    launch_square_tf32x3(st, n, ld, map_hi, map_lo, C32.p, err.p);
+    launch_widen(st, n, ld, C32.p, C.p);
+    int e = 0;
+    CUDA_OK(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(c_out, C.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaGetLastError());
+    if (e) throw Failure{PM7_ERR_CUDA, "tcgen05 squaring: a pipeline wait expired"};
   });
 }
 

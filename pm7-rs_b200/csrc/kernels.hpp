@@ -104,6 +104,25 @@ void launch_stage_pair(cudaStream_t st, const DeviceParams &P, int zi, int zj, c
 }
 
 namespace pm7 {
+// FP32-accuracy (3xTF32) symmetric squaring on tcgen05 (kernels_tf32.cu). Matrices are
+// ld x ld fp32, ld a multiple of 32, zero padded beyond n; the maps come from
+// make_square_map (an opaque 128-byte CUtensorMap each).
+bool make_square_map(const float *base, int ld, void *map_out);
+size_t square_tf32x3_smem();
+void launch_square_tf32x3(cudaStream_t st, int n, int ld, const void *map_hi, const void *map_lo, float *C,
+                          int *error);
+void launch_split_tf32(cudaStream_t st, int n, int ld, const double *X, float *hi, float *lo);
+void launch_widen(cudaStream_t st, int n, int ld, const float *C32, double *C);
+// The fp32 SP2 iteration: start, traces (fp64 sums), update with re-split, density.
+void launch_sp2_init32(cudaStream_t st, int n, int ld, const double *F, const double *bounds, float *X, float *hi,
+                       float *lo);
+void launch_sp2_trace32(cudaStream_t st, int n, int ld, const float *X, const float *X2, double n_occ, double *state);
+void launch_sp2_update32(cudaStream_t st, int n, int ld, float *X, const float *X2, const double *state, float *hi,
+                         float *lo);
+void launch_sp2_density32(cudaStream_t st, int n, int ld, const float *X, double w, double *P);
+}
+
+namespace pm7 {
 // SP2 purification building blocks (kernels_dense.cu).
 void launch_gershgorin(cudaStream_t st, int n, const double *F, double *scratch, double *bounds);
 void launch_sp2_init(cudaStream_t st, int n, const double *F, const double *bounds, double *X);

@@ -1,0 +1,415 @@
+// FP32-accuracy symmetric squaring C = X X on the 5th-generation tensor cores (tcgen05,
+// kind::tf32) for the mixed-precision SP2 purification.
+//
+// X is stored split as X = Xhi + Xlo with Xhi = tf32(X) and Xlo = X - Xhi (both fp32
+// arrays, row-major, leading dimension ld, zero padded to ld); the product is accumulated
+// in fp32 in tensor memory as Xhi Xhi + Xhi Xlo + Xlo Xhi (the "3xTF32" split, about fp32
+// accuracy). X is symmetric, so C = X X^T: both operands are row blocks of X, K-major.
+//
+// One CTA per 128x128 lower tile of C (the upper tiles are mirrored). Warp 0 lane 0 feeds
+// a 3-stage shared-memory ring with TMA (cp.async.bulk.tensor, 128-byte swizzle, no
+// multicast); warp 1 lane 0 issues tcgen05.mma (M=128, N=128, K=8) into a 128-column TMEM
+// accumulator and releases each stage with tcgen05.commit; all four warps read the
+// accumulator back with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = tile rows) and
+// store it. Every mbarrier wait has an iteration limit; on expiry the CTA records an error,
+// stops issuing, frees its TMEM and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "kernels.hpp"
+
+namespace pm7 {
+namespace {
+
+constexpr int TM = 128, TN = 128, TK = 32, STAGES = 3;
+constexpr int TILE_BYTES = TM * TK * 4;            // 16 KB: 128 rows x 32 fp32 (128 B per row)
+constexpr int STAGE_BYTES = 4 * TILE_BYTES;        // Ahi, Alo, Bhi, Blo
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;  // + alignment slack + barriers
+constexpr uint32_t kWaitLimit = 1u << 26;          // try_wait polls before giving up
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// Bounded wait for phase `parity` of an mbarrier; false when the limit expired or the
+// CTA aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
+  const uint32_t addr = smem_u32(bar);
+  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((it & 255) == 255 && *abort_flag) return false;
+  }
+  *abort_flag = 1;
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void *smem_dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+          smem_u32(smem_dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major operand, 128-byte swizzle, 8-row groups 1024 B
+// apart (SBO), version 1 (tcgen05), base offset 0 (stage buffers are 1024-byte aligned).
+__device__ __forceinline__ uint64_t smem_desc(const void *tile) {
+  const uint32_t addr = smem_u32(tile);
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);          // start address
+  d |= (uint64_t)1 << 16;                         // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;               // stride byte offset
+  d |= (uint64_t)1 << 46;                         // version
+  d |= (uint64_t)2 << 61;                         // SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor, kind::tf32: fp32 accumulate, TF32 A and B, both K-major, N=128, M=128.
+constexpr uint32_t kIdesc = (1u << 4)              // c_format F32
+                            | (2u << 7)            // a_format TF32
+                            | (2u << 10)           // b_format TF32
+                            | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__global__ void __launch_bounds__(128) k_square_tf32x3(const __grid_constant__ CUtensorMap map_hi,
+                                                       const __grid_constant__ CUtensorMap map_lo, int n, int ld,
+                                                       float *__restrict__ C, int *__restrict__ error) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // stage buffers on a 1024-byte boundary (128-byte swizzle atoms)
+  unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+  uint64_t *empty = full + STAGES;
+  uint64_t *done = empty + STAGES;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+  // lower tile (bm >= bn) of this CTA
+  int bm = 0;
+  while ((bm + 1) * (bm + 2) / 2 <= (int)blockIdx.x) ++bm;
+  const int bn = blockIdx.x - bm * (bm + 1) / 2;
+  const int m0 = bm * TM, n0 = bn * TN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ktiles = (ld + TK - 1) / TK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // producer: TMA ring
+    for (int kt = 0; kt < ktiles; ++kt) {
+      const int s = kt % STAGES;
+      if (kt >= STAGES && !mbar_wait(&empty[s], (uint32_t)((kt / STAGES - 1) & 1), abort_flag)) break;
+      unsigned char *st = smem + s * STAGE_BYTES;
+      mbar_expect_tx(&full[s], STAGE_BYTES);
+      const int k0 = kt * TK;
+      tma_load_2d(st + 0 * TILE_BYTES, &map_hi, &full[s], k0, m0);
+      tma_load_2d(st + 1 * TILE_BYTES, &map_lo, &full[s], k0, m0);
+      tma_load_2d(st + 2 * TILE_BYTES, &map_hi, &full[s], k0, n0);
+      tma_load_2d(st + 3 * TILE_BYTES, &map_lo, &full[s], k0, n0);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    bool ok = true;
+    for (int kt = 0; kt < ktiles && ok; ++kt) {
+      const int s = kt % STAGES;
+      if (!mbar_wait(&full[s], (uint32_t)((kt / STAGES) & 1), abort_flag)) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      unsigned char *st = smem + s * STAGE_BYTES;
+      const uint64_t ahi = smem_desc(st), alo = smem_desc(st + TILE_BYTES);
+      const uint64_t bhi = smem_desc(st + 2 * TILE_BYTES), blo = smem_desc(st + 3 * TILE_BYTES);
+#pragma unroll
+      for (int j = 0; j < TK / 8; ++j) {
+        const uint64_t off = (uint64_t)(j * 2);  // 8 fp32 = 32 bytes = 2 units of 16 bytes
+        mma_tf32(tmem, ahi + off, bhi + off, (kt > 0 || j > 0) ? 1u : 0u);
+        mma_tf32(tmem, ahi + off, blo + off, 1u);
+        mma_tf32(tmem, alo + off, bhi + off, 1u);
+      }
+      mma_commit(&empty[s]);  // the stage is free once these MMAs have read it
+    }
+    if (ok) mma_commit(done);  // the accumulator is final once every MMA completed
+    else *abort_flag = 1;
+  }
+  __syncwarp();
+  // epilogue: all four warps
+  const bool ok = mbar_wait(done, 0u, abort_flag);
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (ok) {
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll
+    for (int c = 0; c < TN / 32; ++c) {
+      uint32_t r[32];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 32);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+            "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+            "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int q = 0; q < 32; ++q) {
+        const int col = n0 + c * 32 + q;
+        if (row >= n || col >= n || row < col) continue;  // lower triangle, each element once
+        const float v = __uint_as_float(r[q]);
+        C[(size_t)row * ld + col] = v;
+        C[(size_t)col * ld + row] = v;
+      }
+    }
+  } else if (threadIdx.x == 0) {
+    atomicExch(error, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN));
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+using EncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                              const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeFn encode_fn() {
+  static EncodeFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeFn>(p);
+  });
+  return fn;
+}
+
+}  // namespace
+
+// Tensor map of an ld x ld fp32 row-major matrix with 32 x 128 boxes, 128-byte swizzle.
+bool make_square_map(const float *base, int ld, void *map_out) {
+  EncodeFn fn = encode_fn();
+  if (!fn || ld % 32 != 0 || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)ld};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
+  const cuuint32_t box[2] = {TK, TM};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(reinterpret_cast<CUtensorMap *>(map_out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                        const_cast<float *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+size_t square_tf32x3_smem() { return SMEM_BYTES; }
+
+void launch_square_tf32x3(cudaStream_t st, int n, int ld, const void *map_hi, const void *map_lo, float *C,
+                          int *error) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_square_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    attr = true;
+  }
+  const int t = (n + TM - 1) / TM;
+  k_square_tf32x3<<<t * (t + 1) / 2, 128, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap *>(map_hi),
+                                                            *reinterpret_cast<const CUtensorMap *>(map_lo), n, ld, C,
+                                                            error);
+  note_launch();
+}
+
+}  // namespace pm7
+
+namespace pm7 {
+namespace {
+
+// fp64 n x n -> fp32 split pair (hi = tf32 rounding, lo = remainder), ld x ld, zero padded.
+__global__ void k_split_tf32(int n, int ld, const double *__restrict__ X, float *__restrict__ hi,
+                             float *__restrict__ lo) {
+  const size_t len = (size_t)ld * ld;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = e / ld, j = e - i * ld;
+    float h = 0.0f, l = 0.0f;
+    if (i < (size_t)n && j < (size_t)n) {
+      const float x = (float)X[i * n + j];
+      uint32_t t;
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(x));
+      h = __uint_as_float(t);
+      l = x - h;
+    }
+    hi[e] = h;
+    lo[e] = l;
+  }
+}
+
+__global__ void k_widen(int n, int ld, const float *__restrict__ C32, double *__restrict__ C) {
+  const size_t len = (size_t)n * n;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = e / n, j = e - i * n;
+    C[e] = (double)C32[i * ld + j];
+  }
+}
+
+}  // namespace
+
+void launch_split_tf32(cudaStream_t st, int n, int ld, const double *X, float *hi, float *lo) {
+  k_split_tf32<<<1184, 256, 0, st>>>(n, ld, X, hi, lo);
+  note_launch();
+}
+
+void launch_widen(cudaStream_t st, int n, int ld, const float *C32, double *C) {
+  k_widen<<<1184, 256, 0, st>>>(n, ld, C32, C);
+  note_launch();
+}
+
+}  // namespace pm7
+
+// ---- the fp32 SP2 iteration around the tcgen05 squaring ------------------------------
+namespace pm7 {
+namespace {
+
+__device__ __forceinline__ void split_store(float x, float *hi, float *lo, size_t e) {
+  uint32_t t;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(x));
+  const float h = __uint_as_float(t);
+  hi[e] = h;
+  lo[e] = x - h;
+}
+
+// X = (emax I - F) / (emax - emin) in fp32 (ld x ld, padding untouched) and its split.
+__global__ void k_sp2_init32(int n, int ld, const double *__restrict__ F, const double *__restrict__ bounds,
+                             float *__restrict__ X, float *__restrict__ hi, float *__restrict__ lo) {
+  const double emin = bounds[0], emax = bounds[1], inv = 1.0 / (emax - emin);
+  const size_t len = (size_t)n * n;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = e / n, j = e - i * n, q = i * ld + j;
+    const float x = (float)(((i == j ? emax : 0.0) - F[e]) * inv);
+    X[q] = x;
+    split_store(x, hi, lo, q);
+  }
+}
+
+// state[0] = tr X, state[1] = tr X^2 (fp64 sums), state[2] = SP2 branch, state[3] = tr X - tr X^2.
+__global__ void k_sp2_trace32(int n, int ld, const float *__restrict__ X, const float *__restrict__ X2, double n_occ,
+                              double *__restrict__ state) {
+  __shared__ double sa[8], sb[8];
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) {
+    a += (double)X[(size_t)i * ld + i];
+    b += (double)X2[(size_t)i * ld + i];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sa[threadIdx.x >> 5] = a;
+    sb[threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a = 0.0;
+    b = 0.0;
+    for (int w = 0; w < 8; ++w) {
+      a += sa[w];
+      b += sb[w];
+    }
+    state[0] = a;
+    state[1] = b;
+    state[2] = fabs(b - n_occ) < fabs(2.0 * a - b - n_occ) ? 1.0 : 0.0;
+    state[3] = a - b;
+  }
+}
+
+// X <- X^2 or 2X - X^2 by state[2], and its split.
+__global__ void k_sp2_update32(int n, int ld, float *__restrict__ X, const float *__restrict__ X2,
+                               const double *__restrict__ state, float *__restrict__ hi, float *__restrict__ lo) {
+  const bool square = state[2] != 0.0;
+  const size_t len = (size_t)n * n;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = e / n, j = e - i * n, q = i * ld + j;
+    const float x2 = X2[q];
+    const float x = square ? x2 : 2.0f * X[q] - x2;
+    X[q] = x;
+    split_store(x, hi, lo, q);
+  }
+}
+
+// P = w X (fp64 n x n from the fp32 iterate).
+__global__ void k_sp2_density32(int n, int ld, const float *__restrict__ X, double w, double *__restrict__ P) {
+  const size_t len = (size_t)n * n;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = e / n, j = e - i * n;
+    P[e] = w * (double)X[i * ld + j];
+  }
+}
+
+}  // namespace
+
+void launch_sp2_init32(cudaStream_t st, int n, int ld, const double *F, const double *bounds, float *X, float *hi,
+                       float *lo) {
+  k_sp2_init32<<<1184, 256, 0, st>>>(n, ld, F, bounds, X, hi, lo);
+  note_launch();
+}
+void launch_sp2_trace32(cudaStream_t st, int n, int ld, const float *X, const float *X2, double n_occ, double *state) {
+  k_sp2_trace32<<<1, 256, 0, st>>>(n, ld, X, X2, n_occ, state);
+  note_launch();
+}
+void launch_sp2_update32(cudaStream_t st, int n, int ld, float *X, const float *X2, const double *state, float *hi,
+                         float *lo) {
+  k_sp2_update32<<<1184, 256, 0, st>>>(n, ld, X, X2, state, hi, lo);
+  note_launch();
+}
+void launch_sp2_density32(cudaStream_t st, int n, int ld, const float *X, double w, double *P) {
+  k_sp2_density32<<<1184, 256, 0, st>>>(n, ld, X, w, P);
+  note_launch();
+}
+
+}  // namespace pm7

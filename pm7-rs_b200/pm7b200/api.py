@@ -326,3 +326,15 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+def square_tf32(x):
+    """C = X X of a symmetric matrix on the tcgen05 tensor cores (3xTF32 split, fp32
+    accumulation): the squaring of the mixed-precision SP2 purification."""
+    L = lib()
+    L.pm7_stage_square_tf32.argtypes = [C.c_int32, abi.DP, abi.DP]
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n = x.shape[0]
+    out = np.zeros((n, n))
+    _check(L.pm7_stage_square_tf32(n, x.ctypes.data_as(abi.DP), out.ctypes.data_as(abi.DP)))
+    return out

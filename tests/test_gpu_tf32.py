@@ -1,0 +1,53 @@
+"""The tcgen05 (kind::tf32) squaring of the mixed-precision SP2 against fp64.
+
+X is split as tf32(X) + remainder and X X accumulated in fp32 in tensor memory (3xTF32),
+so the product carries about fp32 accuracy; the tensor core's fp32 accumulation is not
+round-to-nearest, so the error grows with the inner dimension: 4e-8 n of the largest
+element is allowed. Checked on symmetric matrices shaped like SP2 iterates (spectrum in
+[0, 1]) at sizes that cover one tile, ragged tiles and several tile rows.
+"""
+import numpy as np
+import pytest
+
+from pm7b200 import api
+
+pytestmark = pytest.mark.gpu
+
+
+def _iterate(n, seed):
+    rng = np.random.default_rng(seed)
+    q, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    lam = rng.uniform(0.0, 1.0, size=n)
+    return (q * lam) @ q.T
+
+
+@pytest.mark.parametrize("n", [40, 128, 131, 300, 517])
+def test_square_matches_fp64(n):
+    x = _iterate(n, n)
+    c = api.square_tf32(x)
+    ref = x @ x
+    err = np.max(np.abs(c - ref)) / np.max(np.abs(ref))
+    assert err < 4e-8 * max(n, 64), err
+    assert np.array_equal(c, c.T)  # written once and mirrored
+
+
+def test_square_is_deterministic():
+    x = _iterate(300, 3)
+    assert np.array_equal(api.square_tf32(x), api.square_tf32(x))
+
+
+def test_mixed_precision_scf_matches_fp64_oracle():
+    # fp32 (tcgen05) densities for the early cycles, fp64 refinement cycles at the end:
+    # the heat of formation within 1e-4 kcal/mol and the charges within 1e-6 e of the oracle
+    from oracle import harness
+    from pm7b200 import geometry as G
+
+    z, x = G.water_cluster(100, seed=2)  # 600 basis functions: the SP2 path
+    r = api.run_pm7(z, x, precision=1)
+    o = harness.run(z, x)
+    assert r["fp32_iterations"] > 0
+    assert r["iterations"] > r["fp32_iterations"]
+    assert abs(r["heat_of_formation_kcal"] - o["heat_of_formation_kcal"]) < 1.0e-4
+    assert np.max(np.abs(r["charges"] - o["charges"])) < 1.0e-6
+    f = api.run_pm7(z, x)
+    assert f["fp32_iterations"] == 0
