@@ -379,7 +379,7 @@ def run_batch_bench(args, world, rank, local):
     from pm7b200 import geometry as G
 
     mols = G.batch(4096, seed=rank)
-    opts = dict(device=local, want_matrices=0)
+    opts = dict(device=local, want_matrices=0, precision=1 if args.precision == "mixed" else 0)
     for _ in range(args.warmup):
         api.run_batch(mols[:128], **opts)
     barrier(world)
@@ -405,7 +405,7 @@ def run_batch_bench(args, world, rank, local):
     value = 4096 * args.steps * world / wall
     rng = np.random.default_rng(7)
     idx = sorted(rng.choice(len(mols), size=48, replace=False).tolist())
-    plain, plain_res = _plain_sample(api, mols, idx, local)
+    plain, plain_res = _plain_sample(api, mols, idx, local)  # plain FP64 path
     dhf = max(abs(res[i]["heat_of_formation_kcal"] - plain_res[i]["heat_of_formation_kcal"]) for i in idx)
     cpu = None
     if not args.no_cpu_baseline:
@@ -419,7 +419,8 @@ def run_batch_bench(args, world, rank, local):
     line = {
         "metric": "PM7 SCF solves/s (batched RHF single points)", "value": value, "unit": "solves/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+        "dtype": "f64" if args.precision == "fp64" else "f32 (tcgen05 3xTF32) + f64 refinement",
         "config": {"workload": "batch4096", "molecules": 4096, "seed": rank, "atoms_min": min(natoms),
                    "atoms_max": max(natoms), "atoms_mean": float(np.mean(natoms)), "failed": failed,
                    "parallelism": f"replicas{world}"},
@@ -439,11 +440,12 @@ def run_stream_bench(args, world, rank, local):
 
     count = args.stream_count
     mols = G.stream(count, seed=rank)
+    prec = 1 if args.precision == "mixed" else 0
     with api.Engine(device=local) as eng:
         # warm-up and capacity: a burst of the first molecules submitted at once
         burst = mols[: min(count, 120)]
         t = time.perf_counter()
-        tk = [eng.submit(z, x, want_matrices=0) for z, x in burst]
+        tk = [eng.submit(z, x, want_matrices=0, precision=prec) for z, x in burst]
         for k in tk:
             eng.poll(k, wait=True)
         capacity = len(burst) / (time.perf_counter() - t)
@@ -463,7 +465,7 @@ def run_stream_bench(args, world, rank, local):
             now = time.perf_counter()
             if due > now:
                 time.sleep(due - now)
-            tickets[i] = eng.submit(z, x, want_matrices=0)
+            tickets[i] = eng.submit(z, x, want_matrices=0, precision=prec)
         res = [eng.poll(tk, wait=True)[1] for tk in tickets]
         wall = time.perf_counter() - t0
         launches = api.launch_count() - launches0
@@ -485,7 +487,8 @@ def run_stream_bench(args, world, rank, local):
     line = {
         "metric": "PM7 SCF solves/s and p50/p99 latency (served stream)", "value": value, "unit": "solves/s",
         "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": wall * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+        "dtype": "f64" if args.precision == "fp64" else "f32 (tcgen05 3xTF32) + f64 refinement",
         "config": {"workload": "stream", "requests": count, "seed": rank, "arrival": "Poisson",
                    "rate_per_s": rate, "burst_capacity_per_s": capacity, "atoms_min": min(natoms),
                    "atoms_max": max(natoms), "failed": count - len(ok), "parallelism": f"replicas{world}"},
@@ -508,6 +511,8 @@ def main():
     ap.add_argument("--workload", default="water334",
                     choices=["water334", "water1000", "decane", "batch4096", "stream"])
     ap.add_argument("--stream-count", type=int, default=600)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="batch4096/stream: fp64, or fp32 tcgen05 purification cycles with fp64 refinement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-peak", action="store_true")
     args = ap.parse_args()

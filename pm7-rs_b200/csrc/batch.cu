@@ -79,6 +79,10 @@ __global__ void __launch_bounds__(RB) k_b_init(BatchList L, const MolDesc *__res
     const size_t r = i / n, c = i - r * n;
     d.P[i] = diag ? (r == c ? diag[r] : 0.0) : d.Pn[i];
   }
+  if (d.X32) {  // the fp32 arrays' padding must stay zero
+    const size_t l32 = (size_t)d.ld32 * d.ld32;
+    for (size_t i = threadIdx.x; i < l32; i += RB) d.X32[i] = d.hi32[i] = d.lo32[i] = d.C32[i] = 0.0f;
+  }
 }
 
 // Core-core energy of each molecule: its pair-sweep partials in fixed order.
@@ -104,22 +108,6 @@ __global__ void k_b_push(int n, const int *__restrict__ slots, MolCtl *__restric
     for (int i = 0; i + 1 < c.n_ord; ++i) c.ord[i] = c.ord[i + 1];
     c.n_ord -= 1;
   }
-}
-
-// Chunk `item` of a chunk list: list position, slot and element range [e0, e1).
-struct ChunkRef {
-  int m, slot, q;
-  size_t e0, e1;
-};
-__device__ __forceinline__ ChunkRef chunk_ref(const BatchList &L, const MolDesc *D, int item) {
-  ChunkRef r;
-  r.m = batch_find(L, item);
-  r.slot = L.slot[r.m];
-  r.q = item - L.prefix[r.m];
-  const size_t nn = mol_nn(D[r.slot]);
-  r.e0 = (size_t)r.q * kChunk;
-  r.e1 = r.e0 + kChunk < nn ? r.e0 + kChunk : nn;
-  return r;
 }
 
 // Partial of E_el = 1/2 sum P (H + F) (scf.rs:1237) into part[0]; in the SCF loop also
@@ -366,10 +354,23 @@ __device__ bool dev_adiis(const MolCtl &c, double *cw) {
 }
 
 // Record the new entry's inner products and choose this iteration's extrapolation.
-__global__ void k_b_control(int n, const int *__restrict__ slots, MolCtl *__restrict__ C) {
+// DIIS error below which a mixed-precision molecule switches to fp64 densities.
+constexpr double kMixedSwitch = 1.0e-3;
+constexpr double kMixedSwitchStep = 1.0e-5;  // rms density step that also ends the fp32 phase
+
+__global__ void k_b_control(int n, const int *__restrict__ slots, MolCtl *__restrict__ C,
+                            unsigned char *__restrict__ use32) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= n) return;
   MolCtl &c = C[slots[m]];
+  // mixed precision: fp32 densities until the DIIS error is small, fp64 from then on
+  // (the first cycles' error says nothing: a SAD guess proportional to I commutes with F;
+  // for a large molecule the commutator norm can stall at the fp32 noise floor while the
+  // density step is already small, so either criterion, or 40 fp32 cycles, ends the phase)
+  if (c.mixed && c.iter >= 2 && (sqrt(c.err2) < kMixedSwitch || c.dp < kMixedSwitchStep || c.fp32_iters >= 40))
+    c.mixed = 0;
+  c.use32 = c.mixed;
+  use32[m] = (unsigned char)c.use32;
   const int s = c.slot, k = c.n_ord;
   for (int i = 0; i < k; ++i) {
     const int o = c.ord[i];
@@ -660,12 +661,13 @@ __global__ void k_b_converge(int n, const int *__restrict__ slots, MolDesc *__re
   d.Pn = t;
   c.e_old = c.e_elec;
   const bool residual_ok = c.shift == 0.0 && sqrt(c.err2) < 1.0e-7;
-  if (c.iter > 0 && de < c.e_tol && (dp < c.p_tol || residual_ok)) {
+  if (!c.use32 && c.iter > 0 && de < c.e_tol && (dp < c.p_tol || residual_ok)) {  // only fp64 cycles end the SCF
     c.converged = 1;
     c.done = 1;
   } else {
     guard_update(c, dp, c.e_elec);
   }
+  if (c.use32) c.fp32_iters += 1;
   c.iter += 1;
   if (!c.done && c.iter >= c.max_scf) c.done = 1;
   flags[m] = (unsigned char)c.done;
@@ -708,7 +710,7 @@ __global__ void k_b_atom_out(BatchList L, const MolDesc *__restrict__ D, DeviceP
 
 // Packs what the host reports of each listed molecule into out + off[m]: 11 control
 // scalars, the orbital energies (nao) and the per-atom outputs (kAtomOut n).
-constexpr int kOutScalars = 11;
+constexpr int kOutScalars = 12;
 __global__ void k_b_gather_out(BatchList L, const MolDesc *__restrict__ D, const MolCtl *__restrict__ C,
                                const long long *__restrict__ off, double *__restrict__ out) {
   const int m = blockIdx.x;
@@ -724,6 +726,7 @@ __global__ void k_b_gather_out(BatchList L, const MolDesc *__restrict__ D, const
     o[4] = c.core_core;
     for (int k = 0; k < 5; ++k) o[5 + k] = c.corr[k];
     o[10] = c.shift;
+    o[11] = c.fp32_iters;
   }
   const int nao = d.g.nao, na = kAtomOut * d.g.n_atoms;
   for (int i = threadIdx.x; i < nao; i += blockDim.x) o[kOutScalars + i] = d.eps_out[i];
@@ -797,6 +800,7 @@ struct BatchMol {
   size_t bytes = 0;
   MolDesc d{};
   int np = 0;  // bucket matrix size
+  bool mixed = false;  // fp32 (tcgen05) SP2 cycles before the fp64 ones
   // outcome
   pm7_status status = PM7_OK;
   std::string error;
@@ -854,6 +858,12 @@ static size_t mol_layout(BatchMol &b, char *base) {
   d.V_out = b.o.want_matrices ? (double *)take(8 * nn) : nullptr;
   d.atom_out = (double *)take(8 * (size_t)kAtomOut * n);
   d.part = (double *)take(8 * (size_t)kPart * std::max(items_chunks(nao), items_rows8(nao)));
+  d.ld32 = b.mixed ? ((nao + 31) / 32) * 32 : 0;
+  const size_t l32 = (size_t)d.ld32 * d.ld32;
+  d.X32 = b.mixed ? (float *)take(4 * l32) : nullptr;
+  d.hi32 = b.mixed ? (float *)take(4 * l32) : nullptr;
+  d.lo32 = b.mixed ? (float *)take(4 * l32) : nullptr;
+  d.C32 = b.mixed ? (float *)take(4 * l32) : nullptr;
   d.corr_scratch = (double *)take(8 * corrections_scratch(n));
   // the uploaded tables, contiguous: xyz | sad | z | aoff | ao_atom | csr_start | csr | near | mask
   const size_t up0 = off;
@@ -934,6 +944,8 @@ class BatchRunner {
     SOLVER_OK(cusolverDnCreate(&solver_));
     SOLVER_OK(cusolverDnSetStream(solver_, st_));
     SOLVER_OK(cusolverDnCreateParams(&sparams_));
+    CUDA_OK(cudaMalloc((void **)&err32_, sizeof(int)));
+    CUDA_OK(cudaMemset(err32_, 0, sizeof(int)));
     // density of each SCF iteration: SP2 purification from sp2_min_nao_ basis functions up,
     // the eigensolver below; PM7_BATCH_DENSITY=eig|sp2 forces one of them for every molecule
     if (const char *e = std::getenv("PM7_BATCH_DENSITY")) {
@@ -953,6 +965,8 @@ class BatchRunner {
     if (flags_d_) cudaFree(flags_d_);
     if (pin_) cudaFreeHost(pin_);
     if (out_d_) cudaFree(out_d_);
+    if (maps_) cudaFree(maps_);
+    if (err32_) cudaFree(err32_);
     cusolverDnDestroyParams(sparams_);
     cusolverDnDestroy(solver_);
     cudaStreamDestroy(st_);
@@ -981,6 +995,7 @@ class BatchRunner {
                                                " is incompatible with multiplicity " + std::to_string(o.multiplicity)};
     b->n_occ = (int)(ni / 2);
     b->dframe = o.force_dpath || b->L.has_d;
+    b->mixed = o.precision == PM7_PRECISION_MIXED && b->L.nao >= sp2_min_nao_;
     b->bytes = mol_layout(*b, nullptr);
     b->np = bucket_size(b->L.nao);
     if (o.initial_density) {
@@ -1040,8 +1055,20 @@ class BatchRunner {
       c.adiis_switch = b->o.adiis_switch;
       c.shift_floor = b->o.level_shift;
       c.shift = b->o.level_shift;
+      c.mixed = b->mixed ? 1 : 0;
       std::memcpy(host + ctl_off + sizeof(MolCtl) * i, &c, sizeof(MolCtl));
     });
+    for (int i = 0; i < n; ++i) {
+      BatchMol *b = in[i];
+      if (!b->mixed) continue;
+      // tensor maps of the split fp32 iterate, read by the grouped tcgen05 squaring
+      alignas(64) unsigned char maps[256];
+      if (!make_square_map(b->d.hi32, b->d.ld32, maps) || !make_square_map(b->d.lo32, b->d.ld32, maps + 128))
+        throw Failure{PM7_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
+      std::memcpy(map_stage_.data() + 256 * (size_t)b->slot, maps, 256);
+      CUDA_OK(cudaMemcpyAsync(maps_ + 256 * (size_t)b->slot, map_stage_.data() + 256 * (size_t)b->slot, 256,
+                              cudaMemcpyHostToDevice, st_));
+    }
     for (int i = 0; i < n; ++i) {
       BatchMol *b = in[i];
       size_t start, bytes;
@@ -1104,40 +1131,79 @@ class BatchRunner {
       Stage s_(st_, "batch_diis");
       k_b_dots_c<<<A.chunks.total, RB, 0, st_>>>(A.chunks, desc_, ctl_);
       k_b_reduce<<<nb, 128, 0, st_>>>(n, A.mol.slot, desc_, ctl_, 0);
-      k_b_control<<<(n + 63) / 64, 64, 0, st_>>>(n, A.mol.slot, ctl_);
+      k_b_control<<<(n + 63) / 64, 64, 0, st_>>>(n, A.mol.slot, ctl_, flags_d_ + 2 * (size_t)cap_);
       note_launch(3);
     }
-    // density: SP2 purification on the tensor cores for the larger molecules, the batched
-    // eigensolver for the small ones (where it is as fast) and for what SP2 leaves
-    std::vector<BatchMol *> fallback, purify;
-    for (BatchMol *b : active_) (b->L.nao >= sp2_min_nao_ ? purify : fallback).push_back(b);
-    if (!purify.empty()) {
+    // which molecules take an fp32 cycle (decided on the device from their DIIS error)
+    bool any_mixed = false;
+    for (const BatchMol *b : active_) any_mixed = any_mixed || b->mixed;
+    if (any_mixed) {
+      CUDA_OK(cudaMemcpyAsync(flags_h_ + 2 * (size_t)cap_, flags_d_ + 2 * (size_t)cap_, n, cudaMemcpyDeviceToHost,
+                              st_));
+      CUDA_OK(cudaStreamSynchronize(st_));
+    }
+    // density: SP2 purification on the tensor cores for the larger molecules (fp32 cycles
+    // on tcgen05, fp64 cycles on DMMA), the batched eigensolver for the small ones (where
+    // it is as fast) and for what SP2 leaves
+    std::vector<BatchMol *> fallback, purify64, purify32;
+    for (int m = 0; m < n; ++m) {
+      BatchMol *b = active_[m];
+      if (b->L.nao < sp2_min_nao_) fallback.push_back(b);
+      else if (any_mixed && flags_h_[2 * (size_t)cap_ + m]) purify32.push_back(b);
+      else purify64.push_back(b);
+    }
+    if (!purify64.empty() || !purify32.empty()) {
       Stage s_(st_, "batch_sp2");
-      Lists S = lists(purify, false, &up_sp2_);
-      const int ns = S.mol.n;
-      k_b_sp2_fuse<<<S.rows.total, RB, 0, st_>>>(S.rows, desc_, ctl_);
-      k_b_sp2_bounds<<<(ns + 127) / 128, 128, 0, st_>>>(ns, S.mol.slot, desc_, ctl_);
-      k_b_sp2_x0<<<S.chunks.total, RB, 0, st_>>>(S.chunks, desc_, ctl_);
-      note_launch(3);
-      const int chunk = 8;
-      bool running = true;
-      for (int step = 0; step < 100 && running; step += chunk) {
-        for (int k = 0; k < chunk; ++k) {
-          launch_b_gemm(st_, S.glow, desc_, ctl_, nullptr, 2);
-          k_b_sp2_decide<<<ns, RB, 0, st_>>>(S.mol, desc_, ctl_, flags_d_);
-          k_b_sp2_apply<<<S.chunks.total, RB, 0, st_>>>(S.chunks, desc_, ctl_);
-          note_launch(2);
-        }
-        CUDA_OK(cudaMemcpyAsync(flags_h_, flags_d_, ns, cudaMemcpyDeviceToHost, st_));
-        CUDA_OK(cudaStreamSynchronize(st_));
-        running = false;
-        for (int m = 0; m < ns; ++m) running = running || flags_h_[m] == 0;
+      Lists S = lists(purify64, false, &up_sp2_);
+      Lists T = lists(purify32, false, &up_sp32_);
+      unsigned char *f64 = flags_d_, *f32 = flags_d_ + cap_;
+      for (const Lists *L : {&S, &T}) {
+        if (L->mol.n == 0) continue;
+        k_b_sp2_fuse<<<L->rows.total, RB, 0, st_>>>(L->rows, desc_, ctl_);
+        k_b_sp2_bounds<<<(L->mol.n + 127) / 128, 128, 0, st_>>>(L->mol.n, L->mol.slot, desc_, ctl_);
+        k_b_sp2_x0<<<L->chunks.total, RB, 0, st_>>>(L->chunks, desc_, ctl_);
+        note_launch(3);
       }
-      for (int m = 0; m < ns; ++m)
+      if (T.mol.n) launch_b_to32(st_, T.chunks, desc_);
+      const int chunk = 8;
+      bool run64 = S.mol.n > 0, run32 = T.mol.n > 0;
+      for (int step = 0; step < 100 && (run64 || run32); step += chunk) {
+        for (int k = 0; k < chunk; ++k) {
+          if (run64) {
+            launch_b_gemm(st_, S.glow, desc_, ctl_, nullptr, 2);
+            k_b_sp2_decide<<<S.mol.n, RB, 0, st_>>>(S.mol, desc_, ctl_, f64);
+            k_b_sp2_apply<<<S.chunks.total, RB, 0, st_>>>(S.chunks, desc_, ctl_);
+            note_launch(2);
+          }
+          if (run32) {
+            launch_b_square_tf32x3(st_, T.tiles, desc_, ctl_, maps_, err32_);
+            launch_b_sp2_decide32(st_, T.mol, desc_, ctl_, f32);
+            launch_b_sp2_apply32(st_, T.chunks, desc_, ctl_);
+          }
+        }
+        CUDA_OK(cudaMemcpyAsync(flags_h_, flags_d_, 2 * (size_t)cap_, cudaMemcpyDeviceToHost, st_));
+        CUDA_OK(cudaStreamSynchronize(st_));
+        run64 = false;
+        for (int m = 0; m < S.mol.n; ++m) run64 = run64 || flags_h_[m] == 0;
+        run32 = false;
+        for (int m = 0; m < T.mol.n; ++m) run32 = run32 || flags_h_[cap_ + m] == 0;
+      }
+      for (int m = 0; m < S.mol.n; ++m)
         if (flags_h_[m] != 1) {
-          fallback.push_back(purify[m]);
+          fallback.push_back(purify64[m]);
           ++sp2_fallbacks_;
         }
+      for (int m = 0; m < T.mol.n; ++m)
+        if (flags_h_[cap_ + m] != 1) {
+          fallback.push_back(purify32[m]);
+          ++sp2_fallbacks_;
+        }
+      if (T.mol.n) {
+        int bad = 0;
+        CUDA_OK(cudaMemcpyAsync(&bad, err32_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+        CUDA_OK(cudaStreamSynchronize(st_));
+        if (bad) throw Failure{PM7_ERR_CUDA, "tcgen05 squaring: a pipeline wait expired"};
+      }
     }
     if (!fallback.empty()) {
       Stage s_(st_, "batch_eigensolve");
@@ -1165,7 +1231,7 @@ class BatchRunner {
 
  private:
   struct Lists {
-    BatchList mol, rows, chunks, near, atoms, gfull, glow, sp_pairs, d_pairs, sp_near, d_near, pairs;
+    BatchList mol, rows, chunks, near, atoms, gfull, glow, tiles, sp_pairs, d_pairs, sp_near, d_near, pairs;
     const EigSlot *eig = nullptr;
     std::vector<EigSlot> eig_h;
     std::map<int, std::vector<int>> buckets;  // np -> list positions
@@ -1190,6 +1256,7 @@ class BatchRunner {
   }
 
   void grow(int cap) {
+    const int old_cap = cap_;
     MolDesc *nd = nullptr;
     MolCtl *nc = nullptr;
     CUDA_OK(cudaMalloc(&nd, sizeof(MolDesc) * cap));
@@ -1207,8 +1274,16 @@ class BatchRunner {
     cap_ = cap;
     if (flags_h_) CUDA_OK(cudaFreeHost(flags_h_));
     if (flags_d_) CUDA_OK(cudaFree(flags_d_));
-    CUDA_OK(cudaMallocHost((void **)&flags_h_, cap));
-    CUDA_OK(cudaMalloc((void **)&flags_d_, cap));
+    CUDA_OK(cudaMallocHost((void **)&flags_h_, 3 * (size_t)cap));
+    CUDA_OK(cudaMalloc((void **)&flags_d_, 3 * (size_t)cap));
+    unsigned char *nm = nullptr;
+    CUDA_OK(cudaMalloc((void **)&nm, 256 * (size_t)cap));
+    if (maps_) {
+      CUDA_OK(cudaMemcpy(nm, maps_, 256 * (size_t)old_cap, cudaMemcpyDeviceToDevice));
+      CUDA_OK(cudaFree(maps_));
+    }
+    maps_ = nm;
+    map_stage_.resize(256 * (size_t)cap);
   }
 
   void release(BatchMol &b) {
@@ -1250,6 +1325,7 @@ class BatchRunner {
         {&A.atoms, [](const BatchMol &b) { return b.m.n; }, all},
         {&A.gfull, [](const BatchMol &b) { return items_gemm_full(b.L.nao); }, all},
         {&A.glow, [](const BatchMol &b) { return items_gemm_lower(b.L.nao); }, all},
+        {&A.tiles, [](const BatchMol &b) { return items_tiles128(b.L.nao); }, all},
         {&A.pairs, [](const BatchMol &b) { return items_pairs_all(b.m.n); }, all},
         {&A.sp_pairs, [](const BatchMol &b) { return items_pairs_all(b.m.n); },
          [](const BatchMol &b) { return !b.dframe; }},
@@ -1435,6 +1511,7 @@ class BatchRunner {
       rp.core_ev = o[4];
       for (int k = 0; k < 5; ++k) rp.corr[k] = o[5 + k];
       rp.n_occ = b.n_occ;
+      rp.fp32_iterations = (int)o[11];
       rp.eps_a.assign(o + kOutScalars, o + kOutScalars + nao);
       const double *ao = o + kOutScalars + nao;
       std::vector<double> pops(b.m.n);
@@ -1476,11 +1553,14 @@ class BatchRunner {
   std::vector<int> free_slots_;
   std::vector<BatchMol *> active_;
   size_t bytes_in_use_ = 0;
-  ListUpload up_, up_fallback_, up_sp2_, ptr_up_;
+  ListUpload up_, up_fallback_, up_sp2_, up_sp32_, ptr_up_;
   char *pin_ = nullptr;
   size_t pin_cap_ = 0;
   double *out_d_ = nullptr;
   size_t out_cap_ = 0;
+  unsigned char *maps_ = nullptr;      // 2 CUtensorMap (128 B each) per slot
+  std::vector<unsigned char> map_stage_;
+  int *err32_ = nullptr;               // set by the tcgen05 squaring when a wait expired
   double *arena_ = nullptr;
   size_t arena_cap_ = 0;
   void *work_ = nullptr;

@@ -29,6 +29,8 @@ struct MolDesc {
   double *eps_out, *V_out;   // reported orbital energies (nao) and vectors (nao^2, optional)
   double *atom_out;          // per atom: population and the hybrid-dipole density elements
   double *part;              // per-item partial sums of the chunked reductions (kPart each)
+  float *X32, *hi32, *lo32, *C32;  // mixed precision: fp32 SP2 iterate, its tf32 split, X^2 (ld32^2)
+  int ld32;
   double *corr_scratch;      // post-SCF corrections scratch
 };
 
@@ -53,6 +55,7 @@ struct MolCtl {
   double ee[kHist + 1], df_row[kHist + 1], df_col[kHist];
   // SP2 purification of this iteration: state 0 running, 1 converged, 2 failed
   int sp2_state, sp2_steps, sp2_fallbacks, sp2_square, sp2_apply;
+  int mixed, use32, fp32_iters;  // mixed precision: still in fp32 cycles, this cycle fp32, count
   double sp2_err[3], sp2_emin, sp2_emax;
   // results
   double core_core, e_final, corr[5];
@@ -89,6 +92,23 @@ __device__ __forceinline__ double *hist_F(const MolDesc &d, int s) { return d.hi
 __device__ __forceinline__ double *hist_E(const MolDesc &d, int s) { return hist_F(d, s) + mol_nn(d); }
 __device__ __forceinline__ double *hist_D(const MolDesc &d, int s) { return hist_F(d, s) + 2 * mol_nn(d); }
 
+// Chunk `item` of a chunk list: list position, slot and element range [e0, e1).
+struct ChunkRef {
+  int m, slot, q;
+  size_t e0, e1;
+};
+constexpr int kChunkElems = 32768;
+__device__ __forceinline__ ChunkRef chunk_ref(const BatchList &L, const MolDesc *D, int item) {
+  ChunkRef r;
+  r.m = batch_find(L, item);
+  r.slot = L.slot[r.m];
+  r.q = item - L.prefix[r.m];
+  const size_t nn = mol_nn(D[r.slot]);
+  r.e0 = (size_t)r.q * kChunkElems;
+  r.e1 = r.e0 + kChunkElems < nn ? r.e0 + kChunkElems : nn;
+  return r;
+}
+
 // ---- batched phase launchers (kernels_*.cu) ----
 // Work items per molecule, for building the prefix arrays on the host.
 inline int items_pairs_all(int n_atoms) { return n_atoms * ((n_atoms + 127) / 128); }
@@ -99,7 +119,7 @@ inline int items_rows8(int nao) { return (nao + 7) / 8; }
 // Matrix-element chunks of the elementwise and reduction kernels: a large molecule is
 // spread over many blocks; each chunk leaves kPart partial sums that a per-molecule pass
 // adds in chunk order.
-constexpr int kChunk = 32768;
+constexpr int kChunk = kChunkElems;
 constexpr int kPart = 32;
 __host__ __device__ inline int items_chunks(int nao) {
   return (int)(((size_t)nao * nao + kChunk - 1) / kChunk);
@@ -123,6 +143,15 @@ void launch_b_fock(cudaStream_t st, const BatchList &Lmol, const BatchList &Lrow
 // op 0: X = F_slot P (full tiles); op 1: Pn = 2 V_occ^T V_occ (lower tiles, mirrored);
 // op 2: Pn = X X for molecules whose SP2 purification is still running (lower tiles).
 void launch_b_gemm(cudaStream_t st, const BatchList &L, const MolDesc *D, const MolCtl *C, const EigSlot *E, int op);
+
+// Mixed precision (kernels_tf32.cu): items_tiles128 per molecule for the squaring; chunks
+// for the conversions and updates; one block per molecule for the decisions.
+inline int items_tiles128(int nao) { const int t = (nao + 127) / 128; return t * (t + 1) / 2; }
+void launch_b_square_tf32x3(cudaStream_t st, const BatchList &L, const MolDesc *D, const MolCtl *C,
+                            const void *maps, int *error);
+void launch_b_to32(cudaStream_t st, const BatchList &L, const MolDesc *D);
+void launch_b_sp2_decide32(cudaStream_t st, const BatchList &L, const MolDesc *D, MolCtl *C, unsigned char *flags);
+void launch_b_sp2_apply32(cudaStream_t st, const BatchList &L, const MolDesc *D, const MolCtl *C);
 
 // Post-SCF corrections of the listed molecules into C[slot].corr (dispersion variant per
 // molecule from MolDesc::smooth_dispersion). Lmol: one item per molecule; Lpairs:

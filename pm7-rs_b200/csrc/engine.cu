@@ -464,6 +464,7 @@ struct Purifier {
 // be forced with PM7_DENSITY_SOLVER=sp2|syevd.
 // DIIS error below which the mixed-precision SCF switches to fp64 densities.
 static constexpr double kMixedSwitch = 1.0e-3;
+static constexpr double kMixedSwitchStep = 1.0e-5;  // rms density step that also ends the fp32 phase
 
 static bool use_sp2(int n) {
   const char *env = std::getenv("PM7_DENSITY_SOLVER");
@@ -649,7 +650,12 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     CUDA_OK(cudaMemcpyAsync(coef.p, pin_cw, sizeof(double) * cw.size(), cudaMemcpyHostToDevice, st));
     { Stage s_(st, "combine"); launch_combine(st, n, (int)fp.size(), ptrs.p + 48, coef.p, out.P.p, 2.0, guard.shift, Fuse.p); }
     bool purified = false;
-    if (phase32 && err_norm < kMixedSwitch) phase32 = false;
+    // (the first cycles' error says nothing: a SAD guess proportional to I commutes with F;
+    // for a large molecule the commutator norm can stall at the fp32 noise floor while the
+    // density step is already small, so either criterion, or 40 fp32 cycles, ends the phase)
+    if (phase32 && iter >= 2 &&
+        (err_norm < kMixedSwitch || out.density_error < kMixedSwitchStep || out.fp32_iterations >= 40))
+      phase32 = false;
     const bool used32 = phase32;
     if (sp2) {
       Stage s_(st, "sp2_purify");

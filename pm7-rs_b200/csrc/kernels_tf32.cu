@@ -102,10 +102,11 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
                : "memory");
 }
 
-__global__ void __launch_bounds__(128) k_square_tf32x3(const __grid_constant__ CUtensorMap map_hi,
-                                                       const __grid_constant__ CUtensorMap map_lo, int n, int ld,
-                                                       float *__restrict__ C, int *__restrict__ error) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
+// One 128x128 lower tile (bm >= bn) of C = X X; `smem_raw` is the CTA's dynamic shared
+// memory (SMEM_BYTES), map_hi / map_lo the tensor maps of the split operand.
+__device__ __forceinline__ void square_tile(int bm, int bn, const CUtensorMap *map_hi, const CUtensorMap *map_lo,
+                                            int n, int ld, float *__restrict__ C, int *__restrict__ error,
+                                            unsigned char *smem_raw) {
   // stage buffers on a 1024-byte boundary (128-byte swizzle atoms)
   unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
@@ -114,10 +115,6 @@ __global__ void __launch_bounds__(128) k_square_tf32x3(const __grid_constant__ C
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
-  // lower tile (bm >= bn) of this CTA
-  int bm = 0;
-  while ((bm + 1) * (bm + 2) / 2 <= (int)blockIdx.x) ++bm;
-  const int bn = blockIdx.x - bm * (bm + 1) / 2;
   const int m0 = bm * TM, n0 = bn * TN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ktiles = (ld + TK - 1) / TK;
@@ -149,10 +146,10 @@ __global__ void __launch_bounds__(128) k_square_tf32x3(const __grid_constant__ C
       unsigned char *st = smem + s * STAGE_BYTES;
       mbar_expect_tx(&full[s], STAGE_BYTES);
       const int k0 = kt * TK;
-      tma_load_2d(st + 0 * TILE_BYTES, &map_hi, &full[s], k0, m0);
-      tma_load_2d(st + 1 * TILE_BYTES, &map_lo, &full[s], k0, m0);
-      tma_load_2d(st + 2 * TILE_BYTES, &map_hi, &full[s], k0, n0);
-      tma_load_2d(st + 3 * TILE_BYTES, &map_lo, &full[s], k0, n0);
+      tma_load_2d(st + 0 * TILE_BYTES, map_hi, &full[s], k0, m0);
+      tma_load_2d(st + 1 * TILE_BYTES, map_lo, &full[s], k0, m0);
+      tma_load_2d(st + 2 * TILE_BYTES, map_hi, &full[s], k0, n0);
+      tma_load_2d(st + 3 * TILE_BYTES, map_lo, &full[s], k0, n0);
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
@@ -213,6 +210,22 @@ __global__ void __launch_bounds__(128) k_square_tf32x3(const __grid_constant__ C
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN));
+}
+
+__device__ __forceinline__ void lower_tile(int t, int &bm, int &bn) {
+  int m = 0;
+  while ((m + 1) * (m + 2) / 2 <= t) ++m;
+  bm = m;
+  bn = t - m * (m + 1) / 2;
+}
+
+__global__ void __launch_bounds__(128) k_square_tf32x3(const __grid_constant__ CUtensorMap map_hi,
+                                                       const __grid_constant__ CUtensorMap map_lo, int n, int ld,
+                                                       float *__restrict__ C, int *__restrict__ error) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  int bm, bn;
+  lower_tile(blockIdx.x, bm, bn);
+  square_tile(bm, bn, &map_hi, &map_lo, n, ld, C, error, smem_raw);
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
@@ -409,6 +422,153 @@ void launch_sp2_update32(cudaStream_t st, int n, int ld, float *X, const float *
 }
 void launch_sp2_density32(cudaStream_t st, int n, int ld, const float *X, double w, double *P) {
   k_sp2_density32<<<1184, 256, 0, st>>>(n, ld, X, w, P);
+  note_launch();
+}
+
+}  // namespace pm7
+
+// ---- batched mixed precision -------------------------------------------------------
+#include "batch.hpp"
+
+namespace pm7 {
+namespace {
+
+// Grouped squaring: item = (molecule, lower 128x128 tile) of the molecules whose fp32
+// purification is still running; each molecule's tensor maps are maps[2 slot], maps[2 slot + 1].
+__global__ void __launch_bounds__(128) k_b_square_tf32x3(BatchList L, const MolDesc *__restrict__ D,
+                                                         const MolCtl *__restrict__ Cc,
+                                                         const CUtensorMap *__restrict__ maps, int *error) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  const int item = blockIdx.x;
+  const int m = batch_find(L, item);
+  const int slot = L.slot[m];
+  if (Cc[slot].sp2_state != 0) return;
+  int bm, bn;
+  lower_tile(item - L.prefix[m], bm, bn);
+  const MolDesc &d = D[slot];
+  square_tile(bm, bn, &maps[2 * slot], &maps[2 * slot + 1], d.g.nao, d.ld32, d.C32, error, smem_raw);
+}
+
+// X32 = fp32 of the (fp64) SP2 start X, and its split. Item = a chunk.
+__global__ void __launch_bounds__(256) k_b_to32(BatchList L, const MolDesc *__restrict__ D) {
+  const ChunkRef r = chunk_ref(L, D, blockIdx.x);
+  const MolDesc &d = D[r.slot];
+  const int n = d.g.nao, ld = d.ld32;
+  for (size_t e = r.e0 + threadIdx.x; e < r.e1; e += 256) {
+    const size_t i = e / n, j = e - i * n, q = i * ld + j;
+    const float x = (float)d.X[e];
+    d.X32[q] = x;
+    split_store(x, d.hi32, d.lo32, q);
+  }
+}
+
+// One fp32 SP2 decision (block per molecule): as the fp64 one, with the fp32 rounding
+// floor (idempotency error stalls below 1e-2 n_occ) and trace tolerance (1e-2 n_occ).
+__global__ void __launch_bounds__(256) k_b_sp2_decide32(BatchList L, const MolDesc *__restrict__ D,
+                                                        MolCtl *__restrict__ C, unsigned char *__restrict__ flags) {
+  const int m = blockIdx.x;
+  const int slot = L.slot[m];
+  const MolDesc &d = D[slot];
+  MolCtl &c = C[slot];
+  if (c.sp2_state != 0) {
+    if (threadIdx.x == 0) c.sp2_apply = 0;
+    return;
+  }
+  const int n = d.g.nao, ld = d.ld32;
+  __shared__ double sa[8], sb[8];
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) {
+    a += (double)d.X32[(size_t)i * ld + i];
+    b += (double)d.C32[(size_t)i * ld + i];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sa[threadIdx.x >> 5] = a;
+    sb[threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a = 0.0;
+    b = 0.0;
+    for (int w = 0; w < 8; ++w) {
+      a += sa[w];
+      b += sb[w];
+    }
+    const double nocc = (double)d.n_occ, scale = fmax(1.0, nocc);
+    c.sp2_square = fabs(b - nocc) < fabs(2.0 * a - b - nocc) ? 1 : 0;
+    const double e = a - b;
+    const int k = c.sp2_steps;
+    int state = 0;
+    if (!isfinite(e)) {
+      state = 2;
+    } else if (fabs(e) <= 1.0e-6 * scale) {
+      state = 1;
+    } else if (k >= 2 && fabs(e) < 1.0e-2 * scale && fabs(e) >= fabs(c.sp2_err[(k + 1) % 3])) {
+      state = 1;  // at the fp32 rounding floor
+    } else if (k + 1 >= 100) {
+      state = 2;
+    }
+    if (state == 1 && fabs(a - nocc) > 1.0e-2 * scale) state = 2;
+    c.sp2_err[k % 3] = e;
+    c.sp2_steps = k + 1;
+    c.sp2_state = state;
+    c.sp2_apply = 1;
+    flags[m] = (unsigned char)state;
+  }
+}
+
+// X32 <- X^2 or 2X - X^2 and its split for the molecules decided this step; Pn = 2 X
+// (fp64) for those that finished. Item = a chunk.
+__global__ void __launch_bounds__(256) k_b_sp2_apply32(BatchList L, const MolDesc *__restrict__ D,
+                                                       const MolCtl *__restrict__ C) {
+  const ChunkRef r = chunk_ref(L, D, blockIdx.x);
+  const MolDesc &d = D[r.slot];
+  const MolCtl &c = C[r.slot];
+  if (!c.sp2_apply) return;
+  const bool sq = c.sp2_square != 0, fin = c.sp2_state == 1;
+  const int n = d.g.nao, ld = d.ld32;
+  for (size_t e = r.e0 + threadIdx.x; e < r.e1; e += 256) {
+    const size_t i = e / n, j = e - i * n, q = i * ld + j;
+    const float x2 = d.C32[q];
+    const float x = sq ? x2 : 2.0f * d.X32[q] - x2;
+    d.X32[q] = x;
+    split_store(x, d.hi32, d.lo32, q);
+    if (fin) d.Pn[e] = 2.0 * (double)x;
+  }
+}
+
+}  // namespace
+
+void launch_b_square_tf32x3(cudaStream_t st, const BatchList &L, const MolDesc *D, const MolCtl *C, const void *maps,
+                            int *error) {
+  if (L.total <= 0) return;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_b_square_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    attr = true;
+  }
+  k_b_square_tf32x3<<<L.total, 128, SMEM_BYTES, st>>>(L, D, C, reinterpret_cast<const CUtensorMap *>(maps), error);
+  note_launch();
+}
+
+void launch_b_to32(cudaStream_t st, const BatchList &L, const MolDesc *D) {
+  if (L.total <= 0) return;
+  k_b_to32<<<L.total, 256, 0, st>>>(L, D);
+  note_launch();
+}
+
+void launch_b_sp2_decide32(cudaStream_t st, const BatchList &L, const MolDesc *D, MolCtl *C, unsigned char *flags) {
+  if (L.n <= 0) return;
+  k_b_sp2_decide32<<<L.n, 256, 0, st>>>(L, D, C, flags);
+  note_launch();
+}
+
+void launch_b_sp2_apply32(cudaStream_t st, const BatchList &L, const MolDesc *D, const MolCtl *C) {
+  if (L.total <= 0) return;
+  k_b_sp2_apply32<<<L.total, 256, 0, st>>>(L, D, C);
   note_launch();
 }
 

@@ -153,3 +153,33 @@ def test_batch_takes_the_single_path_iterations(golden):
         (r,) = api.run_batch([(z, x)])
         s = api.run_pm7(z, x)
         assert abs(r["iterations"] - s["iterations"]) <= 1, (name, r["iterations"], s["iterations"])
+
+
+def test_batch_mixed_precision_within_tolerance():
+    # fp32 purification cycles on the grouped tcgen05 squaring, fp64 cycles to finish:
+    # heat of formation within 1e-4 kcal/mol of the fp64 batch, charges within 1e-5 e
+    mols = [G.water_cluster(k, seed=k) for k in (20, 45, 64)] + [G.alkane(n, seed=n) for n in (17, 30, 40)]
+    mols += [G.water_cluster(5, seed=1), G.alkane(3, seed=2)]  # below the SP2 size: unaffected
+    f64 = api.run_batch(mols)
+    mix = api.run_batch(mols, precision=1)
+    for i, (a, b) in enumerate(zip(f64, mix)):
+        assert abs(a["heat_of_formation_kcal"] - b["heat_of_formation_kcal"]) < 1.0e-4, i
+        assert np.max(np.abs(a["charges"] - b["charges"])) < 1.0e-5, i
+    assert all(b["fp32_iterations"] > 0 for b in mix[:6])
+    assert all(b["fp32_iterations"] == 0 for b in mix[6:])
+    z, x = mols[2]
+    o = harness.run(z, x)
+    assert abs(mix[2]["heat_of_formation_kcal"] - o["heat_of_formation_kcal"]) < 1.0e-4
+
+
+def test_mixed_precision_large_chain_leaves_the_fp32_phase():
+    # a 300+-atom S/Cl chain: the commutator norm stalls at the fp32 floor while the density
+    # step is already small; the switch to fp64 must still happen and the SCF converge
+    rng = np.random.default_rng(5)
+    z, x = G.substituted_chain(110, rng)
+    f = api.run_pm7(z, x, want_matrices=0)
+    (b,) = api.run_batch([(z, x)], want_matrices=0, precision=1)
+    s = api.run_pm7(z, x, want_matrices=0, precision=1)
+    for r in (b, s):
+        assert 0 < r["fp32_iterations"] < r["iterations"]
+        assert abs(r["heat_of_formation_kcal"] - f["heat_of_formation_kcal"]) < 1.0e-4
