@@ -256,6 +256,11 @@ def run_b200(args, world, rank, local):
     z, x, desc = workload(args.workload)
     n_atoms, nao = len(z), nao_of(z)
     opts = dict(device=local, want_matrices=0)
+    if args.precision == "mixed":
+        # the mixed-precision solve is the timed one (fp32 tcgen05 cycles, fp64 refinement)
+        opts["precision"] = 1
+        desc = desc.replace("RHF FP64", "RHF mixed precision")
+        args.no_mixed = True
     for _ in range(args.warmup):
         api.run_pm7(z, x, **opts)
     peaks = measured_peaks()
@@ -279,6 +284,38 @@ def run_b200(args, world, rank, local):
     launches = api.launch_count() - launches0
     prof = api.profile_read()
     api.profile_enable(False)
+    # the same solve in mixed precision: fp32 purification cycles on tcgen05, fp64 refinement
+    mixed = None
+    if not args.no_mixed:
+        api.run_pm7(z, x, precision=1, **opts)
+        api.profile_enable(True)
+        mdev, mres = 0.0, []
+        tm0 = time.perf_counter()
+        for _ in range(args.steps):
+            q = api.run_pm7(z, x, precision=1, **opts)
+            mdev += q["device_ms"]
+            mres.append(q)
+        mwall = time.perf_counter() - tm0
+        mprof = api.profile_read()
+        api.profile_enable(False)
+        mixed = {"value": args.steps / (mdev * 1e-3), "e2e": args.steps / mwall, "unit": "solves/s",
+                 "iterations": mres[-1]["iterations"], "fp32_iterations": mres[-1]["fp32_iterations"],
+                 "dhf_err_vs_fp64_kcal": abs(mres[-1]["heat_of_formation_kcal"] - results[-1]["heat_of_formation_kcal"]),
+                 "max_charge_err_vs_fp64": float(np.max(np.abs(mres[-1]["charges"] - results[-1]["charges"]))),
+                 "stages": {k: {"ms_total": round(v[0], 3), "calls": v[1]} for k, v in mprof.items()}}
+        tf_ms, tf_calls = mprof.get("sp2_square_tf32", (0.0, 0))
+        if tf_calls:
+            ld = ((nao + 31) // 32) * 32
+            t = (nao + 127) // 128
+            flops = 3 * (t * (t + 1) // 2) * 128 * 128 * 2.0 * ld  # issued: 3 MMA products per lower tile
+            alg = 3.0 * float(nao) ** 3                             # algorithmic: 3 symmetric products
+            ach = alg / (tf_ms / tf_calls * 1e-3) / 1e12
+            peak_tf32 = peaks.get("bf16_tflops", 1590.0) / 2.0
+            mixed["roofline"] = {"kernel": "k_square_tf32x3 (tcgen05.mma kind::tf32, TMA, TMEM)", "bound": "tensor",
+                                 "achieved": ach, "peak": peak_tf32, "unit": "TFLOP/s", "frac": ach / peak_tf32,
+                                 "issued_tflops": flops / (tf_ms / tf_calls * 1e-3) / 1e12,
+                                 "ms_avg": tf_ms / tf_calls, "launches": tf_calls,
+                                 "peak_source": "half the measured bf16 dense rate in MEASURED_PEAKS.json (TF32 runs at half the bf16 rate)"}
     clocks = sampler.stop()
     barrier(world)
     dev_s = allreduce_max(dev_ms * 1e-3, world)
@@ -330,7 +367,8 @@ def run_b200(args, world, rank, local):
     line = {
         "metric": "PM7 SCF solves/s (RHF single point)", "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+        "dtype": "f64" if args.precision == "fp64" else "f32 (tcgen05 3xTF32) + f64 refinement",
         "config": {"workload": args.workload, "description": desc, "seed": 0, "n_atoms": n_atoms, "nao": nao,
                    "scf_iterations": r0["iterations"], "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (H, F, P and DIIS history are 32 MB each at nao=2004)"},
@@ -340,6 +378,7 @@ def run_b200(args, world, rank, local):
                        "device_p50": float(np.percentile([q["device_ms"] for q in results], 50))},
         "roofline": roofline,
         "roofline_fock": fock_roof,
+        "mixed_precision": mixed,
         "stages": stages,
         "clocks": clocks,
         "cpu_baseline": cpu,
@@ -515,6 +554,7 @@ def main():
                     help="batch4096/stream: fp64, or fp32 tcgen05 purification cycles with fp64 refinement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-peak", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision solve of the default workload")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU only: rank 0 runs, the other ranks exit without joining a process group

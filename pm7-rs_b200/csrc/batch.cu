@@ -356,7 +356,7 @@ __device__ bool dev_adiis(const MolCtl &c, double *cw) {
 // Record the new entry's inner products and choose this iteration's extrapolation.
 // DIIS error below which a mixed-precision molecule switches to fp64 densities.
 constexpr double kMixedSwitch = 1.0e-3;
-constexpr double kMixedSwitchStep = 1.0e-5;  // rms density step that also ends the fp32 phase
+constexpr double kMixedSwitchStep = 1.0e-6;  // rms density step that also ends the fp32 phase
 
 __global__ void k_b_control(int n, const int *__restrict__ slots, MolCtl *__restrict__ C,
                             unsigned char *__restrict__ use32) {
@@ -946,6 +946,14 @@ class BatchRunner {
     SOLVER_OK(cusolverDnCreateParams(&sparams_));
     CUDA_OK(cudaMalloc((void **)&err32_, sizeof(int)));
     CUDA_OK(cudaMemset(err32_, 0, sizeof(int)));
+    CUDA_OK(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+    for (Side &sd : side_) {
+      CUDA_OK(cudaStreamCreateWithFlags(&sd.st, cudaStreamNonBlocking));
+      SOLVER_OK(cusolverDnCreate(&sd.solver));
+      SOLVER_OK(cusolverDnSetStream(sd.solver, sd.st));
+      CUDA_OK(cudaEventCreateWithFlags(&sd.done, cudaEventDisableTiming));
+      CUDA_OK(cudaMalloc((void **)&sd.info, sizeof(int)));
+    }
     // density of each SCF iteration: SP2 purification from sp2_min_nao_ basis functions up,
     // the eigensolver below; PM7_BATCH_DENSITY=eig|sp2 forces one of them for every molecule
     if (const char *e = std::getenv("PM7_BATCH_DENSITY")) {
@@ -967,6 +975,15 @@ class BatchRunner {
     if (out_d_) cudaFree(out_d_);
     if (maps_) cudaFree(maps_);
     if (err32_) cudaFree(err32_);
+    for (Side &sd : side_) {
+      if (sd.st) cudaStreamSynchronize(sd.st);
+      if (sd.work) cudaFree(sd.work);
+      if (sd.info) cudaFree(sd.info);
+      if (sd.solver) cusolverDnDestroy(sd.solver);
+      if (sd.done) cudaEventDestroy(sd.done);
+      if (sd.st) cudaStreamDestroy(sd.st);
+    }
+    if (fork_) cudaEventDestroy(fork_);
     cusolverDnDestroyParams(sparams_);
     cusolverDnDestroy(solver_);
     cudaStreamDestroy(st_);
@@ -1408,18 +1425,31 @@ class BatchRunner {
         CUDA_OK(cudaMallocAsync((void **)&info_, sizeof(int) * info_cap_, st_));
       }
       if (np >= 512) {
+        // divide and conquer per matrix, spread over the side streams so that several run
+        // at once (one alone leaves most of the GPU idle)
         int lwork = 0;
         SOLVER_OK(cusolverDnDsyevd_bufferSize(solver_, jobz, CUBLAS_FILL_MODE_LOWER, np, in, np, w, &lwork));
         const size_t wd = sizeof(double) * (size_t)lwork;
-        if (wd > work_cap_) {
-          if (work_) CUDA_OK(cudaFreeAsync(work_, st_));
-          work_cap_ = wd + wd / 4;
-          CUDA_OK(cudaMallocAsync(&work_, work_cap_, st_));
+        CUDA_OK(cudaEventRecord(fork_, st_));
+        const int used = std::min(cnt, kSide);
+        for (int k = 0; k < used; ++k) {
+          Side &sd = side_[k];
+          CUDA_OK(cudaStreamWaitEvent(sd.st, fork_, 0));
+          if (wd > sd.cap) {
+            if (sd.work) CUDA_OK(cudaFreeAsync(sd.work, sd.st));
+            sd.cap = wd + wd / 4;
+            CUDA_OK(cudaMallocAsync(&sd.work, sd.cap, sd.st));
+          }
         }
         for (int i = 0; i < cnt; ++i) {
           const EigSlot &e = A.eig_h[kv.second[i]];
-          SOLVER_OK(cusolverDnDsyevd(solver_, jobz, CUBLAS_FILL_MODE_LOWER, np, e.in, np, e.eps, (double *)work_,
-                                     lwork, info_ + i));
+          Side &sd = side_[i % used];
+          SOLVER_OK(cusolverDnDsyevd(sd.solver, jobz, CUBLAS_FILL_MODE_LOWER, np, e.in, np, e.eps, (double *)sd.work,
+                                     lwork, sd.info));
+        }
+        for (int k = 0; k < used; ++k) {
+          CUDA_OK(cudaEventRecord(side_[k].done, side_[k].st));
+          CUDA_OK(cudaStreamWaitEvent(st_, side_[k].done, 0));
         }
         continue;
       }
@@ -1561,6 +1591,18 @@ class BatchRunner {
   unsigned char *maps_ = nullptr;      // 2 CUtensorMap (128 B each) per slot
   std::vector<unsigned char> map_stage_;
   int *err32_ = nullptr;               // set by the tcgen05 squaring when a wait expired
+  // side streams for the large eigendecompositions
+  static constexpr int kSide = 4;
+  struct Side {
+    cudaStream_t st = nullptr;
+    cusolverDnHandle_t solver = nullptr;
+    cudaEvent_t done = nullptr;
+    void *work = nullptr;
+    size_t cap = 0;
+    int *info = nullptr;
+  };
+  Side side_[kSide];
+  cudaEvent_t fork_ = nullptr;
   double *arena_ = nullptr;
   size_t arena_cap_ = 0;
   void *work_ = nullptr;

@@ -464,7 +464,7 @@ struct Purifier {
 // be forced with PM7_DENSITY_SOLVER=sp2|syevd.
 // DIIS error below which the mixed-precision SCF switches to fp64 densities.
 static constexpr double kMixedSwitch = 1.0e-3;
-static constexpr double kMixedSwitchStep = 1.0e-5;  // rms density step that also ends the fp32 phase
+static constexpr double kMixedSwitchStep = 1.0e-6;  // rms density step that also ends the fp32 phase
 
 static bool use_sp2(int n) {
   const char *env = std::getenv("PM7_DENSITY_SOLVER");
