@@ -278,6 +278,16 @@ int32_t pm7_corrections_noalloc_max_atoms(void);
 pm7_status pm7_run_batch(int32_t n_molecules, const pm7_molecule *molecules, const pm7_params *params,
                          const pm7_options *options, pm7_result *results, pm7_status *statuses);
 
+/* Splits a batch over n_ranks GPUs (or processes) for independent pm7_run_batch calls:
+ * greedy longest-processing-time by an estimated cost per molecule (a constant per
+ * solve + nao^3 for the dense SCF work + 1000 per atom pair for the integrals), heaviest
+ * first, each to the least loaded rank (ties: lowest index). rank_of[i] receives the
+ * rank of molecule i; rank_cost (n_ranks entries, may be NULL) the summed cost per rank.
+ * Host only: needs no device. Deterministic for equal inputs. Molecules whose elements
+ * have no parameters count with one orbital per atom (their solve fails at once). */
+pm7_status pm7_batch_partition(int32_t n_molecules, const pm7_molecule *molecules, int32_t method,
+                               int32_t n_ranks, int32_t *rank_of, double *rank_cost);
+
 /* A serving engine: a worker thread on one GPU admits submitted closed-shell RHF
  * requests as HBM (their device footprint against hbm_budget_mb, or 80% of free
  * memory when -1) and max_active (0 = unlimited) allow, advances all admitted

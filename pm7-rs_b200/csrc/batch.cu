@@ -1797,6 +1797,47 @@ pm7_status pm7_run_batch(int32_t n_molecules, const pm7_molecule *molecules, con
   }
 }
 
+pm7_status pm7_batch_partition(int32_t n_molecules, const pm7_molecule *molecules, int32_t method, int32_t n_ranks,
+                               int32_t *rank_of, double *rank_cost) {
+  try {
+    if (n_molecules < 0 || n_ranks < 1 || (n_molecules > 0 && (!molecules || !rank_of)))
+      throw Failure{PM7_ERR_INVALID_INPUT, "pm7_batch_partition: bad counts or null arrays"};
+    if (method < 0 || method > 4) throw Failure{PM7_ERR_INVALID_INPUT, "unknown PM7 method"};
+    const ParamSet &ps = param_set(method);
+    std::vector<double> cost(n_molecules);
+    for (int i = 0; i < n_molecules; ++i) {
+      const pm7_molecule &m = molecules[i];
+      if (m.n_atoms < 0 || (m.n_atoms > 0 && !m.z))
+        throw Failure{PM7_ERR_INVALID_INPUT, "pm7_batch_partition: molecule " + std::to_string(i) + " is malformed"};
+      double nao = 0;
+      for (int a = 0; a < m.n_atoms; ++a) {
+        const ElementRec *e = ps.element(m.z[a]);
+        nao += e ? e->n_orb : 1;
+      }
+      const double pairs = 0.5 * (double)m.n_atoms * (double)(m.n_atoms - 1 > 0 ? m.n_atoms - 1 : 0);
+      cost[i] = 2.0e5 + nao * nao * nao + 1.0e3 * pairs;
+    }
+    std::vector<int> order(n_molecules);
+    for (int i = 0; i < n_molecules; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<double> load(n_ranks, 0.0);
+    for (int i : order) {
+      int best = 0;
+      for (int r = 1; r < n_ranks; ++r)
+        if (load[r] < load[best]) best = r;
+      rank_of[i] = best;
+      load[best] += cost[i];
+    }
+    if (rank_cost)
+      for (int r = 0; r < n_ranks; ++r) rank_cost[r] = load[r];
+    g_last_error.clear();
+    return PM7_OK;
+  } catch (const Failure &f) {
+    g_last_error = f.msg;
+    return f.code;
+  }
+}
+
 void pm7_engine_config_default(pm7_engine_config *c) {
   if (!c) return;
   c->device = 0;

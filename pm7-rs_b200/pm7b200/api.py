@@ -22,7 +22,7 @@ EXPORTED = [
     "pm7_params_load", "pm7_options_default", "pm7_run", "pm7_result_free", "pm7_last_error_message",
     "pm7_device_count", "pm7_stage_core_hamiltonian", "pm7_stage_fock", "pm7_stage_pair", "pm7_stage_core_core",
     "pm7_stage_corrections", "pm7_run_batch", "pm7_engine_config_default", "pm7_engine_create", "pm7_engine_submit",
-    "pm7_engine_poll", "pm7_engine_destroy",
+    "pm7_engine_poll", "pm7_engine_destroy", "pm7_batch_partition",
 ]
 
 
@@ -30,6 +30,11 @@ class Pm7Error(RuntimeError):
     def __init__(self, code, message):
         super().__init__(f"{abi.STATUS_NAMES.get(code, code)}: {message}")
         self.code = code
+        self.message = message
+
+    def __reduce__(self):
+        # results travel between ranks by pickling (host-side gather of a sharded batch)
+        return (Pm7Error, (self.code, self.message))
 
 
 def lib():
@@ -56,6 +61,8 @@ def lib():
     L.pm7_abi_sizes.argtypes = [C.POINTER(C.c_int64)]
     L.pm7_run_batch.argtypes = [C.c_int32, C.POINTER(abi.Molecule), C.c_void_p, C.POINTER(abi.Options),
                                 C.POINTER(abi.Result), C.POINTER(C.c_int32)]
+    L.pm7_batch_partition.argtypes = [C.c_int32, C.POINTER(abi.Molecule), C.c_int32, C.c_int32,
+                                      C.POINTER(C.c_int32), C.POINTER(C.c_double)]
     L.pm7_engine_config_default.argtypes = [C.POINTER(abi.EngineConfig)]
     L.pm7_engine_create.argtypes = [C.POINTER(abi.EngineConfig), C.POINTER(C.c_void_p)]
     L.pm7_engine_submit.argtypes = [C.c_void_p, C.POINTER(abi.Molecule), C.POINTER(abi.Options),
@@ -259,6 +266,21 @@ def run_batch(molecules, options=None, **common):
             out.append(Pm7Error(st[i], "batched solve failed"))
         lib().pm7_result_free(C.byref(res[i]))
     return out
+
+
+def batch_partition(molecules, n_ranks, method=0):
+    """Longest-processing-time split of a batch over `n_ranks` (`pm7_batch_partition`).
+
+    Returns (rank_of, rank_cost): the rank of each molecule and the estimated cost each
+    rank carries. Host only; needs no GPU.
+    """
+    n = len(molecules)
+    mols = [_Mol(z, x) for z, x in molecules]
+    ms = (abi.Molecule * max(n, 1))(*[m.s for m in mols])
+    owner = (C.c_int32 * max(n, 1))()
+    load = (C.c_double * max(int(n_ranks), 1))()
+    _check(lib().pm7_batch_partition(n, ms, int(method), int(n_ranks), owner, load))
+    return np.array(owner[:n], dtype=np.int32), np.array(load[:n_ranks])
 
 
 class Engine:
