@@ -342,7 +342,7 @@ def run_b200(args, world, rank, local):
         traffic = None
         if sq_traffic is not None and cm_traffic is not None:
             traffic = (sq_calls * sq_traffic + cm_calls * cm_traffic) / launches_g
-        roofline = {"kernel": "k_gemm_tn (FP64 DMMA mma.sync.m8n8k4)", "bound": "tensor", "achieved": achieved,
+        roofline = {"kernel": "k_gemm_tn (FP64 DMMA mma.sync.m16n8k8)", "bound": "tensor", "achieved": achieved,
                     "peak": dgemm, "unit": "TFLOP/s", "frac": (achieved / dgemm) if dgemm else None,
                     "traffic": traffic, "launches": launches_g, "ms_avg": gemm_ms / launches_g,
                     "algorithmic_per_launch": f"{flops / launches_g:.4g} flop (SP2 square nao^3, commutator 2 nao^3)",

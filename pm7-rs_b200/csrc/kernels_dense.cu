@@ -12,16 +12,28 @@ namespace pm7 {
 
 // ---------------------------------------------------------------------------
 // FP64 tensor-core GEMM, C = alpha * A^T * B (A: K x M, B: K x N, both row-major).
-// mma.sync m8n8k4 (DMMA) is the FP64 tensor-core instruction on sm_100a; tcgen05
-// has no FP64 kind. 64x64x16 block tiles, 4 warps of 32x32, two-stage cp.async.
+// DMMA (mma.sync .f64, here the m16n8k8 shape) is the FP64 tensor-core instruction on
+// sm_100a; tcgen05 has no FP64 kind. 64x64x16 block tiles, 4 warps of 32x32, a
+// three-stage cp.async ring in dynamic shared memory. Shared rows are 68 doubles long
+// so the fragment loads of a half-warp (4 k-rows x 4 columns) hit 16 distinct bank
+// pairs; tiles move in 16-byte copies when the leading dimensions are even and the
+// bases 16-byte aligned, else in 8-byte copies. Out-of-range elements are zero-filled
+// by the copy itself, so K and M/N edges need no separate masking.
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int BM = 64, BN = 64, BK = 16, PADW = 8;
+constexpr int BM = 64, BN = 64, BK = 16, LDS = 68, STAGES = 3;
+constexpr int STAGE_DOUBLES = 2 * BK * LDS;                    // A and B tiles of one stage
+constexpr int GEMM_SMEM = STAGES * STAGE_DOUBLES * 8;          // 52,224 bytes
 
 __device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
   const int bytes = pred ? 8 : 0;
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+// 16-byte copy of `bytes` (0, 8 or 16) source bytes, the rest of the 16 zero-filled
+__device__ __forceinline__ void cp_async16(double *smem, const double *gmem, int bytes) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
@@ -29,78 +41,116 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
+// D(16x8) += A(16x8) B(8x8), fragments as the PTX ISA lays out .f64 m16n8k8:
+// a0 (g, t) a1 (g+8, t) a2 (g, t+4) a3 (g+8, t+4); b0 (t, g) b1 (t+4, g);
+// d0 (g, 2t) d1 (g, 2t+1) d2 (g+8, 2t) d3 (g+8, 2t+1), g = lane/4, t = lane%4.
+__device__ __forceinline__ void dmma16x8x8(double *d, const double *a, const double *b) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+               "{%0,%1,%2,%3};\n"
+               : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+               : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
-}  // namespace
 
-// sym != 0: only tiles with bm >= bn are computed; the lower triangle is written and
-// mirrored, so the output is exactly symmetric (used for P = w V^T V).
-__device__ __forceinline__ void gemm_tile(int bm, int bn, int M, int N, int K, double alpha,
-                                          const double *__restrict__ A, int lda, const double *__restrict__ B, int ldb,
-                                          double *__restrict__ C, int ldc, int sym) {
-  __shared__ __align__(16) double As[2][BK][BM + PADW];
-  __shared__ __align__(16) double Bs[2][BK][BN + PADW];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 1, wn = warp & 1;
-  const int g = lane >> 2, t = lane & 3;
-  const int m0 = bm * BM, n0 = bn * BN;
-  double acc[4][4][2];
+template <bool VEC>
+__device__ __forceinline__ void load_stage(double *sA, double *sB, int k0, int m0, int n0, int M, int N, int K,
+                                           const double *__restrict__ A, int lda, const double *__restrict__ B,
+                                           int ldb) {
+  const int tid = threadIdx.x;
+  if (VEC) {
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-  auto load_tile = [&](int stage, int k0) {
+    for (int i = 0; i < 4; ++i) {
+      const int e = tid + 128 * i, row = e >> 5, col = (e & 31) * 2;
+      const int kr = k0 + row;
+      const int ra = kr < K ? min(max(M - (m0 + col), 0), 2) * 8 : 0;
+      const int rb = kr < K ? min(max(N - (n0 + col), 0), 2) * 8 : 0;
+      cp_async16(sA + row * LDS + col, ra ? A + (size_t)kr * lda + m0 + col : A, ra);
+      cp_async16(sB + row * LDS + col, rb ? B + (size_t)kr * ldb + n0 + col : B, rb);
+    }
+  } else {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       const int e = tid + 128 * i, row = e >> 6, col = e & 63;
       const int kr = k0 + row;
       const bool pa = kr < K && (m0 + col) < M;
       const bool pb = kr < K && (n0 + col) < N;
-      cp_async8(&As[stage][row][col], pa ? A + (size_t)kr * lda + m0 + col : A, pa);
-      cp_async8(&Bs[stage][row][col], pb ? B + (size_t)kr * ldb + n0 + col : B, pb);
+      cp_async8(sA + row * LDS + col, pa ? A + (size_t)kr * lda + m0 + col : A, pa);
+      cp_async8(sB + row * LDS + col, pb ? B + (size_t)kr * ldb + n0 + col : B, pb);
     }
-    cp_async_commit();
-  };
-
-  const int ktiles = (K + BK - 1) / BK;
-  if (ktiles > 0) load_tile(0, 0);
-  for (int kt = 0; kt < ktiles; ++kt) {
-    const int stage = kt & 1;
-    if (kt + 1 < ktiles) {
-      load_tile(stage ^ 1, (kt + 1) * BK);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < BK; kk += 4) {
-      double a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[stage][kk + t][wm * 32 + i * 8 + g];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[stage][kk + t][wn * 32 + j * 8 + g];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-    }
-    __syncthreads();
   }
+}
+}  // namespace
+
+// sym != 0: only tiles with bm >= bn are computed; the lower triangle is written and
+// mirrored, so the output is exactly symmetric (used for P = w V^T V and X X).
+template <bool VEC>
+__device__ __forceinline__ void gemm_tile_impl(double *smem, int bm, int bn, int M, int N, int K, double alpha,
+                                               const double *__restrict__ A, int lda, const double *__restrict__ B,
+                                               int ldb, double *__restrict__ C, int ldc, int sym) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int g = lane >> 2, t = lane & 3;
+  const int m0 = bm * BM, n0 = bn * BN;
+  double acc[2][4][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int m = m0 + wm * 32 + i * 8 + g;
-        const int n = n0 + wn * 32 + j * 8 + 2 * t + h;
+      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+
+  const int ktiles = (K + BK - 1) / BK;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < ktiles)
+      load_stage<VEC>(smem + s * STAGE_DOUBLES, smem + s * STAGE_DOUBLES + BK * LDS, s * BK, m0, n0, M, N, K, A, lda,
+                      B, ldb);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < ktiles; ++kt) {
+    cp_async_wait<STAGES - 2>();  // tile kt has landed (this thread's copies)
+    __syncthreads();              // ... everyone's, and stage (kt - 1) % STAGES is free
+    const int pf = kt + STAGES - 1;
+    if (pf < ktiles) {
+      double *s = smem + (pf % STAGES) * STAGE_DOUBLES;
+      load_stage<VEC>(s, s + BK * LDS, pf * BK, m0, n0, M, N, K, A, lda, B, ldb);
+    }
+    cp_async_commit();
+    const double *sA = smem + (kt % STAGES) * STAGE_DOUBLES;
+    const double *sB = sA + BK * LDS;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 8) {
+      double a[2][4], b[4][2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const double *pa = sA + (kk + t) * LDS + wm * 32 + i * 16 + g;
+        a[i][0] = pa[0];
+        a[i][1] = pa[8];
+        a[i][2] = pa[4 * LDS];
+        a[i][3] = pa[4 * LDS + 8];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double *pb = sB + (kk + t) * LDS + wn * 32 + j * 8 + g;
+        b[j][0] = pb[0];
+        b[j][1] = pb[4 * LDS];
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma16x8x8(acc[i][j], a[i], b[j]);
+    }
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int m = m0 + wm * 32 + i * 16 + g + (q >> 1) * 8;
+        const int n = n0 + wn * 32 + j * 8 + 2 * t + (q & 1);
         if (m >= M || n >= N) continue;
-        const double v = alpha * acc[i][j][h];
+        const double v = alpha * acc[i][j][q];
         if (!sym) {
           C[(size_t)m * ldc + n] = v;
         } else if (m >= n) {
@@ -110,19 +160,34 @@ __device__ __forceinline__ void gemm_tile(int bm, int bn, int M, int N, int K, d
       }
 }
 
-__global__ void __launch_bounds__(128) k_gemm_tn(int M, int N, int K, double alpha, const double *__restrict__ A,
+__device__ __forceinline__ bool gemm_vec_ok(const double *A, int lda, const double *B, int ldb) {
+  return ((lda | ldb) & 1) == 0 && ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) == 0;
+}
+
+__device__ __forceinline__ void gemm_tile(double *smem, int bm, int bn, int M, int N, int K, double alpha,
+                                          const double *__restrict__ A, int lda, const double *__restrict__ B, int ldb,
+                                          double *__restrict__ C, int ldc, int sym) {
+  if (gemm_vec_ok(A, lda, B, ldb))
+    gemm_tile_impl<true>(smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym);
+  else
+    gemm_tile_impl<false>(smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym);
+}
+
+__global__ void __launch_bounds__(128, 4) k_gemm_tn(int M, int N, int K, double alpha, const double *__restrict__ A,
                                                  int lda, const double *__restrict__ B, int ldb,
                                                  double *__restrict__ C, int ldc, int sym) {
+  extern __shared__ __align__(16) double gemm_smem[];
   const int bn = blockIdx.x, bm = blockIdx.y;
   if (sym && bm < bn) return;
-  gemm_tile(bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym);
+  gemm_tile(gemm_smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym);
 }
 
 // Grouped over molecules: item = one 64x64 tile of one molecule's product.
 // op 0: X = F_slot P (F symmetric, so F^T P = F P), all tiles.
 // op 1: Pn = 2 V_occ^T V_occ from this iteration's eigenvectors, lower tiles mirrored.
-__global__ void __launch_bounds__(128) k_b_gemm(BatchList L, const MolDesc *__restrict__ D,
+__global__ void __launch_bounds__(128, 4) k_b_gemm(BatchList L, const MolDesc *__restrict__ D,
                                                 const MolCtl *__restrict__ Cc, const EigSlot *__restrict__ E, int op) {
+  extern __shared__ __align__(16) double gemm_smem[];
   const int item = blockIdx.x;
   const int m = batch_find(L, item);
   const int slot = L.slot[m];
@@ -131,26 +196,39 @@ __global__ void __launch_bounds__(128) k_b_gemm(BatchList L, const MolDesc *__re
   const int local = item - L.prefix[m];
   if (op == 0) {
     const int bm = local / tiles, bn = local - bm * tiles;
-    gemm_tile(bm, bn, n, n, n, 1.0, hist_F(d, Cc[slot].slot), n, d.P, n, d.X, n, 0);
+    gemm_tile(gemm_smem, bm, bn, n, n, n, 1.0, hist_F(d, Cc[slot].slot), n, d.P, n, d.X, n, 0);
   } else {
     int bm = 0;
     while ((bm + 1) * (bm + 2) / 2 <= local) ++bm;
     const int bn = local - bm * (bm + 1) / 2;
-    if (op == 1) gemm_tile(bm, bn, n, n, d.n_occ, 2.0, E[m].in, E[m].ldv, E[m].in, E[m].ldv, d.Pn, n, 1);
-    else if (Cc[slot].sp2_state == 0) gemm_tile(bm, bn, n, n, n, 1.0, d.X, n, d.X, n, d.Pn, n, 1);
+    if (op == 1) gemm_tile(gemm_smem, bm, bn, n, n, d.n_occ, 2.0, E[m].in, E[m].ldv, E[m].in, E[m].ldv, d.Pn, n, 1);
+    else if (Cc[slot].sp2_state == 0) gemm_tile(gemm_smem, bm, bn, n, n, n, 1.0, d.X, n, d.X, n, d.Pn, n, 1);
   }
+}
+
+// Opt the GEMM kernels in to more than 48 KB of dynamic shared memory (once per device).
+static void gemm_smem_attr() {
+  static bool done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || done[dev]) return;
+  cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
+  cudaFuncSetAttribute(k_b_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
+  done[dev] = true;
 }
 
 void launch_b_gemm(cudaStream_t st, const BatchList &L, const MolDesc *D, const MolCtl *C, const EigSlot *E, int op) {
   if (L.total <= 0) return;
-  k_b_gemm<<<L.total, 128, 0, st>>>(L, D, C, E, op);
+  gemm_smem_attr();
+  k_b_gemm<<<L.total, 128, GEMM_SMEM, st>>>(L, D, C, E, op);
   note_launch();
 }
 
 void launch_gemm_tn(cudaStream_t st, int M, int N, int K, double alpha, const double *A, int lda, const double *B,
                     int ldb, double *C, int ldc) {
   dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-  k_gemm_tn<<<grid, 128, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc, 0);
+  gemm_smem_attr();
+  k_gemm_tn<<<grid, 128, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc, 0);
   note_launch();
 }
 
@@ -160,7 +238,8 @@ void launch_density(cudaStream_t st, int n, int k, double w, const double *V, in
     return;
   }
   dim3 grid((n + BN - 1) / BN, (n + BM - 1) / BM);
-  k_gemm_tn<<<grid, 128, 0, st>>>(n, n, k, w, V, ldv, V, ldv, P, n, 1);
+  gemm_smem_attr();
+  k_gemm_tn<<<grid, 128, GEMM_SMEM, st>>>(n, n, k, w, V, ldv, V, ldv, P, n, 1);
   note_launch();
 }
 
@@ -489,7 +568,8 @@ void launch_sp2_init(cudaStream_t st, int n, const double *F, const double *boun
 
 void launch_sp2_square(cudaStream_t st, int n, const double *X, double *X2) {
   dim3 grid((n + BN - 1) / BN, (n + BM - 1) / BM);
-  k_gemm_tn<<<grid, 128, 0, st>>>(n, n, n, 1.0, X, n, X, n, X2, n, 1);
+  gemm_smem_attr();
+  k_gemm_tn<<<grid, 128, GEMM_SMEM, st>>>(n, n, n, 1.0, X, n, X, n, X2, n, 1);
   note_launch();
 }
 
