@@ -326,7 +326,7 @@ def run_b200(args, world, rank, local):
     value = total / dev_s
     e2e = total / wall
     r0 = results[-1]
-    # dominant kernel of ours and its roofline: the FP64 DMMA GEMM (k_gemm_tn), timed per
+    # dominant kernels of ours and their roofline: the FP64 DMMA GEMMs (k_gemm_sym, k_gemm_tn), timed per
     # launch with CUDA events on the engine's stream
     stages = {k: {"ms_total": round(v[0], 3), "calls": v[1], "ms_avg": round(v[0] / max(v[1], 1), 4)}
               for k, v in prof.items()}
@@ -342,7 +342,7 @@ def run_b200(args, world, rank, local):
         traffic = None
         if sq_traffic is not None and cm_traffic is not None:
             traffic = (sq_calls * sq_traffic + cm_calls * cm_traffic) / launches_g
-        roofline = {"kernel": "k_gemm_tn (FP64 DMMA mma.sync.m16n8k8)", "bound": "tensor", "achieved": achieved,
+        roofline = {"kernel": "k_gemm_sym (SP2 squares) + k_gemm_tn (F.P), FP64 DMMA mma.sync.m16n8k8", "bound": "tensor", "achieved": achieved,
                     "peak": dgemm, "unit": "TFLOP/s", "frac": (achieved / dgemm) if dgemm else None,
                     "traffic": traffic, "launches": launches_g, "ms_avg": gemm_ms / launches_g,
                     "algorithmic_per_launch": f"{flops / launches_g:.4g} flop (SP2 square nao^3, commutator 2 nao^3)",

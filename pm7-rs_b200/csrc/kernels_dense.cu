@@ -2,6 +2,7 @@
 // P = w V_occ^T V_occ and the DIIS commutator F P) and the HBM-bound reductions
 // around them. All reductions write fixed per-block partials that are summed in a
 // fixed order, so results are bitwise reproducible.
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -13,17 +14,29 @@ namespace pm7 {
 // ---------------------------------------------------------------------------
 // FP64 tensor-core GEMM, C = alpha * A^T * B (A: K x M, B: K x N, both row-major).
 // DMMA (mma.sync .f64, here the m16n8k8 shape) is the FP64 tensor-core instruction on
-// sm_100a; tcgen05 has no FP64 kind. 64x64x16 block tiles, 4 warps of 32x32, a
-// three-stage cp.async ring in dynamic shared memory. Shared rows are 68 doubles long
-// so the fragment loads of a half-warp (4 k-rows x 4 columns) hit 16 distinct bank
-// pairs; tiles move in 16-byte copies when the leading dimensions are even and the
-// bases 16-byte aligned, else in 8-byte copies. Out-of-range elements are zero-filled
-// by the copy itself, so K and M/N edges need no separate masking.
+// sm_100a; tcgen05 has no FP64 kind. Block tiles BM x BN x 16 over 4 warps, a
+// three-stage cp.async ring in dynamic shared memory. Shared rows are BM + 4 (BN + 4)
+// doubles long, so the fragment loads of a half-warp (4 k-rows x 4 columns) hit 16
+// distinct bank pairs; tiles move in 16-byte copies when the leading dimensions are
+// even and the bases 16-byte aligned, else in 8-byte copies. Out-of-range elements are
+// zero-filled by the copy itself, so K and M/N edges need no separate masking.
+// Two shapes: 64x64 (warp tile 32x32, four CTAs per SM) for full products, and 128x64
+// (warp tile 64x32, two CTAs per SM) over an enumerated lower triangle for symmetric
+// ones, whose fewer, larger tiles fill the SMs more evenly at nao ~ 2,000.
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int BM = 64, BN = 64, BK = 16, LDS = 68, STAGES = 3;
-constexpr int STAGE_DOUBLES = 2 * BK * LDS;                    // A and B tiles of one stage
-constexpr int GEMM_SMEM = STAGES * STAGE_DOUBLES * 8;          // 52,224 bytes
+constexpr int BK = 16, STAGES = 3;
+constexpr int BM = 64, BN = 64;  // full-product tile (also the batched kernel's)
+
+template <int TBM, int TBN>
+struct GemmShape {
+  static constexpr int LA = TBM + 4, LB = TBN + 4;
+  static constexpr int STAGE = BK * (LA + LB);          // doubles per stage
+  static constexpr int SMEM = STAGES * STAGE * 8;       // bytes
+};
+constexpr int GEMM_SMEM = GemmShape<64, 64>::SMEM;       // 52,224 bytes
+constexpr int SYM_BM = 128, SYM_BN = 64;
+constexpr int SYM_SMEM = GemmShape<SYM_BM, SYM_BN>::SMEM;  // 76,800 bytes
 
 __device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -51,59 +64,71 @@ __device__ __forceinline__ void dmma16x8x8(double *d, const double *a, const dou
                : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-template <bool VEC>
+// One k-slab (16 rows) of the A and B tiles into shared memory, 128 threads.
+template <int TBM, int TBN, bool VEC>
 __device__ __forceinline__ void load_stage(double *sA, double *sB, int k0, int m0, int n0, int M, int N, int K,
                                            const double *__restrict__ A, int lda, const double *__restrict__ B,
                                            int ldb) {
+  using S = GemmShape<TBM, TBN>;
   const int tid = threadIdx.x;
   if (VEC) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int e = tid + 128 * i, row = e >> 5, col = (e & 31) * 2;
-      const int kr = k0 + row;
-      const int ra = kr < K ? min(max(M - (m0 + col), 0), 2) * 8 : 0;
-      const int rb = kr < K ? min(max(N - (n0 + col), 0), 2) * 8 : 0;
-      cp_async16(sA + row * LDS + col, ra ? A + (size_t)kr * lda + m0 + col : A, ra);
-      cp_async16(sB + row * LDS + col, rb ? B + (size_t)kr * ldb + n0 + col : B, rb);
+    for (int e = tid; e < BK * TBM / 2; e += 128) {
+      const int row = e / (TBM / 2), col = (e % (TBM / 2)) * 2, kr = k0 + row;
+      const int r = kr < K ? min(max(M - (m0 + col), 0), 2) * 8 : 0;
+      cp_async16(sA + row * S::LA + col, r ? A + (size_t)kr * lda + m0 + col : A, r);
+    }
+#pragma unroll
+    for (int e = tid; e < BK * TBN / 2; e += 128) {
+      const int row = e / (TBN / 2), col = (e % (TBN / 2)) * 2, kr = k0 + row;
+      const int r = kr < K ? min(max(N - (n0 + col), 0), 2) * 8 : 0;
+      cp_async16(sB + row * S::LB + col, r ? B + (size_t)kr * ldb + n0 + col : B, r);
     }
   } else {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int e = tid + 128 * i, row = e >> 6, col = e & 63;
-      const int kr = k0 + row;
-      const bool pa = kr < K && (m0 + col) < M;
-      const bool pb = kr < K && (n0 + col) < N;
-      cp_async8(sA + row * LDS + col, pa ? A + (size_t)kr * lda + m0 + col : A, pa);
-      cp_async8(sB + row * LDS + col, pb ? B + (size_t)kr * ldb + n0 + col : B, pb);
+    for (int e = tid; e < BK * TBM; e += 128) {
+      const int row = e / TBM, col = e % TBM, kr = k0 + row;
+      const bool p = kr < K && (m0 + col) < M;
+      cp_async8(sA + row * S::LA + col, p ? A + (size_t)kr * lda + m0 + col : A, p);
+    }
+#pragma unroll
+    for (int e = tid; e < BK * TBN; e += 128) {
+      const int row = e / TBN, col = e % TBN, kr = k0 + row;
+      const bool p = kr < K && (n0 + col) < N;
+      cp_async8(sB + row * S::LB + col, p ? B + (size_t)kr * ldb + n0 + col : B, p);
     }
   }
 }
 }  // namespace
 
-// sym != 0: only tiles with bm >= bn are computed; the lower triangle is written and
-// mirrored, so the output is exactly symmetric (used for P = w V^T V and X X).
-template <bool VEC>
+// One TBM x TBN tile, 4 warps as 2 x 2 of (TBM/2) x (TBN/2). sym != 0: only elements
+// with m >= n are written, each also mirrored to (n, m), so the output is exactly
+// symmetric (P = w V^T V and X X).
+template <int TBM, int TBN, bool VEC>
 __device__ __forceinline__ void gemm_tile_impl(double *smem, int bm, int bn, int M, int N, int K, double alpha,
                                                const double *__restrict__ A, int lda, const double *__restrict__ B,
                                                int ldb, double *__restrict__ C, int ldc, int sym) {
+  using S = GemmShape<TBM, TBN>;
+  constexpr int TM = TBM / 2, TN = TBN / 2, FM = TM / 16, FN = TN / 8;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
   const int g = lane >> 2, t = lane & 3;
-  const int m0 = bm * BM, n0 = bn * BN;
-  double acc[2][4][4];
+  const int m0 = bm * TBM, n0 = bn * TBN;
+  double acc[FM][FN][4];
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < FM; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < FN; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
 
   const int ktiles = (K + BK - 1) / BK;
 #pragma unroll
   for (int s = 0; s < STAGES - 1; ++s) {
-    if (s < ktiles)
-      load_stage<VEC>(smem + s * STAGE_DOUBLES, smem + s * STAGE_DOUBLES + BK * LDS, s * BK, m0, n0, M, N, K, A, lda,
-                      B, ldb);
+    if (s < ktiles) {
+      double *st = smem + s * S::STAGE;
+      load_stage<TBM, TBN, VEC>(st, st + BK * S::LA, s * BK, m0, n0, M, N, K, A, lda, B, ldb);
+    }
     cp_async_commit();
   }
   for (int kt = 0; kt < ktiles; ++kt) {
@@ -111,44 +136,44 @@ __device__ __forceinline__ void gemm_tile_impl(double *smem, int bm, int bn, int
     __syncthreads();              // ... everyone's, and stage (kt - 1) % STAGES is free
     const int pf = kt + STAGES - 1;
     if (pf < ktiles) {
-      double *s = smem + (pf % STAGES) * STAGE_DOUBLES;
-      load_stage<VEC>(s, s + BK * LDS, pf * BK, m0, n0, M, N, K, A, lda, B, ldb);
+      double *st = smem + (pf % STAGES) * S::STAGE;
+      load_stage<TBM, TBN, VEC>(st, st + BK * S::LA, pf * BK, m0, n0, M, N, K, A, lda, B, ldb);
     }
     cp_async_commit();
-    const double *sA = smem + (kt % STAGES) * STAGE_DOUBLES;
-    const double *sB = sA + BK * LDS;
+    const double *sA = smem + (kt % STAGES) * S::STAGE;
+    const double *sB = sA + BK * S::LA;
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 8) {
-      double a[2][4], b[4][2];
+      double a[FM][4], b[FN][2];
 #pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const double *pa = sA + (kk + t) * LDS + wm * 32 + i * 16 + g;
+      for (int i = 0; i < FM; ++i) {
+        const double *pa = sA + (kk + t) * S::LA + wm * TM + i * 16 + g;
         a[i][0] = pa[0];
         a[i][1] = pa[8];
-        a[i][2] = pa[4 * LDS];
-        a[i][3] = pa[4 * LDS + 8];
+        a[i][2] = pa[4 * S::LA];
+        a[i][3] = pa[4 * S::LA + 8];
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const double *pb = sB + (kk + t) * LDS + wn * 32 + j * 8 + g;
+      for (int j = 0; j < FN; ++j) {
+        const double *pb = sB + (kk + t) * S::LB + wn * TN + j * 8 + g;
         b[j][0] = pb[0];
-        b[j][1] = pb[4 * LDS];
+        b[j][1] = pb[4 * S::LB];
       }
 #pragma unroll
-      for (int i = 0; i < 2; ++i)
+      for (int i = 0; i < FM; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) dmma16x8x8(acc[i][j], a[i], b[j]);
+        for (int j = 0; j < FN; ++j) dmma16x8x8(acc[i][j], a[i], b[j]);
     }
   }
   cp_async_wait<0>();
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < FM; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < FN; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const int m = m0 + wm * 32 + i * 16 + g + (q >> 1) * 8;
-        const int n = n0 + wn * 32 + j * 8 + 2 * t + (q & 1);
+        const int m = m0 + wm * TM + i * 16 + g + (q >> 1) * 8;
+        const int n = n0 + wn * TN + j * 8 + 2 * t + (q & 1);
         if (m >= M || n >= N) continue;
         const double v = alpha * acc[i][j][q];
         if (!sym) {
@@ -164,22 +189,51 @@ __device__ __forceinline__ bool gemm_vec_ok(const double *A, int lda, const doub
   return ((lda | ldb) & 1) == 0 && ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) == 0;
 }
 
+template <int TBM, int TBN>
+__device__ __forceinline__ void gemm_tile_t(double *smem, int bm, int bn, int M, int N, int K, double alpha,
+                                            const double *__restrict__ A, int lda, const double *__restrict__ B,
+                                            int ldb, double *__restrict__ C, int ldc, int sym) {
+  if (gemm_vec_ok(A, lda, B, ldb))
+    gemm_tile_impl<TBM, TBN, true>(smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym);
+  else
+    gemm_tile_impl<TBM, TBN, false>(smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym);
+}
+
 __device__ __forceinline__ void gemm_tile(double *smem, int bm, int bn, int M, int N, int K, double alpha,
                                           const double *__restrict__ A, int lda, const double *__restrict__ B, int ldb,
                                           double *__restrict__ C, int ldc, int sym) {
-  if (gemm_vec_ok(A, lda, B, ldb))
-    gemm_tile_impl<true>(smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym);
-  else
-    gemm_tile_impl<false>(smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym);
+  gemm_tile_t<BM, BN>(smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym);
 }
 
 __global__ void __launch_bounds__(128, 4) k_gemm_tn(int M, int N, int K, double alpha, const double *__restrict__ A,
-                                                 int lda, const double *__restrict__ B, int ldb,
-                                                 double *__restrict__ C, int ldc, int sym) {
+                                                    int lda, const double *__restrict__ B, int ldb,
+                                                    double *__restrict__ C, int ldc) {
   extern __shared__ __align__(16) double gemm_smem[];
-  const int bn = blockIdx.x, bm = blockIdx.y;
-  if (sym && bm < bn) return;
-  gemm_tile(gemm_smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym);
+  gemm_tile(gemm_smem, blockIdx.y, blockIdx.x, M, N, K, alpha, A, lda, B, ldb, C, ldc, 0);
+}
+
+// Number of SYM_BM x SYM_BN tiles that hold elements with m >= n of an n x n product.
+static inline int sym_tiles(int n) {
+  const int rows = (n + SYM_BM - 1) / SYM_BM, cols = (n + SYM_BN - 1) / SYM_BN;
+  int t = 0;
+  for (int r = 0; r < rows; ++r) t += std::min(((r + 1) * SYM_BM + SYM_BN - 1) / SYM_BN, cols);
+  return t;
+}
+
+// Symmetric n x n product over the enumerated lower-triangle tiles (row block r holds
+// column blocks 0 .. ceil((r+1) SYM_BM / SYM_BN) - 1).
+__global__ void __launch_bounds__(128, 2) k_gemm_sym(int n, int K, double alpha, const double *__restrict__ A,
+                                                     int lda, const double *__restrict__ B, int ldb,
+                                                     double *__restrict__ C, int ldc) {
+  extern __shared__ __align__(16) double gemm_smem[];
+  const int cols = (n + SYM_BN - 1) / SYM_BN;
+  int t = blockIdx.x, r = 0;
+  for (;; ++r) {
+    const int nc = min(((r + 1) * SYM_BM + SYM_BN - 1) / SYM_BN, cols);
+    if (t < nc) break;
+    t -= nc;
+  }
+  gemm_tile_t<SYM_BM, SYM_BN>(gemm_smem, r, t, n, n, K, alpha, A, lda, B, ldb, C, ldc, 1);
 }
 
 // Grouped over molecules: item = one 64x64 tile of one molecule's product.
@@ -213,6 +267,7 @@ static void gemm_smem_attr() {
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64 || done[dev]) return;
   cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
+  cudaFuncSetAttribute(k_gemm_sym, cudaFuncAttributeMaxDynamicSharedMemorySize, SYM_SMEM);
   cudaFuncSetAttribute(k_b_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
   done[dev] = true;
 }
@@ -228,7 +283,7 @@ void launch_gemm_tn(cudaStream_t st, int M, int N, int K, double alpha, const do
                     int ldb, double *C, int ldc) {
   dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
   gemm_smem_attr();
-  k_gemm_tn<<<grid, 128, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc, 0);
+  k_gemm_tn<<<grid, 128, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
   note_launch();
 }
 
@@ -237,9 +292,8 @@ void launch_density(cudaStream_t st, int n, int k, double w, const double *V, in
     cudaMemsetAsync(P, 0, sizeof(double) * (size_t)n * n, st);
     return;
   }
-  dim3 grid((n + BN - 1) / BN, (n + BM - 1) / BM);
   gemm_smem_attr();
-  k_gemm_tn<<<grid, 128, GEMM_SMEM, st>>>(n, n, k, w, V, ldv, V, ldv, P, n, 1);
+  k_gemm_sym<<<sym_tiles(n), 128, SYM_SMEM, st>>>(n, k, w, V, ldv, V, ldv, P, n);
   note_launch();
 }
 
@@ -567,9 +621,8 @@ void launch_sp2_init(cudaStream_t st, int n, const double *F, const double *boun
 }
 
 void launch_sp2_square(cudaStream_t st, int n, const double *X, double *X2) {
-  dim3 grid((n + BN - 1) / BN, (n + BM - 1) / BM);
   gemm_smem_attr();
-  k_gemm_tn<<<grid, 128, GEMM_SMEM, st>>>(n, n, n, 1.0, X, n, X, n, X2, n, 1);
+  k_gemm_sym<<<sym_tiles(n), 128, SYM_SMEM, st>>>(n, n, 1.0, X, n, X, n, X2, n);
   note_launch();
 }
 
