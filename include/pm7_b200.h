@@ -211,6 +211,15 @@ pm7_status pm7_stage_pair(const pm7_params *params, int32_t z_i, int32_t z_j, co
  * counterpart in pm7-rs (its density step diagonalises). */
 pm7_status pm7_stage_square_tf32(int32_t n, const double *x, double *c_out);
 
+/* Eigenvalues (ascending, no eigenvectors) of `count` symmetric matrices, the stage that
+ * gives the reported MO energies when no orbitals are returned. Replaces the eigenvalue
+ * half of `symmetric_eigen` (src/linalg.rs:231-278, faer self_adjoint_eigen) as used by
+ * run_pm7's final step (src/scf.rs:1299-1305). Matrices are packed row-major one after
+ * another (orders[i]^2 doubles each; order <= 8192), eigenvalues likewise (orders[i]
+ * each). Host buffers; runs on `device`. */
+pm7_status pm7_stage_eigenvalues(int32_t count, const int32_t *orders, const double *a, double *w,
+                                 int32_t device);
+
 /* Core-core repulsion energy in eV (`core_core_energy`, src/repulsion.rs:16-36). */
 pm7_status pm7_stage_core_core(const pm7_molecule *molecule, const pm7_params *params,
                                double *energy_ev);

@@ -965,6 +965,8 @@ class BatchRunner {
     cudaSetDevice(ctx_.device);
     cudaStreamSynchronize(st_);
     for (auto &kv : active_) release(*kv);
+    eig_scr_.release(st_);
+    cudaStreamSynchronize(st_);
     if (desc_) cudaFree(desc_);
     if (ctl_) cudaFree(ctl_);
     if (arena_) cudaFree(arena_);
@@ -1411,8 +1413,12 @@ class BatchRunner {
   // Eigendecomposition of every bucket matrix (eigenvalues ascending; with `vectors`,
   // eigenvector k in row k, in place): one batched call per bucket size, or one
   // divide-and-conquer call per matrix for the large sizes.
-  void eigensolve(const Lists &A, bool vectors = true) {
+  // Eigensolves of the bucket matrices with order >= min_np. Orders from 512 go to the
+  // side streams; when min_np > 0 the caller joins them (join_side) after queuing its own
+  // work on the main stream.
+  void eigensolve(const Lists &A, bool vectors = true, int min_np = 0) {
     for (auto &kv : A.buckets) {
+      if (kv.first < min_np) continue;
       // the batched routine is faster with vectors than without at these sizes; the
       // divide-and-conquer one saves its back-transformation when only values are needed
       const cusolverEigMode_t jobz =
@@ -1447,10 +1453,8 @@ class BatchRunner {
           SOLVER_OK(cusolverDnDsyevd(sd.solver, jobz, CUBLAS_FILL_MODE_LOWER, np, e.in, np, e.eps, (double *)sd.work,
                                      lwork, sd.info));
         }
-        for (int k = 0; k < used; ++k) {
-          CUDA_OK(cudaEventRecord(side_[k].done, side_[k].st));
-          CUDA_OK(cudaStreamWaitEvent(st_, side_[k].done, 0));
-        }
+        side_used_ = std::max(side_used_, used);
+        if (min_np == 0) join_side();
         continue;
       }
       size_t wd = 0, wh = 0;
@@ -1466,6 +1470,15 @@ class BatchRunner {
                                        CUDA_R_64F, w, CUDA_R_64F, work_, work_cap_,
                                        host_work_.empty() ? nullptr : host_work_.data(), wh, info_, cnt));
     }
+  }
+
+  // The main stream waits for the side streams' eigensolves.
+  void join_side() {
+    for (int k = 0; k < side_used_; ++k) {
+      CUDA_OK(cudaEventRecord(side_[k].done, side_[k].st));
+      CUDA_OK(cudaStreamWaitEvent(st_, side_[k].done, 0));
+    }
+    side_used_ = 0;
   }
 
   // Final Fock and energy, corrections, reported orbitals and per-atom outputs of the
@@ -1491,7 +1504,20 @@ class BatchRunner {
       // Fock when a level shift was active (scf.rs:1299-1305)
       Stage s_(st_, "batch_orbitals");
       k_b_to_bucket<<<n, RB, 0, st_>>>(A.mol, desc_, ctl_, A.eig, 2);
-      eigensolve(A, vectors);
+      if (vectors) {
+        eigensolve(A, true);
+      } else {
+        // Energies only. Orders from kLeanEig up: the library's divide and conquer, one
+        // matrix per side stream; below: all at once through the cluster tridiagonalisation
+        // (the top-left nao x nao block of each bucket matrix) on this stream, meanwhile.
+        eigensolve(A, false, kLeanEig);
+        std::vector<EigvalsRequest> req;
+        for (auto &kv : A.buckets)
+          if (kv.first < kLeanEig)
+            for (int m : kv.second) req.push_back({A.eig_h[m].in, R[m]->L.nao, A.eig_h[m].ldv, A.eig_h[m].eps});
+        eigvals_device(st_, req, eig_scr_);
+        join_side();
+      }
       k_b_save_orbitals<<<n, RB, 0, st_>>>(A.mol, desc_, A.eig);
       note_launch(2);
     }
@@ -1605,6 +1631,9 @@ class BatchRunner {
   cudaEvent_t fork_ = nullptr;
   double *arena_ = nullptr;
   size_t arena_cap_ = 0;
+  EigvalsScratch eig_scr_;  // eigenvalue solves at retirement
+  int side_used_ = 0;       // side streams with queued eigensolves not yet joined
+  static constexpr int kLeanEig = 512;  // from this order the library solver, below the cluster one
   void *work_ = nullptr;
   size_t work_cap_ = 0;
   std::vector<char> host_work_;

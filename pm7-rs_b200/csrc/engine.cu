@@ -17,6 +17,7 @@
 #include <cstring>
 #include <functional>
 #include <limits>
+#include <map>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -703,6 +704,82 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   out.n_occ = n_occ;
 }
 
+void eigvals_device(cudaStream_t st, const std::vector<EigvalsRequest> &req, EigvalsScratch &scr) {
+  if (req.empty()) return;
+  std::map<int, std::vector<int>> groups;  // cluster size -> requests
+  size_t work = 0;
+  for (size_t i = 0; i < req.size(); ++i) {
+    const int n = req[i].n;
+    if (!eigvals_supported(n) || req[i].ld < n)
+      throw Failure{PM7_ERR_INVALID_INPUT, "eigenvalue solve: order " + std::to_string(n) + " not supported"};
+    groups[tridiag_cluster_size(n)].push_back((int)i);
+    work += (eigvals_work_doubles(n) + 31) / 32 * 32;
+  }
+  // per group: its tasks, then its prefix sums (int), in one uploaded block
+  std::vector<unsigned char> meta;
+  struct G {
+    int c, count, max_n, total;
+    size_t tasks_off, prefix_off;
+  };
+  std::vector<G> gs;
+  std::vector<std::vector<EigvalsTask>> tasks_of;
+  for (auto &kv : groups) {
+    G g{kv.first, (int)kv.second.size(), 0, 0, 0, 0};
+    std::vector<int> prefix;
+    for (int i : kv.second) {
+      prefix.push_back(g.total);
+      g.total += req[i].n;
+      g.max_n = std::max(g.max_n, req[i].n);
+    }
+    g.tasks_off = (meta.size() + 63) / 64 * 64;
+    meta.resize(g.tasks_off + sizeof(EigvalsTask) * kv.second.size());
+    g.prefix_off = (meta.size() + 63) / 64 * 64;
+    meta.resize(g.prefix_off + sizeof(int) * prefix.size());
+    std::memcpy(meta.data() + g.prefix_off, prefix.data(), sizeof(int) * prefix.size());
+    gs.push_back(g);
+  }
+  if (work > scr.cap) {
+    if (scr.work) CUDA_OK(cudaFreeAsync(scr.work, st));
+    scr.cap = work + work / 4;
+    CUDA_OK(cudaMallocAsync((void **)&scr.work, sizeof(double) * scr.cap, st));
+  }
+  if (!scr.uploaded) CUDA_OK(cudaEventCreateWithFlags(&scr.uploaded, cudaEventDisableTiming));
+  CUDA_OK(cudaEventSynchronize(scr.uploaded));  // the previous table was read: pinned is free
+  if (meta.size() > scr.meta_cap) {
+    if (scr.meta) CUDA_OK(cudaFreeAsync(scr.meta, st));
+    if (scr.pinned) CUDA_OK(cudaFreeHost(scr.pinned));
+    scr.meta_cap = meta.size() + meta.size() / 4 + 256;
+    CUDA_OK(cudaMallocAsync((void **)&scr.meta, scr.meta_cap, st));
+    CUDA_OK(cudaMallocHost((void **)&scr.pinned, scr.meta_cap));
+  }
+  size_t woff = 0;
+  size_t k = 0;
+  for (auto &kv : groups) {
+    EigvalsTask *out = reinterpret_cast<EigvalsTask *>(meta.data() + gs[k].tasks_off);
+    for (size_t q = 0; q < kv.second.size(); ++q) {
+      const EigvalsRequest &r = req[kv.second[q]];
+      EigvalsTask t{};
+      t.src = r.src;
+      t.n = r.n;
+      t.ld = r.ld;
+      t.eps = r.eps;
+      eigvals_task_layout(t, scr.work + woff);
+      woff += (eigvals_work_doubles(t.n) + 31) / 32 * 32;
+      std::memcpy(out + q, &t, sizeof(t));
+    }
+    ++k;
+  }
+  std::memcpy(scr.pinned, meta.data(), meta.size());
+  CUDA_OK(cudaMemcpyAsync(scr.meta, scr.pinned, meta.size(), cudaMemcpyHostToDevice, st));
+  CUDA_OK(cudaEventRecord(scr.uploaded, st));
+  for (const G &g : gs) {
+    const cudaError_t err =
+        launch_eigvals(st, reinterpret_cast<const EigvalsTask *>(scr.meta + g.tasks_off), g.count, g.c, g.max_n,
+                       reinterpret_cast<const int *>(scr.meta + g.prefix_off), g.total);
+    if (err != cudaSuccess) throw Failure{PM7_ERR_CUDA, std::string("eigenvalue solve: ") + cudaGetErrorString(err)};
+  }
+}
+
 static void run_uhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D, const Molecule &m,
                     const Layout &L, const ParamSet &ps, int n_alpha, int n_beta, const pm7_options &o,
                     ScfOut &out) {
@@ -1327,6 +1404,40 @@ pm7_status pm7_stage_square_tf32(int32_t n, const double *x, double *c_out) {
     CUDA_OK(cudaStreamSynchronize(st));
     CUDA_OK(cudaGetLastError());
     if (e) throw Failure{PM7_ERR_CUDA, "tcgen05 squaring: a pipeline wait expired"};
+  });
+}
+
+pm7_status pm7_stage_eigenvalues(int32_t count, const int32_t *orders, const double *a, double *w,
+                                 int32_t device) {
+  return guarded([&] {
+    if (count < 0 || (count > 0 && (!orders || !a || !w)))
+      throw Failure{PM7_ERR_INVALID_INPUT, "eigenvalues: bad count or null arrays"};
+    if (count == 0) return;
+    DeviceContext &ctx = context_for(device);
+    std::lock_guard<std::mutex> lock(ctx.run_mutex);
+    CUDA_OK(cudaSetDevice(ctx.device));
+    cudaStream_t st = ctx.stream;
+    size_t na = 0, nw = 0;
+    for (int i = 0; i < count; ++i) {
+      if (!eigvals_supported(orders[i]))
+        throw Failure{PM7_ERR_INVALID_INPUT, "eigenvalues: order " + std::to_string(orders[i]) + " outside 1..4096"};
+      na += (size_t)orders[i] * orders[i];
+      nw += orders[i];
+    }
+    DevBuf<double> A, E;
+    upload(A, std::vector<double>(a, a + na), st);
+    E.alloc(nw, st);
+    std::vector<EigvalsRequest> req;
+    size_t oa = 0, ow = 0;
+    for (int i = 0; i < count; ++i) {
+      req.push_back({A.p + oa, orders[i], orders[i], E.p + ow});
+      oa += (size_t)orders[i] * orders[i];
+      ow += orders[i];
+    }
+    eigvals_device(st, req, ctx.eig_scratch);
+    CUDA_OK(cudaMemcpyAsync(w, E.p, sizeof(double) * nw, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaGetLastError());
   });
 }
 

@@ -109,6 +109,29 @@ struct Stage {
   ~Stage() { g_prof.end(st, token); }
 };
 
+// Grow-only device scratch of the eigenvalue solver (stream-ordered growth): repeated
+// solves reuse it instead of re-allocating their workspace every call.
+struct EigvalsScratch {
+  double *work = nullptr;
+  size_t cap = 0;  // doubles
+  unsigned char *meta = nullptr;
+  size_t meta_cap = 0;  // bytes
+  unsigned char *pinned = nullptr;  // host staging of the task table (same capacity)
+  cudaEvent_t uploaded = nullptr;   // the last upload from `pinned` has been read
+  // stream-ordered release (the owner's stream); the owner calls it before it goes away
+  void release(cudaStream_t st) {
+    if (uploaded) cudaEventSynchronize(uploaded);
+    if (work) cudaFreeAsync(work, st);
+    if (meta) cudaFreeAsync(meta, st);
+    if (pinned) cudaFreeHost(pinned);
+    if (uploaded) cudaEventDestroy(uploaded);
+    work = nullptr;
+    meta = pinned = nullptr;
+    uploaded = nullptr;
+    cap = meta_cap = 0;
+  }
+};
+
 struct DeviceContext {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -119,6 +142,7 @@ struct DeviceContext {
   // Pinned staging area for the small per-iteration transfers (pointer lists,
   // extrapolation weights, scalars), so they never go through pageable memory.
   unsigned char *pinned = nullptr;
+  EigvalsScratch eig_scratch;  // eigenvalue solves of this context's stream
 };
 static constexpr size_t kPinnedBytes = 1 << 16;
 
@@ -190,6 +214,18 @@ struct ResultParts {
 void fill_result(pm7_result *res, const Molecule &m, const Layout &L, const ParamSet &ps, const pm7_options &o,
                  const ResultParts &S, const std::vector<double> &pops,
                  const std::function<double(int, int, int)> &Pm);
+
+// One symmetric device matrix (order n, leading dimension ld) whose eigenvalues go,
+// ascending, to the device array eps.
+struct EigvalsRequest {
+  const double *src;
+  int n, ld;
+  double *eps;
+};
+// Eigenvalues only, many matrices at once (kernels_eig.cu): grouped by cluster size, one
+// tridiagonalisation and one Sturm launch per group; workspace from `scr` (grown in
+// stream order as needed). Every order must satisfy eigvals_supported().
+void eigvals_device(cudaStream_t st, const std::vector<EigvalsRequest> &req, EigvalsScratch &scr);
 
 template <class T>
 inline void upload(DevBuf<T> &b, const std::vector<T> &v, cudaStream_t st) {

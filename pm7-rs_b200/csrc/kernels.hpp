@@ -130,3 +130,34 @@ void launch_sp2_square(cudaStream_t st, int n, const double *X, double *X2);
 void launch_sp2_trace(cudaStream_t st, int n, const double *X, const double *X2, double n_occ, double *state);
 void launch_sp2_update(cudaStream_t st, int n, double *X, const double *X2, const double *state);
 }
+
+namespace pm7 {
+// Eigenvalues of symmetric matrices, no eigenvectors (kernels_eig.cu): Householder
+// tridiagonalisation with one thread-block cluster per matrix, then Sturm multisection.
+constexpr int kTriPanel = 32;       // reflectors per panel
+constexpr int kTriMaxCluster = 16;  // CTAs per matrix at most
+constexpr int kTriMaxN = 4096;      // largest order accepted
+
+struct EigvalsTask {
+  const double *src;  // n x n symmetric, row-major, leading dimension ld; read only
+  double *a;          // workspace (eigvals_task_layout): n x n copy, panel vectors, ...
+  double *V, *W;      // panel vectors of all rows, n x kTriPanel each
+  double *vec, *part; // e^2 (n); Gershgorin interval and pivot floor (3)
+  double *d, *e;      // the tridiagonal matrix
+  double *eps;        // n eigenvalues, ascending (output)
+  int n, ld;
+};
+
+// Doubles of workspace one task of order n needs; eigvals_task_layout carves it.
+size_t eigvals_work_doubles(int n);
+void eigvals_task_layout(EigvalsTask &t, double *work);
+// CTAs per matrix for order n (1 .. 16; 8 at most where 16-CTA clusters cannot run).
+int tridiag_cluster_size(int n);
+// Whether order n runs here (order and the per-CTA shared memory it needs); larger
+// matrices go to the library eigensolver.
+bool eigvals_supported(int n);
+// All tasks share one cluster size; prefix[t] = sum of the orders of tasks before t,
+// total = sum of all orders (device arrays / values). Returns the launch status.
+cudaError_t launch_eigvals(cudaStream_t st, const EigvalsTask *tasks, int n_tasks, int cluster, int max_n,
+                           const int *prefix, int total);
+}

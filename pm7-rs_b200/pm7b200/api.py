@@ -22,7 +22,7 @@ EXPORTED = [
     "pm7_params_load", "pm7_options_default", "pm7_run", "pm7_result_free", "pm7_last_error_message",
     "pm7_device_count", "pm7_stage_core_hamiltonian", "pm7_stage_fock", "pm7_stage_pair", "pm7_stage_core_core",
     "pm7_stage_corrections", "pm7_run_batch", "pm7_engine_config_default", "pm7_engine_create", "pm7_engine_submit",
-    "pm7_engine_poll", "pm7_engine_destroy", "pm7_batch_partition",
+    "pm7_engine_poll", "pm7_engine_destroy", "pm7_batch_partition", "pm7_stage_eigenvalues",
 ]
 
 
@@ -63,6 +63,7 @@ def lib():
                                 C.POINTER(abi.Result), C.POINTER(C.c_int32)]
     L.pm7_batch_partition.argtypes = [C.c_int32, C.POINTER(abi.Molecule), C.c_int32, C.c_int32,
                                       C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+    L.pm7_stage_eigenvalues.argtypes = [C.c_int32, C.POINTER(C.c_int32), abi.DP, abi.DP, C.c_int32]
     L.pm7_engine_config_default.argtypes = [C.POINTER(abi.EngineConfig)]
     L.pm7_engine_create.argtypes = [C.POINTER(abi.EngineConfig), C.POINTER(C.c_void_p)]
     L.pm7_engine_submit.argtypes = [C.c_void_p, C.POINTER(abi.Molecule), C.POINTER(abi.Options),
@@ -348,6 +349,24 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+def eigenvalues(matrices, device=0):
+    """Ascending eigenvalues of symmetric matrices on the GPU (`pm7_stage_eigenvalues`).
+
+    `matrices` is a list of square arrays; returns one array of eigenvalues per matrix.
+    """
+    mats = [np.ascontiguousarray(m, dtype=np.float64) for m in matrices]
+    orders = np.array([m.shape[0] for m in mats], dtype=np.int32)
+    packed = np.concatenate([m.reshape(-1) for m in mats]) if mats else np.zeros(1)
+    out = np.zeros(max(int(orders.sum()), 1))
+    _check(lib().pm7_stage_eigenvalues(len(mats), orders.ctypes.data_as(C.POINTER(C.c_int32)),
+                                       packed.ctypes.data_as(abi.DP), out.ctypes.data_as(abi.DP), int(device)))
+    res, off = [], 0
+    for n in orders:
+        res.append(out[off:off + n].copy())
+        off += n
+    return res
 
 
 def square_tf32(x):
