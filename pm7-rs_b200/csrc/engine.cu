@@ -338,10 +338,10 @@ struct Eigen {
     info.alloc(1, ctx.stream);
   }
   // In place: A (n x n symmetric) becomes the eigenvectors, one per row when read
-  // row-major; eigenvalues ascending in eps.
-  void solve(double *A) {
-    SOLVER_OK(cusolverDnDsyevd(ctx.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A, n, eps.p, work.p,
-                               lwork, info.p));
+  // row-major (vectors = true; else A is overwritten); eigenvalues ascending in eps.
+  void solve(double *A, bool vectors = true) {
+    SOLVER_OK(cusolverDnDsyevd(ctx.solver, vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR,
+                               CUBLAS_FILL_MODE_LOWER, n, A, n, eps.p, work.p, lwork, info.p));
   }
 };
 
@@ -353,13 +353,13 @@ struct Purifier {
   int n;
   DevBuf<double> X, X2, scratch, bounds, state;
   int last_iterations = 0;
-  double *pin = nullptr;  // 4 pinned doubles for the per-step state
+  double *pin = nullptr;  // kSp2Len pinned doubles for the purification state
   Purifier(cudaStream_t s, int n_, double *pinned_state) : st(s), n(n_), pin(pinned_state) {
     X.alloc((size_t)n * n, st);
     X2.alloc((size_t)n * n, st);
     scratch.alloc(1024, st);
     bounds.alloc(2, st);
-    state.alloc(4, st);
+    state.alloc(kSp2Len, st);
   }
   // fp32 iterate of the mixed-precision purification: X, its tf32 split, X^2 (ld x ld)
   int ld = 0;
@@ -379,6 +379,28 @@ struct Purifier {
     if (!make_square_map(hi32.p, ld, map_hi) || !make_square_map(lo32.p, ld, map_lo))
       throw Failure{PM7_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
   }
+  // Queue SP2 steps in chunks and read the device state once per chunk: the device stops
+  // the purification itself (Sp2Rule) and skips the steps queued after that. The first
+  // chunk is sized from the previous purification's step count. Returns the steps run.
+  static constexpr int kMaxSteps = 100;
+  int hint64 = 0, hint32 = 0;
+  template <class Launch>
+  int run_chunks(Launch launch_step, const char *gemm_stage, int &hint) {
+    launch_sp2_reset(st, state.p);
+    int launched = 0, chunk = std::max(4, hint + 1);
+    while (launched < kMaxSteps) {
+      for (int c = 0; c < chunk && launched < kMaxSteps; ++c) launch_step(launched++);
+      CUDA_OK(cudaMemcpyAsync(pin, state.p, kSp2Len * sizeof(double), cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaStreamSynchronize(st));
+      if (pin[kSp2Stop] < 1.0e8) break;
+      chunk = 4;
+    }
+    const int steps = pin[kSp2Stop] < 1.0e8 ? (int)pin[kSp2Stop] + 1 : launched;
+    g_prof.drop_last(gemm_stage, launched - steps);
+    hint = steps;
+    return steps;
+  }
+
   // SP2 with the squarings on the tcgen05 tensor cores (3xTF32, fp32 accumulation). The
   // fp32 iterate reaches idempotency only to its rounding floor, so the density carries
   // about 1e-5 relative error: the SCF uses it for its early cycles only.
@@ -386,34 +408,21 @@ struct Purifier {
     ensure32();
     launch_gershgorin(st, n, F, scratch.p, bounds.p);
     launch_sp2_init32(st, n, ld, F, bounds.p, X32.p, hi32.p, lo32.p);
-    std::vector<double> err;
-    bool ok = false;
     const double scale = std::max(1, n_occ);
-    for (int it = 0; it < 100; ++it) {
-      {
-        Stage g_(st, "sp2_square_tf32");
-        launch_square_tf32x3(st, n, ld, map_hi, map_lo, C32.p, err32.p);
-      }
-      launch_sp2_trace32(st, n, ld, X32.p, C32.p, (double)n_occ, state.p);
-      launch_sp2_update32(st, n, ld, X32.p, C32.p, state.p, hi32.p, lo32.p);
-      double *s = pin;
-      CUDA_OK(cudaMemcpyAsync(s, state.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
-      CUDA_OK(cudaStreamSynchronize(st));
-      const double e = s[3];
-      err.push_back(e);
-      last_iterations = it + 1;
-      const size_t k = err.size();
-      if (!std::isfinite(e)) break;
-      if (std::fabs(e) <= 1.0e-6 * scale) {
-        ok = true;
-        break;
-      }
-      if (k >= 3 && std::fabs(e) < 1.0e-2 * scale && std::fabs(e) >= std::fabs(err[k - 3])) {
-        ok = true;  // at the fp32 rounding floor
-        break;
-      }
-    }
-    if (ok && std::fabs(pin[0] - (double)n_occ) > 1.0e-2 * scale) ok = false;
+    const Sp2Rule rule{1.0e-6 * scale, 1.0e-2 * scale, kMaxSteps};
+    last_iterations = run_chunks(
+        [&](int s) {
+          {
+            Stage g_(st, "sp2_square_tf32");
+            launch_square_tf32x3(st, n, ld, map_hi, map_lo, C32.p, err32.p, state.p, s);
+          }
+          launch_sp2_trace32(st, n, ld, X32.p, C32.p, (double)n_occ, state.p, s, rule);
+          launch_sp2_update32(st, n, ld, X32.p, C32.p, state.p, hi32.p, lo32.p, s);
+        },
+        "sp2_square_tf32", hint32);
+    bool ok = pin[kSp2Ok] != 0.0;
+    // an idempotent X whose trace is not n_occ is a wrong projector (degenerate frontier)
+    if (ok && std::fabs(pin[kSp2TrX] - (double)n_occ) > 1.0e-2 * scale) ok = false;
     int bad = 0;
     CUDA_OK(cudaMemcpyAsync(&bad, err32.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
@@ -426,34 +435,20 @@ struct Purifier {
   bool project(const double *F, int n_occ, double w, double *P) {
     launch_gershgorin(st, n, F, scratch.p, bounds.p);
     launch_sp2_init(st, n, F, bounds.p, X.p);
-    std::vector<double> err;
-    bool ok = false;
-    for (int it = 0; it < 100; ++it) {
-      {
-        Stage g_(st, "sp2_square_gemm");
-        launch_sp2_square(st, n, X.p, X2.p);
-      }
-      launch_sp2_trace(st, n, X.p, X2.p, (double)n_occ, state.p);
-      launch_sp2_update(st, n, X.p, X2.p, state.p);
-      double *s = pin;
-      CUDA_OK(cudaMemcpyAsync(s, state.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
-      CUDA_OK(cudaStreamSynchronize(st));
-      const double e = s[3];
-      err.push_back(e);
-      last_iterations = it + 1;
-      const size_t k = err.size();
-      if (!std::isfinite(e)) break;
-      if (std::fabs(e) <= 1.0e-13 * std::max(1, n_occ)) {
-        ok = true;
-        break;
-      }
-      if (k >= 3 && std::fabs(e) < 1.0e-6 && std::fabs(e) >= std::fabs(err[k - 3])) {
-        ok = true;  // at the rounding floor: no further progress
-        break;
-      }
-    }
+    const Sp2Rule rule{1.0e-13 * std::max(1, n_occ), 1.0e-6, kMaxSteps};
+    last_iterations = run_chunks(
+        [&](int s) {
+          {
+            Stage g_(st, "sp2_square_gemm");
+            launch_sp2_square(st, n, X.p, X2.p, state.p, s);
+          }
+          launch_sp2_trace(st, n, X.p, X2.p, (double)n_occ, state.p, s, rule);
+          launch_sp2_update(st, n, X.p, X2.p, state.p, s);
+        },
+        "sp2_square_gemm", hint64);
+    bool ok = pin[kSp2Ok] != 0.0;
     // an idempotent X whose trace is not n_occ is a wrong projector (degenerate frontier)
-    if (ok && std::fabs(pin[0] - (double)n_occ) > 1.0e-3) ok = false;
+    if (ok && std::fabs(pin[kSp2TrX] - (double)n_occ) > 1.0e-3) ok = false;
     if (!ok) return false;
     launch_scale(st, (size_t)n * n, w, X.p, P);
     return true;
@@ -688,16 +683,20 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, out.P.p, out.P.p, 0.5, F.p, D.pop.p, D.jbuf.p); }
   size_t ne = launch_energy(st, nn, out.P.p, D.H.p, F.p, partials.p);
   out.electronic_ev = 0.5 * host_sum(partials, ne, dscal.p, st);
-  out.Va.alloc(nn, st);
   // Reported orbitals: the eigenvectors of the last extrapolated Fock, or of the real
-  // Fock when a level shift was active (scf.rs:1299-1305).
+  // Fock when a level shift was active (scf.rs:1299-1305); their energies alone when no
+  // matrices are returned.
+  const bool vectors = o.want_matrices != 0;
   if (guard.shift > 0.0) {
     CUDA_OK(cudaMemcpyAsync(Fuse.p, F.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
-    { Stage s_(st, "eigensolve"); eig.solve(Fuse.p); }
+    { Stage s_(st, "eigensolve"); eig.solve(Fuse.p, vectors); }
   } else if (!diagonalised) {
-    { Stage s_(st, "eigensolve"); eig.solve(Fuse.p); }
+    { Stage s_(st, "eigensolve"); eig.solve(Fuse.p, vectors); }
   }
-  CUDA_OK(cudaMemcpyAsync(out.Va.p, Fuse.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+  if (vectors) {
+    out.Va.alloc(nn, st);
+    CUDA_OK(cudaMemcpyAsync(out.Va.p, Fuse.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+  }
   out.eps_a.resize(n);
   CUDA_OK(cudaMemcpyAsync(out.eps_a.data(), eig.eps.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaStreamSynchronize(st));

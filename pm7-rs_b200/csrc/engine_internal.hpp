@@ -76,12 +76,26 @@ struct StageProfiler {
     std::lock_guard<std::mutex> g(mu);
     if (token < (int)pending.size()) cudaEventRecord(pending[token].b, st);
   }
+  // Forget the last `count` pending measurements of stage `name` (launches whose work the
+  // device skipped, e.g. SP2 steps queued past the step that stopped the purification).
+  void drop_last(const char *name, int count) {
+    std::lock_guard<std::mutex> g(mu);
+    if (!on || count <= 0) return;
+    int idx = -1;
+    for (size_t i = 0; i < names.size(); ++i)
+      if (names[i] == name) idx = (int)i;
+    for (int i = (int)pending.size() - 1; i >= 0 && count > 0 && idx >= 0; --i)
+      if (pending[i].stage == idx) {
+        pending[i].stage = -1;
+        --count;
+      }
+  }
   void flush() {
     std::lock_guard<std::mutex> g(mu);
     for (Open &o : pending) {
       cudaEventSynchronize(o.b);
       float ms = 0.0f;
-      if (cudaEventElapsedTime(&ms, o.a, o.b) == cudaSuccess) {
+      if (o.stage >= 0 && cudaEventElapsedTime(&ms, o.a, o.b) == cudaSuccess) {
         total_ms[o.stage] += ms;
         calls[o.stage] += 1;
       }

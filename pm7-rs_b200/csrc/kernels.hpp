@@ -104,21 +104,43 @@ void launch_stage_pair(cudaStream_t st, const DeviceParams &P, int zi, int zj, c
 }
 
 namespace pm7 {
+// Device-side SP2 control: every step kernel gets its step index and does nothing once
+// an earlier step has stopped the purification (state[kSp2Stop] = that step), so steps
+// can be queued in chunks without a host round trip per step.
+enum Sp2State {
+  kSp2TrX = 0, kSp2TrX2 = 1, kSp2Square = 2, kSp2Err = 3,  // traces, branch, tr X - tr X^2
+  kSp2Stop = 4,                                            // step at which it stopped (1e9: running)
+  kSp2Ok = 5,                                              // 1: converged, 0: failed
+  kSp2Ring = 6,                                            // errors of the last three steps
+  kSp2Len = 12
+};
+// Stopping rule of one purification: converged when |err| <= tol_done, or at the rounding
+// floor when |err| < tol_floor and no smaller than two steps before; failed on a
+// non-finite error or after max_steps.
+struct Sp2Rule {
+  double tol_done, tol_floor;
+  int max_steps;
+};
+}
+
+namespace pm7 {
 // FP32-accuracy (3xTF32) symmetric squaring on tcgen05 (kernels_tf32.cu). Matrices are
 // ld x ld fp32, ld a multiple of 32, zero padded beyond n; the maps come from
 // make_square_map (an opaque 128-byte CUtensorMap each).
 bool make_square_map(const float *base, int ld, void *map_out);
 size_t square_tf32x3_smem();
+// state/step: as the fp64 SP2 steps (state may be null: always runs).
 void launch_square_tf32x3(cudaStream_t st, int n, int ld, const void *map_hi, const void *map_lo, float *C,
-                          int *error);
+                          int *error, const double *state = nullptr, int step = 0);
 void launch_split_tf32(cudaStream_t st, int n, int ld, const double *X, float *hi, float *lo);
 void launch_widen(cudaStream_t st, int n, int ld, const float *C32, double *C);
 // The fp32 SP2 iteration: start, traces (fp64 sums), update with re-split, density.
 void launch_sp2_init32(cudaStream_t st, int n, int ld, const double *F, const double *bounds, float *X, float *hi,
                        float *lo);
-void launch_sp2_trace32(cudaStream_t st, int n, int ld, const float *X, const float *X2, double n_occ, double *state);
+void launch_sp2_trace32(cudaStream_t st, int n, int ld, const float *X, const float *X2, double n_occ, double *state,
+                        int step, Sp2Rule rule);
 void launch_sp2_update32(cudaStream_t st, int n, int ld, float *X, const float *X2, const double *state, float *hi,
-                         float *lo);
+                         float *lo, int step);
 void launch_sp2_density32(cudaStream_t st, int n, int ld, const float *X, double w, double *P);
 }
 
@@ -126,9 +148,11 @@ namespace pm7 {
 // SP2 purification building blocks (kernels_dense.cu).
 void launch_gershgorin(cudaStream_t st, int n, const double *F, double *scratch, double *bounds);
 void launch_sp2_init(cudaStream_t st, int n, const double *F, const double *bounds, double *X);
-void launch_sp2_square(cudaStream_t st, int n, const double *X, double *X2);
-void launch_sp2_trace(cudaStream_t st, int n, const double *X, const double *X2, double n_occ, double *state);
-void launch_sp2_update(cudaStream_t st, int n, double *X, const double *X2, const double *state);
+void launch_sp2_reset(cudaStream_t st, double *state);
+void launch_sp2_square(cudaStream_t st, int n, const double *X, double *X2, const double *state, int step);
+void launch_sp2_trace(cudaStream_t st, int n, const double *X, const double *X2, double n_occ, double *state, int step,
+                      Sp2Rule rule);
+void launch_sp2_update(cudaStream_t st, int n, double *X, const double *X2, const double *state, int step);
 }
 
 namespace pm7 {

@@ -224,8 +224,10 @@ static inline int sym_tiles(int n) {
 // column blocks 0 .. ceil((r+1) SYM_BM / SYM_BN) - 1).
 __global__ void __launch_bounds__(128, 2) k_gemm_sym(int n, int K, double alpha, const double *__restrict__ A,
                                                      int lda, const double *__restrict__ B, int ldb,
-                                                     double *__restrict__ C, int ldc) {
+                                                     double *__restrict__ C, int ldc, const double *__restrict__ sp2,
+                                                     int step) {
   extern __shared__ __align__(16) double gemm_smem[];
+  if (!sp2_active(sp2, step)) return;  // an SP2 step after the purification stopped
   const int cols = (n + SYM_BN - 1) / SYM_BN;
   int t = blockIdx.x, r = 0;
   for (;; ++r) {
@@ -293,7 +295,7 @@ void launch_density(cudaStream_t st, int n, int k, double w, const double *V, in
     return;
   }
   gemm_smem_attr();
-  k_gemm_sym<<<sym_tiles(n), 128, SYM_SMEM, st>>>(n, k, w, V, ldv, V, ldv, P, n);
+  k_gemm_sym<<<sym_tiles(n), 128, SYM_SMEM, st>>>(n, k, w, V, ldv, V, ldv, P, n, nullptr, 0);
   note_launch();
 }
 
@@ -581,9 +583,11 @@ __global__ void k_sp2_init(int n, const double *__restrict__ F, const double *__
 }
 
 // Traces of X and X^2 and the SP2 branch: state[0] = tr X, state[1] = tr X^2,
-// state[2] = 1 when squaring brings the trace closer to n_occ, state[3] = tr X - tr X^2.
+// state[2] = 1 when squaring brings the trace closer to n_occ, state[3] = tr X - tr X^2;
+// then the stopping rule.
 __global__ void k_sp2_trace(int n, const double *__restrict__ X, const double *__restrict__ X2, double n_occ,
-                            double *__restrict__ state) {
+                            double *__restrict__ state, int step, Sp2Rule rule) {
+  if (!sp2_active(state, step)) return;
   double a = 0.0, b = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     a += X[(size_t)i * n + i];
@@ -592,19 +596,26 @@ __global__ void k_sp2_trace(int n, const double *__restrict__ X, const double *_
   a = block_sum<256>(a);
   b = block_sum<256>(b);
   if (threadIdx.x == 0) {
-    state[0] = a;
-    state[1] = b;
-    state[2] = fabs(b - n_occ) < fabs(2.0 * a - b - n_occ) ? 1.0 : 0.0;
-    state[3] = a - b;
+    state[kSp2TrX] = a;
+    state[kSp2TrX2] = b;
+    state[kSp2Square] = fabs(b - n_occ) < fabs(2.0 * a - b - n_occ) ? 1.0 : 0.0;
+    state[kSp2Err] = a - b;
+    sp2_control(state, step, a - b, rule);
   }
 }
 
 // X <- X^2 or 2X - X^2 according to state[2].
 __global__ void k_sp2_update(size_t len, double *__restrict__ X, const double *__restrict__ X2,
-                             const double *__restrict__ state) {
-  const bool square = state[2] != 0.0;
+                             const double *__restrict__ state, int step) {
+  if (!sp2_active(state, step)) return;
+  const bool square = state[kSp2Square] != 0.0;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x)
     X[e] = square ? X2[e] : 2.0 * X[e] - X2[e];
+}
+
+__global__ void k_sp2_reset(double *state) {
+  const int i = threadIdx.x;
+  if (i < kSp2Len) state[i] = i == kSp2Stop ? 1.0e9 : 0.0;
 }
 
 void launch_gershgorin(cudaStream_t st, int n, const double *F, double *scratch, double *bounds) {
@@ -620,19 +631,25 @@ void launch_sp2_init(cudaStream_t st, int n, const double *F, const double *boun
   note_launch();
 }
 
-void launch_sp2_square(cudaStream_t st, int n, const double *X, double *X2) {
+void launch_sp2_reset(cudaStream_t st, double *state) {
+  k_sp2_reset<<<1, 32, 0, st>>>(state);
+  note_launch();
+}
+
+void launch_sp2_square(cudaStream_t st, int n, const double *X, double *X2, const double *state, int step) {
   gemm_smem_attr();
-  k_gemm_sym<<<sym_tiles(n), 128, SYM_SMEM, st>>>(n, n, 1.0, X, n, X, n, X2, n);
+  k_gemm_sym<<<sym_tiles(n), 128, SYM_SMEM, st>>>(n, n, 1.0, X, n, X, n, X2, n, state, step);
   note_launch();
 }
 
-void launch_sp2_trace(cudaStream_t st, int n, const double *X, const double *X2, double n_occ, double *state) {
-  k_sp2_trace<<<1, 256, 0, st>>>(n, X, X2, n_occ, state);
+void launch_sp2_trace(cudaStream_t st, int n, const double *X, const double *X2, double n_occ, double *state, int step,
+                      Sp2Rule rule) {
+  k_sp2_trace<<<1, 256, 0, st>>>(n, X, X2, n_occ, state, step, rule);
   note_launch();
 }
 
-void launch_sp2_update(cudaStream_t st, int n, double *X, const double *X2, const double *state) {
-  k_sp2_update<<<RED_BLOCKS * 2, 256, 0, st>>>((size_t)n * n, X, X2, state);
+void launch_sp2_update(cudaStream_t st, int n, double *X, const double *X2, const double *state, int step) {
+  k_sp2_update<<<RED_BLOCKS * 2, 256, 0, st>>>((size_t)n * n, X, X2, state, step);
   note_launch();
 }
 

@@ -19,6 +19,7 @@
 #include <cstdint>
 #include <mutex>
 
+#include "common.cuh"
 #include "kernels.hpp"
 
 namespace pm7 {
@@ -221,8 +222,12 @@ __device__ __forceinline__ void lower_tile(int t, int &bm, int &bn) {
 
 __global__ void __launch_bounds__(128) k_square_tf32x3(const __grid_constant__ CUtensorMap map_hi,
                                                        const __grid_constant__ CUtensorMap map_lo, int n, int ld,
-                                                       float *__restrict__ C, int *__restrict__ error) {
+                                                       float *__restrict__ C, int *__restrict__ error,
+                                                       const double *__restrict__ sp2, int step) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // an SP2 step after the purification stopped: the whole CTA leaves before any barrier,
+  // tensor-memory or copy set-up
+  if (!sp2_active(sp2, step)) return;
   int bm, bn;
   lower_tile(blockIdx.x, bm, bn);
   square_tile(bm, bn, &map_hi, &map_lo, n, ld, C, error, smem_raw);
@@ -265,7 +270,7 @@ bool make_square_map(const float *base, int ld, void *map_out) {
 size_t square_tf32x3_smem() { return SMEM_BYTES; }
 
 void launch_square_tf32x3(cudaStream_t st, int n, int ld, const void *map_hi, const void *map_lo, float *C,
-                          int *error) {
+                          int *error, const double *state, int step) {
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_square_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
@@ -274,7 +279,7 @@ void launch_square_tf32x3(cudaStream_t st, int n, int ld, const void *map_hi, co
   const int t = (n + TM - 1) / TM;
   k_square_tf32x3<<<t * (t + 1) / 2, 128, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap *>(map_hi),
                                                             *reinterpret_cast<const CUtensorMap *>(map_lo), n, ld, C,
-                                                            error);
+                                                            error, state, step);
   note_launch();
 }
 
@@ -351,7 +356,8 @@ __global__ void k_sp2_init32(int n, int ld, const double *__restrict__ F, const 
 
 // state[0] = tr X, state[1] = tr X^2 (fp64 sums), state[2] = SP2 branch, state[3] = tr X - tr X^2.
 __global__ void k_sp2_trace32(int n, int ld, const float *__restrict__ X, const float *__restrict__ X2, double n_occ,
-                              double *__restrict__ state) {
+                              double *__restrict__ state, int step, Sp2Rule rule) {
+  if (!sp2_active(state, step)) return;
   __shared__ double sa[8], sb[8];
   double a = 0.0, b = 0.0;
   for (int i = threadIdx.x; i < n; i += 256) {
@@ -378,12 +384,15 @@ __global__ void k_sp2_trace32(int n, int ld, const float *__restrict__ X, const 
     state[1] = b;
     state[2] = fabs(b - n_occ) < fabs(2.0 * a - b - n_occ) ? 1.0 : 0.0;
     state[3] = a - b;
+    sp2_control(state, step, a - b, rule);
   }
 }
 
 // X <- X^2 or 2X - X^2 by state[2], and its split.
 __global__ void k_sp2_update32(int n, int ld, float *__restrict__ X, const float *__restrict__ X2,
-                               const double *__restrict__ state, float *__restrict__ hi, float *__restrict__ lo) {
+                               const double *__restrict__ state, float *__restrict__ hi, float *__restrict__ lo,
+                               int step) {
+  if (!sp2_active(state, step)) return;
   const bool square = state[2] != 0.0;
   const size_t len = (size_t)n * n;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x) {
@@ -411,13 +420,14 @@ void launch_sp2_init32(cudaStream_t st, int n, int ld, const double *F, const do
   k_sp2_init32<<<1184, 256, 0, st>>>(n, ld, F, bounds, X, hi, lo);
   note_launch();
 }
-void launch_sp2_trace32(cudaStream_t st, int n, int ld, const float *X, const float *X2, double n_occ, double *state) {
-  k_sp2_trace32<<<1, 256, 0, st>>>(n, ld, X, X2, n_occ, state);
+void launch_sp2_trace32(cudaStream_t st, int n, int ld, const float *X, const float *X2, double n_occ, double *state,
+                        int step, Sp2Rule rule) {
+  k_sp2_trace32<<<1, 256, 0, st>>>(n, ld, X, X2, n_occ, state, step, rule);
   note_launch();
 }
 void launch_sp2_update32(cudaStream_t st, int n, int ld, float *X, const float *X2, const double *state, float *hi,
-                         float *lo) {
-  k_sp2_update32<<<1184, 256, 0, st>>>(n, ld, X, X2, state, hi, lo);
+                         float *lo, int step) {
+  k_sp2_update32<<<1184, 256, 0, st>>>(n, ld, X, X2, state, hi, lo, step);
   note_launch();
 }
 void launch_sp2_density32(cudaStream_t st, int n, int ld, const float *X, double w, double *P) {
