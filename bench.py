@@ -424,8 +424,8 @@ def run_batch_bench(args, world, rank, local):
     every = G.batch(4096 * world, seed=0)
     mols = [every[i] for i in shard.shard_of(every, rank, world)]
     opts = dict(device=local, want_matrices=0, precision=1 if args.precision == "mixed" else 0)
-    for _ in range(args.warmup):
-        api.run_batch(mols[:128], **opts)
+    for _ in range(args.warmup):  # full batches: the grow-only device and pinned buffers reach size
+        api.run_batch(mols, **opts)
     barrier(world)
     sampler = ClockSampler(local)
     sampler.start()
