@@ -947,6 +947,8 @@ class BatchRunner {
     CUDA_OK(cudaMalloc((void **)&err32_, sizeof(int)));
     CUDA_OK(cudaMemset(err32_, 0, sizeof(int)));
     CUDA_OK(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+    CUDA_OK(cudaStreamCreateWithFlags(&eig_st_, cudaStreamNonBlocking));
+    CUDA_OK(cudaEventCreateWithFlags(&eig_done_, cudaEventDisableTiming));
     for (Side &sd : side_) {
       CUDA_OK(cudaStreamCreateWithFlags(&sd.st, cudaStreamNonBlocking));
       SOLVER_OK(cusolverDnCreate(&sd.solver));
@@ -964,9 +966,15 @@ class BatchRunner {
   ~BatchRunner() {
     cudaSetDevice(ctx_.device);
     cudaStreamSynchronize(st_);
+    cudaStreamSynchronize(eig_st_);
+    for (Side &sd : side_)
+      if (sd.st) cudaStreamSynchronize(sd.st);
     for (auto &kv : active_) release(*kv);
-    eig_scr_.release(st_);
+    for (BatchMol *b : retiring_) release(*b);
+    eig_scr_.release(eig_st_);
+    cudaStreamSynchronize(eig_st_);
     cudaStreamSynchronize(st_);
+    if (rarena_) cudaFree(rarena_);
     if (desc_) cudaFree(desc_);
     if (ctl_) cudaFree(ctl_);
     if (arena_) cudaFree(arena_);
@@ -986,6 +994,8 @@ class BatchRunner {
       if (sd.st) cudaStreamDestroy(sd.st);
     }
     if (fork_) cudaEventDestroy(fork_);
+    if (eig_done_) cudaEventDestroy(eig_done_);
+    if (eig_st_) cudaStreamDestroy(eig_st_);
     cusolverDnDestroyParams(sparams_);
     cusolverDnDestroy(solver_);
     cudaStreamDestroy(st_);
@@ -1127,8 +1137,8 @@ class BatchRunner {
   // (their results filled, device memory released).
   std::vector<BatchMol *> iterate() {
     std::vector<BatchMol *> finished;
-    if (active_.empty()) return finished;
     CUDA_OK(cudaSetDevice(ctx_.device));
+    if (active_.empty()) return retiring_.empty() ? finished : retire_end();
     Lists A = lists(active_, false);
     const int n = A.mol.n;
     const int nb = (n + 127) / 128;
@@ -1244,9 +1254,25 @@ class BatchRunner {
     std::vector<BatchMol *> keep;
     for (int m = 0; m < n; ++m) (flags_h_[m] ? finished : keep).push_back(active_[m]);
     active_.swap(keep);
-    if (!finished.empty()) retire(finished);
-    return finished;
+    // the previous iteration's retirement (its eigensolves ran alongside this step)
+    std::vector<BatchMol *> done;
+    if (!retiring_.empty()) done = retire_end();
+    if (!finished.empty()) {
+      bool vectors = false;
+      for (const BatchMol *b : finished) vectors = vectors || b->o.want_matrices;
+      if (vectors) {
+        retire(finished);
+        done.insert(done.end(), finished.begin(), finished.end());
+      } else {
+        retire_begin(finished);
+      }
+    }
+    return done;
   }
+
+  // Molecules whose retirement eigensolves are still running.
+  int retiring_count() const { return (int)retiring_.size(); }
+  bool busy() const { return !active_.empty() || !retiring_.empty(); }
 
  private:
   struct Lists {
@@ -1325,8 +1351,11 @@ class BatchRunner {
   // Each ListUpload backs at most one list set in flight: the host writes its pinned
   // buffer immediately, so a second set on the same buffer before a stream sync would
   // overwrite what queued copies have not yet read.
-  Lists lists(const std::vector<BatchMol *> &mols, bool with_eig, ListUpload *upl = nullptr) {
+  Lists lists(const std::vector<BatchMol *> &mols, bool with_eig, ListUpload *upl = nullptr,
+              bool retire_arena = false) {
     ListUpload &up_ = upl ? *upl : this->up_;
+    double *&arena = retire_arena ? rarena_ : arena_;  // bucket matrices
+    size_t &arena_cap = retire_arena ? rarena_cap_ : arena_cap_;
     Lists A;
     const int n = (int)mols.size();
     up_.begin();
@@ -1378,13 +1407,13 @@ class BatchRunner {
       for (int m = 0; m < n; ++m) A.buckets[mols[m]->np].push_back(m);
       size_t total = 0;
       for (auto &kv : A.buckets) total += kv.second.size() * ((size_t)kv.first * kv.first + kv.first);
-      if (total > arena_cap_) {
-        if (arena_) CUDA_OK(cudaFreeAsync(arena_, st_));
-        arena_cap_ = total + total / 4;
-        CUDA_OK(cudaMallocAsync((void **)&arena_, 8 * arena_cap_, st_));
+      if (total > arena_cap) {
+        if (arena) CUDA_OK(cudaFreeAsync(arena, st_));
+        arena_cap = total + total / 4;
+        CUDA_OK(cudaMallocAsync((void **)&arena, 8 * arena_cap, st_));
       }
       A.eig_h.resize(n);
-      double *p = arena_;
+      double *p = arena;
       for (auto &kv : A.buckets) {
         const int np = kv.first, cnt = (int)kv.second.size();
         double *in = p, *w = p + (size_t)cnt * np * np;
@@ -1489,16 +1518,7 @@ class BatchRunner {
     const int n = A.mol.n;
     bool vectors = false;
     for (const BatchMol *b : R) vectors = vectors || b->o.want_matrices;
-    {
-      Stage s_(st_, "batch_finish");
-      launch_b_fock(st_, A.mol, A.rows, A.near, A.atoms, desc_, ctl_, *P_, 1);
-      k_b_energy_c<<<A.chunks.total, RB, 0, st_>>>(A.chunks, desc_, ctl_, 1);
-      k_b_reduce<<<(n + 127) / 128, 128, 0, st_>>>(n, A.mol.slot, desc_, ctl_, 1);
-      note_launch(2);
-      launch_b_corrections(st_, A.mol, A.pairs, desc_, ctl_, method_, A.max_atoms);
-      k_b_atom_out<<<n, 128, 0, st_>>>(A.mol, desc_, *P_);
-      note_launch();
-    }
+    finish_scf(A);
     {
       // reported orbitals: eigenvectors of the last extrapolated Fock, or of the final
       // Fock when a level shift was active (scf.rs:1299-1305)
@@ -1521,6 +1541,93 @@ class BatchRunner {
       k_b_save_orbitals<<<n, RB, 0, st_>>>(A.mol, desc_, A.eig);
       note_launch(2);
     }
+    finish_outputs(R, A, vectors);
+  }
+
+  // Final Fock and energy, corrections and per-atom outputs (the SCF's last step of the
+  // finished molecules), on the main stream.
+  void finish_scf(const Lists &A) {
+    const int n = A.mol.n;
+    Stage s_(st_, "batch_finish");
+    launch_b_fock(st_, A.mol, A.rows, A.near, A.atoms, desc_, ctl_, *P_, 1);
+    k_b_energy_c<<<A.chunks.total, RB, 0, st_>>>(A.chunks, desc_, ctl_, 1);
+    k_b_reduce<<<(n + 127) / 128, 128, 0, st_>>>(n, A.mol.slot, desc_, ctl_, 1);
+    note_launch(2);
+    launch_b_corrections(st_, A.mol, A.pairs, desc_, ctl_, method_, A.max_atoms);
+    k_b_atom_out<<<n, 128, 0, st_>>>(A.mol, desc_, *P_);
+    note_launch();
+  }
+
+  // Retirement without returned matrices, first half: the SCF's last step, the reported
+  // Fock into the retirement buckets, and the eigenvalue solves queued off the main stream
+  // (orders from kLeanEig: dsyevd on the side streams, on the nao x nao block of each
+  // bucket; below: the cluster kernel on eig_st_), writing straight into each molecule's
+  // eps_out. The next SCF step of the other molecules overlaps them; retire_end finishes.
+  void retire_begin(std::vector<BatchMol *> &R) {
+    Lists A = lists(R, true, nullptr, true);
+    const int n = A.mol.n;
+    finish_scf(A);
+    {
+      Stage s_(st_, "batch_orbitals");
+      k_b_to_bucket<<<n, RB, 0, st_>>>(A.mol, desc_, ctl_, A.eig, 2);
+      note_launch();
+    }
+    CUDA_OK(cudaEventRecord(fork_, st_));
+    std::vector<EigvalsRequest> small;
+    for (auto &kv : A.buckets) {
+      const int np = kv.first;
+      if (np < kLeanEig) {
+        for (int m : kv.second) small.push_back({A.eig_h[m].in, R[m]->L.nao, np, R[m]->d.eps_out});
+        continue;
+      }
+      int lwork = 0;
+      SOLVER_OK(cusolverDnDsyevd_bufferSize(solver_, CUSOLVER_EIG_MODE_NOVECTOR, CUBLAS_FILL_MODE_LOWER, np,
+                                            A.eig_h[kv.second[0]].in, np, A.eig_h[kv.second[0]].eps, &lwork));
+      const size_t wd = sizeof(double) * (size_t)lwork;
+      for (size_t i = 0; i < kv.second.size(); ++i) {
+        const int m = kv.second[i];
+        Side &sd = side_[rside_ % kSide];
+        ++rside_;
+        CUDA_OK(cudaStreamWaitEvent(sd.st, fork_, 0));
+        if (wd > sd.cap) {
+          if (sd.work) CUDA_OK(cudaFreeAsync(sd.work, sd.st));
+          sd.cap = wd + wd / 4;
+          CUDA_OK(cudaMallocAsync(&sd.work, sd.cap, sd.st));
+        }
+        SOLVER_OK(cusolverDnDsyevd(sd.solver, CUSOLVER_EIG_MODE_NOVECTOR, CUBLAS_FILL_MODE_LOWER, R[m]->L.nao,
+                                   A.eig_h[m].in, np, R[m]->d.eps_out, (double *)sd.work, lwork, sd.info));
+      }
+    }
+    if (!small.empty()) {
+      CUDA_OK(cudaStreamWaitEvent(eig_st_, fork_, 0));
+      Stage s_(eig_st_, "batch_orbitals_side");
+      eigvals_device(eig_st_, small, eig_scr_);
+    }
+    // the lists' pinned and device buffers are reused by the next step's lists
+    CUDA_OK(cudaStreamSynchronize(st_));
+    retiring_ = R;
+  }
+
+  // Second half: the main stream waits for the eigenvalue solves, then the packed outputs
+  // and the results. Returns the retired molecules.
+  std::vector<BatchMol *> retire_end() {
+    std::vector<BatchMol *> R;
+    R.swap(retiring_);
+    for (int k = 0; k < kSide; ++k) {
+      CUDA_OK(cudaEventRecord(side_[k].done, side_[k].st));
+      CUDA_OK(cudaStreamWaitEvent(st_, side_[k].done, 0));
+    }
+    CUDA_OK(cudaEventRecord(eig_done_, eig_st_));
+    CUDA_OK(cudaStreamWaitEvent(st_, eig_done_, 0));
+    Lists A = lists(R, false);
+    finish_outputs(R, A, false);
+    return R;
+  }
+
+  // Packed read-back of the retired molecules' outputs, their results on the host, and
+  // the release of their device memory.
+  void finish_outputs(std::vector<BatchMol *> &R, const Lists &A, bool vectors) {
+    const int n = A.mol.n;
     std::vector<long long> off(n + 1, 0);
     for (int m = 0; m < n; ++m)
       off[m + 1] = off[m] + kOutScalars + R[m]->L.nao + (long long)kAtomOut * R[m]->m.n;
@@ -1632,6 +1739,12 @@ class BatchRunner {
   double *arena_ = nullptr;
   size_t arena_cap_ = 0;
   EigvalsScratch eig_scr_;  // eigenvalue solves at retirement
+  std::vector<BatchMol *> retiring_;  // retirement eigensolves in flight (retire_begin)
+  double *rarena_ = nullptr;          // their bucket matrices
+  size_t rarena_cap_ = 0;
+  cudaStream_t eig_st_ = nullptr;     // the cluster eigenvalue kernel of retirements
+  cudaEvent_t eig_done_ = nullptr;
+  unsigned rside_ = 0;                // round robin over the side streams
   int side_used_ = 0;       // side streams with queued eigensolves not yet joined
   static constexpr int kLeanEig = 512;  // from this order the library solver, below the cluster one
   void *work_ = nullptr;
@@ -1692,7 +1805,7 @@ static void run_batch_impl(int n, const pm7_molecule *mols, const pm7_params *pa
   size_t next = 0;
   double t_admit = 0.0, t_iter = 0.0;
   int n_iter = 0;
-  while (next < pending.size() || runner.active_count() > 0) {
+  while (next < pending.size() || runner.busy()) {
     std::vector<BatchMol *> admit;
     size_t used = runner.bytes_in_use();
     while (next < pending.size() && (used + pending[next]->bytes <= budget || (runner.active_count() == 0 && admit.empty()))) {
@@ -1760,8 +1873,8 @@ static void engine_loop(pm7_engine *E) {
       std::vector<BatchMol *> admit;
       {
         std::unique_lock<std::mutex> lk(E->mu);
-        E->cv.wait(lk, [&] { return E->stop || !E->queue.empty() || E->runner->active_count() > 0; });
-        if (E->stop && E->runner->active_count() == 0) break;
+        E->cv.wait(lk, [&] { return E->stop || !E->queue.empty() || E->runner->busy(); });
+        if (E->stop && !E->runner->busy()) break;
         size_t used = E->runner->bytes_in_use();
         int active = E->runner->active_count();
         while (!E->queue.empty()) {
