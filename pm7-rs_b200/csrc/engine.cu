@@ -1172,14 +1172,25 @@ static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm
   R.fp32_iterations = S.fp32_iterations;
   const int nao = L.nao;
   const size_t nn = (size_t)nao * nao;
-  std::vector<double> Ph;
+  // The density back on the host: all of it when it is returned, else only the atom
+  // blocks the dipole needs (a full nao^2 copy is ~30 MB at 2,000 basis functions).
+  std::vector<double> Ph, blocks;
   if (S.converged) {
-    Ph.resize(nn);
-    CUDA_OK(cudaMemcpyAsync(Ph.data(), S.P.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+    if (o.want_matrices) {
+      Ph.resize(nn);
+      CUDA_OK(cudaMemcpyAsync(Ph.data(), S.P.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+    } else {
+      DevBuf<double> B;
+      B.alloc((size_t)81 * m.n, st);
+      launch_atom_blocks(st, m.n, D.aoff.p, D.z.p, P, nao, S.P.p, B.p);
+      blocks.resize((size_t)81 * m.n);
+      CUDA_OK(cudaMemcpyAsync(blocks.data(), B.p, sizeof(double) * blocks.size(), cudaMemcpyDeviceToHost, st));
+    }
     CUDA_OK(cudaStreamSynchronize(st));
   }
-  fill_result(res, m, L, ps, o, R, diag_blocks,
-              [&](int a, int i, int j) { return Ph[(size_t)(L.aoff[a] + i) * nao + L.aoff[a] + j]; });
+  fill_result(res, m, L, ps, o, R, diag_blocks, [&](int a, int i, int j) {
+    return o.want_matrices ? Ph[(size_t)(L.aoff[a] + i) * nao + L.aoff[a] + j] : blocks[(size_t)81 * a + 9 * i + j];
+  });
   if (o.want_matrices) {
     res->density = host_vec(Ph);
     if (S.unrestricted) res->spin_density = host_copy(S.Pspin.p, nn, st);

@@ -89,6 +89,9 @@ void launch_axpby(cudaStream_t st, size_t len, double a, const double *x, double
 void launch_set_diag(cudaStream_t st, int n, const double *diag, double *M);
 void launch_atom_pop(cudaStream_t st, int n_atoms, const int *aoff, const int *z, const DeviceParams &P,
                      int nao, const double *Pm, double *pop);
+// out[81 a + 9 i + j] = Pm of atom a's diagonal block (i, j < n_orb; 0 elsewhere).
+void launch_atom_blocks(cudaStream_t st, int n_atoms, const int *aoff, const int *z, const DeviceParams &P, int nao,
+                        const double *Pm, double *out);
 
 // ---- corrections (kernels_corr.cu) ----
 // out[0] dispersion, out[1] H-bond, out[2] C#C, out[3] Si-O-H, out[4] PM7-HH (kcal/mol).

@@ -29,6 +29,18 @@ __global__ void k_atom_pop(int n_atoms, const int *__restrict__ aoff, const int 
   pop[A] = s;
 }
 
+// The atom-diagonal density blocks, 9 x 9 per atom (n_orb x n_orb used), for the reported
+// dipole's hybrid terms without reading the whole density back.
+__global__ void k_atom_blocks(int n_atoms, const int *__restrict__ aoff, const int *__restrict__ z, DeviceParams P,
+                              int nao, const double *__restrict__ Pm, double *__restrict__ out) {
+  const int A = blockIdx.x;
+  const int off = aoff[A], no = P.elements[z[A]].n_orb;
+  for (int e = threadIdx.x; e < 81; e += blockDim.x) {
+    const int i = e / 9, j = e % 9;
+    out[(size_t)A * 81 + e] = (i < no && j < no) ? Pm[(size_t)(off + i) * nao + off + j] : 0.0;
+  }
+}
+
 __device__ __forceinline__ void fock_far_elem(const FockGeometry &g, const double *__restrict__ H,
                                               const double *__restrict__ Ps, double s_scale, double *__restrict__ F,
                                               int i, int j) {
@@ -246,6 +258,13 @@ void launch_b_fock(cudaStream_t st, const BatchList &Lmol, const BatchList &Lrow
   if (Lnear.total > 0) k_b_fock_near<<<Lnear.total, 128, 0, st>>>(Lnear, D, C, P, final_pass);
   note_launch();
   if (Latoms.total > 0) k_b_fock_atom<<<Latoms.total, ATOM_THREADS, 0, st>>>(Latoms, D, C, P, final_pass);
+  note_launch();
+}
+
+void launch_atom_blocks(cudaStream_t st, int n_atoms, const int *aoff, const int *z, const DeviceParams &P, int nao,
+                        const double *Pm, double *out) {
+  if (n_atoms <= 0) return;
+  k_atom_blocks<<<n_atoms, 96, 0, st>>>(n_atoms, aoff, z, P, nao, Pm, out);
   note_launch();
 }
 
