@@ -211,6 +211,11 @@ pm7_status pm7_stage_pair(const pm7_params *params, int32_t z_i, int32_t z_j, co
  * counterpart in pm7-rs (its density step diagonalises). */
 pm7_status pm7_stage_square_tf32(int32_t n, const double *x, double *c_out);
 
+/* C = A B of two symmetric n x n matrices on the tcgen05 tensor cores (3xTF32), the DIIS
+ * commutator product F P of the mixed-precision fp32 cycles; a stage for accuracy tests.
+ * Replaces, in those cycles, the product of `commutator_into` (src/scf.rs:1148-1156). */
+pm7_status pm7_stage_product_tf32(int32_t n, const double *a, const double *b, double *c_out);
+
 /* Eigenvalues (ascending, no eigenvectors) of `count` symmetric matrices, the stage that
  * gives the reported MO energies when no orbitals are returned. Replaces the eigenvalue
  * half of `symmetric_eigen` (src/linalg.rs:231-278, faer self_adjoint_eigen) as used by

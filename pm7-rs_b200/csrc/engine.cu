@@ -379,6 +379,28 @@ struct Purifier {
     if (!make_square_map(hi32.p, ld, map_hi) || !make_square_map(lo32.p, ld, map_lo))
       throw Failure{PM7_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
   }
+  // X = F P at fp32 accuracy on the tcgen05 tensor cores (3xTF32), for the DIIS error of
+  // the fp32 cycles: F into its own split pair, P into the SP2 split buffers (free between
+  // purifications; the next purification re-initialises them).
+  DevBuf<float> Fhi32, Flo32;
+  alignas(64) unsigned char mapF_hi[128], mapF_lo[128];
+  void product32(const double *F, const double *Pm, double *X) {
+    ensure32();
+    if (!Fhi32.p) {
+      const size_t ll = (size_t)ld * ld;
+      for (DevBuf<float> *b : {&Fhi32, &Flo32}) {
+        b->alloc(ll, st);
+        CUDA_OK(cudaMemsetAsync(b->p, 0, sizeof(float) * ll, st));
+      }
+      if (!make_square_map(Fhi32.p, ld, mapF_hi) || !make_square_map(Flo32.p, ld, mapF_lo))
+        throw Failure{PM7_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
+    }
+    launch_split_tf32(st, n, ld, F, Fhi32.p, Flo32.p);
+    launch_split_tf32(st, n, ld, Pm, hi32.p, lo32.p);
+    launch_product_tf32x3(st, n, ld, mapF_hi, mapF_lo, map_hi, map_lo, C32.p, err32.p);
+    launch_widen(st, n, ld, C32.p, X);
+  }
+
   // Queue SP2 steps in chunks and read the device state once per chunk: the device stops
   // the purification itself (Sp2Rule) and skips the steps queued after that. The first
   // chunk is sized from the previous purification's step count. Returns the steps run.
@@ -586,7 +608,14 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     launch_sum(st, partials.p, ne, dscal.p + 0);
     CUDA_OK(cudaMemcpyAsync(hD[slot].p, out.P.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
     // DIIS error e = F P - P F = F P - (F P)^T
-    { Stage s_(st, "commutator_gemm"); launch_gemm_tn(st, n, n, n, 1.0, Fk, n, out.P.p, n, X.p, n); }
+    if (phase32) {
+      // fp32 cycles: the product at fp32 accuracy (tcgen05), like their densities
+      Stage s_(st, "commutator_tf32");
+      pur.product32(Fk, out.P.p, X.p);
+    } else {
+      Stage s_(st, "commutator_gemm");
+      launch_gemm_tn(st, n, n, n, 1.0, Fk, n, out.P.p, n, X.p, n);
+    }
     size_t na = launch_antisym(st, n, X.p, hE[slot].p, partials.p);
     launch_sum(st, partials.p, na, dscal.p + 1);
     // inner products of the new entry with the history (chronological, newest last)
@@ -1414,6 +1443,41 @@ pm7_status pm7_stage_square_tf32(int32_t n, const double *x, double *c_out) {
     CUDA_OK(cudaStreamSynchronize(st));
     CUDA_OK(cudaGetLastError());
     if (e) throw Failure{PM7_ERR_CUDA, "tcgen05 squaring: a pipeline wait expired"};
+  });
+}
+
+pm7_status pm7_stage_product_tf32(int32_t n, const double *a, const double *b, double *c_out) {
+  return guarded([&] {
+    if (n < 1 || !a || !b || !c_out) throw Failure{PM7_ERR_INVALID_INPUT, "product_tf32 needs n >= 1 and buffers"};
+    DeviceContext &ctx = context_for(0);
+    std::lock_guard<std::mutex> lock(ctx.run_mutex);
+    CUDA_OK(cudaSetDevice(ctx.device));
+    cudaStream_t st = ctx.stream;
+    const int ld = ((n + 31) / 32) * 32;
+    const size_t nn = (size_t)n * n, ll = (size_t)ld * ld;
+    DevBuf<double> A, B, Cm;
+    DevBuf<float> ahi, alo, bhi, blo, C32;
+    DevBuf<int> err;
+    upload(A, std::vector<double>(a, a + nn), st);
+    upload(B, std::vector<double>(b, b + nn), st);
+    for (DevBuf<float> *q : {&ahi, &alo, &bhi, &blo, &C32}) q->alloc(ll, st);
+    Cm.alloc(nn, st);
+    err.alloc(1, st);
+    CUDA_OK(cudaMemsetAsync(err.p, 0, sizeof(int), st));
+    launch_split_tf32(st, n, ld, A.p, ahi.p, alo.p);
+    launch_split_tf32(st, n, ld, B.p, bhi.p, blo.p);
+    alignas(64) unsigned char m_ahi[128], m_alo[128], m_bhi[128], m_blo[128];
+    if (!make_square_map(ahi.p, ld, m_ahi) || !make_square_map(alo.p, ld, m_alo) ||
+        !make_square_map(bhi.p, ld, m_bhi) || !make_square_map(blo.p, ld, m_blo))
+      throw Failure{PM7_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
+    launch_product_tf32x3(st, n, ld, m_ahi, m_alo, m_bhi, m_blo, C32.p, err.p);
+    launch_widen(st, n, ld, C32.p, Cm.p);
+    int e = 0;
+    CUDA_OK(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(c_out, Cm.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaGetLastError());
+    if (e) throw Failure{PM7_ERR_CUDA, "tcgen05 product: a pipeline wait expired"};
   });
 }
 

@@ -135,6 +135,9 @@ size_t square_tf32x3_smem();
 // state/step: as the fp64 SP2 steps (state may be null: always runs).
 void launch_square_tf32x3(cudaStream_t st, int n, int ld, const void *map_hi, const void *map_lo, float *C,
                           int *error, const double *state = nullptr, int step = 0);
+// C = A B for symmetric A, B given as split tensor maps (all 128x128 tiles, no mirror).
+void launch_product_tf32x3(cudaStream_t st, int n, int ld, const void *a_hi, const void *a_lo, const void *b_hi,
+                           const void *b_lo, float *C, int *error);
 void launch_split_tf32(cudaStream_t st, int n, int ld, const double *X, float *hi, float *lo);
 void launch_widen(cudaStream_t st, int n, int ld, const float *C32, double *C);
 // The fp32 SP2 iteration: start, traces (fp64 sums), update with re-split, density.

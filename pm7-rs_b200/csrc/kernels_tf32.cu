@@ -1,5 +1,6 @@
-// FP32-accuracy symmetric squaring C = X X on the 5th-generation tensor cores (tcgen05,
-// kind::tf32) for the mixed-precision SP2 purification.
+// FP32-accuracy products of symmetric matrices on the 5th-generation tensor cores (tcgen05,
+// kind::tf32) for the mixed-precision SCF cycles: the SP2 squaring C = X X and the DIIS
+// commutator product F P.
 //
 // X is stored split as X = Xhi + Xlo with Xhi = tf32(X) and Xlo = X - Xhi (both fp32
 // arrays, row-major, leading dimension ld, zero padded to ld); the product is accumulated
@@ -103,11 +104,15 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
                : "memory");
 }
 
-// One 128x128 lower tile (bm >= bn) of C = X X; `smem_raw` is the CTA's dynamic shared
-// memory (SMEM_BYTES), map_hi / map_lo the tensor maps of the split operand.
-__device__ __forceinline__ void square_tile(int bm, int bn, const CUtensorMap *map_hi, const CUtensorMap *map_lo,
-                                            int n, int ld, float *__restrict__ C, int *__restrict__ error,
-                                            unsigned char *smem_raw) {
+// One 128x128 tile (bm, bn) of C = A B for symmetric A, B (so B's columns are its rows:
+// both operands K-major row blocks). `smem_raw` is the CTA's dynamic shared memory
+// (SMEM_BYTES); a_hi / a_lo and b_hi / b_lo the tensor maps of the split operands. With
+// `mirror` (the squaring, A = B, lower tiles bm >= bn only) each element of the lower
+// triangle is written with its mirror; without, the tile is written as it is.
+__device__ __forceinline__ void product_tile(int bm, int bn, const CUtensorMap *a_hi, const CUtensorMap *a_lo,
+                                             const CUtensorMap *b_hi, const CUtensorMap *b_lo, bool mirror, int n,
+                                             int ld, float *__restrict__ C, int *__restrict__ error,
+                                             unsigned char *smem_raw) {
   // stage buffers on a 1024-byte boundary (128-byte swizzle atoms)
   unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
@@ -147,10 +152,10 @@ __device__ __forceinline__ void square_tile(int bm, int bn, const CUtensorMap *m
       unsigned char *st = smem + s * STAGE_BYTES;
       mbar_expect_tx(&full[s], STAGE_BYTES);
       const int k0 = kt * TK;
-      tma_load_2d(st + 0 * TILE_BYTES, map_hi, &full[s], k0, m0);
-      tma_load_2d(st + 1 * TILE_BYTES, map_lo, &full[s], k0, m0);
-      tma_load_2d(st + 2 * TILE_BYTES, map_hi, &full[s], k0, n0);
-      tma_load_2d(st + 3 * TILE_BYTES, map_lo, &full[s], k0, n0);
+      tma_load_2d(st + 0 * TILE_BYTES, a_hi, &full[s], k0, m0);
+      tma_load_2d(st + 1 * TILE_BYTES, a_lo, &full[s], k0, m0);
+      tma_load_2d(st + 2 * TILE_BYTES, b_hi, &full[s], k0, n0);
+      tma_load_2d(st + 3 * TILE_BYTES, b_lo, &full[s], k0, n0);
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
@@ -199,10 +204,14 @@ __device__ __forceinline__ void square_tile(int bm, int bn, const CUtensorMap *m
 #pragma unroll
       for (int q = 0; q < 32; ++q) {
         const int col = n0 + c * 32 + q;
-        if (row >= n || col >= n || row < col) continue;  // lower triangle, each element once
+        if (row >= n || col >= n) continue;
         const float v = __uint_as_float(r[q]);
-        C[(size_t)row * ld + col] = v;
-        C[(size_t)col * ld + row] = v;
+        if (!mirror) {
+          C[(size_t)row * ld + col] = v;
+        } else if (row >= col) {  // lower triangle, each element once, and its mirror
+          C[(size_t)row * ld + col] = v;
+          C[(size_t)col * ld + row] = v;
+        }
       }
     }
   } else if (threadIdx.x == 0) {
@@ -230,7 +239,19 @@ __global__ void __launch_bounds__(128) k_square_tf32x3(const __grid_constant__ C
   if (!sp2_active(sp2, step)) return;
   int bm, bn;
   lower_tile(blockIdx.x, bm, bn);
-  square_tile(bm, bn, &map_hi, &map_lo, n, ld, C, error, smem_raw);
+  product_tile(bm, bn, &map_hi, &map_lo, &map_hi, &map_lo, true, n, ld, C, error, smem_raw);
+}
+
+// C = A B of two symmetric split operands, every 128x128 tile (the DIIS commutator F P of
+// the fp32 cycles).
+__global__ void __launch_bounds__(128) k_product_tf32x3(const __grid_constant__ CUtensorMap a_hi,
+                                                        const __grid_constant__ CUtensorMap a_lo,
+                                                        const __grid_constant__ CUtensorMap b_hi,
+                                                        const __grid_constant__ CUtensorMap b_lo, int n, int ld,
+                                                        float *__restrict__ C, int *__restrict__ error) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  const int t = (n + TM - 1) / TM;
+  product_tile(blockIdx.x / t, blockIdx.x % t, &a_hi, &a_lo, &b_hi, &b_lo, false, n, ld, C, error, smem_raw);
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
@@ -268,6 +289,20 @@ bool make_square_map(const float *base, int ld, void *map_out) {
 }
 
 size_t square_tf32x3_smem() { return SMEM_BYTES; }
+
+void launch_product_tf32x3(cudaStream_t st, int n, int ld, const void *a_hi, const void *a_lo, const void *b_hi,
+                           const void *b_lo, float *C, int *error) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_product_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    attr = true;
+  }
+  const int t = (n + TM - 1) / TM;
+  k_product_tf32x3<<<t * t, 128, SMEM_BYTES, st>>>(
+      *reinterpret_cast<const CUtensorMap *>(a_hi), *reinterpret_cast<const CUtensorMap *>(a_lo),
+      *reinterpret_cast<const CUtensorMap *>(b_hi), *reinterpret_cast<const CUtensorMap *>(b_lo), n, ld, C, error);
+  note_launch();
+}
 
 void launch_square_tf32x3(cudaStream_t st, int n, int ld, const void *map_hi, const void *map_lo, float *C,
                           int *error, const double *state, int step) {
@@ -456,7 +491,8 @@ __global__ void __launch_bounds__(128) k_b_square_tf32x3(BatchList L, const MolD
   int bm, bn;
   lower_tile(item - L.prefix[m], bm, bn);
   const MolDesc &d = D[slot];
-  square_tile(bm, bn, &maps[2 * slot], &maps[2 * slot + 1], d.g.nao, d.ld32, d.C32, error, smem_raw);
+  product_tile(bm, bn, &maps[2 * slot], &maps[2 * slot + 1], &maps[2 * slot], &maps[2 * slot + 1], true, d.g.nao,
+               d.ld32, d.C32, error, smem_raw);
 }
 
 // X32 = fp32 of the (fp64) SP2 start X, and its split. Item = a chunk.

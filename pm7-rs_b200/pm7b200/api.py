@@ -23,6 +23,7 @@ EXPORTED = [
     "pm7_device_count", "pm7_stage_core_hamiltonian", "pm7_stage_fock", "pm7_stage_pair", "pm7_stage_core_core",
     "pm7_stage_corrections", "pm7_run_batch", "pm7_engine_config_default", "pm7_engine_create", "pm7_engine_submit",
     "pm7_engine_poll", "pm7_engine_destroy", "pm7_batch_partition", "pm7_stage_eigenvalues",
+    "pm7_stage_product_tf32",
 ]
 
 
@@ -367,6 +368,19 @@ def eigenvalues(matrices, device=0):
         res.append(out[off:off + n].copy())
         off += n
     return res
+
+
+def product_tf32(a, b):
+    """C = A B of two symmetric matrices on the tcgen05 tensor cores (3xTF32 split, fp32
+    accumulation): the commutator product of the mixed-precision fp32 cycles."""
+    L = lib()
+    L.pm7_stage_product_tf32.argtypes = [C.c_int32, abi.DP, abi.DP, abi.DP]
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    n = a.shape[0]
+    out = np.zeros((n, n))
+    _check(L.pm7_stage_product_tf32(n, a.ctypes.data_as(abi.DP), b.ctypes.data_as(abi.DP), out.ctypes.data_as(abi.DP)))
+    return out
 
 
 def square_tf32(x):

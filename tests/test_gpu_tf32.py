@@ -31,6 +31,21 @@ def test_square_matches_fp64(n):
     assert np.array_equal(c, c.T)  # written once and mirrored
 
 
+@pytest.mark.parametrize("n", [40, 128, 131, 300, 517])
+def test_product_matches_fp64(n):
+    # the DIIS commutator product F P of the fp32 cycles: two different symmetric operands,
+    # a Fock-like one with a wide spectrum and an SP2-like one in [0, 1]
+    rng = np.random.default_rng(n + 1)
+    f = rng.normal(size=(n, n))
+    f = 0.5 * (f + f.T) * 10.0 + np.diag(np.linspace(-40.0, 20.0, n))
+    p = _iterate(n, n + 2)
+    c = api.product_tf32(f, p)
+    ref = f @ p
+    err = np.max(np.abs(c - ref)) / np.max(np.abs(ref))
+    assert err < 4e-8 * max(n, 64), err
+    assert not np.array_equal(c, c.T)  # every tile written, no mirror
+
+
 def test_square_is_deterministic():
     x = _iterate(300, 3)
     assert np.array_equal(api.square_tf32(x), api.square_tf32(x))
