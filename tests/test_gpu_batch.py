@@ -183,3 +183,29 @@ def test_mixed_precision_large_chain_leaves_the_fp32_phase():
     for r in (b, s):
         assert 0 < r["fp32_iterations"] < r["iterations"]
         assert abs(r["heat_of_formation_kcal"] - f["heat_of_formation_kcal"]) < 1.0e-4
+
+
+def test_engine_without_matrices_retires_asynchronously_and_alone_equals_mixed():
+    # without returned matrices a retirement's eigenvalue solves run beside the next SCF
+    # step and its outputs are gathered one step later; results must not change
+    target = G.water_cluster(14, seed=5)
+    big = G.water_cluster(180, seed=6)  # order >= 512: the library eigensolver on a side stream
+    others = [G.alkane(n, seed=n) for n in (3, 11, 26)] + [G.water_cluster(k, seed=k) for k in (8, 40)] + [big]
+    with api.Engine() as eng:
+        t = eng.submit(*target, want_matrices=0)
+        done, alone = eng.poll(t, wait=True)
+        assert done and not isinstance(alone, Exception)
+        tickets = [eng.submit(*m, want_matrices=0) for m in others[:3]]
+        t2 = eng.submit(*target, want_matrices=0)
+        tickets += [eng.submit(*m, want_matrices=0) for m in others[3:]]
+        done, mixed = eng.poll(t2, wait=True)
+        rest = [eng.poll(tk, wait=True)[1] for tk in tickets]
+    assert all(not isinstance(r, Exception) for r in rest)
+    assert abs(alone["heat_of_formation_kcal"] - mixed["heat_of_formation_kcal"]) < 1e-9
+    np.testing.assert_array_equal(alone["mo_energies"], mixed["mo_energies"])
+    o = harness.run(*target)
+    assert abs(mixed["heat_of_formation_kcal"] - o["heat_of_formation_kcal"]) < DHF_TOL
+    assert abs(mixed["homo_ev"] - o["homo_ev"]) < 1e-5 and abs(mixed["lumo_ev"] - o["lumo_ev"]) < 1e-5
+    full = api.run_pm7(*big, want_matrices=1)
+    np.testing.assert_allclose(rest[-1]["mo_energies"], full["mo_energies"], rtol=0, atol=1e-8)
+    assert abs(rest[-1]["heat_of_formation_kcal"] - full["heat_of_formation_kcal"]) < 1e-7
