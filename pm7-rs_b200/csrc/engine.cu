@@ -454,26 +454,42 @@ struct Purifier {
     return true;
   }
 
+  // Lanczos workspace for the tighter interval; once a refined interval has failed, this
+  // purifier keeps to Gershgorin.
+  DevBuf<double> lz;
+  bool tight = true;
   bool project(const double *F, int n_occ, double w, double *P) {
-    launch_gershgorin(st, n, F, scratch.p, bounds.p);
-    launch_sp2_init(st, n, F, bounds.p, X.p);
-    const Sp2Rule rule{1.0e-13 * std::max(1, n_occ), 1.0e-6, kMaxSteps};
-    last_iterations = run_chunks(
-        [&](int s) {
-          {
-            Stage g_(st, "sp2_square_gemm");
-            launch_sp2_square(st, n, X.p, X2.p, state.p, s);
-          }
-          launch_sp2_trace(st, n, X.p, X2.p, (double)n_occ, state.p, s, rule);
-          launch_sp2_update(st, n, X.p, X2.p, state.p, s);
-        },
-        "sp2_square_gemm", hint64);
-    bool ok = pin[kSp2Ok] != 0.0;
-    // an idempotent X whose trace is not n_occ is a wrong projector (degenerate frontier)
-    if (ok && std::fabs(pin[kSp2TrX] - (double)n_occ) > 1.0e-3) ok = false;
-    if (!ok) return false;
-    launch_scale(st, (size_t)n * n, w, X.p, P);
-    return true;
+    if (tight && !lz.p) lz.alloc(lanczos_doubles(n), st);
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      const bool refine = tight && attempt == 0;
+      launch_gershgorin(st, n, F, scratch.p, bounds.p);
+      if (refine) {
+        Stage l_(st, "sp2_bounds");
+        launch_lanczos_bounds(st, n, F, lz.p, bounds.p);
+      }
+      launch_sp2_init(st, n, F, bounds.p, X.p);
+      const Sp2Rule rule{1.0e-13 * std::max(1, n_occ), 1.0e-6, kMaxSteps};
+      last_iterations = run_chunks(
+          [&](int s) {
+            {
+              Stage g_(st, "sp2_square_gemm");
+              launch_sp2_square(st, n, X.p, X2.p, state.p, s);
+            }
+            launch_sp2_trace(st, n, X.p, X2.p, (double)n_occ, state.p, s, rule);
+            launch_sp2_update(st, n, X.p, X2.p, state.p, s);
+          },
+          "sp2_square_gemm", hint64);
+      bool ok = pin[kSp2Ok] != 0.0;
+      // an idempotent X whose trace is not n_occ is a wrong projector (degenerate frontier)
+      if (ok && std::fabs(pin[kSp2TrX] - (double)n_occ) > 1.0e-3) ok = false;
+      if (ok) {
+        launch_scale(st, (size_t)n * n, w, X.p, P);
+        return true;
+      }
+      if (!refine) return false;
+      tight = false;  // the refined interval missed part of the spectrum: Gershgorin from now on
+    }
+    return false;
   }
 };
 

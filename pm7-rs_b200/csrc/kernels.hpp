@@ -154,6 +154,12 @@ namespace pm7 {
 // SP2 purification building blocks (kernels_dense.cu).
 void launch_gershgorin(cudaStream_t st, int n, const double *F, double *scratch, double *bounds);
 void launch_sp2_init(cudaStream_t st, int n, const double *F, const double *bounds, double *X);
+// Lanczos refinement of the SP2 interval in bounds[0..1] (which holds the Gershgorin one):
+// kLzSteps steps on F, workspace lanczos_doubles(n). Matrices below 2 kLzSteps keep the
+// Gershgorin interval.
+constexpr int kLzSteps = 16;
+size_t lanczos_doubles(int n);
+void launch_lanczos_bounds(cudaStream_t st, int n, const double *F, double *lz, double *bounds);
 void launch_sp2_reset(cudaStream_t st, double *state);
 void launch_sp2_square(cudaStream_t st, int n, const double *X, double *X2, const double *state, int step);
 void launch_sp2_trace(cudaStream_t st, int n, const double *X, const double *X2, double n_occ, double *state, int step,
