@@ -513,6 +513,134 @@ __global__ void k_b_sp2_bounds(int n, const int *__restrict__ slots, const MolDe
   c.sp2_apply = 0;
 }
 
+// Per molecule (one 1,024-thread CTA): kLzSteps Lanczos steps on its extrapolated Fock
+// (d.X, before the SP2 map), the vectors in shared memory (3 nao doubles), and the SP2
+// interval narrowed to [theta_min - 3% R, theta_max + 5% R] inside the Gershgorin one that
+// k_b_sp2_bounds left in sp2_emin / sp2_emax (widened like it). Orders below 2 kLzSteps or
+// above kLzMaxOrder keep the Gershgorin interval. Deterministic: fixed-order reductions.
+constexpr int kLzMaxOrder = 4096;
+__device__ __forceinline__ double lz_block_sum(double v, double *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    double s = red[lane];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[32] = s;
+  }
+  __syncthreads();
+  return red[32];
+}
+__device__ int lz_sturm(const double *a, const double *b, int m, double x) {
+  int c = 0;
+  double q = a[0] - x;
+  if (q == 0.0) q = -1.0e-300;
+  c += q < 0.0;
+  for (int i = 1; i < m; ++i) {
+    q = a[i] - x - b[i] * b[i] / q;
+    if (q == 0.0) q = -1.0e-300;
+    c += q < 0.0;
+  }
+  return c;
+}
+__global__ void __launch_bounds__(1024) k_b_lanczos(BatchList L, const MolDesc *__restrict__ D,
+                                                    MolCtl *__restrict__ C) {
+  extern __shared__ double lzs[];
+  const int m = blockIdx.x;
+  const int slot = L.slot[m];
+  const MolDesc &d = D[slot];
+  MolCtl &c = C[slot];
+  const int n = d.g.nao;
+  if (n < 2 * kLzSteps || n > kLzMaxOrder) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double *vp = lzs, *v = lzs + n, *w = lzs + 2 * n, *red = lzs + 3 * n;
+  __shared__ double alpha[kLzSteps], beta[kLzSteps + 1];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += 1024) {
+    const double x = 1.0 + 0.5 * sin(0.7 * i);
+    v[i] = x;
+    vp[i] = 0.0;
+    s += x * x;
+  }
+  s = lz_block_sum(s, red);
+  const double inv0 = 1.0 / sqrt(s);
+  for (int i = threadIdx.x; i < n; i += 1024) v[i] *= inv0;
+  double bj = 0.0;
+  for (int j = 0; j < kLzSteps; ++j) {
+    __syncthreads();
+    for (int i = warp; i < n; i += 32) {  // w = X v, a warp per row
+      const double *xi = d.X + (size_t)i * n;
+      double acc = 0.0;
+      for (int base = lane; base < n; base += 256) {
+        double t[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int k = base + 32 * u;
+          t[u] = k < n ? xi[k] * v[k] : 0.0;
+        }
+        acc += ((t[0] + t[1]) + (t[2] + t[3])) + ((t[4] + t[5]) + (t[6] + t[7]));
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) w[i] = acc;
+    }
+    __syncthreads();
+    double a = 0.0;
+    for (int i = threadIdx.x; i < n; i += 1024) a += w[i] * v[i];
+    a = lz_block_sum(a, red);
+    double q = 0.0;
+    for (int i = threadIdx.x; i < n; i += 1024) {
+      const double x = w[i] - a * v[i] - bj * vp[i];
+      w[i] = x;
+      q += x * x;
+    }
+    q = lz_block_sum(q, red);
+    const double b = sqrt(q);
+    if (threadIdx.x == 0) {
+      alpha[j] = a;
+      beta[j + 1] = b;
+    }
+    const double inv = b > 1.0e-280 ? 1.0 / b : 0.0;
+    for (int i = threadIdx.x; i < n; i += 1024) {
+      vp[i] = v[i];
+      v[i] = w[i] * inv;
+    }
+    bj = b;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double g_lo = 1.0e300, g_hi = -1.0e300;
+  for (int i = 0; i < kLzSteps; ++i) {
+    const double r = (i > 0 ? fabs(beta[i]) : 0.0) + (i + 1 < kLzSteps ? fabs(beta[i + 1]) : 0.0);
+    g_lo = fmin(g_lo, alpha[i] - r);
+    g_hi = fmax(g_hi, alpha[i] + r);
+  }
+  double lo = g_lo, hi = g_hi;
+  for (int it = 0; it < 100; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (lz_sturm(alpha, beta, kLzSteps, mid) >= 1) hi = mid;
+    else lo = mid;
+  }
+  const double tmin = hi;
+  lo = g_lo;
+  hi = g_hi;
+  for (int it = 0; it < 100; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (lz_sturm(alpha, beta, kLzSteps, mid) >= kLzSteps) hi = mid;
+    else lo = mid;
+  }
+  const double tmax = hi, R = tmax - tmin;
+  if (!(R > 0.0) || !isfinite(R)) return;
+  const double elo = fmax(tmin - 0.03 * R, c.sp2_emin), ehi = fmin(tmax + 0.05 * R, c.sp2_emax);
+  const double pad = 1.0e-3 * (ehi - elo) + 1.0e-6;
+  c.sp2_emin = fmax(elo - pad, c.sp2_emin);
+  c.sp2_emax = fmin(ehi + pad, c.sp2_emax);
+}
+
 // X <- (emax I - X) / (emax - emin): spectrum in [0, 1], occupied levels near 1. Item = a chunk.
 __global__ void __launch_bounds__(RB) k_b_sp2_x0(BatchList L, const MolDesc *__restrict__ D,
                                                  const MolCtl *__restrict__ C) {
@@ -1190,6 +1318,7 @@ class BatchRunner {
         if (L->mol.n == 0) continue;
         k_b_sp2_fuse<<<L->rows.total, RB, 0, st_>>>(L->rows, desc_, ctl_);
         k_b_sp2_bounds<<<(L->mol.n + 127) / 128, 128, 0, st_>>>(L->mol.n, L->mol.slot, desc_, ctl_);
+        launch_b_lanczos(*L, L == &S ? purify64 : purify32);
         k_b_sp2_x0<<<L->chunks.total, RB, 0, st_>>>(L->chunks, desc_, ctl_);
         note_launch(3);
       }
@@ -1501,6 +1630,20 @@ class BatchRunner {
     }
   }
 
+  // Lanczos-narrowed SP2 intervals for the molecules of list set L (vectors in shared memory).
+  void launch_b_lanczos(const Lists &L, const std::vector<BatchMol *> &mols) {
+    int nmax = 0;
+    for (const BatchMol *b : mols) nmax = std::max(nmax, std::min(b->L.nao, kLzMaxOrder));
+    if (nmax < 2 * kLzSteps) return;
+    const size_t smem = sizeof(double) * (3 * (size_t)nmax + 33);
+    if (smem > lz_smem_) {
+      CUDA_OK(cudaFuncSetAttribute(k_b_lanczos, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      lz_smem_ = smem;
+    }
+    k_b_lanczos<<<L.mol.n, 1024, smem, st_>>>(L.mol, desc_, ctl_);
+    note_launch();
+  }
+
   // The main stream waits for the side streams' eigensolves.
   void join_side() {
     for (int k = 0; k < side_used_; ++k) {
@@ -1746,6 +1889,7 @@ class BatchRunner {
   cudaEvent_t eig_done_ = nullptr;
   unsigned rside_ = 0;                // round robin over the side streams
   int side_used_ = 0;       // side streams with queued eigensolves not yet joined
+  size_t lz_smem_ = 48 * 1024;  // dynamic shared memory k_b_lanczos is set up for
   static constexpr int kLeanEig = 512;  // from this order the library solver, below the cluster one
   void *work_ = nullptr;
   size_t work_cap_ = 0;
