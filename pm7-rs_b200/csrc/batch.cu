@@ -421,6 +421,8 @@ __device__ __forceinline__ double fuse_elem(const MolDesc &d, const MolCtl &c, c
 // The molecule's padded bucket matrix from: the extrapolated Fock (src 0), the final
 // Fock in X (src 1), or, for reporting orbitals, the final Fock when a level shift was
 // active and the last extrapolated Fock otherwise (src 2, scf.rs:1299-1305).
+// Grid: x = molecule, y = blocks sharing its matrix (kBucketBlocks).
+constexpr int kBucketBlocks = 32;
 __global__ void __launch_bounds__(RB) k_b_to_bucket(BatchList L, const MolDesc *__restrict__ D,
                                                     const MolCtl *__restrict__ C, const EigSlot *__restrict__ E,
                                                     int src) {
@@ -434,7 +436,7 @@ __global__ void __launch_bounds__(RB) k_b_to_bucket(BatchList L, const MolDesc *
   const double *Fs[kHist];
   for (int i = 0; i < kHist; ++i) Fs[i] = hist_F(d, i < c.ncoef ? c.csrc[i] : 0);
   const size_t len = (size_t)np * np;
-  for (size_t e = threadIdx.x; e < len; e += RB) {
+  for (size_t e = (size_t)blockIdx.y * RB + threadIdx.x; e < len; e += (size_t)gridDim.y * RB) {
     const int r = (int)(e / np), col = (int)(e - (size_t)r * np);
     double v;
     if (r < n && col < n) v = src == 1 ? d.X[(size_t)r * n + col] : fuse_elem(d, c, Fs, r, col);
@@ -1366,7 +1368,7 @@ class BatchRunner {
     if (!fallback.empty()) {
       Stage s_(st_, "batch_eigensolve");
       Lists B = lists(fallback, true, &up_fallback_);
-      k_b_to_bucket<<<B.mol.n, RB, 0, st_>>>(B.mol, desc_, ctl_, B.eig, 0);
+      k_b_to_bucket<<<dim3(B.mol.n, kBucketBlocks), RB, 0, st_>>>(B.mol, desc_, ctl_, B.eig, 0);
       note_launch();
       eigensolve(B);
       launch_b_gemm(st_, B.glow, desc_, ctl_, B.eig, 1);
@@ -1666,7 +1668,7 @@ class BatchRunner {
       // reported orbitals: eigenvectors of the last extrapolated Fock, or of the final
       // Fock when a level shift was active (scf.rs:1299-1305)
       Stage s_(st_, "batch_orbitals");
-      k_b_to_bucket<<<n, RB, 0, st_>>>(A.mol, desc_, ctl_, A.eig, 2);
+      k_b_to_bucket<<<dim3(n, kBucketBlocks), RB, 0, st_>>>(A.mol, desc_, ctl_, A.eig, 2);
       if (vectors) {
         eigensolve(A, true);
       } else {
@@ -1712,7 +1714,7 @@ class BatchRunner {
     finish_scf(A);
     {
       Stage s_(st_, "batch_orbitals");
-      k_b_to_bucket<<<n, RB, 0, st_>>>(A.mol, desc_, ctl_, A.eig, 2);
+      k_b_to_bucket<<<dim3(n, kBucketBlocks), RB, 0, st_>>>(A.mol, desc_, ctl_, A.eig, 2);
       note_launch();
     }
     CUDA_OK(cudaEventRecord(fork_, st_));
