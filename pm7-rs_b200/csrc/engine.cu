@@ -18,6 +18,7 @@
 #include <functional>
 #include <limits>
 #include <map>
+#include <thread>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -183,29 +184,44 @@ Layout build_layout(const Molecule &m, const ParamSet &ps) {
                (long long)std::floor(m.xyz[3 * i + 2] / cut)};
     cells[key[i]].push_back(i);
   }
-  std::vector<int> partners;
-  for (int u = 0; u < m.n; ++u) {
-    partners.clear();
-    for (int dx = -1; dx <= 1; ++dx)
-      for (int dy = -1; dy <= 1; ++dy)
-        for (int dz = -1; dz <= 1; ++dz) {
-          auto it = cells.find(K{key[u].a + dx, key[u].b + dy, key[u].c + dz});
-          if (it == cells.end()) continue;
-          for (int v : it->second) {
-            if (v <= u) continue;
-            const double ex = m.xyz[3 * v] - m.xyz[3 * u], ey = m.xyz[3 * v + 1] - m.xyz[3 * u + 1],
-                         ez = m.xyz[3 * v + 2] - m.xyz[3 * u + 2];
-            if (std::sqrt(ex * ex + ey * ey + ez * ez) * kA0 < 7.0) partners.push_back(v);
+  // partners of each atom, on several host threads for large molecules (atom ranges,
+  // concatenated in atom order: the pair list is the same as a serial scan's)
+  const int workers = m.n >= 512 ? (int)std::min(8u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+  std::vector<std::vector<NearPair>> part(workers);
+  auto scan = [&](int w) {
+    const int a0 = (int)((long long)m.n * w / workers), a1 = (int)((long long)m.n * (w + 1) / workers);
+    std::vector<int> partners;
+    for (int u = a0; u < a1; ++u) {
+      partners.clear();
+      for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dz = -1; dz <= 1; ++dz) {
+            auto it = cells.find(K{key[u].a + dx, key[u].b + dy, key[u].c + dz});
+            if (it == cells.end()) continue;
+            for (int v : it->second) {
+              if (v <= u) continue;
+              const double ex = m.xyz[3 * v] - m.xyz[3 * u], ey = m.xyz[3 * v + 1] - m.xyz[3 * u + 1],
+                           ez = m.xyz[3 * v + 2] - m.xyz[3 * u + 2];
+              if (std::sqrt(ex * ex + ey * ey + ez * ez) * kA0 < 7.0) partners.push_back(v);
+            }
           }
-        }
-    std::sort(partners.begin(), partners.end());
-    for (int v : partners) {
-      NearPair q;
-      q.u = u;
-      q.v = v;
-      L.near.push_back(q);
+      std::sort(partners.begin(), partners.end());
+      for (int v : partners) {
+        NearPair q;
+        q.u = u;
+        q.v = v;
+        part[w].push_back(q);
+      }
     }
+  };
+  if (workers == 1) {
+    scan(0);
+  } else {
+    std::vector<std::thread> th;
+    for (int w = 0; w < workers; ++w) th.emplace_back(scan, w);
+    for (auto &t : th) t.join();
   }
+  for (auto &pp : part) L.near.insert(L.near.end(), pp.begin(), pp.end());
   std::vector<std::vector<int2>> lists(m.n);
   int64_t woff = 0;
   int32_t eoff = 0;
@@ -1115,11 +1131,32 @@ void fill_result(pm7_result *res, const Molecule &m, const Layout &L, const Para
   if (S.unrestricted) res->mo_energies_beta = host_vec(S.eps_b);
 }
 
+// Host-side phase times of one pm7_run on stderr (PM7_HOST_TRACE set): where the wall time
+// beyond the device's goes.
+struct HostTrace {
+  bool on = std::getenv("PM7_HOST_TRACE") != nullptr;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  std::string line;
+  void mark(const char *what) {
+    if (!on) return;
+    const auto now = std::chrono::steady_clock::now();
+    char buf[64];
+    std::snprintf(buf, sizeof buf, " %s %.3f", what, std::chrono::duration<double, std::milli>(now - t).count());
+    line += buf;
+    t = now;
+  }
+  ~HostTrace() {
+    if (on) std::fprintf(stderr, "pm7_run host ms:%s\n", line.c_str());
+  }
+};
+
 static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm7_options *opt, pm7_result *res) {
   if (!opt || !res || !params) throw Failure{PM7_ERR_INVALID_INPUT, "null argument"};
+  HostTrace ht;
   const pm7_options &o = *opt;
   Molecule m = to_molecule(mol);
   validate(m, o);
+  ht.mark("validate");
   const int pmethod = *reinterpret_cast<const int *>(params);
   if (o.method != pmethod)
     throw Failure{PM7_ERR_INVALID_INPUT, "options method does not match parameter method"};
@@ -1128,6 +1165,7 @@ static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm
     throw Failure{PM7_ERR_INVALID_INPUT, "unknown precision mode"};
   const ParamSet &ps = param_set(o.method);
   Layout L = build_layout(m, ps);
+  ht.mark("layout");
   DeviceContext &ctx = context_for(o.device);
   std::lock_guard<std::mutex> lock(ctx.run_mutex);
   CUDA_OK(cudaSetDevice(ctx.device));
@@ -1151,6 +1189,7 @@ static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm
   CUDA_OK(cudaEventRecord(t0, st));
   DeviceMolecule D;
   { Stage s_(st, "build"); build_device_molecule(D, m, L, P, o.force_dpath || L.has_d, st); }
+  ht.mark("build_queued");
   // electron count and spin (scf.rs:588-627)
   double n_elec = 0.0;
   for (int zz : m.z) n_elec += ps.element(zz)->core;
@@ -1176,6 +1215,7 @@ static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm
   ScfOut S;
   if (uhf) run_uhf(ctx, P, D, m, L, ps, n_alpha, n_beta, o, S);
   else run_rhf(ctx, P, D, m, L, ps, n_alpha, o, S);
+  ht.mark("scf");
   // post-SCF corrections on the device (scf.rs:907-932)
   DevBuf<double> cscratch, cout;
   cscratch.alloc(corrections_scratch(m.n), st);
@@ -1195,6 +1235,7 @@ static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm
   }
   CUDA_OK(cudaEventRecord(t1, st));
   CUDA_OK(cudaEventSynchronize(t1));
+  ht.mark("corrections");
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, t0, t1);
   g_prof.flush();
@@ -1233,9 +1274,11 @@ static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm
     }
     CUDA_OK(cudaStreamSynchronize(st));
   }
+  ht.mark("readback");
   fill_result(res, m, L, ps, o, R, diag_blocks, [&](int a, int i, int j) {
     return o.want_matrices ? Ph[(size_t)(L.aoff[a] + i) * nao + L.aoff[a] + j] : blocks[(size_t)81 * a + 9 * i + j];
   });
+  ht.mark("result");
   if (o.want_matrices) {
     res->density = host_vec(Ph);
     if (S.unrestricted) res->spin_density = host_copy(S.Pspin.p, nn, st);
