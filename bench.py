@@ -69,12 +69,19 @@ def nao_of(z):
 
 def near_w_doubles(z, x):
     """Sum of npair(u)*npair(v) over atom pairs closer than 7 Angstrom (the stored blocks)."""
+    return near_pairs(z, x)[1]
+
+
+def near_pairs(z, x):
+    """(atom pairs closer than 7 Angstrom, their stored two-electron doubles)."""
     npair = np.array([1 if int(v) == 1 else 10 for v in z], dtype=np.int64)
-    tot = 0
+    count, tot = 0, 0
     for i in range(len(z)):
         d = np.linalg.norm(x[i + 1:] - x[i], axis=1) * A0
-        tot += int(np.sum(npair[i] * npair[i + 1:][d < 7.0]))
-    return tot
+        near = d < 7.0
+        count += int(np.sum(near))
+        tot += int(np.sum(npair[i] * npair[i + 1:][near]))
+    return count, tot
 
 
 class ClockSampler:
@@ -354,6 +361,17 @@ def run_b200(args, world, rank, local):
                     "traffic": traffic, "launches": launches_g, "ms_avg": gemm_ms / launches_g,
                     "algorithmic_per_launch": f"{flops / launches_g:.4g} flop (SP2 square nao^3, commutator 2 nao^3)",
                     "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)"}
+    # pair integrals: the build stage computes every pair's overlap/resonance and core-core
+    # terms and the multipole two-electron blocks of the pairs inside 7 Angstrom
+    pair_rate = None
+    b_ms, b_calls = prof.get("build", (0.0, 0))
+    if b_calls:
+        n_near, w_near = near_pairs(z, x)
+        n_all = len(z) * (len(z) - 1) // 2
+        per = b_ms / b_calls * 1e-3
+        pair_rate = {"pairs_all": n_all, "pairs_near": n_near, "w_doubles_near": w_near, "build_ms": per * 1e3,
+                     "pairs_per_s": n_all / per, "near_pairs_per_s": n_near / per,
+                     "note": "build stage (k_pairs_all + k_near_integrals + k_hcore_diag) per solve"}
     fock_ms, fock_calls = prof.get("fock", (0.0, 0))
     fock_roof = None
     if fock_calls:
@@ -385,6 +403,7 @@ def run_b200(args, world, rank, local):
                        "device_p50": float(np.percentile([q["device_ms"] for q in results], 50))},
         "roofline": roofline,
         "roofline_fock": fock_roof,
+        "pair_integrals": pair_rate,
         "mixed_precision": mixed,
         "stages": stages,
         "clocks": clocks,
