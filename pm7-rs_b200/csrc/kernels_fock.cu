@@ -61,18 +61,23 @@ __global__ void k_fock_far(FockGeometry g, const double *__restrict__ H, const d
   fock_far_elem(g, H, Ps, s_scale, F, i, j);
 }
 
+// One near pair's Fock terms, a warp per pair: lanes over the pair's outputs — the exchange
+// block F_uv (n_u x n_v elements), then the packed Coulomb partials of u from P_vv and of v
+// from P_uu (summed per atom by the atom kernel). Every output is one lane's sum in a fixed
+// order, so the result does not depend on the launch shape.
 __device__ __forceinline__ void fock_near_pair(const FockGeometry &g, const DeviceParams &P,
                                                const double *__restrict__ H, const double *__restrict__ Pt,
                                                const double *__restrict__ Ps, double s_scale,
-                                               double *__restrict__ F, double *__restrict__ jbuf, int p) {
+                                               double *__restrict__ F, double *__restrict__ jbuf, int p, int lane) {
   const NearPair q = g.np[p];
   const int nu_ = P.elements[g.z[q.u]].n_orb, nv = P.elements[g.z[q.v]].n_orb;
   const int ou = g.aoff[q.u], ov = g.aoff[q.v], nao = g.nao;
   const int npv = nv * (nv + 1) / 2, npu = nu_ * (nu_ + 1) / 2;
   const double *w = g.w + q.woff;
-  // exchange block
-  for (int mu = 0; mu < nu_; ++mu)
-    for (int la = 0; la < nv; ++la) {
+  const int nx = nu_ * nv, total = nx + npu + npv;
+  for (int t = lane; t < total; t += 32) {
+    if (t < nx) {  // exchange element (mu, la)
+      const int mu = t / nv, la = t - mu * nv;
       double acc = 0.0;
       for (int nu = 0; nu < nu_; ++nu) {
         const double *row = w + dpack(mu, nu) * npv;
@@ -82,36 +87,37 @@ __device__ __forceinline__ void fock_near_pair(const FockGeometry &g, const Devi
       const size_t e1 = (size_t)(ou + mu) * nao + ov + la, e2 = (size_t)(ov + la) * nao + ou + mu;
       F[e1] = H[e1] + kv;
       F[e2] = H[e2] + kv;
-    }
-  // Coulomb on u from P_vv
-  double *ju = jbuf + q.eoff_u;
-  for (int mu = 0; mu < nu_; ++mu)
-    for (int nu = 0; nu <= mu; ++nu) {
-      const double *row = w + dpack(mu, nu) * npv;
+    } else if (t < nx + npu) {  // Coulomb on u from P_vv, packed element k = (mu >= nu)
+      const int k = t - nx;
+      int mu = 0;
+      while ((mu + 1) * (mu + 2) / 2 <= k) ++mu;
+      const double *row = w + k * npv;
       double acc = 0.0;
       for (int la = 0; la < nv; ++la)
         for (int si = 0; si < nv; ++si) acc += Pt[(size_t)(ov + la) * nao + ov + si] * row[dpack(la, si)];
-      ju[dpack(mu, nu)] = acc;
-    }
-  // Coulomb on v from P_uu
-  double *jv = jbuf + q.eoff_v;
-  for (int la = 0; la < nv; ++la)
-    for (int si = 0; si <= la; ++si) {
-      const int col = dpack(la, si);
+      jbuf[q.eoff_u + k] = acc;
+    } else {  // Coulomb on v from P_uu, packed element col
+      const int col = t - nx - npu;
       double acc = 0.0;
       for (int mu = 0; mu < nu_; ++mu)
         for (int nu = 0; nu < nu_; ++nu) acc += Pt[(size_t)(ou + mu) * nao + ou + nu] * w[dpack(mu, nu) * npv + col];
-      jv[col] = acc;
+      jbuf[q.eoff_v + col] = acc;
     }
-  (void)npu;
+  }
 }
 
-__global__ void k_fock_near(FockGeometry g, DeviceParams P, const double *__restrict__ H,
-                            const double *__restrict__ Pt, const double *__restrict__ Ps, double s_scale,
-                            double *__restrict__ F, double *__restrict__ jbuf) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= g.n_near) return;
-  fock_near_pair(g, P, H, Pt, Ps, s_scale, F, jbuf, p);
+// 32 warps per block, each warp a near pair at a time: pairs 128 b .. 128 b + 127.
+constexpr int NEAR_THREADS = 1024;
+__global__ void __launch_bounds__(NEAR_THREADS, 1) k_fock_near(FockGeometry g, DeviceParams P,
+                                                            const double *__restrict__ H,
+                                                            const double *__restrict__ Pt,
+                                                            const double *__restrict__ Ps, double s_scale,
+                                                            double *__restrict__ F, double *__restrict__ jbuf) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int r = 0; r < 4; ++r) {
+    const int p = blockIdx.x * 128 + warp + 32 * r;
+    if (p < g.n_near) fock_near_pair(g, P, H, Pt, Ps, s_scale, F, jbuf, p, lane);
+  }
 }
 
 // One-centre two-electron integral (a b | c d) of an sp atom (fock.rs:69-107).
@@ -127,33 +133,33 @@ __device__ __forceinline__ double oc_sp(int a, int b, int c, int d, const Elemen
   return 0.0;
 }
 
-// One block per atom: the far point-charge Coulomb (threads over partner atoms, fixed
-// block reduction), the near Coulomb contributions summed in partner order (threads
-// over packed elements), then the one-centre terms (threads over block elements).
-constexpr int ATOM_THREADS = 128;
-__device__ __forceinline__ void fock_atom_block(const FockGeometry &g, const DeviceParams &P,
-                                                const double *__restrict__ H, const double *__restrict__ Pt,
-                                                const double *__restrict__ Ps, double s_scale,
-                                                const double *__restrict__ pop, const double *__restrict__ jbuf,
-                                                double *__restrict__ F, int A) {
+// One warp per atom: the far point-charge Coulomb (lanes over partner atoms, fixed shuffle
+// tree), the near Coulomb partials summed in partner order (lanes over packed elements), then
+// the one-centre terms and the assembly of the atom's diagonal block (lanes over its
+// elements). `jacc` is the warp's 45 doubles of shared memory. No block-wide barrier.
+constexpr int ATOM_WARPS = 8;
+__device__ __forceinline__ void fock_atom_warp(const FockGeometry &g, const DeviceParams &P,
+                                               const double *__restrict__ H, const double *__restrict__ Pt,
+                                               const double *__restrict__ Ps, double s_scale,
+                                               const double *__restrict__ pop, const double *__restrict__ jbuf,
+                                               double *__restrict__ F, int A, double *jacc) {
+  const int lane = threadIdx.x & 31;
   const ElementRec &e = P.elements[g.z[A]];
   const int no = e.n_orb, off = g.aoff[A], nao = g.nao;
   if (no == 0) return;
   const int npk = no * (no + 1) / 2;
-  __shared__ double s_far;
-  __shared__ double jacc[45];
   const double xa = g.xyz[3 * A], ya = g.xyz[3 * A + 1], za = g.xyz[3 * A + 2];
   const unsigned char *mask = g.near_mask + (size_t)A * g.n_atoms;
   double far = 0.0;
-  for (int B = threadIdx.x; B < g.n_atoms; B += ATOM_THREADS) {
+  for (int B = lane; B < g.n_atoms; B += 32) {
     if (B == A || mask[B]) continue;
     const double dx = g.xyz[3 * B] - xa, dy = g.xyz[3 * B + 1] - ya, dz = g.xyz[3 * B + 2] - za;
     far += ((1.0 / sqrt(dx * dx + dy * dy + dz * dz)) * kEv) * pop[B];
   }
-  far = block_sum<ATOM_THREADS>(far);
-  if (threadIdx.x == 0) s_far = far;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) far += __shfl_xor_sync(0xffffffffu, far, o);
   const int c0 = g.csr_start[A], c1 = g.csr_start[A + 1];
-  for (int k = threadIdx.x; k < npk; k += ATOM_THREADS) {
+  for (int k = lane; k < npk; k += 32) {
     double acc = 0.0;
     for (int c = c0; c < c1; ++c) {
       const NearPair q = g.np[g.csr[c].y];
@@ -161,9 +167,9 @@ __device__ __forceinline__ void fock_atom_block(const FockGeometry &g, const Dev
     }
     jacc[k] = acc;
   }
-  __syncthreads();
+  __syncwarp();
   const double *oc = (no == 9 && e.onecenter_slot >= 0) ? P.onecenter + (size_t)e.onecenter_slot * 2025 : nullptr;
-  for (int idx = threadIdx.x; idx < no * no; idx += ATOM_THREADS) {
+  for (int idx = lane; idx < no * no; idx += 32) {
     const int mu = idx / no, nu = idx - mu * no;
     double acc = 0.0;
     for (int la = 0; la < no; ++la)
@@ -179,20 +185,23 @@ __device__ __forceinline__ void fock_atom_block(const FockGeometry &g, const Dev
         }
       }
     double v = acc + jacc[dpack(mu, nu)];
-    if (mu == nu) v += s_far;
+    if (mu == nu) v += far;
     const size_t ij = (size_t)(off + mu) * nao + off + nu;
     F[ij] = H[ij] + v;
   }
 }
 
-__global__ void __launch_bounds__(ATOM_THREADS) k_fock_atom(FockGeometry g, DeviceParams P,
-                                                            const double *__restrict__ H,
-                                                            const double *__restrict__ Pt,
-                                                            const double *__restrict__ Ps, double s_scale,
-                                                            const double *__restrict__ pop,
-                                                            const double *__restrict__ jbuf,
-                                                            double *__restrict__ F) {
-  fock_atom_block(g, P, H, Pt, Ps, s_scale, pop, jbuf, F, blockIdx.x);
+__global__ void __launch_bounds__(32 * ATOM_WARPS) k_fock_atom(FockGeometry g, DeviceParams P,
+                                                               const double *__restrict__ H,
+                                                               const double *__restrict__ Pt,
+                                                               const double *__restrict__ Ps, double s_scale,
+                                                               const double *__restrict__ pop,
+                                                               const double *__restrict__ jbuf,
+                                                               double *__restrict__ F) {
+  __shared__ double jacc[ATOM_WARPS][45];
+  const int warp = threadIdx.x >> 5;
+  const int A = blockIdx.x * ATOM_WARPS + warp;
+  if (A < g.n_atoms) fock_atom_warp(g, P, H, Pt, Ps, s_scale, pop, jbuf, F, A, jacc[warp]);
 }
 
 // ---- batched Fock (RHF: P_spin = P/2) ----------------------------------------------
@@ -225,27 +234,35 @@ __global__ void __launch_bounds__(256) k_b_fock_far(BatchList L, const MolDesc *
   for (int j = threadIdx.x & 31; j < d.g.nao; j += 32) fock_far_elem(d.g, d.H, d.P, 0.5, F, i, j);
 }
 
-// Item = 128 near pairs of one molecule (thread per pair).
-__global__ void k_b_fock_near(BatchList L, const MolDesc *__restrict__ D, const MolCtl *__restrict__ C,
-                              DeviceParams P, int final_pass) {
-  const int item = blockIdx.x;
-  const int m = batch_find(L, item);
-  const int slot = L.slot[m];
-  const MolDesc &d = D[slot];
-  const int p = (item - L.prefix[m]) * 128 + threadIdx.x;
-  if (p >= d.g.n_near) return;
-  fock_near_pair(d.g, P, d.H, d.P, d.P, 0.5, fock_target(d, C[slot], final_pass), d.jbuf, p);
-}
-
-// Item = an atom of one molecule (block per atom).
-__global__ void __launch_bounds__(ATOM_THREADS) k_b_fock_atom(BatchList L, const MolDesc *__restrict__ D,
+// Item = 128 near pairs of one molecule (32 warps, a warp per pair at a time).
+__global__ void __launch_bounds__(NEAR_THREADS, 1) k_b_fock_near(BatchList L, const MolDesc *__restrict__ D,
                                                               const MolCtl *__restrict__ C, DeviceParams P,
                                                               int final_pass) {
   const int item = blockIdx.x;
   const int m = batch_find(L, item);
   const int slot = L.slot[m];
   const MolDesc &d = D[slot];
-  fock_atom_block(d.g, P, d.H, d.P, d.P, 0.5, d.pop, d.jbuf, fock_target(d, C[slot], final_pass), item - L.prefix[m]);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double *F = fock_target(d, C[slot], final_pass);
+  for (int r = 0; r < 4; ++r) {
+    const int p = (item - L.prefix[m]) * 128 + warp + 32 * r;
+    if (p < d.g.n_near) fock_near_pair(d.g, P, d.H, d.P, d.P, 0.5, F, d.jbuf, p, lane);
+  }
+}
+
+// Item = an atom of one molecule (a warp per item, eight per block).
+__global__ void __launch_bounds__(32 * ATOM_WARPS) k_b_fock_atom(BatchList L, const MolDesc *__restrict__ D,
+                                                                 const MolCtl *__restrict__ C, DeviceParams P,
+                                                                 int final_pass) {
+  __shared__ double jacc[ATOM_WARPS][45];
+  const int warp = threadIdx.x >> 5;
+  const int item = blockIdx.x * ATOM_WARPS + warp;
+  if (item >= L.total) return;
+  const int m = batch_find(L, item);
+  const int slot = L.slot[m];
+  const MolDesc &d = D[slot];
+  fock_atom_warp(d.g, P, d.H, d.P, d.P, 0.5, d.pop, d.jbuf, fock_target(d, C[slot], final_pass), item - L.prefix[m],
+                 jacc[warp]);
 }
 
 void launch_b_fock(cudaStream_t st, const BatchList &Lmol, const BatchList &Lrows, const BatchList &Lnear,
@@ -255,9 +272,10 @@ void launch_b_fock(cudaStream_t st, const BatchList &Lmol, const BatchList &Lrow
   note_launch();
   if (Lrows.total > 0) k_b_fock_far<<<Lrows.total, 256, 0, st>>>(Lrows, D, C, final_pass);
   note_launch();
-  if (Lnear.total > 0) k_b_fock_near<<<Lnear.total, 128, 0, st>>>(Lnear, D, C, P, final_pass);
+  if (Lnear.total > 0) k_b_fock_near<<<Lnear.total, NEAR_THREADS, 0, st>>>(Lnear, D, C, P, final_pass);
   note_launch();
-  if (Latoms.total > 0) k_b_fock_atom<<<Latoms.total, ATOM_THREADS, 0, st>>>(Latoms, D, C, P, final_pass);
+  if (Latoms.total > 0)
+    k_b_fock_atom<<<(Latoms.total + ATOM_WARPS - 1) / ATOM_WARPS, 32 * ATOM_WARPS, 0, st>>>(Latoms, D, C, P, final_pass);
   note_launch();
 }
 
@@ -280,9 +298,10 @@ void launch_fock(cudaStream_t st, const FockGeometry &g, const DeviceParams &P, 
   dim3 blk(32, 8), grd((g.nao + 31) / 32, (g.nao + 7) / 8);
   k_fock_far<<<grd, blk, 0, st>>>(g, H, Ps, s_scale, F);
   note_launch();
-  if (g.n_near > 0) k_fock_near<<<(g.n_near + 127) / 128, 128, 0, st>>>(g, P, H, Pt, Ps, s_scale, F, jbuf);
+  if (g.n_near > 0) k_fock_near<<<(g.n_near + 127) / 128, NEAR_THREADS, 0, st>>>(g, P, H, Pt, Ps, s_scale, F, jbuf);
   note_launch();
-  k_fock_atom<<<g.n_atoms, ATOM_THREADS, 0, st>>>(g, P, H, Pt, Ps, s_scale, pop, jbuf, F);
+  k_fock_atom<<<(g.n_atoms + ATOM_WARPS - 1) / ATOM_WARPS, 32 * ATOM_WARPS, 0, st>>>(g, P, H, Pt, Ps, s_scale, pop, jbuf,
+                                                                                     F);
   note_launch();
 }
 
