@@ -241,6 +241,12 @@ pm7_status pm7_stage_corrections(const pm7_molecule *molecule, int32_t method,
 /* Number of CUDA kernels this library has launched since the process started. */
 int64_t pm7_launch_count(void);
 
+/* The autotuner's decisions so far in this process, as JSON: {"<device>|<kernel key>":
+ * variant, ...}. Result-identical launch variants (GEMM tile shapes, warps per block) are
+ * timed on first use per size bucket; PM7_AUTOTUNE_CACHE names a JSON file that keeps them
+ * across processes. No counterpart in pm7-rs. */
+const char *pm7_autotune_report(void);
+
 /* Per-stage device timing with CUDA events on the engine's stream: enable (1) resets
  * and starts recording, 0 stops. Stages: "build", "fock", "commutator_gemm",
  * "density_gemm", "eigensolve", "diis_dots", "combine", "corrections". */

@@ -1077,6 +1077,9 @@ class BatchRunner {
     CUDA_OK(cudaMalloc((void **)&err32_, sizeof(int)));
     CUDA_OK(cudaMemset(err32_, 0, sizeof(int)));
     CUDA_OK(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+    // kernel attributes of the SP2 steps, before any of them is captured into a graph
+    prepare_gemm_kernels();
+    prepare_tf32_kernels();
     CUDA_OK(cudaStreamCreateWithFlags(&eig_st_, cudaStreamNonBlocking));
     CUDA_OK(cudaEventCreateWithFlags(&eig_done_, cudaEventDisableTiming));
     for (Side &sd : side_) {
@@ -1327,19 +1330,48 @@ class BatchRunner {
       if (T.mol.n) launch_b_to32(st_, T.chunks, desc_);
       const int chunk = 8;
       bool run64 = S.mol.n > 0, run32 = T.mol.n > 0;
-      for (int step = 0; step < 100 && (run64 || run32); step += chunk) {
+      // A chunk is `chunk` purification steps of every molecule still purifying (steps of a
+      // molecule that has stopped do nothing on the device), the same launches each time
+      // within this iteration: captured once as a CUDA graph and replayed (the kernels'
+      // attributes were set in the constructor, outside any capture).
+      auto queue_chunk = [&](bool r64, bool r32) {
         for (int k = 0; k < chunk; ++k) {
-          if (run64) {
+          if (r64) {
             launch_b_gemm(st_, S.glow, desc_, ctl_, nullptr, 2);
             k_b_sp2_decide<<<S.mol.n, RB, 0, st_>>>(S.mol, desc_, ctl_, f64);
             k_b_sp2_apply<<<S.chunks.total, RB, 0, st_>>>(S.chunks, desc_, ctl_);
             note_launch(2);
           }
-          if (run32) {
+          if (r32) {
             launch_b_square_tf32x3(st_, T.tiles, desc_, ctl_, maps_, err32_);
             launch_b_sp2_decide32(st_, T.mol, desc_, ctl_, f32);
             launch_b_sp2_apply32(st_, T.chunks, desc_, ctl_);
           }
+        }
+      };
+      cudaGraphExec_t exec = nullptr;
+      bool g64 = false, g32 = false;
+      int nodes = 0;
+      for (int step = 0; step < 100 && (run64 || run32); step += chunk) {
+        {
+          if (!exec || g64 != run64 || g32 != run32) {
+            if (exec) CUDA_OK(cudaGraphExecDestroy(exec));
+            exec = nullptr;
+            const long long before = pm7_launch_count();
+            cudaGraph_t graph = nullptr;
+            CUDA_OK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+            queue_chunk(run64, run32);
+            CUDA_OK(cudaStreamEndCapture(st_, &graph));
+            nodes = (int)(pm7_launch_count() - before);
+            note_launch(-nodes);  // counted when replayed
+            const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            CUDA_OK(ie);
+            g64 = run64;
+            g32 = run32;
+          }
+          CUDA_OK(cudaGraphLaunch(exec, st_));
+          note_launch(nodes);
         }
         CUDA_OK(cudaMemcpyAsync(flags_h_, flags_d_, 2 * (size_t)cap_, cudaMemcpyDeviceToHost, st_));
         CUDA_OK(cudaStreamSynchronize(st_));
@@ -1348,6 +1380,7 @@ class BatchRunner {
         run32 = false;
         for (int m = 0; m < T.mol.n; ++m) run32 = run32 || flags_h_[cap_ + m] == 0;
       }
+      if (exec) CUDA_OK(cudaGraphExecDestroy(exec));
       for (int m = 0; m < S.mol.n; ++m)
         if (flags_h_[m] != 1) {
           fallback.push_back(purify64[m]);

@@ -28,6 +28,7 @@
 #include "params.hpp"
 #include "pm7_b200.h"
 #include "scf_host.hpp"
+#include "autotune.hpp"
 #include "engine_internal.hpp"
 
 namespace pm7 {
@@ -1612,6 +1613,12 @@ pm7_status pm7_stage_corrections(const pm7_molecule *molecule, int32_t method, i
 }
 
 int64_t pm7_launch_count(void) { return g_launches.load(); }
+
+const char *pm7_autotune_report(void) {
+  static thread_local std::string r;
+  r = autotune_report();
+  return r.c_str();
+}
 
 void pm7_profile_enable(int32_t on) { g_prof.reset(on != 0); }
 

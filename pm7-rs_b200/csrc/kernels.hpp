@@ -62,6 +62,8 @@ void launch_fock(cudaStream_t st, const FockGeometry &g, const DeviceParams &P, 
 
 // ---- dense algebra (kernels_dense.cu) ----
 // C[M x N] = alpha * A^T B, A: K x M row-major (lda), B: K x N row-major (ldb), C row-major (ldc). FP64 DMMA.
+// Sets the DMMA GEMM kernels' shared-memory attributes on the current device (idempotent).
+void prepare_gemm_kernels();
 void launch_gemm_tn(cudaStream_t st, int M, int N, int K, double alpha, const double *A, int lda, const double *B,
                     int ldb, double *C, int ldc);
 // P = w * V^T V for the first k rows of V (n columns, row stride ldv); symmetric output.
@@ -131,6 +133,8 @@ namespace pm7 {
 // ld x ld fp32, ld a multiple of 32, zero padded beyond n; the maps come from
 // make_square_map (an opaque 128-byte CUtensorMap each).
 bool make_square_map(const float *base, int ld, void *map_out);
+// Sets the tcgen05 kernels' shared-memory attributes on the current device (idempotent).
+void prepare_tf32_kernels();
 size_t square_tf32x3_smem();
 // state/step: as the fp64 SP2 steps (state may be null: always runs).
 void launch_square_tf32x3(cudaStream_t st, int n, int ld, const void *map_hi, const void *map_lo, float *C,

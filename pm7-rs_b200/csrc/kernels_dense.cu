@@ -8,6 +8,7 @@
 #include "common.cuh"
 #include "batch.hpp"
 #include "kernels.hpp"
+#include "autotune.hpp"
 
 namespace pm7 {
 
@@ -220,6 +221,19 @@ static inline int sym_tiles(int n) {
   return t;
 }
 
+// Symmetric n x n product on 64x64 tiles of the lower triangle (four CTAs per SM): more,
+// smaller tiles than k_gemm_sym, the faster shape when 128x64 tiles leave SMs idle.
+__global__ void __launch_bounds__(128, 4) k_gemm_sym64(int n, int K, double alpha, const double *__restrict__ A,
+                                                       int lda, const double *__restrict__ B, int ldb,
+                                                       double *__restrict__ C, int ldc, const double *__restrict__ sp2,
+                                                       int step) {
+  extern __shared__ __align__(16) double gemm_smem[];
+  if (!sp2_active(sp2, step)) return;
+  int t = blockIdx.x, r = 0;
+  while ((r + 1) * (r + 2) / 2 <= t) ++r;
+  gemm_tile_t<BM, BN>(gemm_smem, r, t - r * (r + 1) / 2, n, n, K, alpha, A, lda, B, ldb, C, ldc, 1);
+}
+
 // Symmetric n x n product over the enumerated lower-triangle tiles (row block r holds
 // column blocks 0 .. ceil((r+1) SYM_BM / SYM_BN) - 1).
 __global__ void __launch_bounds__(128, 2) k_gemm_sym(int n, int K, double alpha, const double *__restrict__ A,
@@ -270,9 +284,12 @@ static void gemm_smem_attr() {
   if (dev < 0 || dev >= 64 || done[dev]) return;
   cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
   cudaFuncSetAttribute(k_gemm_sym, cudaFuncAttributeMaxDynamicSharedMemorySize, SYM_SMEM);
+  cudaFuncSetAttribute(k_gemm_sym64, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
   cudaFuncSetAttribute(k_b_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
   done[dev] = true;
 }
+
+void prepare_gemm_kernels() { gemm_smem_attr(); }
 
 void launch_b_gemm(cudaStream_t st, const BatchList &L, const MolDesc *D, const MolCtl *C, const EigSlot *E, int op) {
   if (L.total <= 0) return;
@@ -289,14 +306,29 @@ void launch_gemm_tn(cudaStream_t st, int M, int N, int K, double alpha, const do
   note_launch();
 }
 
+// Symmetric product C = alpha A^T B (n x n, inner dimension K) on the tile shape the
+// autotuner picked for this size: 0 = 128x64 (k_gemm_sym), 1 = 64x64 (k_gemm_sym64).
+static void launch_sym(cudaStream_t st, const char *what, int n, int K, double alpha, const double *A, int lda,
+                       const double *B, int ldb, double *C, int ldc, const double *sp2, int step) {
+  gemm_smem_attr();
+  const int bucket = ((n + 255) / 256) * 256;
+  autotune(st, std::string(what) + "|n" + std::to_string(bucket), 2, [&](int v) {
+    if (v == 0) {
+      k_gemm_sym<<<sym_tiles(n), 128, SYM_SMEM, st>>>(n, K, alpha, A, lda, B, ldb, C, ldc, sp2, step);
+    } else {
+      const int t = (n + BM - 1) / BM;
+      k_gemm_sym64<<<t * (t + 1) / 2, 128, GEMM_SMEM, st>>>(n, K, alpha, A, lda, B, ldb, C, ldc, sp2, step);
+    }
+    note_launch();
+  });
+}
+
 void launch_density(cudaStream_t st, int n, int k, double w, const double *V, int ldv, double *P) {
   if (k == 0) {
     cudaMemsetAsync(P, 0, sizeof(double) * (size_t)n * n, st);
     return;
   }
-  gemm_smem_attr();
-  k_gemm_sym<<<sym_tiles(n), 128, SYM_SMEM, st>>>(n, k, w, V, ldv, V, ldv, P, n, nullptr, 0);
-  note_launch();
+  launch_sym(st, "density_sym", n, k, w, V, ldv, V, ldv, P, n, nullptr, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -790,9 +822,7 @@ void launch_sp2_reset(cudaStream_t st, double *state) {
 }
 
 void launch_sp2_square(cudaStream_t st, int n, const double *X, double *X2, const double *state, int step) {
-  gemm_smem_attr();
-  k_gemm_sym<<<sym_tiles(n), 128, SYM_SMEM, st>>>(n, n, 1.0, X, n, X, n, X2, n, state, step);
-  note_launch();
+  launch_sym(st, "sp2_square", n, n, 1.0, X, n, X, n, X2, n, state, step);
 }
 
 void launch_sp2_trace(cudaStream_t st, int n, const double *X, const double *X2, double n_occ, double *state, int step,

@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "batch.hpp"
 #include "kernels.hpp"
+#include "autotune.hpp"
 #include "nddo_sp.cuh"
 
 namespace pm7 {
@@ -61,10 +62,11 @@ __global__ void k_fock_far(FockGeometry g, const double *__restrict__ H, const d
   fock_far_elem(g, H, Ps, s_scale, F, i, j);
 }
 
-// One near pair's Fock terms, a warp per pair: lanes over the pair's outputs — the exchange
-// block F_uv (n_u x n_v elements), then the packed Coulomb partials of u from P_vv and of v
-// from P_uu (summed per atom by the atom kernel). Every output is one lane's sum in a fixed
-// order, so the result does not depend on the launch shape.
+// One near pair's Fock terms, a group of G lanes per pair: lanes over the pair's outputs —
+// the exchange block F_uv (n_u x n_v elements), then the packed Coulomb partials of u from
+// P_vv and of v from P_uu (summed per atom by the atom kernel). Every output is one lane's
+// sum in a fixed order, so the result does not depend on G or the block size.
+template <int G>
 __device__ __forceinline__ void fock_near_pair(const FockGeometry &g, const DeviceParams &P,
                                                const double *__restrict__ H, const double *__restrict__ Pt,
                                                const double *__restrict__ Ps, double s_scale,
@@ -75,7 +77,7 @@ __device__ __forceinline__ void fock_near_pair(const FockGeometry &g, const Devi
   const int npv = nv * (nv + 1) / 2, npu = nu_ * (nu_ + 1) / 2;
   const double *w = g.w + q.woff;
   const int nx = nu_ * nv, total = nx + npu + npv;
-  for (int t = lane; t < total; t += 32) {
+  for (int t = lane; t < total; t += G) {
     if (t < nx) {  // exchange element (mu, la)
       const int mu = t / nv, la = t - mu * nv;
       double acc = 0.0;
@@ -106,19 +108,27 @@ __device__ __forceinline__ void fock_near_pair(const FockGeometry &g, const Devi
   }
 }
 
-// 32 warps per block, each warp a near pair at a time: pairs 128 b .. 128 b + 127.
-constexpr int NEAR_THREADS = 1024;
-__global__ void __launch_bounds__(NEAR_THREADS, 1) k_fock_near(FockGeometry g, DeviceParams P,
-                                                            const double *__restrict__ H,
-                                                            const double *__restrict__ Pt,
-                                                            const double *__restrict__ Ps, double s_scale,
-                                                            double *__restrict__ F, double *__restrict__ jbuf) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int r = 0; r < 4; ++r) {
-    const int p = blockIdx.x * 128 + warp + 32 * r;
-    if (p < g.n_near) fock_near_pair(g, P, H, Pt, Ps, s_scale, F, jbuf, p, lane);
+// A block of T threads per 128 near pairs (pairs 128 b .. 128 b + 127), in groups of G lanes
+// that take a pair at a time. (G, T) is an autotuned launch shape with identical results:
+// whole warps suit the 9-orbital pairs, narrow groups the hydrogen-rich sp pairs (3 to 36
+// outputs each).
+template <int G, int T>
+__global__ void __launch_bounds__(T, 1) k_fock_near(FockGeometry g, DeviceParams P, const double *__restrict__ H,
+                                                    const double *__restrict__ Pt, const double *__restrict__ Ps,
+                                                    double s_scale, double *__restrict__ F,
+                                                    double *__restrict__ jbuf) {
+  constexpr int NG = T / G;
+  static_assert(128 % NG == 0, "groups per block must divide 128");
+  const int lane = threadIdx.x % G, grp = threadIdx.x / G;
+  for (int r = 0; r < 128 / NG; ++r) {
+    const int p = blockIdx.x * 128 + grp + NG * r;
+    if (p < g.n_near) fock_near_pair<G>(g, P, H, Pt, Ps, s_scale, F, jbuf, p, lane);
   }
 }
+
+// The near-pair launch shapes, X(variant, G lanes per pair, T threads per block).
+#define PM7_NEAR_SHAPES(X) X(0, 32, 1024) X(1, 32, 256) X(2, 8, 256) X(3, 4, 128) X(4, 1, 128)
+constexpr int kNearVariants = 5;
 
 // One-centre two-electron integral (a b | c d) of an sp atom (fock.rs:69-107).
 __device__ __forceinline__ double oc_sp(int a, int b, int c, int d, const ElementRec &e) {
@@ -133,33 +143,53 @@ __device__ __forceinline__ double oc_sp(int a, int b, int c, int d, const Elemen
   return 0.0;
 }
 
-// One warp per atom: the far point-charge Coulomb (lanes over partner atoms, fixed shuffle
-// tree), the near Coulomb partials summed in partner order (lanes over packed elements), then
-// the one-centre terms and the assembly of the atom's diagonal block (lanes over its
-// elements). `jacc` is the warp's 45 doubles of shared memory. No block-wide barrier.
-constexpr int ATOM_WARPS = 8;
-__device__ __forceinline__ void fock_atom_warp(const FockGeometry &g, const DeviceParams &P,
-                                               const double *__restrict__ H, const double *__restrict__ Pt,
-                                               const double *__restrict__ Ps, double s_scale,
-                                               const double *__restrict__ pop, const double *__restrict__ jbuf,
-                                               double *__restrict__ F, int A, double *jacc) {
-  const int lane = threadIdx.x & 31;
+// One group of G lanes per atom: the far point-charge Coulomb (32 partial sums over partner
+// atoms, B = v, v + 32, ..., combined by a fixed xor tree; with G < 32 each lane holds 32/G of
+// the partials and does the upper tree levels in registers, so every G gives the same bits),
+// the near Coulomb partials summed in partner order (lanes over packed elements), then the
+// one-centre terms and the assembly of the atom's diagonal block (lanes over its elements).
+// `jacc` is the group's 45 doubles of shared memory; `gmask` the group's lanes. No block-wide
+// barrier.
+template <int G>
+__device__ __forceinline__ void fock_atom_group(const FockGeometry &g, const DeviceParams &P,
+                                                const double *__restrict__ H, const double *__restrict__ Pt,
+                                                const double *__restrict__ Ps, double s_scale,
+                                                const double *__restrict__ pop, const double *__restrict__ jbuf,
+                                                double *__restrict__ F, int A, double *jacc, int lane,
+                                                unsigned gmask) {
+  constexpr int V = 32 / G;
   const ElementRec &e = P.elements[g.z[A]];
   const int no = e.n_orb, off = g.aoff[A], nao = g.nao;
   if (no == 0) return;
   const int npk = no * (no + 1) / 2;
   const double xa = g.xyz[3 * A], ya = g.xyz[3 * A + 1], za = g.xyz[3 * A + 2];
   const unsigned char *mask = g.near_mask + (size_t)A * g.n_atoms;
-  double far = 0.0;
-  for (int B = lane; B < g.n_atoms; B += 32) {
-    if (B == A || mask[B]) continue;
-    const double dx = g.xyz[3 * B] - xa, dy = g.xyz[3 * B + 1] - ya, dz = g.xyz[3 * B + 2] - za;
-    far += ((1.0 / sqrt(dx * dx + dy * dy + dz * dz)) * kEv) * pop[B];
-  }
+  double part[V];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) far += __shfl_xor_sync(0xffffffffu, far, o);
+  for (int k = 0; k < V; ++k) part[k] = 0.0;
+  for (int B0 = 0; B0 < g.n_atoms; B0 += 32) {
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+      const int B = B0 + lane + G * k;  // partial v = lane + G k
+      if (B >= g.n_atoms || B == A || mask[B]) continue;
+      const double dx = g.xyz[3 * B] - xa, dy = g.xyz[3 * B + 1] - ya, dz = g.xyz[3 * B + 2] - za;
+      part[k] += ((1.0 / sqrt(dx * dx + dy * dy + dz * dz)) * kEv) * pop[B];
+    }
+  }
+  // xor tree over the 32 partials: levels o >= G pair partials of one lane, o < G cross lanes
+#pragma unroll
+  for (int o = 16; o >= G; o >>= 1) {
+    double t[V];
+#pragma unroll
+    for (int k = 0; k < V; ++k) t[k] = part[k] + part[k ^ (o / G)];
+#pragma unroll
+    for (int k = 0; k < V; ++k) part[k] = t[k];
+  }
+  double far = part[0];
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) far += __shfl_xor_sync(gmask, far, o, G);
   const int c0 = g.csr_start[A], c1 = g.csr_start[A + 1];
-  for (int k = lane; k < npk; k += 32) {
+  for (int k = lane; k < npk; k += G) {
     double acc = 0.0;
     for (int c = c0; c < c1; ++c) {
       const NearPair q = g.np[g.csr[c].y];
@@ -167,9 +197,9 @@ __device__ __forceinline__ void fock_atom_warp(const FockGeometry &g, const Devi
     }
     jacc[k] = acc;
   }
-  __syncwarp();
+  __syncwarp(gmask);
   const double *oc = (no == 9 && e.onecenter_slot >= 0) ? P.onecenter + (size_t)e.onecenter_slot * 2025 : nullptr;
-  for (int idx = lane; idx < no * no; idx += 32) {
+  for (int idx = lane; idx < no * no; idx += G) {
     const int mu = idx / no, nu = idx - mu * no;
     double acc = 0.0;
     for (int la = 0; la < no; ++la)
@@ -191,18 +221,30 @@ __device__ __forceinline__ void fock_atom_warp(const FockGeometry &g, const Devi
   }
 }
 
-__global__ void __launch_bounds__(32 * ATOM_WARPS) k_fock_atom(FockGeometry g, DeviceParams P,
-                                                               const double *__restrict__ H,
-                                                               const double *__restrict__ Pt,
-                                                               const double *__restrict__ Ps, double s_scale,
-                                                               const double *__restrict__ pop,
-                                                               const double *__restrict__ jbuf,
-                                                               double *__restrict__ F) {
-  __shared__ double jacc[ATOM_WARPS][45];
-  const int warp = threadIdx.x >> 5;
-  const int A = blockIdx.x * ATOM_WARPS + warp;
-  if (A < g.n_atoms) fock_atom_warp(g, P, H, Pt, Ps, s_scale, pop, jbuf, F, A, jacc[warp]);
+// The lanes of this thread's aligned group of G within its warp.
+template <int G>
+__device__ __forceinline__ unsigned group_mask() {
+  if constexpr (G == 32) return 0xffffffffu;
+  else return ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
 }
+
+// A block of T threads, T/G atoms (a group of G lanes each).
+template <int G, int T>
+__global__ void __launch_bounds__(T) k_fock_atom(FockGeometry g, DeviceParams P, const double *__restrict__ H,
+                                                 const double *__restrict__ Pt, const double *__restrict__ Ps,
+                                                 double s_scale, const double *__restrict__ pop,
+                                                 const double *__restrict__ jbuf, double *__restrict__ F) {
+  constexpr int NG = T / G;
+  __shared__ double jacc[NG][45];
+  const int grp = threadIdx.x / G;
+  const int A = blockIdx.x * NG + grp;
+  if (A < g.n_atoms)
+    fock_atom_group<G>(g, P, H, Pt, Ps, s_scale, pop, jbuf, F, A, jacc[grp], threadIdx.x % G, group_mask<G>());
+}
+
+// The atom launch shapes, X(variant, G lanes per atom, T threads per block).
+#define PM7_ATOM_SHAPES(X) X(0, 32, 256) X(1, 8, 256) X(2, 4, 128)
+constexpr int kAtomVariants = 3;
 
 // ---- batched Fock (RHF: P_spin = P/2) ----------------------------------------------
 
@@ -234,36 +276,42 @@ __global__ void __launch_bounds__(256) k_b_fock_far(BatchList L, const MolDesc *
   for (int j = threadIdx.x & 31; j < d.g.nao; j += 32) fock_far_elem(d.g, d.H, d.P, 0.5, F, i, j);
 }
 
-// Item = 128 near pairs of one molecule (32 warps, a warp per pair at a time).
-__global__ void __launch_bounds__(NEAR_THREADS, 1) k_b_fock_near(BatchList L, const MolDesc *__restrict__ D,
-                                                              const MolCtl *__restrict__ C, DeviceParams P,
-                                                              int final_pass) {
+// Item = 128 near pairs of one molecule (groups of G lanes, a pair per group at a time).
+template <int G, int T>
+__global__ void __launch_bounds__(T, 1) k_b_fock_near(BatchList L, const MolDesc *__restrict__ D,
+                                                      const MolCtl *__restrict__ C, DeviceParams P, int final_pass) {
+  constexpr int NG = T / G;
+  static_assert(128 % NG == 0, "groups per block must divide 128");
   const int item = blockIdx.x;
   const int m = batch_find(L, item);
   const int slot = L.slot[m];
   const MolDesc &d = D[slot];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x % G, grp = threadIdx.x / G;
   double *F = fock_target(d, C[slot], final_pass);
-  for (int r = 0; r < 4; ++r) {
-    const int p = (item - L.prefix[m]) * 128 + warp + 32 * r;
-    if (p < d.g.n_near) fock_near_pair(d.g, P, d.H, d.P, d.P, 0.5, F, d.jbuf, p, lane);
+  for (int r = 0; r < 128 / NG; ++r) {
+    const int p = (item - L.prefix[m]) * 128 + grp + NG * r;
+    if (p < d.g.n_near) fock_near_pair<G>(d.g, P, d.H, d.P, d.P, 0.5, F, d.jbuf, p, lane);
   }
 }
 
-// Item = an atom of one molecule (a warp per item, eight per block).
-__global__ void __launch_bounds__(32 * ATOM_WARPS) k_b_fock_atom(BatchList L, const MolDesc *__restrict__ D,
-                                                                 const MolCtl *__restrict__ C, DeviceParams P,
-                                                                 int final_pass) {
-  __shared__ double jacc[ATOM_WARPS][45];
-  const int warp = threadIdx.x >> 5;
-  const int item = blockIdx.x * ATOM_WARPS + warp;
+// Item = an atom of one molecule (a group of G lanes per item, T/G per block).
+template <int G, int T>
+__global__ void __launch_bounds__(T) k_b_fock_atom(BatchList L, const MolDesc *__restrict__ D,
+                                                   const MolCtl *__restrict__ C, DeviceParams P, int final_pass) {
+  constexpr int NG = T / G;
+  __shared__ double jacc[NG][45];
+  const int grp = threadIdx.x / G;
+  const int item = blockIdx.x * NG + grp;
   if (item >= L.total) return;
   const int m = batch_find(L, item);
   const int slot = L.slot[m];
   const MolDesc &d = D[slot];
-  fock_atom_warp(d.g, P, d.H, d.P, d.P, 0.5, d.pop, d.jbuf, fock_target(d, C[slot], final_pass), item - L.prefix[m],
-                 jacc[warp]);
+  fock_atom_group<G>(d.g, P, d.H, d.P, d.P, 0.5, d.pop, d.jbuf, fock_target(d, C[slot], final_pass),
+                     item - L.prefix[m], jacc[grp], threadIdx.x % G, group_mask<G>());
 }
+
+// Size bucket of an autotune key: the next power of two above n.
+static int pow2_bucket(int n) { return n <= 0 ? 1 : 1 << (32 - __builtin_clz((unsigned)n)); }
 
 void launch_b_fock(cudaStream_t st, const BatchList &Lmol, const BatchList &Lrows, const BatchList &Lnear,
                    const BatchList &Latoms, const MolDesc *D, const MolCtl *C, const DeviceParams &P, int final_pass) {
@@ -272,11 +320,26 @@ void launch_b_fock(cudaStream_t st, const BatchList &Lmol, const BatchList &Lrow
   note_launch();
   if (Lrows.total > 0) k_b_fock_far<<<Lrows.total, 256, 0, st>>>(Lrows, D, C, final_pass);
   note_launch();
-  if (Lnear.total > 0) k_b_fock_near<<<Lnear.total, NEAR_THREADS, 0, st>>>(Lnear, D, C, P, final_pass);
-  note_launch();
+  if (Lnear.total > 0)
+    autotune(st, "b_fock_near|items" + std::to_string(pow2_bucket(Lnear.total)), kNearVariants, [&](int v) {
+      switch (v) {
+#define PM7_LAUNCH(i, G, T) \
+  case i: k_b_fock_near<G, T><<<Lnear.total, T, 0, st>>>(Lnear, D, C, P, final_pass); break;
+        PM7_NEAR_SHAPES(PM7_LAUNCH)
+#undef PM7_LAUNCH
+      }
+      note_launch();
+    });
   if (Latoms.total > 0)
-    k_b_fock_atom<<<(Latoms.total + ATOM_WARPS - 1) / ATOM_WARPS, 32 * ATOM_WARPS, 0, st>>>(Latoms, D, C, P, final_pass);
-  note_launch();
+    autotune(st, "b_fock_atom|items" + std::to_string(pow2_bucket(Latoms.total)), kAtomVariants, [&](int v) {
+      switch (v) {
+#define PM7_LAUNCH(i, G, T) \
+  case i: k_b_fock_atom<G, T><<<(Latoms.total + T / G - 1) / (T / G), T, 0, st>>>(Latoms, D, C, P, final_pass); break;
+        PM7_ATOM_SHAPES(PM7_LAUNCH)
+#undef PM7_LAUNCH
+      }
+      note_launch();
+    });
 }
 
 void launch_atom_blocks(cudaStream_t st, int n_atoms, const int *aoff, const int *z, const DeviceParams &P, int nao,
@@ -298,11 +361,27 @@ void launch_fock(cudaStream_t st, const FockGeometry &g, const DeviceParams &P, 
   dim3 blk(32, 8), grd((g.nao + 31) / 32, (g.nao + 7) / 8);
   k_fock_far<<<grd, blk, 0, st>>>(g, H, Ps, s_scale, F);
   note_launch();
-  if (g.n_near > 0) k_fock_near<<<(g.n_near + 127) / 128, NEAR_THREADS, 0, st>>>(g, P, H, Pt, Ps, s_scale, F, jbuf);
-  note_launch();
-  k_fock_atom<<<(g.n_atoms + ATOM_WARPS - 1) / ATOM_WARPS, 32 * ATOM_WARPS, 0, st>>>(g, P, H, Pt, Ps, s_scale, pop, jbuf,
-                                                                                     F);
-  note_launch();
+  if (g.n_near > 0) {
+    const int blocks = (g.n_near + 127) / 128;
+    autotune(st, "fock_near|pairs" + std::to_string(pow2_bucket(g.n_near)), kNearVariants, [&](int v) {
+      switch (v) {
+#define PM7_LAUNCH(i, G, T) \
+  case i: k_fock_near<G, T><<<blocks, T, 0, st>>>(g, P, H, Pt, Ps, s_scale, F, jbuf); break;
+        PM7_NEAR_SHAPES(PM7_LAUNCH)
+#undef PM7_LAUNCH
+      }
+      note_launch();
+    });
+  }
+  autotune(st, "fock_atom|atoms" + std::to_string(pow2_bucket(g.n_atoms)), kAtomVariants, [&](int v) {
+    switch (v) {
+#define PM7_LAUNCH(i, G, T) \
+  case i: k_fock_atom<G, T><<<(g.n_atoms + T / G - 1) / (T / G), T, 0, st>>>(g, P, H, Pt, Ps, s_scale, pop, jbuf, F); break;
+      PM7_ATOM_SHAPES(PM7_LAUNCH)
+#undef PM7_LAUNCH
+    }
+    note_launch();
+  });
 }
 
 }  // namespace pm7

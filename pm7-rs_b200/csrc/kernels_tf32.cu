@@ -292,11 +292,7 @@ size_t square_tf32x3_smem() { return SMEM_BYTES; }
 
 void launch_product_tf32x3(cudaStream_t st, int n, int ld, const void *a_hi, const void *a_lo, const void *b_hi,
                            const void *b_lo, float *C, int *error) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_product_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    attr = true;
-  }
+  prepare_tf32_kernels();
   const int t = (n + TM - 1) / TM;
   k_product_tf32x3<<<t * t, 128, SMEM_BYTES, st>>>(
       *reinterpret_cast<const CUtensorMap *>(a_hi), *reinterpret_cast<const CUtensorMap *>(a_lo),
@@ -306,11 +302,7 @@ void launch_product_tf32x3(cudaStream_t st, int n, int ld, const void *a_hi, con
 
 void launch_square_tf32x3(cudaStream_t st, int n, int ld, const void *map_hi, const void *map_lo, float *C,
                           int *error, const double *state, int step) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_square_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    attr = true;
-  }
+  prepare_tf32_kernels();
   const int t = (n + TM - 1) / TM;
   k_square_tf32x3<<<t * (t + 1) / 2, 128, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap *>(map_hi),
                                                             *reinterpret_cast<const CUtensorMap *>(map_lo), n, ld, C,
@@ -588,14 +580,25 @@ __global__ void __launch_bounds__(256) k_b_sp2_apply32(BatchList L, const MolDes
 
 }  // namespace
 
+// The tcgen05 kernels' dynamic shared memory limit, once per device (kernel attributes are
+// per device). Called by every launcher and by the batched engine before any graph capture.
+void prepare_tf32_kernels() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev < 0 || dev >= 64 || done[dev]) return;
+  cudaFuncSetAttribute(k_square_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  cudaFuncSetAttribute(k_product_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  cudaFuncSetAttribute(k_b_square_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  done[dev] = true;
+}
+
 void launch_b_square_tf32x3(cudaStream_t st, const BatchList &L, const MolDesc *D, const MolCtl *C, const void *maps,
                             int *error) {
   if (L.total <= 0) return;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_b_square_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    attr = true;
-  }
+  prepare_tf32_kernels();
   k_b_square_tf32x3<<<L.total, 128, SMEM_BYTES, st>>>(L, D, C, reinterpret_cast<const CUtensorMap *>(maps), error);
   note_launch();
 }

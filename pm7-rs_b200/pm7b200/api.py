@@ -23,7 +23,7 @@ EXPORTED = [
     "pm7_device_count", "pm7_stage_core_hamiltonian", "pm7_stage_fock", "pm7_stage_pair", "pm7_stage_core_core",
     "pm7_stage_corrections", "pm7_run_batch", "pm7_engine_config_default", "pm7_engine_create", "pm7_engine_submit",
     "pm7_engine_poll", "pm7_engine_destroy", "pm7_batch_partition", "pm7_stage_eigenvalues",
-    "pm7_stage_product_tf32",
+    "pm7_stage_product_tf32", "pm7_autotune_report",
 ]
 
 
@@ -201,6 +201,15 @@ def abi_sizes():
     out = (C.c_int64 * 3)()
     lib().pm7_abi_sizes(out)
     return tuple(out)
+
+
+def autotune_report():
+    """The autotuner's choices so far in this process ({"<device>|<key>": variant})."""
+    import json
+
+    L = lib()
+    L.pm7_autotune_report.restype = C.c_char_p
+    return json.loads(L.pm7_autotune_report().decode())
 
 
 def launch_count():
