@@ -91,8 +91,9 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device):
+    def __init__(self, device, interval_ms=200):
         self.device = device
+        self.interval_ms = interval_ms
         self.rows = []
         self.proc = None
 
@@ -100,7 +101,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(self.interval_ms)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except (OSError, FileNotFoundError):
@@ -454,7 +455,7 @@ def run_batch_bench(args, world, rank, local):
     for _ in range(args.warmup):  # full batches: the grow-only device and pinned buffers reach size
         api.run_batch(mols, **opts)
     barrier(world)
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(local, interval_ms=500)  # multi-second timed region; driver queries stall CUDA calls
     sampler.start()
     launches0 = api.launch_count()
     walls = []
@@ -533,7 +534,7 @@ def run_stream_bench(args, world, rank, local):
         rng = np.random.default_rng(11)
         gaps = rng.exponential(1.0 / rate, size=count)
         barrier(world)
-        sampler = ClockSampler(local)
+        sampler = ClockSampler(local, interval_ms=500)  # multi-second timed region; driver queries stall CUDA calls
         sampler.start()
         launches0 = api.launch_count()
         tickets = [None] * count

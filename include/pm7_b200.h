@@ -171,6 +171,32 @@ void pm7_options_default(pm7_options *options);
 pm7_status pm7_run(const pm7_molecule *molecule, const pm7_params *params,
                    const pm7_options *options, pm7_result *result);
 
+/* ---- nuclear gradient ------------------------------------------------------------
+ * Hellmann-Feynman gradient dE/dR in eV/Bohr, laid out gradient[3*atom + axis]. */
+
+/* Replaces `closed_form_gradient` (src/gradient.rs:500-561): runs the SCF exactly as
+ * pm7_run does (`*result` filled on PM7_OK, same errors) and returns the gradient of
+ * result->total_ev at the converged density: core-core, electronic pair terms (RHF, or the
+ * spin-resolved UHF form of src/gradient.rs:1249-1350) and the post-SCF corrections
+ * (:208-261). `forces` of the reference's GradientResult are -gradient; `max_gradient`
+ * (may be NULL) receives the largest |component|. `gradient` holds 3 * n_atoms doubles. */
+pm7_status pm7_gradient(const pm7_molecule *molecule, const pm7_params *params,
+                        const pm7_options *options, pm7_result *result, double *gradient,
+                        double *max_gradient);
+
+/* Replaces `fixed_density_gradient_with` (src/gradient.rs:638-700) and, with a spin
+ * density, `fixed_density_gradient_uhf_with` (:1263-1350): core-core plus electronic
+ * gradient at a given density, no corrections. `p_total` (nao^2, row-major) is the total
+ * density; `p_spin` is P_alpha - P_beta, or NULL for a closed shell. Host buffers; device 0. */
+pm7_status pm7_fixed_density_gradient(const pm7_molecule *molecule, const pm7_params *params,
+                                      int32_t force_dpath, const double *p_total,
+                                      const double *p_spin, double *gradient);
+
+/* Replaces `correction_gradient` (src/gradient.rs:208-261): the gradient of the post-SCF
+ * corrections (dispersion, H-bond, C#C, Si-O-H, PM7-HH H-H) in eV/Bohr; zero for PM7-minus. */
+pm7_status pm7_correction_gradient(const pm7_molecule *molecule, int32_t method,
+                                   int32_t smooth_dispersion, double *gradient);
+
 /* Release the arrays of a result filled by pm7_run (or the engine). */
 void pm7_result_free(pm7_result *result);
 

@@ -59,6 +59,9 @@ def lib():
     L.pm7_oracle_core_core.argtypes = [C.POINTER(abi.Molecule), C.c_int, abi.DP]
     L.pm7_oracle_corrections.argtypes = [C.POINTER(abi.Molecule), C.c_int, C.c_int, abi.DP]
     L.pm7_oracle_element.argtypes = [C.c_int, C.c_int, abi.DP]
+    L.pm7_oracle_fixed_density_gradient.argtypes = [C.POINTER(abi.Molecule), C.c_int, C.c_int, abi.DP, abi.DP,
+                                                    C.c_double, abi.DP]
+    L.pm7_oracle_correction_gradient.argtypes = [C.POINTER(abi.Molecule), C.c_int, C.c_int, C.c_double, abi.DP]
     libs = sorted(glob.glob(os.path.join(os.path.dirname(np.__file__) + ".libs", "libscipy_openblas64_*.so")))
     if libs:
         L.pm7_oracle_set_lapack(libs[0].encode(), int(os.environ.get("PM7_ORACLE_BLAS_THREADS", "0")))
@@ -192,6 +195,57 @@ def corrections(z, xyz_bohr, method=0, smooth=False):
     out = np.zeros(5)
     _check(lib().pm7_oracle_corrections(C.byref(m.s), method, int(smooth), out.ctypes.data_as(abi.DP)))
     return out
+
+
+def fixed_density_gradient(z, xyz_bohr, p_total, p_spin=None, method=0, force_dpath=False, step=1.0e-3):
+    """Core-core + electronic gradient (eV/Bohr) at a fixed density: the five-point difference
+    of `energy_at_fixed_density_with` (src/gradient.rs:312-432)."""
+    m = _Mol(z, xyz_bohr)
+    pt = np.ascontiguousarray(p_total, dtype=np.float64)
+    ps = None if p_spin is None else np.ascontiguousarray(p_spin, dtype=np.float64)
+    g = np.zeros((len(m.z), 3))
+    _check(lib().pm7_oracle_fixed_density_gradient(C.byref(m.s), method, int(force_dpath), pt.ctypes.data_as(abi.DP),
+                                                   None if ps is None else ps.ctypes.data_as(abi.DP), step,
+                                                   g.ctypes.data_as(abi.DP)))
+    return g
+
+
+def correction_gradient(z, xyz_bohr, method=0, smooth=False, step=1.0e-5):
+    """Post-SCF correction gradient (eV/Bohr, src/gradient.rs:208-261) by the five-point
+    difference of the correction energy. The step is small because the EH+ H-bond energy
+    has kinks (hard switches); a wider stencil can straddle one."""
+    m = _Mol(z, xyz_bohr)
+    g = np.zeros((len(m.z), 3))
+    _check(lib().pm7_oracle_correction_gradient(C.byref(m.s), method, int(smooth), step, g.ctypes.data_as(abi.DP)))
+    return g
+
+
+def gradient(z, xyz_bohr, step=1.0e-3, corr_step=1.0e-5, **options):
+    """The closed-form gradient's quantities (src/gradient.rs:500-561) from the oracle: its
+    SCF, then the fixed-density and correction gradients at the converged density."""
+    r = run(z, xyz_bohr, want_matrices=1, **options)
+    method = options.get("method", 0)
+    g = fixed_density_gradient(z, xyz_bohr, r["density"], r["spin_density"] if r["unrestricted"] else None,
+                               method=method, force_dpath=options.get("force_dpath", False), step=step)
+    g = g + correction_gradient(z, xyz_bohr, method=method, smooth=options.get("smooth_dispersion", False),
+                                step=corr_step)
+    return r, g
+
+
+def numerical_gradient(z, xyz_bohr, step=1.0e-4, **options):
+    """`numerical_gradient` (src/gradient.rs:454-498): central difference of the full SCF's
+    total energy."""
+    x0 = np.array(xyz_bohr, dtype=np.float64).reshape(-1, 3)
+    g = np.zeros_like(x0)
+    for a in range(len(x0)):
+        for k in range(3):
+            e = []
+            for t in (step, -step):
+                x = x0.copy()
+                x[a, k] += t
+                e.append(run(z, x, want_matrices=0, **options)["total_ev"])
+            g[a, k] = (e[0] - e[1]) / (2.0 * step)
+    return g
 
 
 def element(z, method=0):

@@ -1007,6 +1007,32 @@ static pm7_status guarded(F f) {
 
 using namespace oracle;
 
+// Fixed-density energy and the five-point difference of the gradient entry points below.
+static double fixed_density_energy(const Molecule &mol, const Params &p, bool force_dpath, const Mat &pt,
+                                   const Mat &pa, const Mat &pb) {
+  Basis b = build_basis(mol, p);
+  CoreHamiltonian core = build_core(mol, b, p, force_dpath);
+  Mat fa = build_fock_spin(mol, b, p, core, pt, pa);
+  Mat fb = build_fock_spin(mol, b, p, core, pt, pb);
+  return 0.5 * (frob(pt, core.h) + frob(pa, fa) + frob(pb, fb)) + core_core_energy(mol, p);
+}
+
+template <class Energy>
+static void five_point_gradient(const Molecule &mol, double h, Energy energy, double *grad) {
+  const double t[4] = {1.0, -1.0, 2.0, -2.0};
+  for (int a = 0; a < mol.size(); ++a)
+    for (int k = 0; k < 3; ++k) {
+      double e[4];
+      for (int j = 0; j < 4; ++j) {
+        Molecule m2 = mol;
+        Vec3 &r = m2.pos[a];
+        (k == 0 ? r.x : (k == 1 ? r.y : r.z)) += t[j] * h;
+        e[j] = energy(m2);
+      }
+      grad[3 * a + k] = (8.0 * (e[0] - e[1]) - (e[2] - e[3])) / (12.0 * h);
+    }
+}
+
 extern "C" {
 
 int pm7_oracle_set_lapack(const char *path, int threads) { return set_lapack(path, threads) ? 1 : 0; }
@@ -1124,6 +1150,47 @@ pm7_status pm7_oracle_corrections(const pm7_molecule *m, int method, int smooth,
     o.method = method;
     o.smooth_dispersion = smooth;
     correction_energy(to_molecule(m), o, out);
+  });
+}
+
+// ---- nuclear gradient (src/gradient.rs) ----------------------------------------
+// The oracle restates the reference's *independent* check of its closed-form gradient,
+// `analytic_gradient` (src/gradient.rs:365-432): the electronic energy at a fixed density
+// (`energy_at_fixed_density_with`, :312-363: 1/2 [tr(P H) + tr(P^a F^a) + tr(P^b F^b)] from a
+// full core build, plus core-core) differentiated by central differences of the geometry,
+// here the five-point form (8 [E(+h) - E(-h)] - [E(+2h) - E(-2h)]) / 12h per component; and
+// the correction gradient (:208-261) as the same difference of the correction energy.
+
+// Core-core + electronic gradient at the density p_total (spin density p_spin, or null for
+// a closed shell: P^a = P^b = P / 2), eV/Bohr.
+pm7_status pm7_oracle_fixed_density_gradient(const pm7_molecule *m, int method, int force_dpath, const double *pt,
+                                             const double *ps, double step, double *grad) {
+  return guarded([&] {
+    Molecule mol = to_molecule(m);
+    const Params &p = params_for(method);
+    const int nao = build_basis(mol, p).nao;
+    Mat PT(nao), PA(nao), PB(nao);
+    std::memcpy(PT.a.data(), pt, sizeof(double) * PT.a.size());
+    for (size_t i = 0; i < PT.a.size(); ++i) {
+      const double s = ps ? ps[i] : 0.0;
+      PA.a[i] = 0.5 * (PT.a[i] + s);
+      PB.a[i] = 0.5 * (PT.a[i] - s);
+    }
+    five_point_gradient(mol, step, [&](const Molecule &x) { return fixed_density_energy(x, p, force_dpath != 0, PT, PA, PB); },
+                        grad);
+  });
+}
+
+// Post-SCF correction gradient, eV/Bohr.
+pm7_status pm7_oracle_correction_gradient(const pm7_molecule *m, int method, int smooth, double step, double *grad) {
+  return guarded([&] {
+    pm7_options o;
+    std::memset(&o, 0, sizeof o);
+    o.method = method;
+    o.smooth_dispersion = smooth;
+    double parts[5];
+    five_point_gradient(to_molecule(m), step,
+                        [&](const Molecule &x) { return correction_energy(x, o, parts) * KCAL_TO_EV; }, grad);
   });
 }
 

@@ -24,6 +24,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "gradient.cuh"
 #include "kernels.hpp"
 #include "params.hpp"
 #include "pm7_b200.h"
@@ -1132,6 +1133,73 @@ void fill_result(pm7_result *res, const Molecule &m, const Layout &L, const Para
   if (S.unrestricted) res->mo_energies_beta = host_vec(S.eps_b);
 }
 
+// Displaced geometry copies per pass of the correction gradient: all 12 n at once when they fit
+// in ~1 GB of device memory (and the grid's z extent), else as many as do.
+static int correction_copies(int n, int smooth) {
+  const size_t per = corrections_gradient_work(n, 1, smooth) - corrections_gradient_work(n, 0, smooth);
+  return (int)std::max<size_t>(1, std::min<size_t>({(size_t)kStencil * n, (size_t)65535, ((size_t)1 << 27) / per}));
+}
+
+// Nuclear gradient (eV/Bohr) at the density Pt (total) / Ps (spin, null for a closed shell) of
+// the built device molecule D: core-core + electronic pair terms (src/gradient.rs:654-700,
+// 1082-1247) and, with `corrections`, the post-SCF correction gradient (:208-261).
+static std::vector<double> device_gradient(cudaStream_t st, const DeviceParams &P, const DeviceMolecule &D, bool dpath,
+                                           const double *Pt, const double *Ps, int method, int smooth,
+                                           bool corrections) {
+  const int n = D.n;
+  std::vector<double> grad(3 * (size_t)n, 0.0);
+  if (n == 0) return grad;
+  const size_t npairs = (size_t)n * (size_t)(n - 1) / 2;
+  DevBuf<double> E, G;
+  DevBuf<int> status;
+  E.alloc(npairs * kStencil, st);
+  G.alloc(3 * (size_t)n, st);
+  status.alloc(1, st);
+  CUDA_OK(cudaMemsetAsync(status.p, 0, sizeof(int), st));
+  GradGeometry g;
+  g.n_atoms = n;
+  g.nao = D.nao;
+  g.n_near = D.n_near;
+  g.z = D.z.p;
+  g.aoff = D.aoff.p;
+  g.xyz = D.xyz.p;
+  g.near_mask = D.mask.p;
+  g.np = D.near.p;
+  g.Pt = Pt;
+  g.Ps = Ps;
+  g.E = E.p;
+  g.status = status.p;
+  {
+    Stage s_(st, "gradient_pairs");
+    if (dpath) {
+      launch_grad_pairs_d(st, g, P);
+      launch_grad_near_d(st, g, P);
+    } else {
+      launch_grad_pairs_sp(st, g, P);
+      launch_grad_near_sp(st, g, P);
+    }
+    launch_grad_atoms(st, g, G.p);
+  }
+  if (corrections && method != 3) {
+    Stage s_(st, "gradient_corrections");
+    const int copies = correction_copies(n, smooth);
+    DevBuf<double> work, energies, cg;
+    work.alloc(corrections_gradient_work(n, copies, smooth), st);
+    energies.alloc((size_t)kStencil * n, st);
+    cg.alloc(3 * (size_t)n, st);
+    launch_corrections_gradient(st, n, D.z.p, D.xyz.p, method, smooth, copies, work.p, energies.p, cg.p);
+    launch_grad_add(st, n, kKcalToEv, cg.p, G.p);
+  }
+  int bad = 0;
+  CUDA_OK(cudaMemcpyAsync(grad.data(), G.p, sizeof(double) * grad.size(), cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(&bad, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  CUDA_OK(cudaGetLastError());
+  if (bad & 1) throw Failure{PM7_ERR_UNSUPPORTED, "gradient: a shell pair without an overlap formula"};
+  if (bad & 2) throw Failure{PM7_ERR_INVALID_INPUT, "gradient: d-shell pair in the sp frame"};
+  return grad;
+}
+
 // Host-side phase times of one pm7_run on stderr (PM7_HOST_TRACE set): where the wall time
 // beyond the device's goes.
 struct HostTrace {
@@ -1151,7 +1219,8 @@ struct HostTrace {
   }
 };
 
-static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm7_options *opt, pm7_result *res) {
+static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm7_options *opt, pm7_result *res,
+                     std::vector<double> *gradient = nullptr) {
   if (!opt || !res || !params) throw Failure{PM7_ERR_INVALID_INPUT, "null argument"};
   HostTrace ht;
   const pm7_options &o = *opt;
@@ -1276,6 +1345,9 @@ static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm
     CUDA_OK(cudaStreamSynchronize(st));
   }
   ht.mark("readback");
+  if (gradient && S.converged)
+    *gradient = device_gradient(st, P, D, o.force_dpath || L.has_d, S.P.p, S.unrestricted ? S.Pspin.p : nullptr,
+                                o.method, o.smooth_dispersion, true);
   fill_result(res, m, L, ps, o, R, diag_blocks, [&](int a, int i, int j) {
     return o.want_matrices ? Ph[(size_t)(L.aoff[a] + i) * nao + L.aoff[a] + j] : blocks[(size_t)81 * a + 9 * i + j];
   });
@@ -1341,6 +1413,55 @@ static void stage_core(const pm7_molecule *mol, const pm7_params *params, int fo
   CUDA_OK(cudaStreamSynchronize(st));
 }
 
+// Fixed-density gradient of host densities (src/gradient.rs:626-700 and the UHF form :1249-1350).
+static void stage_gradient(const pm7_molecule *mol, const pm7_params *params, int force_dpath, const double *p_total,
+                           const double *p_spin, double *grad_out) {
+  Molecule m = to_molecule(mol);
+  const int method = *reinterpret_cast<const int *>(params);
+  const ParamSet &ps = param_set(method);
+  Layout L = build_layout(m, ps);
+  DeviceContext &ctx = context_for(0);
+  std::lock_guard<std::mutex> lock(ctx.run_mutex);
+  CUDA_OK(cudaSetDevice(ctx.device));
+  const DeviceParams &P = device_params(ctx, method);
+  cudaStream_t st = ctx.stream;
+  DeviceMolecule D;
+  const bool dpath = force_dpath || L.has_d;
+  build_device_molecule(D, m, L, P, dpath, st);
+  const size_t nn = (size_t)L.nao * L.nao;
+  DevBuf<double> Pt, Ps;
+  upload(Pt, std::vector<double>(p_total, p_total + nn), st);
+  if (p_spin) upload(Ps, std::vector<double>(p_spin, p_spin + nn), st);
+  const std::vector<double> g = device_gradient(st, P, D, dpath, Pt.p, p_spin ? Ps.p : nullptr, method, 0, false);
+  std::memcpy(grad_out, g.data(), sizeof(double) * g.size());
+}
+
+// Correction-energy gradient alone, eV/Bohr (src/gradient.rs:208-261).
+static void stage_correction_gradient(const pm7_molecule *mol, int method, int smooth, double *grad_out) {
+  Molecule m = to_molecule(mol);
+  DeviceContext &ctx = context_for(0);
+  std::lock_guard<std::mutex> lock(ctx.run_mutex);
+  CUDA_OK(cudaSetDevice(ctx.device));
+  cudaStream_t st = ctx.stream;
+  const int n = m.n;
+  if (n == 0) return;
+  DevBuf<int> z;
+  DevBuf<double> xyz, work, energies, cg, G;
+  upload(z, m.z, st);
+  upload(xyz, m.xyz, st);
+  const int copies = correction_copies(n, smooth);
+  work.alloc(corrections_gradient_work(n, copies, smooth), st);
+  energies.alloc((size_t)kStencil * n, st);
+  cg.alloc(3 * (size_t)n, st);
+  G.alloc(3 * (size_t)n, st);
+  CUDA_OK(cudaMemsetAsync(G.p, 0, sizeof(double) * 3 * n, st));
+  launch_corrections_gradient(st, n, z.p, xyz.p, method, smooth, copies, work.p, energies.p, cg.p);
+  launch_grad_add(st, n, kKcalToEv, cg.p, G.p);
+  CUDA_OK(cudaMemcpyAsync(grad_out, G.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  CUDA_OK(cudaGetLastError());
+}
+
 }  // namespace pm7
 
 // ---------------------------------------------------------------------------
@@ -1400,6 +1521,38 @@ void pm7_options_default(pm7_options *o) {
 pm7_status pm7_run(const pm7_molecule *molecule, const pm7_params *params, const pm7_options *options,
                    pm7_result *result) {
   return guarded([&] { run_impl(molecule, params, options, result); });
+}
+
+pm7_status pm7_gradient(const pm7_molecule *molecule, const pm7_params *params, const pm7_options *options,
+                        pm7_result *result, double *gradient, double *max_gradient) {
+  return guarded([&] {
+    if (!gradient) throw Failure{PM7_ERR_INVALID_INPUT, "null gradient buffer"};
+    std::vector<double> g;
+    run_impl(molecule, params, options, result, &g);
+    std::memcpy(gradient, g.data(), sizeof(double) * g.size());
+    if (max_gradient) {
+      double mx = 0.0;
+      for (double v : g) mx = std::max(mx, std::fabs(v));
+      *max_gradient = mx;
+    }
+  });
+}
+
+pm7_status pm7_fixed_density_gradient(const pm7_molecule *molecule, const pm7_params *params, int32_t force_dpath,
+                                      const double *p_total, const double *p_spin, double *gradient) {
+  return guarded([&] {
+    if (!params || !p_total || !gradient) throw Failure{PM7_ERR_INVALID_INPUT, "null argument"};
+    stage_gradient(molecule, params, force_dpath, p_total, p_spin, gradient);
+  });
+}
+
+pm7_status pm7_correction_gradient(const pm7_molecule *molecule, int32_t method, int32_t smooth_dispersion,
+                                   double *gradient) {
+  return guarded([&] {
+    if (!gradient) throw Failure{PM7_ERR_INVALID_INPUT, "null gradient buffer"};
+    if (method < 0 || method > 4) throw Failure{PM7_ERR_INVALID_INPUT, "unknown PM7 method"};
+    stage_correction_gradient(molecule, method, smooth_dispersion, gradient);
+  });
 }
 
 void pm7_result_free(pm7_result *r) {

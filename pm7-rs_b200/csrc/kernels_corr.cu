@@ -8,6 +8,7 @@
 
 #include "common.cuh"
 #include "batch.hpp"
+#include "gradient.cuh"
 #include "kernels.hpp"
 
 namespace pm7 {
@@ -116,37 +117,43 @@ __device__ __forceinline__ void c6_atom(int n, const int *__restrict__ z, const 
   }
 }
 
+// The pair terms of atoms of numbers zu, zv (C6 coefficients c6u, c6v) at distance r (Bohr):
+// dispersion, the C#C switch (counted 12 kcal/mol per full bond by the caller) and PM7-HH.
+__device__ __forceinline__ void pair_corr_r(int zu, int zv, double c6u, double c6v, int hh, double r, double &ed,
+                                            double &ey, double &eh) {
+  ed = pair_dispersion(zu, zv, c6u, c6v, r);
+  ey = 0.0;
+  eh = 0.0;
+  const double ra = r * kA0;
+  if (zu == 6 && zv == 6 && ra < 1.33) {
+    if (ra < 1.21) {
+      ey = 1.0;
+    } else {
+      const double x = (ra - 1.21) / (1.33 - 1.21);
+      const double x3 = x * x * x, x4 = x3 * x, x5 = x4 * x, x6 = x5 * x;
+      ey = (1.0 - 10.0 * x3 + 15.0 * x4 - 6.0 * x5) + (-5.0 + 25.0 * x) * (x3 - 3.0 * x4 + 3.0 * x5 - x6);
+    }
+  }
+  if (hh && zu == 1 && zv == 1) {
+    if (ra <= 1.0) eh = 25.46293603147693;
+    else if (ra < 1.5) {
+      const double r2 = ra * ra, r3 = r2 * ra, r4 = r3 * ra, r5 = r4 * ra;
+      eh = r5 * (-2714.9523516034697) + r4 * 17103.650110591705 + r3 * (-42511.85798221796) +
+           r2 * 52063.19679913834 + ra * (-31430.65833597229) + 7516.08469609514;
+    } else {
+      eh = exp(pow(ra, 1.72905) * (-1.53965)) * 118.7326;
+    }
+  }
+}
+
 // Pair terms of every u < v: dispersion, C#C and PM7-HH. Grid (ceil(N/128), N).
 __device__ __forceinline__ void pair_corr_elem(int n, const int *__restrict__ z, const double *__restrict__ xyz,
                                                const double *__restrict__ c6, int hh, int u, int v, double &ed,
                                                double &ey, double &eh) {
-  ed = 0.0;
-  ey = 0.0;
-  eh = 0.0;
+  ed = ey = eh = 0.0;
   if (v > u && v < n) {
     const double dx = xyz[3 * v] - xyz[3 * u], dy = xyz[3 * v + 1] - xyz[3 * u + 1], dz = xyz[3 * v + 2] - xyz[3 * u + 2];
-    const double r = sqrt(dx * dx + dy * dy + dz * dz);
-    ed = pair_dispersion(z[u], z[v], c6[u], c6[v], r);
-    const double ra = r * kA0;
-    if (z[u] == 6 && z[v] == 6 && ra < 1.33) {
-      if (ra < 1.21) {
-        ey = 1.0;
-      } else {
-        const double x = (ra - 1.21) / (1.33 - 1.21);
-        const double x3 = x * x * x, x4 = x3 * x, x5 = x4 * x, x6 = x5 * x;
-        ey = (1.0 - 10.0 * x3 + 15.0 * x4 - 6.0 * x5) + (-5.0 + 25.0 * x) * (x3 - 3.0 * x4 + 3.0 * x5 - x6);
-      }
-    }
-    if (hh && z[u] == 1 && z[v] == 1) {
-      if (ra <= 1.0) eh = 25.46293603147693;
-      else if (ra < 1.5) {
-        const double r2 = ra * ra, r3 = r2 * ra, r4 = r3 * ra, r5 = r4 * ra;
-        eh = r5 * (-2714.9523516034697) + r4 * 17103.650110591705 + r3 * (-42511.85798221796) +
-             r2 * 52063.19679913834 + ra * (-31430.65833597229) + 7516.08469609514;
-      } else {
-        eh = exp(pow(ra, 1.72905) * (-1.53965)) * 118.7326;
-      }
-    }
+    pair_corr_r(z[u], z[v], c6[u], c6[v], hh, sqrt(dx * dx + dy * dy + dz * dz), ed, ey, eh);
   }
 }
 
@@ -601,7 +608,244 @@ __global__ void k_b_finish(BatchList L, const MolDesc *__restrict__ D, MolCtl *_
   finish_block((int)v.parts, v.pd, v.py, v.ph, v.n, v.ehb, v.esioh, C[slot].corr);
 }
 
+// ---- gradient of the correction energy (src/gradient.rs:208-261) ----------------------
+// Central differences (five-point, step kCorrStep) of the correction energy. With the
+// default discrete C6 (bond counts, src/dispersion.rs:297-330: fixed under a small
+// displacement, as the reference's gradient treats them) the pair terms (dispersion, C#C,
+// PM7-HH) are differentiated pair by pair in r, and only the many-body H-bond and Si-O-H
+// items are re-evaluated at displaced copies of the geometry -- and only those within reach
+// of the moved atom, the others being bit-identical to the base values (covalent neighbour
+// lists, a discrete choice, are taken at the base geometry). With the smooth C6
+// (src/dispersion.rs:428-) every term is re-evaluated at every copy. The step is small
+// (1e-5 Bohr) because the EH+ H-bond energy has kinks (hard switches of hbond.rs:525-620):
+// a stencil that straddles one mixes both branches; differencing the changed items only
+// keeps the rounding error near 1e-10 kcal/mol per Bohr.
+constexpr double kCorrStep = 1.0e-5;   // Bohr
+constexpr double kSiohReachAng = 2.5;  // Si within 2.4 A, H within 1.4 A of the oxygen
+
+// How far (Angstrom) the H-bond energies that depend on atom A reach, or -1 for none. The
+// energy of hydrogen j (hbonds_warp) depends on j, its donors (N/O within 1.4 A), their
+// acceptors (N/O within 7 A of the donor, so within 8.4 A of j) and the covalent neighbours of
+// both (neighbour lists fixed at the base geometry). So A reaches 0 (itself, a hydrogen),
+// 8.4 A (an N or O) and 8.4 A + |A - X| for each N/O atom X that lists A as a neighbour.
+__global__ void k_hb_reach(int n, const int *__restrict__ z, const double *__restrict__ xyz,
+                           const int *__restrict__ nbr, const int *__restrict__ nbc, double *__restrict__ reach) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  double r = z[a] == 1 ? 0.0 : -1.0;
+  if (is_acceptor(z[a])) r = fmax(r, 8.4);
+  for (int x = 0; x < n; ++x) {
+    if (!is_acceptor(z[x])) continue;
+    for (int q = 0; q < nbc[x]; ++q)
+      if (nbr[4 * x + q] == a) r = fmax(r, 8.4 + dist_ang(xyz, x, a));
+  }
+  reach[a] = r;
+}
+
+// Copy c of a pass holds stencil point s = s0 + c: atom s / 12 moved by stencil_offset(s % 12).
+__global__ void k_fd_displace(int n, const double *__restrict__ xyz, int s0, size_t stride, double *__restrict__ work) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (i >= 3 * n) return;
+  const int s = s0 + c;
+  double o[3];
+  stencil_offset(s % kStencil, kCorrStep, o);
+  work[(size_t)c * stride + i] = xyz[i] + (i / 3 == s / kStencil ? o[i % 3] : 0.0);
+}
+
+// ... full path: the whole correction energy per copy (coordinates, corrections scratch, parts).
+struct FdCopy {
+  double *xyz;
+  CorrView v;
+  double *out;
+};
+__device__ __forceinline__ FdCopy fd_copy(int n, double *work, size_t stride, int c) {
+  FdCopy f;
+  f.xyz = work + (size_t)c * stride;
+  f.v = corr_view(n, f.xyz + 3 * (size_t)n);
+  const size_t parts = (size_t)((n + 127) / 128) * (size_t)(n > 0 ? n : 1);
+  f.out = f.xyz + 3 * (size_t)n + 3 * parts + 11 * (size_t)n;
+  return f;
+}
+__global__ void k_fd_c6(int n, const int *__restrict__ z, int smooth, double *work, size_t stride) {
+  const FdCopy f = fd_copy(n, work, stride, blockIdx.z);
+  c6_atom(n, z, f.xyz, smooth, f.v.c6, blockIdx.x * blockDim.x + threadIdx.x);
+}
+__global__ void k_fd_pair_corr(int n, const int *__restrict__ z, int hh, double *work, size_t stride) {
+  const FdCopy f = fd_copy(n, work, stride, blockIdx.z);
+  pair_corr_block(n, z, f.xyz, f.v.c6, hh, blockIdx.y, blockIdx.x, (size_t)blockIdx.y * gridDim.x + blockIdx.x,
+                  f.v.pd, f.v.py, f.v.ph);
+}
+__global__ void k_fd_hb_neighbours(int n, const int *__restrict__ z, double *work, size_t stride) {
+  const FdCopy f = fd_copy(n, work, stride, blockIdx.z);
+  hb_neighbours_atom(n, z, f.xyz, f.v.nbr, f.v.nbc, blockIdx.x * blockDim.x + threadIdx.x);
+}
+__global__ void k_fd_hbonds(int n, const int *__restrict__ z, double *work, size_t stride) {
+  const FdCopy f = fd_copy(n, work, stride, blockIdx.z);
+  hbonds_warp(n, z, f.xyz, f.v.nbr, f.v.nbc, f.v.ehb, blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+}
+__global__ void k_fd_sioh(int n, const int *__restrict__ z, double *work, size_t stride) {
+  const FdCopy f = fd_copy(n, work, stride, blockIdx.z);
+  sioh_atom(n, z, f.xyz, f.v.esioh, blockIdx.x * blockDim.x + threadIdx.x);
+}
+// The copy's total correction, summed in the order the result uses (scf.rs:907-932).
+__global__ void k_fd_finish(int n, double *work, size_t stride, int s0, double *__restrict__ energies) {
+  const FdCopy f = fd_copy(n, work, stride, blockIdx.x);
+  finish_block((int)f.v.parts, f.v.pd, f.v.py, f.v.ph, n, f.v.ehb, f.v.esioh, f.out);
+  if (threadIdx.x == 0) {
+    double e = f.out[0];
+    e += f.out[1];
+    e += f.out[4];
+    e += f.out[2];
+    e += f.out[3];
+    energies[s0 + blockIdx.x] = e;
+  }
+}
+
+// ... local path: per copy, coordinates and the H-bond / Si-O-H energy of every atom.
+struct FdLocal {
+  double *xyz, *hb, *so;
+};
+__device__ __forceinline__ FdLocal fd_local(int n, double *work, size_t stride, int c) {
+  FdLocal f;
+  f.xyz = work + (size_t)c * stride;
+  f.hb = f.xyz + 3 * (size_t)n;
+  f.so = f.hb + n;
+  return f;
+}
+// A warp per atom j of copy blockIdx.z: its H-bond energy, re-evaluated when j is a hydrogen
+// within reach of the moved atom, else the base value.
+__global__ void k_fd_hbonds_local(int n, const int *__restrict__ z, const int *__restrict__ nbr,
+                                  const int *__restrict__ nbc, const double *__restrict__ ehb0,
+                                  const double *__restrict__ reach, int s0, double *work, size_t stride) {
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (j >= n) return;
+  const FdLocal f = fd_local(n, work, stride, blockIdx.z);
+  const int A = (s0 + (int)blockIdx.z) / kStencil;
+  if (z[j] != 1 || reach[A] < 0.0 || dist_ang(f.xyz, j, A) > reach[A] + 0.01) {
+    if ((threadIdx.x & 31) == 0) f.hb[j] = ehb0[j];
+    return;
+  }
+  hbonds_warp(n, z, f.xyz, nbr, nbc, f.hb, j);
+}
+__global__ void k_fd_sioh_local(int n, const int *__restrict__ z, const double *__restrict__ esioh0, int s0, double *work,
+                                size_t stride) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= n) return;
+  const FdLocal f = fd_local(n, work, stride, blockIdx.z);
+  const int A = (s0 + (int)blockIdx.z) / kStencil;
+  if (z[o] != 8 || dist_ang(f.xyz, o, A) > kSiohReachAng) f.so[o] = esioh0[o];
+  else sioh_atom(n, z, f.xyz, f.so, o);
+}
+// The copy's change of the H-bond + Si-O-H energy (fixed order).
+__global__ void k_fd_finish_local(int n, const double *__restrict__ ehb0, const double *__restrict__ esioh0, double *work,
+                                  size_t stride, int s0, double *__restrict__ energies) {
+  const FdLocal f = fd_local(n, work, stride, blockIdx.x);
+  double d = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) d += (f.hb[i] - ehb0[i]) + (f.so[i] - esioh0[i]);
+  d = block_sum<256>(d);
+  if (threadIdx.x == 0) energies[s0 + blockIdx.x] = d;
+}
+
+// A warp per atom A: the pair terms' derivative along every pair (A, B) at fixed C6, by the
+// five-point difference in r; lanes over partners, fixed xor tree. kcal/mol per Bohr.
+__global__ void k_corr_pair_grad(int n, const int *__restrict__ z, const double *__restrict__ xyz,
+                                 const double *__restrict__ c6, int hh, double *__restrict__ grad) {
+  const int A = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (A >= n) return;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int B = lane; B < n; B += 32) {
+    if (B == A) continue;
+    const int u = A < B ? A : B, v = A < B ? B : A;
+    const double d[3] = {xyz[3 * A] - xyz[3 * B], xyz[3 * A + 1] - xyz[3 * B + 1], xyz[3 * A + 2] - xyz[3 * B + 2]};
+    const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    double e4[4];
+    const double t[4] = {1.0, -1.0, 2.0, -2.0};
+    for (int q = 0; q < 4; ++q) {
+      double ed, ey, eh;
+      pair_corr_r(z[u], z[v], c6[u], c6[v], hh, r + t[q] * kCorrStep, ed, ey, eh);
+      e4[q] = ed + 12.0 * ey + eh;
+    }
+    const double dedr = stencil_derivative(e4, kCorrStep);
+    for (int k = 0; k < 3; ++k) acc[k] += dedr * (d[k] / r);
+  }
+  for (int k = 0; k < 3; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+  }
+  if (lane == 0)
+    for (int k = 0; k < 3; ++k) grad[3 * A + k] = acc[k];
+}
+
+__global__ void k_fd_grad(int n, const double *__restrict__ energies, int add, double *__restrict__ grad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * n) return;
+  const double g = stencil_derivative(energies + (size_t)(i / 3) * kStencil + 4 * (i % 3), kCorrStep);
+  grad[i] = add ? grad[i] + g : g;
+}
+
+// Work layout: a base block (the local path's C6, base H-bond and Si-O-H energies, reach,
+// neighbour lists) then `copies` slices of `corr_copy_stride` doubles.
+size_t corr_base_doubles(int n) { return 9 * (size_t)n + 8; }
+size_t corr_copy_stride(int n, int smooth) {
+  return smooth ? 3 * (size_t)n + corrections_scratch(n) + 8 : 5 * (size_t)n + 8;
+}
+
 }  // namespace
+
+size_t corrections_gradient_work(int n_atoms, int copies, int smooth) {
+  return corr_base_doubles(n_atoms) + (size_t)copies * corr_copy_stride(n_atoms, smooth);
+}
+
+void launch_corrections_gradient(cudaStream_t st, int n, const int *z, const double *xyz, int method, int smooth,
+                                 int copies, double *work, double *energies, double *grad) {
+  if (n <= 0) return;
+  if (method == 3) {  // PM7-minus carries no post-SCF corrections
+    cudaMemsetAsync(grad, 0, 3 * sizeof(double) * (size_t)n, st);
+    return;
+  }
+  const int hh = method == 4;
+  const size_t stride = corr_copy_stride(n, smooth);
+  double *base = work, *copy0 = work + corr_base_doubles(n);
+  const int total = kStencil * n;
+  const int ga = (n + 127) / 128;
+  if (smooth) {
+    for (int s0 = 0; s0 < total; s0 += copies) {
+      const int c = copies < total - s0 ? copies : total - s0;
+      k_fd_displace<<<dim3((3 * n + 127) / 128, c), 128, 0, st>>>(n, xyz, s0, stride, copy0);
+      k_fd_c6<<<dim3(ga, 1, c), 128, 0, st>>>(n, z, smooth, copy0, stride);
+      k_fd_pair_corr<<<dim3(ga, n, c), 128, 0, st>>>(n, z, hh, copy0, stride);
+      k_fd_hb_neighbours<<<dim3(ga, 1, c), 128, 0, st>>>(n, z, copy0, stride);
+      k_fd_hbonds<<<dim3((n + 3) / 4, 1, c), 128, 0, st>>>(n, z, copy0, stride);
+      k_fd_sioh<<<dim3(ga, 1, c), 128, 0, st>>>(n, z, copy0, stride);
+      k_fd_finish<<<c, 256, 0, st>>>(n, copy0, stride, s0, energies);
+      note_launch(7);
+    }
+    k_fd_grad<<<(3 * n + 127) / 128, 128, 0, st>>>(n, energies, 0, grad);
+    note_launch();
+    return;
+  }
+  // base quantities of the local path
+  double *c6 = base, *ehb0 = c6 + n, *esioh0 = ehb0 + n, *reach = esioh0 + n;
+  int *nbr = reinterpret_cast<int *>(reach + n), *nbc = nbr + 4 * n;
+  k_c6<<<ga, 128, 0, st>>>(n, z, xyz, 0, c6);
+  k_hb_neighbours<<<ga, 128, 0, st>>>(n, z, xyz, nbr, nbc);
+  k_hbonds<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, nbr, nbc, ehb0);
+  k_sioh<<<ga, 128, 0, st>>>(n, z, xyz, esioh0);
+  k_hb_reach<<<ga, 128, 0, st>>>(n, z, xyz, nbr, nbc, reach);
+  k_corr_pair_grad<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, c6, hh, grad);
+  note_launch(6);
+  for (int s0 = 0; s0 < total; s0 += copies) {
+    const int c = copies < total - s0 ? copies : total - s0;
+    k_fd_displace<<<dim3((3 * n + 127) / 128, c), 128, 0, st>>>(n, xyz, s0, stride, copy0);
+    k_fd_hbonds_local<<<dim3((n + 3) / 4, 1, c), 128, 0, st>>>(n, z, nbr, nbc, ehb0, reach, s0, copy0, stride);
+    k_fd_sioh_local<<<dim3(ga, 1, c), 128, 0, st>>>(n, z, esioh0, s0, copy0, stride);
+    k_fd_finish_local<<<c, 256, 0, st>>>(n, ehb0, esioh0, copy0, stride, s0, energies);
+    note_launch(4);
+  }
+  k_fd_grad<<<(3 * n + 127) / 128, 128, 0, st>>>(n, energies, 1, grad);
+  note_launch();
+}
 
 size_t corrections_scratch(int n_atoms) {
   const size_t parts = (size_t)((n_atoms + 127) / 128) * (size_t)(n_atoms > 0 ? n_atoms : 1);

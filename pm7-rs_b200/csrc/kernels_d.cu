@@ -17,8 +17,13 @@
 #include "common.cuh"
 #include "core_repulsion.cuh"
 #include "batch.hpp"
+#include "gradient.cuh"
 #include "kernels.hpp"
 #include "nddo_sp.cuh"
+
+#include <mutex>
+#include <set>
+#include <utility>
 
 namespace pm7 {
 namespace {
@@ -1078,6 +1083,79 @@ __global__ void __launch_bounds__(32) k_stage_pair_d(DeviceParams P, int zi, int
   }
 }
 
+// ---- nuclear gradient at a fixed density, MNDO/d frame (gradient.cuh) ----------------
+
+// Every pair u < v and stencil point s: core-core, beta*S from the d-frame overlap and the
+// point-charge terms beyond the feather range. Grid (ceil((N - 1) * 12 / 128), N), blockIdx.y = u.
+__global__ void k_grad_pairs_d(GradGeometry g, DeviceParams P) {
+  const int u = blockIdx.y;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int v = u + 1 + t / kStencil, s = t % kStencil;
+  if (v >= g.n_atoms) return;
+  const StencilPair q = stencil_pair(g, P, u, v, s);
+  const ElementRec &ea = P.elements[g.z[q.a]];
+  const ElementRec &eb = P.elements[g.z[q.b]];
+  double E = pair_core_energy(P, ea, eb, q.r);
+  const int oa = g.aoff[q.a], ob = g.aoff[q.b];
+  diat_overlap(ea, eb, q.d[0], q.d[1], q.d[2], [&](int i, int j, double sv) {
+    E += g.Pt[(size_t)(oa + i - 1) * g.nao + ob + j - 1] * (beta_of(ea, i - 1) + beta_of(eb, j - 1)) * sv;
+  });
+  if (!g.near_mask[(size_t)u * g.n_atoms + v])
+    E += ((1.0 / q.r) * kEv) * far_bracket(g, oa, ea.n_orb, ob, eb.n_orb, ea.core, eb.core);
+  g.E[tri_index(g.n_atoms, u, v) * kStencil + s] = E;
+}
+
+// Near pair p and stencil point s, a warp per item: w and the electron-core blocks of the
+// warp-per-pair kernel at the displaced separation, contracted with the density (lanes over
+// elements, fixed xor tree), added to the pair's stencil energy.
+__global__ void __launch_bounds__(32 * kDWarps) k_grad_near_d(GradGeometry g, DeviceParams P) {
+  extern __shared__ double smem_d[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long item = (long long)blockIdx.x * kDWarps + warp;
+  const int p = (int)(item / kStencil), s = (int)(item % kStencil);
+  if (p >= g.n_near) return;
+  DPairShared &S = reinterpret_cast<DPairShared *>(smem_d)[warp];
+  const NearPair np = g.np[p];
+  const int u = np.u < np.v ? np.u : np.v, v = np.u < np.v ? np.v : np.u;
+  const StencilPair q = stencil_pair(g, P, u, v, s);
+  const ElementRec &ea = P.elements[g.z[q.a]];
+  const ElementRec &eb = P.elements[g.z[q.b]];
+  warp_pair_d(S, P.tab, ea, eb, q.d[0], q.d[1], q.d[2], lane);
+  const int oa = g.aoff[q.a], ob = g.aoff[q.b];
+  const int limij = ea.n_orb * (ea.n_orb + 1) / 2, limkl = eb.n_orb * (eb.n_orb + 1) / 2;
+  double E = 0.0;
+  for (int t = lane; t < limij * limkl; t += 32) {
+    const int pi = t / limkl, pj = t - pi * limkl;
+    int mu, nu, la, si;
+    unpack(pi, mu, nu);
+    unpack(pj, la, si);
+    E += two_e_coef(g, oa, ob, mu, nu, la, si) * S.ww[t + 1];
+  }
+  for (int t = lane; t < limij + limkl; t += 32) {
+    int mu, nu;
+    if (t < limij) {
+      unpack(t, mu, nu);
+      E += ecore_coef(g, oa, mu, nu) * elenuc(S, P.tab, 1, mu + 1, nu + 1);
+    } else {
+      unpack(t - limij, mu, nu);
+      E += ecore_coef(g, ob, mu, nu) * elenuc(S, P.tab, 2, mu + 1, nu + 1);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) E += __shfl_xor_sync(0xffffffffu, E, o);
+  if (lane == 0) g.E[tri_index(g.n_atoms, u, v) * kStencil + s] += E;
+}
+
+// Sets a kernel's dynamic shared-memory limit once per (kernel, device).
+void ensure_smem(const void *fn, size_t bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<const void *, int>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.insert({fn, dev}).second) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 }  // namespace
 
 // ---- host launchers ------------------------------------------------------
@@ -1094,11 +1172,7 @@ void launch_near_integrals_d(cudaStream_t st, int n_near, const int *z, const do
                              const DeviceParams &P, double *w, double *ecore) {
   if (n_near == 0) return;
   const size_t smem = sizeof(DPairShared) * kDWarps;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_near_integrals_d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  ensure_smem((const void *)k_near_integrals_d, smem);
   k_near_integrals_d<<<(n_near + kDWarps - 1) / kDWarps, 32 * kDWarps, smem, st>>>(n_near, z, xyz, np, P, w, ecore);
   note_launch();
 }
@@ -1112,12 +1186,24 @@ void launch_b_pairs_all_d(cudaStream_t st, const BatchList &L, const MolDesc *D,
 void launch_b_near_integrals_d(cudaStream_t st, const BatchList &L, const MolDesc *D, const DeviceParams &P) {
   if (L.total <= 0) return;
   const size_t smem = sizeof(DPairShared) * kDWarps;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_b_near_integrals_d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  ensure_smem((const void *)k_b_near_integrals_d, smem);
   k_b_near_integrals_d<<<L.total, 32 * kDWarps, smem, st>>>(L, D, P);
+  note_launch();
+}
+
+void launch_grad_pairs_d(cudaStream_t st, const GradGeometry &g, const DeviceParams &P) {
+  if (g.n_atoms < 2) return;
+  const dim3 grid((unsigned)(((size_t)(g.n_atoms - 1) * kStencil + 127) / 128), (unsigned)g.n_atoms);
+  k_grad_pairs_d<<<grid, 128, 0, st>>>(g, P);
+  note_launch();
+}
+
+void launch_grad_near_d(cudaStream_t st, const GradGeometry &g, const DeviceParams &P) {
+  if (g.n_near <= 0) return;
+  const size_t smem = sizeof(DPairShared) * kDWarps;
+  ensure_smem((const void *)k_grad_near_d, smem);
+  const size_t items = (size_t)g.n_near * kStencil;
+  k_grad_near_d<<<(unsigned)((items + kDWarps - 1) / kDWarps), 32 * kDWarps, smem, st>>>(g, P);
   note_launch();
 }
 

@@ -23,7 +23,8 @@ EXPORTED = [
     "pm7_device_count", "pm7_stage_core_hamiltonian", "pm7_stage_fock", "pm7_stage_pair", "pm7_stage_core_core",
     "pm7_stage_corrections", "pm7_run_batch", "pm7_engine_config_default", "pm7_engine_create", "pm7_engine_submit",
     "pm7_engine_poll", "pm7_engine_destroy", "pm7_batch_partition", "pm7_stage_eigenvalues",
-    "pm7_stage_product_tf32", "pm7_autotune_report",
+    "pm7_stage_product_tf32", "pm7_autotune_report", "pm7_gradient", "pm7_fixed_density_gradient",
+    "pm7_correction_gradient",
 ]
 
 
@@ -64,6 +65,10 @@ def lib():
                                 C.POINTER(abi.Result), C.POINTER(C.c_int32)]
     L.pm7_batch_partition.argtypes = [C.c_int32, C.POINTER(abi.Molecule), C.c_int32, C.c_int32,
                                       C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+    L.pm7_gradient.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, C.POINTER(abi.Options), C.POINTER(abi.Result),
+                               abi.DP, abi.DP]
+    L.pm7_fixed_density_gradient.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, C.c_int32, abi.DP, abi.DP, abi.DP]
+    L.pm7_correction_gradient.argtypes = [C.POINTER(abi.Molecule), C.c_int32, C.c_int32, abi.DP]
     L.pm7_stage_eigenvalues.argtypes = [C.c_int32, C.POINTER(C.c_int32), abi.DP, abi.DP, C.c_int32]
     L.pm7_engine_config_default.argtypes = [C.POINTER(abi.EngineConfig)]
     L.pm7_engine_create.argtypes = [C.POINTER(abi.EngineConfig), C.POINTER(C.c_void_p)]
@@ -148,6 +153,54 @@ def run_pm7(z, xyz_bohr, **options):
         return result_to_dict(r)
     finally:
         lib().pm7_result_free(C.byref(r))
+
+
+def closed_form_gradient(z, xyz_bohr, **options):
+    """`closed_form_gradient` (src/gradient.rs:500-561) on the device: the SCF of `run_pm7`
+    and the gradient of its total energy in eV/Bohr. Returns the fields of the reference's
+    `GradientResult`: scf (the result dict), energy_ev, gradient (N x 3), forces (= -gradient)
+    and max_gradient."""
+    m = _Mol(z, xyz_bohr)
+    keep = []
+    for k in ("initial_density", "initial_spin_density"):
+        if options.get(k) is not None:
+            a = np.ascontiguousarray(options[k], dtype=np.float64)
+            keep.append(a)
+            options[k] = a.ctypes.data_as(abi.DP)
+    o = abi.default_options(**options)
+    h = params(o.method)
+    r = abi.Result()
+    g = np.zeros((len(m.z), 3))
+    mx = C.c_double()
+    code = lib().pm7_gradient(C.byref(m.s), h, C.byref(o), C.byref(r), g.ctypes.data_as(abi.DP), C.byref(mx))
+    if code != 0:
+        raise Pm7Error(code, lib().pm7_last_error_message().decode())
+    try:
+        scf = result_to_dict(r)
+    finally:
+        lib().pm7_result_free(C.byref(r))
+    return {"scf": scf, "energy_ev": scf["total_ev"], "gradient": g, "forces": -g, "max_gradient": mx.value}
+
+
+def fixed_density_gradient(z, xyz_bohr, p_total, p_spin=None, method=0, force_dpath=False):
+    """`fixed_density_gradient_with` (src/gradient.rs:638-700), or with a spin density
+    (P_alpha - P_beta) the UHF form (:1263-1350): core-core + electronic gradient, eV/Bohr."""
+    m = _Mol(z, xyz_bohr)
+    pt = np.ascontiguousarray(p_total, dtype=np.float64)
+    ps = None if p_spin is None else np.ascontiguousarray(p_spin, dtype=np.float64)
+    g = np.zeros((len(m.z), 3))
+    _check(lib().pm7_fixed_density_gradient(C.byref(m.s), params(method), int(force_dpath), pt.ctypes.data_as(abi.DP),
+                                            None if ps is None else ps.ctypes.data_as(abi.DP),
+                                            g.ctypes.data_as(abi.DP)))
+    return g
+
+
+def correction_gradient(z, xyz_bohr, method=0, smooth=False):
+    """`correction_gradient` (src/gradient.rs:208-261): post-SCF correction gradient, eV/Bohr."""
+    m = _Mol(z, xyz_bohr)
+    g = np.zeros((len(m.z), 3))
+    _check(lib().pm7_correction_gradient(C.byref(m.s), int(method), int(smooth), g.ctypes.data_as(abi.DP)))
+    return g
 
 
 def core_hamiltonian(z, xyz_bohr, method=0, force_dpath=False):
