@@ -331,6 +331,27 @@ def run_b200(args, world, rank, local):
                                  "issued_tflops": flops / (tf_ms / tf_calls * 1e-3) / 1e12,
                                  "ms_avg": tf_ms / tf_calls, "launches": tf_calls,
                                  "peak_source": "half the measured bf16 dense rate in MEASURED_PEAKS.json (TF32 runs at half the bf16 rate)"}
+    # the nuclear gradient of the same solve through pm7_gradient (closed_form_gradient: the SCF
+    # and the gradient of its total energy), wall clock with host buffers; the device split of
+    # the gradient stages from one more, untimed call with stage events
+    grad = None
+    if not args.no_gradient:
+        api.closed_form_gradient(z, x, **opts)
+        gw, go = [], None
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            go = api.closed_form_gradient(z, x, **opts)
+            gw.append(time.perf_counter() - t)
+        api.profile_enable(True)
+        api.closed_form_gradient(z, x, **opts)
+        gp = api.profile_read()
+        api.profile_enable(False)
+        gpair, gcorr = gp.get("gradient_pairs", (0.0, 0))[0], gp.get("gradient_corrections", (0.0, 0))[0]
+        grad = {"value": args.steps / sum(gw), "unit": "SCF+gradient/s (pm7_gradient, host buffers)",
+                "gradient_device_ms": gpair + gcorr, "pairs_ms": gpair, "corrections_ms": gcorr,
+                "pair_stencil_energies": len(z) * (len(z) - 1) // 2 * 12,
+                "max_gradient_ev_bohr": go["max_gradient"],
+                "net_force_ev_bohr": float(np.max(np.abs(go["gradient"].sum(axis=0))))}
     clocks = sampler.stop()
     barrier(world)
     dev_s = allreduce_max(dev_ms * 1e-3, world)
@@ -407,6 +428,7 @@ def run_b200(args, world, rank, local):
         "pair_integrals": pair_rate,
         "autotune": api.autotune_report(),
         "mixed_precision": mixed,
+        "gradient": grad,
         "stages": stages,
         "clocks": clocks,
         "cpu_baseline": cpu,
@@ -602,6 +624,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-peak", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision solve of the default workload")
+    ap.add_argument("--no-gradient", action="store_true", help="skip the nuclear-gradient figure of the default workload")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU only: rank 0 runs, the other ranks exit without joining a process group

@@ -1032,6 +1032,18 @@ static void five_point_gradient(const Molecule &mol, double h, Energy energy, do
       grad[3 * a + k] = (8.0 * (e[0] - e[1]) - (e[2] - e[3])) / (12.0 * h);
     }
 }
+// The derivative rule for energies with hard switches (the post-SCF corrections): from the
+// energies at -2h, -h, 0, +h, +2h, the five-point formula when both third differences stay
+// below `tol` (one smooth curve), else the second-order one-sided formula of the side whose
+// second difference is the smaller -- the side without the break, i.e. the derivative of the
+// branch the geometry is on, which is what the reference's analytic gradient gives there.
+static double break_aware_derivative(double em2, double em1, double e0, double ep1, double ep2, double h, double tol) {
+  const double d0 = em1 - em2, d1 = e0 - em1, d2 = ep1 - e0, d3 = ep2 - ep1;
+  const double t1 = (d2 - d1) - (d1 - d0), t2 = (d3 - d2) - (d2 - d1);
+  if (std::fabs(t1) <= tol && std::fabs(t2) <= tol) return (8.0 * (ep1 - em1) - (ep2 - em2)) / (12.0 * h);
+  if (std::fabs(d3 - d2) <= std::fabs(d1 - d0)) return (-3.0 * e0 + 4.0 * ep1 - ep2) / (2.0 * h);
+  return (3.0 * e0 - 4.0 * em1 + em2) / (2.0 * h);
+}
 
 extern "C" {
 
@@ -1181,7 +1193,8 @@ pm7_status pm7_oracle_fixed_density_gradient(const pm7_molecule *m, int method, 
   });
 }
 
-// Post-SCF correction gradient, eV/Bohr.
+// Post-SCF correction gradient, eV/Bohr: differences of the correction energy under the
+// break-aware rule above (its EH+ H-bond term has jumps and kinks).
 pm7_status pm7_oracle_correction_gradient(const pm7_molecule *m, int method, int smooth, double step, double *grad) {
   return guarded([&] {
     pm7_options o;
@@ -1189,8 +1202,21 @@ pm7_status pm7_oracle_correction_gradient(const pm7_molecule *m, int method, int
     o.method = method;
     o.smooth_dispersion = smooth;
     double parts[5];
-    five_point_gradient(to_molecule(m), step,
-                        [&](const Molecule &x) { return correction_energy(x, o, parts) * KCAL_TO_EV; }, grad);
+    const Molecule mol = to_molecule(m);
+    const double e0 = correction_energy(mol, o, parts);
+    const double t[4] = {-2.0, -1.0, 1.0, 2.0};
+    for (int a = 0; a < mol.size(); ++a)
+      for (int k = 0; k < 3; ++k) {
+        double e[4];
+        for (int j = 0; j < 4; ++j) {
+          Molecule m2 = mol;
+          Vec3 &r = m2.pos[a];
+          (k == 0 ? r.x : (k == 1 ? r.y : r.z)) += t[j] * step;
+          e[j] = correction_energy(m2, o, parts);
+        }
+        // kcal/mol; a smooth term's third differences stay far below 1e-9 kcal/mol
+        grad[3 * a + k] = break_aware_derivative(e[0], e[1], e0, e[2], e[3], step, 1.0e-9) * KCAL_TO_EV;
+      }
   });
 }
 

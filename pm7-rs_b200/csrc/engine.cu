@@ -1137,7 +1137,7 @@ void fill_result(pm7_result *res, const Molecule &m, const Layout &L, const Para
 // in ~1 GB of device memory (and the grid's z extent), else as many as do.
 static int correction_copies(int n, int smooth) {
   const size_t per = corrections_gradient_work(n, 1, smooth) - corrections_gradient_work(n, 0, smooth);
-  return (int)std::max<size_t>(1, std::min<size_t>({(size_t)kStencil * n, (size_t)65535, ((size_t)1 << 27) / per}));
+  return (int)std::max<size_t>(1, std::min<size_t>({(size_t)kStencil * n + 1, (size_t)65535, ((size_t)1 << 27) / per}));
 }
 
 // Nuclear gradient (eV/Bohr) at the density Pt (total) / Ps (spin, null for a closed shell) of
@@ -1185,7 +1185,7 @@ static std::vector<double> device_gradient(cudaStream_t st, const DeviceParams &
     const int copies = correction_copies(n, smooth);
     DevBuf<double> work, energies, cg;
     work.alloc(corrections_gradient_work(n, copies, smooth), st);
-    energies.alloc((size_t)kStencil * n, st);
+    energies.alloc((size_t)kStencil * n + 1, st);
     cg.alloc(3 * (size_t)n, st);
     launch_corrections_gradient(st, n, D.z.p, D.xyz.p, method, smooth, copies, work.p, energies.p, cg.p);
     launch_grad_add(st, n, kKcalToEv, cg.p, G.p);
@@ -1451,7 +1451,7 @@ static void stage_correction_gradient(const pm7_molecule *mol, int method, int s
   upload(xyz, m.xyz, st);
   const int copies = correction_copies(n, smooth);
   work.alloc(corrections_gradient_work(n, copies, smooth), st);
-  energies.alloc((size_t)kStencil * n, st);
+  energies.alloc((size_t)kStencil * n + 1, st);
   cg.alloc(3 * (size_t)n, st);
   G.alloc(3 * (size_t)n, st);
   CUDA_OK(cudaMemsetAsync(G.p, 0, sizeof(double) * 3 * n, st));

@@ -41,6 +41,21 @@ __host__ __device__ inline double stencil_derivative(const double *e4, double h)
   return (8.0 * (e4[0] - e4[1]) - (e4[2] - e4[3])) / (12.0 * h);
 }
 
+// Derivative at 0 from energies at -2h, -h, 0, +h, +2h that may hold a jump or kink (the
+// post-SCF corrections' hard switches): with all four one-step differences on one smooth curve
+// (both third differences below `tol`, about h^3 times the third derivative for a smooth f)
+// the five-point formula; else the second-order one-sided formula of the side whose second
+// difference is the smaller, which holds no break and so gives the derivative of the branch
+// that 0 lies on.
+__host__ __device__ inline double robust_derivative(double em2, double em1, double e0, double ep1, double ep2, double h,
+                                                    double tol) {
+  const double d0 = em1 - em2, d1 = e0 - em1, d2 = ep1 - e0, d3 = ep2 - ep1;
+  const double t1 = (d2 - d1) - (d1 - d0), t2 = (d3 - d2) - (d2 - d1);
+  if (fabs(t1) <= tol && fabs(t2) <= tol) return (8.0 * (ep1 - em1) - (ep2 - em2)) / (12.0 * h);
+  if (fabs(d3 - d2) <= fabs(d1 - d0)) return (-3.0 * e0 + 4.0 * ep1 - ep2) / (2.0 * h);
+  return (3.0 * e0 - 4.0 * em1 + em2) / (2.0 * h);
+}
+
 // Index of the pair u < v in the row-major upper triangle of an n-atom molecule.
 __host__ __device__ inline size_t tri_index(int n, int u, int v) {
   return (size_t)u * (size_t)n - (size_t)u * (size_t)(u + 1) / 2 + (size_t)(v - u - 1);
@@ -141,7 +156,7 @@ void launch_grad_add(cudaStream_t st, int n, double scale, const double *extra, 
 // Correction-energy gradient (kcal/mol per Bohr) by five-point differences of the correction
 // energy (kernels_corr.cu): the pair terms pair by pair, the many-body terms over displaced
 // copies of the geometry (`copies` per pass, >= 1). `work` holds
-// corrections_gradient_work(n, copies, smooth) doubles, `energies` 12 n.
+// corrections_gradient_work(n, copies, smooth) doubles, `energies` 12 n + 1.
 size_t corrections_gradient_work(int n_atoms, int copies, int smooth);
 void launch_corrections_gradient(cudaStream_t st, int n_atoms, const int *z, const double *xyz, int method, int smooth,
                                  int copies, double *work, double *energies, double *grad);

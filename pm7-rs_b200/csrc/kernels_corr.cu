@@ -616,11 +616,15 @@ __global__ void k_b_finish(BatchList L, const MolDesc *__restrict__ D, MolCtl *_
 // items are re-evaluated at displaced copies of the geometry -- and only those within reach
 // of the moved atom, the others being bit-identical to the base values (covalent neighbour
 // lists, a discrete choice, are taken at the base geometry). With the smooth C6
-// (src/dispersion.rs:428-) every term is re-evaluated at every copy. The step is small
-// (1e-5 Bohr) because the EH+ H-bond energy has kinks (hard switches of hbond.rs:525-620):
-// a stencil that straddles one mixes both branches; differencing the changed items only
-// keeps the rounding error near 1e-10 kcal/mol per Bohr.
-constexpr double kCorrStep = 1.0e-5;   // Bohr
+// (src/dispersion.rs:428-) every term is re-evaluated at every copy (plus one undisplaced
+// copy for the base energy). The EH+ H-bond energy has jumps and kinks (the hard switches of
+// hbond.rs:525-620), and in a large cluster some stencil always lands on one: the derivative
+// is taken by robust_derivative (gradient.cuh), which falls back to the one-sided formula of
+// the unbroken side -- the derivative of the branch the geometry is on, as the reference's
+// analytic gradient gives it. The step is small (1e-5 Bohr) so that breaks are rarely inside
+// a stencil; differencing only the changed items keeps the rounding error near 1e-12 kcal/mol.
+constexpr double kCorrStep = 1.0e-5;  // Bohr
+constexpr double kBreakTol = 1.0e-9;  // kcal/mol: third differences of a smooth term stay below it
 constexpr double kSiohReachAng = 2.5;  // Si within 2.4 A, H within 1.4 A of the oxygen
 
 // How far (Angstrom) the H-bond energies that depend on atom A reach, or -1 for none. The
@@ -642,13 +646,14 @@ __global__ void k_hb_reach(int n, const int *__restrict__ z, const double *__res
   reach[a] = r;
 }
 
-// Copy c of a pass holds stencil point s = s0 + c: atom s / 12 moved by stencil_offset(s % 12).
+// Copy c of a pass holds stencil point s = s0 + c: atom s / 12 moved by stencil_offset(s % 12);
+// s = 12 n is the undisplaced geometry.
 __global__ void k_fd_displace(int n, const double *__restrict__ xyz, int s0, size_t stride, double *__restrict__ work) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
   if (i >= 3 * n) return;
   const int s = s0 + c;
-  double o[3];
-  stencil_offset(s % kStencil, kCorrStep, o);
+  double o[3] = {0.0, 0.0, 0.0};
+  if (s < kStencil * n) stencil_offset(s % kStencil, kCorrStep, o);
   work[(size_t)c * stride + i] = xyz[i] + (i / 3 == s / kStencil ? o[i % 3] : 0.0);
 }
 
@@ -746,8 +751,9 @@ __global__ void k_fd_finish_local(int n, const double *__restrict__ ehb0, const 
   if (threadIdx.x == 0) energies[s0 + blockIdx.x] = d;
 }
 
-// A warp per atom A: the pair terms' derivative along every pair (A, B) at fixed C6, by the
-// five-point difference in r; lanes over partners, fixed xor tree. kcal/mol per Bohr.
+// A warp per atom A: the pair terms' derivative along every pair (A, B) at fixed C6, by
+// differences in r (robust_derivative: the PM7-HH term is piecewise); lanes over partners,
+// fixed xor tree. kcal/mol per Bohr.
 __global__ void k_corr_pair_grad(int n, const int *__restrict__ z, const double *__restrict__ xyz,
                                  const double *__restrict__ c6, int hh, double *__restrict__ grad) {
   const int A = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -759,14 +765,13 @@ __global__ void k_corr_pair_grad(int n, const int *__restrict__ z, const double 
     const int u = A < B ? A : B, v = A < B ? B : A;
     const double d[3] = {xyz[3 * A] - xyz[3 * B], xyz[3 * A + 1] - xyz[3 * B + 1], xyz[3 * A + 2] - xyz[3 * B + 2]};
     const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-    double e4[4];
-    const double t[4] = {1.0, -1.0, 2.0, -2.0};
-    for (int q = 0; q < 4; ++q) {
+    double e5[5];  // r - 2h .. r + 2h
+    for (int q = 0; q < 5; ++q) {
       double ed, ey, eh;
-      pair_corr_r(z[u], z[v], c6[u], c6[v], hh, r + t[q] * kCorrStep, ed, ey, eh);
-      e4[q] = ed + 12.0 * ey + eh;
+      pair_corr_r(z[u], z[v], c6[u], c6[v], hh, r + (q - 2) * kCorrStep, ed, ey, eh);
+      e5[q] = ed + 12.0 * ey + eh;
     }
-    const double dedr = stencil_derivative(e4, kCorrStep);
+    const double dedr = robust_derivative(e5[0], e5[1], e5[2], e5[3], e5[4], kCorrStep, kBreakTol);
     for (int k = 0; k < 3; ++k) acc[k] += dedr * (d[k] / r);
   }
   for (int k = 0; k < 3; ++k) {
@@ -777,10 +782,13 @@ __global__ void k_corr_pair_grad(int n, const int *__restrict__ z, const double 
     for (int k = 0; k < 3; ++k) grad[3 * A + k] = acc[k];
 }
 
+// energies[12 a + 4 k + j]: atom a moved along axis k by +h, -h, +2h, -2h (j = 0..3); the
+// base energy is energies[12 n] (zero on the local path, which holds changes).
 __global__ void k_fd_grad(int n, const double *__restrict__ energies, int add, double *__restrict__ grad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= 3 * n) return;
-  const double g = stencil_derivative(energies + (size_t)(i / 3) * kStencil + 4 * (i % 3), kCorrStep);
+  const double *e = energies + (size_t)(i / 3) * kStencil + 4 * (i % 3);
+  const double g = robust_derivative(e[3], e[1], energies[(size_t)kStencil * n], e[0], e[2], kCorrStep, kBreakTol);
   grad[i] = add ? grad[i] + g : g;
 }
 
@@ -810,8 +818,8 @@ void launch_corrections_gradient(cudaStream_t st, int n, const int *z, const dou
   const int total = kStencil * n;
   const int ga = (n + 127) / 128;
   if (smooth) {
-    for (int s0 = 0; s0 < total; s0 += copies) {
-      const int c = copies < total - s0 ? copies : total - s0;
+    for (int s0 = 0; s0 <= total; s0 += copies) {  // s = total: the base geometry
+      const int c = copies < total + 1 - s0 ? copies : total + 1 - s0;
       k_fd_displace<<<dim3((3 * n + 127) / 128, c), 128, 0, st>>>(n, xyz, s0, stride, copy0);
       k_fd_c6<<<dim3(ga, 1, c), 128, 0, st>>>(n, z, smooth, copy0, stride);
       k_fd_pair_corr<<<dim3(ga, n, c), 128, 0, st>>>(n, z, hh, copy0, stride);
@@ -834,6 +842,7 @@ void launch_corrections_gradient(cudaStream_t st, int n, const int *z, const dou
   k_sioh<<<ga, 128, 0, st>>>(n, z, xyz, esioh0);
   k_hb_reach<<<ga, 128, 0, st>>>(n, z, xyz, nbr, nbc, reach);
   k_corr_pair_grad<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, c6, hh, grad);
+  cudaMemsetAsync(energies + total, 0, sizeof(double), st);  // the local path holds changes
   note_launch(6);
   for (int s0 = 0; s0 < total; s0 += copies) {
     const int c = copies < total - s0 ? copies : total - s0;

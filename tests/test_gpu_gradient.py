@@ -164,3 +164,36 @@ def test_gradient_errors_and_edge_cases():
     z, x, _ = small("water")
     with pytest.raises(api.Pm7Error):
         api.closed_form_gradient(z, x, multiplicity=2, reference=1)  # RHF with an open shell
+
+
+def _break_aware(e, h):
+    # the rule of the device and the oracle: five-point on a smooth stencil, else the one-sided
+    # formula of the side without the break
+    em2, em1, e0, ep1, ep2 = e
+    d = [em1 - em2, e0 - em1, ep1 - e0, ep2 - ep1]
+    t1, t2 = (d[2] - d[1]) - (d[1] - d[0]), (d[3] - d[2]) - (d[2] - d[1])
+    if abs(t1) <= 1e-9 and abs(t2) <= 1e-9:
+        return (8 * (ep1 - em1) - (ep2 - em2)) / (12 * h)
+    if abs(d[3] - d[2]) <= abs(d[1] - d[0]):
+        return (-3 * e0 + 4 * ep1 - ep2) / (2 * h)
+    return (3 * e0 - 4 * em1 + em2) / (2 * h)
+
+
+def test_correction_gradient_across_an_hbond_switch_3000_atoms():
+    # In the 1,000-water cluster (seed 0) the EH+ energy jumps by 0.17 kcal/mol when O 1131
+    # moves by +1.5e-5..2e-5 Bohr along x: inside the +2h point of the stencil. The gradient
+    # must be the derivative of the branch the geometry is on (the oracle's correction energy,
+    # evaluated at the five points, under the same rule), not the 60 eV/Bohr a plain five-point
+    # difference gives; and the whole cluster's correction forces must still sum to zero.
+    z, x = G.water_cluster(1000, seed=0)
+    g = api.correction_gradient(z, x)
+    h, a = 1.0e-5, 1131
+    e = []
+    for t in (-2, -1, 0, 1, 2):
+        y = x.copy()
+        y[a, 0] += t * h
+        e.append(float(np.sum(H.corrections(z, y))))
+    ref = _break_aware(e, h) / 23.06054783061903
+    assert abs(g[a, 0] - ref) < FIXED_TOL, (g[a, 0], ref)
+    assert abs(g[a, 0]) < 1.0
+    assert np.max(np.abs(g.sum(axis=0))) < 1.0e-6
