@@ -6,6 +6,8 @@
 // in a fixed order.
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "common.cuh"
 #include "batch.hpp"
 #include "gradient.cuh"
@@ -453,6 +455,17 @@ __device__ double eh_plus(int n, const int *z, const double *xyz, const int *nbr
 
 __device__ __forceinline__ bool is_acceptor(int z) { return z == 7 || z == 8; }
 
+// Whether acceptor k forms an H-bond term with donor di and hydrogen j (hbond.rs:263-406): an
+// N or O within 7 A of the donor, D-H...A angle above 90 degrees, and not a second donor of j
+// of lower index (that pair is taken as (k, j, di)).
+__device__ __forceinline__ bool hb_acceptor_ok(const int *z, const double *xyz, int j, int di, int k) {
+  if (k == di || !is_acceptor(z[k])) return false;
+  if (!(dist2_ang(xyz, k, di) < 7.0 * 7.0)) return false;
+  if (bangle(xyz, k, j, di) <= kPi * 0.5) return false;
+  if (k < di && dist2_ang(xyz, k, j) < 1.4 * 1.4) return false;  // already taken as (k, j, di)
+  return true;
+}
+
 // One warp per hydrogen j: every donor i (N/O within 1.4 A of j, in atom order) and
 // acceptor k (N/O within 7 A of i, D-H...A angle above 90 degrees, lanes over k), each
 // unordered {i,k} once with the lower-index donor taking the bond as in the reference's
@@ -464,7 +477,7 @@ __device__ __forceinline__ void hbonds_warp(int n, const int *__restrict__ z, co
   if (j >= n) return;
   double e = 0.0;
   if (z[j] == 1) {
-    const double rah2 = 1.4 * 1.4, cut2 = 7.0 * 7.0;
+    const double rah2 = 1.4 * 1.4;
     for (int base = 0; base < n; base += 32) {
       const int i = base + lane;
       const bool donor = i < n && is_acceptor(z[i]) && dist2_ang(xyz, i, j) < rah2;
@@ -472,13 +485,8 @@ __device__ __forceinline__ void hbonds_warp(int n, const int *__restrict__ z, co
       while (m) {
         const int di = base + __ffs(m) - 1;
         m &= m - 1;
-        for (int k = lane; k < n; k += 32) {
-          if (k == di || !is_acceptor(z[k])) continue;
-          if (!(dist2_ang(xyz, k, di) < cut2)) continue;
-          if (bangle(xyz, k, j, di) <= kPi * 0.5) continue;
-          if (k < di && dist2_ang(xyz, k, j) < rah2) continue;  // already taken as (k, j, di)
-          e += eh_plus(n, z, xyz, nbr, nbc, di, j, k);
-        }
+        for (int k = lane; k < n; k += 32)
+          if (hb_acceptor_ok(z, xyz, j, di, k)) e += eh_plus(n, z, xyz, nbr, nbc, di, j, k);
       }
     }
   }
@@ -741,14 +749,140 @@ __global__ void k_fd_sioh_local(int n, const int *__restrict__ z, const double *
   if (z[o] != 8 || dist_ang(f.xyz, o, A) > kSiohReachAng) f.so[o] = esioh0[o];
   else sioh_atom(n, z, f.xyz, f.so, o);
 }
-// The copy's change of the H-bond + Si-O-H energy (fixed order).
-__global__ void k_fd_finish_local(int n, const double *__restrict__ ehb0, const double *__restrict__ esioh0, double *work,
-                                  size_t stride, int s0, double *__restrict__ energies) {
+// ... H-bond terms by triple. The H-bond energy is a sum of eh_plus(donor i, hydrogen j,
+// acceptor k) over the triples hbonds_warp selects; moving atom A changes only the triples
+// whose evaluation reads A: i, j, k, the covalent neighbours of i and k and, for a side with a
+// single neighbour y, the atoms bonded to y (assign_refs' second shell). The triples are
+// selected once at the base geometry (a discrete choice, like the neighbour lists), each
+// copy re-evaluates only its atom's triples, and the changes are summed.
+constexpr int kHbDeps = 40;  // atoms a triple's value can depend on (3 + 4 + 4 + two shells)
+
+__global__ void k_hb_tcount(int n, const int *__restrict__ z, const double *__restrict__ xyz, int *__restrict__ cnt) {
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= n) return;
+  int c = 0;
+  if (z[j] == 1) {
+    for (int base = 0; base < n; base += 32) {
+      const int i = base + lane;
+      const bool donor = i < n && is_acceptor(z[i]) && dist2_ang(xyz, i, j) < 1.4 * 1.4;
+      unsigned m = __ballot_sync(0xffffffffu, donor);
+      while (m) {
+        const int di = base + __ffs(m) - 1;
+        m &= m - 1;
+        for (int k = lane; k < n; k += 32) c += hb_acceptor_ok(z, xyz, j, di, k) ? 1 : 0;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if (lane == 0) cnt[j] = c;
+}
+
+// The triples of hydrogen j from position off[j] on (donor order, then acceptor order), with
+// their base-geometry values.
+__global__ void k_hb_tfill(int n, const int *__restrict__ z, const double *__restrict__ xyz,
+                           const int *__restrict__ nbr, const int *__restrict__ nbc, const int *__restrict__ off,
+                           int4 *__restrict__ tri, double *__restrict__ e0) {
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= n || z[j] != 1) return;
+  int pos = off[j];
+  for (int base = 0; base < n; base += 32) {
+    const int i = base + lane;
+    const bool donor = i < n && is_acceptor(z[i]) && dist2_ang(xyz, i, j) < 1.4 * 1.4;
+    unsigned m = __ballot_sync(0xffffffffu, donor);
+    while (m) {
+      const int di = base + __ffs(m) - 1;
+      m &= m - 1;
+      for (int kb = 0; kb < n; kb += 32) {
+        const int k = kb + lane;
+        const bool sel = k < n && hb_acceptor_ok(z, xyz, j, di, k);
+        const unsigned b = __ballot_sync(0xffffffffu, sel);
+        if (sel) {
+          const int t = pos + __popc(b & ((1u << lane) - 1u));
+          tri[t] = make_int4(di, j, k, 0);
+          e0[t] = eh_plus(n, z, xyz, nbr, nbc, di, j, k);
+        }
+        pos += __popc(b);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ int add_dep(int *d, int c, int a) {
+  for (int q = 0; q < c && q < kHbDeps; ++q)
+    if (d[q] == a) return c;
+  if (c < kHbDeps) d[c] = a;
+  return c + 1;
+}
+
+// The atoms triple t's value reads (bonding test with a 0.05 A margin for the second shell).
+__global__ void k_hb_tdeps(int T, int n, const int *__restrict__ z, const double *__restrict__ xyz,
+                           const int *__restrict__ nbr, const int *__restrict__ nbc, const int4 *__restrict__ tri,
+                           int *__restrict__ deps, int *__restrict__ overflow) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  const int4 q = tri[t];
+  int d[kHbDeps];
+  int c = 0;
+  c = add_dep(d, c, q.x);
+  c = add_dep(d, c, q.y);
+  c = add_dep(d, c, q.z);
+  const int side[2] = {q.x, q.z};
+  for (int sd = 0; sd < 2; ++sd) {
+    const int x = side[sd];
+    for (int p = 0; p < nbc[x]; ++p) c = add_dep(d, c, nbr[4 * x + p]);
+    if (nbc[x] == 1) {
+      const int y = nbr[4 * x];
+      for (int a = 0; a < n; ++a)
+        if (a != y && dist_ang(xyz, a, y) < bonding(z, a, y) + 0.05) c = add_dep(d, c, a);
+    }
+  }
+  if (c > kHbDeps) atomicOr(overflow, 1);
+  for (int p = 0; p < kHbDeps; ++p) deps[(size_t)t * kHbDeps + p] = p < c && p < kHbDeps ? d[p] : -1;
+}
+
+// A warp per copy: the change of the H-bond energy, summed over the moved atom's triples.
+__global__ void k_fd_hb_triples(int n, const int *__restrict__ z, const int *__restrict__ nbr,
+                                const int *__restrict__ nbc, const int4 *__restrict__ tri,
+                                const double *__restrict__ e0, const int *__restrict__ list_off,
+                                const int *__restrict__ list, int s0, int copies, double *work, size_t stride,
+                                double *__restrict__ energies) {
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= copies) return;
+  const int s = s0 + c, A = s / kStencil;
+  const double *X = work + (size_t)c * stride;
+  double e = 0.0;
+  for (int p = list_off[A] + lane; p < list_off[A + 1]; p += 32) {
+    const int t = list[p];
+    const int4 q = tri[t];
+    e += eh_plus(n, z, X, nbr, nbc, q.x, q.y, q.z) - e0[t];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+  if (lane == 0) energies[s] = e;
+}
+
+// The copy's change of the H-bond energy from whole-hydrogen re-evaluation (k_fd_hbonds_local).
+__global__ void k_fd_finish_hb(int n, const double *__restrict__ ehb0, double *work, size_t stride, int s0,
+                               double *__restrict__ energies) {
   const FdLocal f = fd_local(n, work, stride, blockIdx.x);
   double d = 0.0;
-  for (int i = threadIdx.x; i < n; i += 256) d += (f.hb[i] - ehb0[i]) + (f.so[i] - esioh0[i]);
+  for (int i = threadIdx.x; i < n; i += 256) d += f.hb[i] - ehb0[i];
   d = block_sum<256>(d);
   if (threadIdx.x == 0) energies[s0 + blockIdx.x] = d;
+}
+
+// Adds the copy's change of the Si-O-H energy.
+__global__ void k_fd_finish_sioh(int n, const double *__restrict__ esioh0, double *work, size_t stride, int s0,
+                                 double *__restrict__ energies) {
+  const FdLocal f = fd_local(n, work, stride, blockIdx.x);
+  double d = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) d += f.so[i] - esioh0[i];
+  d = block_sum<256>(d);
+  if (threadIdx.x == 0) energies[s0 + blockIdx.x] += d;
 }
 
 // A warp per atom A: the pair terms' derivative along every pair (A, B) at fixed C6, by
@@ -844,14 +978,75 @@ void launch_corrections_gradient(cudaStream_t st, int n, const int *z, const dou
   k_corr_pair_grad<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, c6, hh, grad);
   cudaMemsetAsync(energies + total, 0, sizeof(double), st);  // the local path holds changes
   note_launch(6);
+  // the H-bond triples at the base geometry, their dependency atoms, and each atom's triples
+  std::vector<int> cnt(n), off(n + 1, 0);
+  int *d_cnt = nullptr;
+  cudaMallocAsync((void **)&d_cnt, sizeof(int) * (n + 1), st);
+  k_hb_tcount<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, d_cnt);
+  note_launch();
+  cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  for (int j = 0; j < n; ++j) off[j + 1] = off[j] + cnt[j];
+  const int T = off[n];
+  int4 *d_tri = nullptr;
+  double *d_e0 = nullptr;
+  int *d_deps = nullptr, *d_flag = nullptr, *d_list_off = nullptr, *d_list = nullptr;
+  bool by_triple = true;
+  if (T > 0) {
+    cudaMallocAsync((void **)&d_tri, sizeof(int4) * T, st);
+    cudaMallocAsync((void **)&d_e0, sizeof(double) * T, st);
+    cudaMallocAsync((void **)&d_deps, sizeof(int) * (size_t)T * kHbDeps, st);
+    cudaMallocAsync((void **)&d_flag, sizeof(int), st);
+    cudaMemsetAsync(d_flag, 0, sizeof(int), st);
+    cudaMemcpyAsync(d_cnt, off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st);
+    k_hb_tfill<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, nbr, nbc, d_cnt, d_tri, d_e0);
+    k_hb_tdeps<<<(T + 127) / 128, 128, 0, st>>>(T, n, z, xyz, nbr, nbc, d_tri, d_deps, d_flag);
+    note_launch(2);
+    std::vector<int> deps((size_t)T * kHbDeps);
+    int flag = 0;
+    cudaMemcpyAsync(deps.data(), d_deps, sizeof(int) * deps.size(), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    by_triple = flag == 0;
+    if (by_triple) {
+      std::vector<int> loff(n + 1, 0), list;
+      for (size_t q = 0; q < deps.size(); ++q)
+        if (deps[q] >= 0) ++loff[deps[q] + 1];
+      for (int a = 0; a < n; ++a) loff[a + 1] += loff[a];
+      list.resize(loff[n]);
+      std::vector<int> fill(loff.begin(), loff.end() - 1);
+      for (int t = 0; t < T; ++t)  // ascending t within every atom's list
+        for (int p = 0; p < kHbDeps; ++p) {
+          const int a = deps[(size_t)t * kHbDeps + p];
+          if (a >= 0) list[fill[a]++] = t;
+        }
+      cudaMallocAsync((void **)&d_list_off, sizeof(int) * (n + 1), st);
+      cudaMallocAsync((void **)&d_list, sizeof(int) * (list.empty() ? 1 : list.size()), st);
+      cudaMemcpyAsync(d_list_off, loff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st);
+      if (!list.empty()) cudaMemcpyAsync(d_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, st);
+      cudaStreamSynchronize(st);  // the host vectors are about to go
+    }
+  }
   for (int s0 = 0; s0 < total; s0 += copies) {
     const int c = copies < total - s0 ? copies : total - s0;
     k_fd_displace<<<dim3((3 * n + 127) / 128, c), 128, 0, st>>>(n, xyz, s0, stride, copy0);
-    k_fd_hbonds_local<<<dim3((n + 3) / 4, 1, c), 128, 0, st>>>(n, z, nbr, nbc, ehb0, reach, s0, copy0, stride);
+    if (T == 0) {
+      cudaMemsetAsync(energies + s0, 0, sizeof(double) * c, st);
+    } else if (by_triple) {
+      k_fd_hb_triples<<<(c + 3) / 4, 128, 0, st>>>(n, z, nbr, nbc, d_tri, d_e0, d_list_off, d_list, s0, c, copy0, stride,
+                                                   energies);
+    } else {  // a triple reads more atoms than kept: re-evaluate every hydrogen within reach
+      k_fd_hbonds_local<<<dim3((n + 3) / 4, 1, c), 128, 0, st>>>(n, z, nbr, nbc, ehb0, reach, s0, copy0, stride);
+      k_fd_finish_hb<<<c, 256, 0, st>>>(n, ehb0, copy0, stride, s0, energies);
+      note_launch();
+    }
     k_fd_sioh_local<<<dim3(ga, 1, c), 128, 0, st>>>(n, z, esioh0, s0, copy0, stride);
-    k_fd_finish_local<<<c, 256, 0, st>>>(n, ehb0, esioh0, copy0, stride, s0, energies);
-    note_launch(4);
+    k_fd_finish_sioh<<<c, 256, 0, st>>>(n, esioh0, copy0, stride, s0, energies);
+    note_launch(T > 0 && by_triple ? 4 : 3);
   }
+  for (void *p : {(void *)d_cnt, (void *)d_tri, (void *)d_e0, (void *)d_deps, (void *)d_flag, (void *)d_list_off,
+                  (void *)d_list})
+    if (p) cudaFreeAsync(p, st);
   k_fd_grad<<<(3 * n + 127) / 128, 128, 0, st>>>(n, energies, 1, grad);
   note_launch();
 }
