@@ -1145,7 +1145,7 @@ static int correction_copies(int n, int smooth) {
 // 1082-1247) and, with `corrections`, the post-SCF correction gradient (:208-261).
 static std::vector<double> device_gradient(cudaStream_t st, const DeviceParams &P, const DeviceMolecule &D, bool dpath,
                                            const double *Pt, const double *Ps, int method, int smooth,
-                                           bool corrections) {
+                                           bool corrections, bool any_si) {
   const int n = D.n;
   std::vector<double> grad(3 * (size_t)n, 0.0);
   if (n == 0) return grad;
@@ -1187,7 +1187,7 @@ static std::vector<double> device_gradient(cudaStream_t st, const DeviceParams &
     work.alloc(corrections_gradient_work(n, copies, smooth), st);
     energies.alloc((size_t)kStencil * n + 1, st);
     cg.alloc(3 * (size_t)n, st);
-    launch_corrections_gradient(st, n, D.z.p, D.xyz.p, method, smooth, copies, work.p, energies.p, cg.p);
+    launch_corrections_gradient(st, n, D.z.p, D.xyz.p, method, smooth, any_si, copies, work.p, energies.p, cg.p);
     launch_grad_add(st, n, kKcalToEv, cg.p, G.p);
   }
   int bad = 0;
@@ -1347,7 +1347,8 @@ static void run_impl(const pm7_molecule *mol, const pm7_params *params, const pm
   ht.mark("readback");
   if (gradient && S.converged)
     *gradient = device_gradient(st, P, D, o.force_dpath || L.has_d, S.P.p, S.unrestricted ? S.Pspin.p : nullptr,
-                                o.method, o.smooth_dispersion, true);
+                                o.method, o.smooth_dispersion, true,
+                                std::find(m.z.begin(), m.z.end(), 14) != m.z.end());
   fill_result(res, m, L, ps, o, R, diag_blocks, [&](int a, int i, int j) {
     return o.want_matrices ? Ph[(size_t)(L.aoff[a] + i) * nao + L.aoff[a] + j] : blocks[(size_t)81 * a + 9 * i + j];
   });
@@ -1432,7 +1433,7 @@ static void stage_gradient(const pm7_molecule *mol, const pm7_params *params, in
   DevBuf<double> Pt, Ps;
   upload(Pt, std::vector<double>(p_total, p_total + nn), st);
   if (p_spin) upload(Ps, std::vector<double>(p_spin, p_spin + nn), st);
-  const std::vector<double> g = device_gradient(st, P, D, dpath, Pt.p, p_spin ? Ps.p : nullptr, method, 0, false);
+  const std::vector<double> g = device_gradient(st, P, D, dpath, Pt.p, p_spin ? Ps.p : nullptr, method, 0, false, false);
   std::memcpy(grad_out, g.data(), sizeof(double) * g.size());
 }
 
@@ -1455,7 +1456,8 @@ static void stage_correction_gradient(const pm7_molecule *mol, int method, int s
   cg.alloc(3 * (size_t)n, st);
   G.alloc(3 * (size_t)n, st);
   CUDA_OK(cudaMemsetAsync(G.p, 0, sizeof(double) * 3 * n, st));
-  launch_corrections_gradient(st, n, z.p, xyz.p, method, smooth, copies, work.p, energies.p, cg.p);
+  launch_corrections_gradient(st, n, z.p, xyz.p, method, smooth, std::find(m.z.begin(), m.z.end(), 14) != m.z.end(),
+                              copies, work.p, energies.p, cg.p);
   launch_grad_add(st, n, kKcalToEv, cg.p, G.p);
   CUDA_OK(cudaMemcpyAsync(grad_out, G.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaStreamSynchronize(st));

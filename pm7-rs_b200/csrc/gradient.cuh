@@ -158,7 +158,8 @@ void launch_grad_add(cudaStream_t st, int n, double scale, const double *extra, 
 // copies of the geometry (`copies` per pass, >= 1). `work` holds
 // corrections_gradient_work(n, copies, smooth) doubles, `energies` 12 n + 1.
 size_t corrections_gradient_work(int n_atoms, int copies, int smooth);
+// `any_si`: whether the molecule holds silicon (without it the Si-O-H term is zero).
 void launch_corrections_gradient(cudaStream_t st, int n_atoms, const int *z, const double *xyz, int method, int smooth,
-                                 int copies, double *work, double *energies, double *grad);
+                                 int any_si, int copies, double *work, double *energies, double *grad);
 
 }  // namespace pm7

@@ -560,9 +560,62 @@ __global__ void k_pair_corr(int n, const int *__restrict__ z, const double *__re
 __global__ void k_sioh(int n, const int *__restrict__ z, const double *__restrict__ xyz, double *__restrict__ e_out) {
   sioh_atom(n, z, xyz, e_out, blockIdx.x * blockDim.x + threadIdx.x);
 }
-__global__ void k_hb_neighbours(int n, const int *__restrict__ z, const double *__restrict__ xyz,
-                                int *__restrict__ nbr, int *__restrict__ nbc) {
-  hb_neighbours_atom(n, z, xyz, nbr, nbc, blockIdx.x * blockDim.x + threadIdx.x);
+// A warp per atom i: the discrete covalent-neighbour count (an integer, so the lanes' order
+// does not matter) and the C6 it selects -- c6_atom's discrete branch.
+__global__ void k_c6_discrete_warp(int n, const int *__restrict__ z, const double *__restrict__ xyz,
+                                   double *__restrict__ c6) {
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  int cnt = 0;
+  const double ri = covalent(z[i]);
+  for (int j = lane; j < n; j += 32) {
+    if (j == i) continue;
+    const double dx = xyz[3 * j] - xyz[3 * i], dy = xyz[3 * j + 1] - xyz[3 * i + 1], dz = xyz[3 * j + 2] - xyz[3 * i + 2];
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    const double rc = 1.3 * (ri + covalent(z[j]));
+    if (r * kA0 < rc) ++cnt;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if (lane == 0) c6[i] = z[i] != 6 ? c6_of(z[i]) : (cnt == 4 ? 0.95 : 1.65);
+}
+
+// A warp per atom a: hb_neighbours_atom's ascending scan (a fifth neighbour evicts the longest),
+// candidates found 32 at a time and taken in ascending order by every lane alike.
+__global__ void k_hb_neighbours_warp(int n, const int *__restrict__ z, const double *__restrict__ xyz,
+                                     int *__restrict__ nbr, int *__restrict__ nbc) {
+  const int a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (a >= n) return;
+  int list[5];
+  int cnt = 0;
+  for (int base = 0; base < n; base += 32) {
+    const int j = base + lane;
+    const bool cand = j < n && j != a && dist_ang(xyz, j, a) < bonding(z, j, a);
+    unsigned m = __ballot_sync(0xffffffffu, cand);
+    while (m) {
+      list[cnt++] = base + __ffs(m) - 1;
+      m &= m - 1;
+      if (cnt == 5) {
+        int worst = 0;
+        double wd = -1.0;
+        for (int q = 0; q < 5; ++q) {
+          const double dd = dist_ang(xyz, a, list[q]);
+          if (dd > wd) {
+            wd = dd;
+            worst = q;
+          }
+        }
+        for (int q = worst; q < 4; ++q) list[q] = list[q + 1];
+        cnt = 4;
+      }
+    }
+  }
+  if (lane == 0) {
+    for (int q = 0; q < 4; ++q) nbr[4 * a + q] = q < cnt ? list[q] : -1;
+    nbc[a] = cnt;
+  }
 }
 __global__ void k_hbonds(int n, const int *__restrict__ z, const double *__restrict__ xyz, const int *__restrict__ nbr,
                          const int *__restrict__ nbc, double *__restrict__ e_out) {
@@ -940,7 +993,7 @@ size_t corrections_gradient_work(int n_atoms, int copies, int smooth) {
 }
 
 void launch_corrections_gradient(cudaStream_t st, int n, const int *z, const double *xyz, int method, int smooth,
-                                 int copies, double *work, double *energies, double *grad) {
+                                 int any_si, int copies, double *work, double *energies, double *grad) {
   if (n <= 0) return;
   if (method == 3) {  // PM7-minus carries no post-SCF corrections
     cudaMemsetAsync(grad, 0, 3 * sizeof(double) * (size_t)n, st);
@@ -970,14 +1023,12 @@ void launch_corrections_gradient(cudaStream_t st, int n, const int *z, const dou
   // base quantities of the local path
   double *c6 = base, *ehb0 = c6 + n, *esioh0 = ehb0 + n, *reach = esioh0 + n;
   int *nbr = reinterpret_cast<int *>(reach + n), *nbc = nbr + 4 * n;
-  k_c6<<<ga, 128, 0, st>>>(n, z, xyz, 0, c6);
-  k_hb_neighbours<<<ga, 128, 0, st>>>(n, z, xyz, nbr, nbc);
-  k_hbonds<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, nbr, nbc, ehb0);
-  k_sioh<<<ga, 128, 0, st>>>(n, z, xyz, esioh0);
-  k_hb_reach<<<ga, 128, 0, st>>>(n, z, xyz, nbr, nbc, reach);
+  k_c6_discrete_warp<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, c6);
+  k_hb_neighbours_warp<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, nbr, nbc);
+  if (any_si) k_sioh<<<ga, 128, 0, st>>>(n, z, xyz, esioh0);  // without Si the term is zero
   k_corr_pair_grad<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, c6, hh, grad);
   cudaMemsetAsync(energies + total, 0, sizeof(double), st);  // the local path holds changes
-  note_launch(6);
+  note_launch(any_si ? 4 : 3);
   // the H-bond triples at the base geometry, their dependency atoms, and each atom's triples
   std::vector<int> cnt(n), off(n + 1, 0);
   int *d_cnt = nullptr;
@@ -1008,7 +1059,11 @@ void launch_corrections_gradient(cudaStream_t st, int n, const int *z, const dou
     cudaMemcpyAsync(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
     by_triple = flag == 0;
-    if (by_triple) {
+    if (!by_triple) {  // the fallback's inputs: base H-bond energy per hydrogen, each atom's reach
+      k_hbonds<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, nbr, nbc, ehb0);
+      k_hb_reach<<<ga, 128, 0, st>>>(n, z, xyz, nbr, nbc, reach);
+      note_launch(2);
+    } else {
       std::vector<int> loff(n + 1, 0), list;
       for (size_t q = 0; q < deps.size(); ++q)
         if (deps[q] >= 0) ++loff[deps[q] + 1];
@@ -1040,9 +1095,12 @@ void launch_corrections_gradient(cudaStream_t st, int n, const int *z, const dou
       k_fd_finish_hb<<<c, 256, 0, st>>>(n, ehb0, copy0, stride, s0, energies);
       note_launch();
     }
-    k_fd_sioh_local<<<dim3(ga, 1, c), 128, 0, st>>>(n, z, esioh0, s0, copy0, stride);
-    k_fd_finish_sioh<<<c, 256, 0, st>>>(n, esioh0, copy0, stride, s0, energies);
-    note_launch(T > 0 && by_triple ? 4 : 3);
+    if (any_si) {
+      k_fd_sioh_local<<<dim3(ga, 1, c), 128, 0, st>>>(n, z, esioh0, s0, copy0, stride);
+      k_fd_finish_sioh<<<c, 256, 0, st>>>(n, esioh0, copy0, stride, s0, energies);
+      note_launch(2);
+    }
+    note_launch(T > 0 && by_triple ? 2 : 1);
   }
   for (void *p : {(void *)d_cnt, (void *)d_tri, (void *)d_e0, (void *)d_deps, (void *)d_flag, (void *)d_list_off,
                   (void *)d_list})
@@ -1085,11 +1143,12 @@ void launch_corrections(cudaStream_t st, int n, const int *z, const double *xyz,
   double *pd = scratch, *py = pd + parts, *ph = py + parts, *c6 = ph + parts, *ehb = c6 + n, *esioh = ehb + n;
   int *nbr = reinterpret_cast<int *>(esioh + n);
   int *nbc = nbr + 4 * n;
-  k_c6<<<(n + 127) / 128, 128, 0, st>>>(n, z, xyz, smooth, c6);
+  if (smooth) k_c6<<<(n + 127) / 128, 128, 0, st>>>(n, z, xyz, smooth, c6);
+  else k_c6_discrete_warp<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, c6);
   note_launch();
   k_pair_corr<<<dim3(gx, n), 128, 0, st>>>(n, z, xyz, c6, method == 4, pd, py, ph);
   note_launch();
-  k_hb_neighbours<<<(n + 127) / 128, 128, 0, st>>>(n, z, xyz, nbr, nbc);
+  k_hb_neighbours_warp<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, nbr, nbc);
   note_launch();
   k_hbonds<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, nbr, nbc, ehb);
   note_launch();
