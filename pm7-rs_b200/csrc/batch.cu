@@ -1019,6 +1019,8 @@ static size_t mol_layout(BatchMol &b, char *base) {
   d.g.csr_start = csr_start;
   d.g.csr = csr;
   d.g.w = d.w;
+  d.g.gfar = nullptr;  // the batched Fock kernels evaluate EV / r themselves
+  d.g.csr_eoff = nullptr;
   d.n_occ = b.n_occ;
   d.dframe = b.dframe;
   d.cc_nx = gx;

@@ -249,14 +249,20 @@ Layout build_layout(const Molecule &m, const ParamSet &ps) {
   }
   L.csr.reserve(L.csr_start[m.n]);
   for (int a = 0; a < m.n; ++a) L.csr.insert(L.csr.end(), lists[a].begin(), lists[a].end());
+  L.csr_eoff.resize(L.csr.size());
+  for (int a = 0; a < m.n; ++a)
+    for (int c = L.csr_start[a]; c < L.csr_start[a + 1]; ++c) {
+      const NearPair &q = L.near[L.csr[c].y];
+      L.csr_eoff[c] = q.u == a ? q.eoff_u : q.eoff_v;
+    }
   return L;
 }
 
 struct DeviceMolecule {
   cudaStream_t st;
   int n = 0, nao = 0, n_near = 0;
-  DevBuf<int> z, aoff, ao_atom, csr_start;
-  DevBuf<double> xyz, H, w, ecore, jbuf, pop, cc_partial, scal;
+  DevBuf<int> z, aoff, ao_atom, csr_start, csr_eoff;
+  DevBuf<double> xyz, H, w, ecore, jbuf, pop, cc_partial, scal, gfar;
   DevBuf<NearPair> near;
   DevBuf<int2> csr;
   DevBuf<unsigned char> mask;
@@ -276,7 +282,9 @@ struct DeviceMolecule {
     g.np = near.p;
     g.csr_start = csr_start.p;
     g.csr = csr.p;
+    g.csr_eoff = csr_eoff.p;
     g.w = w.p;
+    g.gfar = gfar.p;
     return g;
   }
 };
@@ -303,9 +311,12 @@ static void build_device_molecule(DeviceMolecule &D, const Molecule &m, const La
   upload(D.csr_start, L.csr_start, st);
   upload(D.near, L.near, st);
   upload(D.csr, L.csr, st);
+  upload(D.csr_eoff, L.csr_eoff, st);
   D.mask.alloc((size_t)m.n * m.n, st);
   CUDA_OK(cudaMemsetAsync(D.mask.p, 0, (size_t)m.n * m.n, st));
   if (D.n_near) k_fill_mask<<<(D.n_near + 255) / 256, 256, 0, st>>>(D.n_near, m.n, D.near.p, D.mask.p);
+  D.gfar.alloc((size_t)m.n * m.n, st);
+  launch_far_coulomb(st, m.n, D.xyz.p, D.mask.p, D.gfar.p);
   const size_t nao2 = (size_t)L.nao * L.nao;
   D.H.alloc(nao2, st);
   CUDA_OK(cudaMemsetAsync(D.H.p, 0, sizeof(double) * nao2, st));

@@ -196,6 +196,7 @@ struct Layout {
   std::vector<NearPair> near;
   std::vector<int> csr_start;
   std::vector<int2> csr;
+  std::vector<int> csr_eoff;  // per csr entry: the packed Coulomb partials of the row's atom in that pair
   int64_t w_len = 0;
   int32_t e_len = 0;
   bool has_d = false;

@@ -54,8 +54,15 @@ struct FockGeometry {
   const NearPair *np;
   const int *csr_start;
   const int2 *csr;  // (partner atom, near-pair index), sorted by partner
+  const int *csr_eoff;  // per csr entry: offset of the row atom's packed partials in jbuf (or null)
   const double *w;
+  // n_atoms^2: EV / r of every pair beyond the feather range (0 for an atom with itself and
+  // for near pairs), precomputed once per molecule; null to evaluate it in the Fock kernels
+  const double *gfar;
 };
+// EV / r of the far pairs into gfar (n x n), the same expression the Fock kernels evaluate.
+void launch_far_coulomb(cudaStream_t st, int n_atoms, const double *xyz, const unsigned char *near_mask,
+                        double *gfar);
 // F = H + J(Pt) - K(s * Ps). `pop` (n_atoms) and `jbuf` (packed, like ecore) are scratch.
 void launch_fock(cudaStream_t st, const FockGeometry &g, const DeviceParams &P, const double *H, const double *Pt,
                  const double *Ps, double s_scale, double *F, double *pop, double *jbuf);

@@ -47,9 +47,14 @@ __device__ __forceinline__ void fock_far_elem(const FockGeometry &g, const doubl
                                               int i, int j) {
   const int A = g.ao_atom[i], B = g.ao_atom[j];
   if (A == B || g.near_mask[(size_t)A * g.n_atoms + B]) return;
-  const double dx = g.xyz[3 * B] - g.xyz[3 * A], dy = g.xyz[3 * B + 1] - g.xyz[3 * A + 1],
-               dz = g.xyz[3 * B + 2] - g.xyz[3 * A + 2];
-  const double v = (1.0 / sqrt(dx * dx + dy * dy + dz * dz)) * kEv;
+  double v;
+  if (g.gfar) {
+    v = g.gfar[(size_t)A * g.n_atoms + B];
+  } else {
+    const double dx = g.xyz[3 * B] - g.xyz[3 * A], dy = g.xyz[3 * B + 1] - g.xyz[3 * A + 1],
+                 dz = g.xyz[3 * B + 2] - g.xyz[3 * A + 2];
+    v = (1.0 / sqrt(dx * dx + dy * dy + dz * dz)) * kEv;
+  }
   const size_t ij = (size_t)i * g.nao + j;
   F[ij] = H[ij] - s_scale * Ps[ij] * v;
 }
@@ -167,13 +172,27 @@ __device__ __forceinline__ void fock_atom_group(const FockGeometry &g, const Dev
   double part[V];
 #pragma unroll
   for (int k = 0; k < V; ++k) part[k] = 0.0;
-  for (int B0 = 0; B0 < g.n_atoms; B0 += 32) {
+  if (g.gfar) {
+    // gfar is exactly 0 for A itself and its near partners and populations are >= 0, so those
+    // terms add +0.0 and change no partial: no branch, independent loads
+    const double *grow = g.gfar + (size_t)A * g.n_atoms;
+#pragma unroll 2
+    for (int B0 = 0; B0 < g.n_atoms; B0 += 32) {
 #pragma unroll
-    for (int k = 0; k < V; ++k) {
-      const int B = B0 + lane + G * k;  // partial v = lane + G k
-      if (B >= g.n_atoms || B == A || mask[B]) continue;
-      const double dx = g.xyz[3 * B] - xa, dy = g.xyz[3 * B + 1] - ya, dz = g.xyz[3 * B + 2] - za;
-      part[k] += ((1.0 / sqrt(dx * dx + dy * dy + dz * dz)) * kEv) * pop[B];
+      for (int k = 0; k < V; ++k) {
+        const int B = B0 + lane + G * k;  // partial v = lane + G k
+        if (B < g.n_atoms) part[k] += grow[B] * pop[B];
+      }
+    }
+  } else {
+    for (int B0 = 0; B0 < g.n_atoms; B0 += 32) {
+#pragma unroll
+      for (int k = 0; k < V; ++k) {
+        const int B = B0 + lane + G * k;  // partial v = lane + G k
+        if (B >= g.n_atoms || B == A || mask[B]) continue;
+        const double dx = g.xyz[3 * B] - xa, dy = g.xyz[3 * B + 1] - ya, dz = g.xyz[3 * B + 2] - za;
+        part[k] += ((1.0 / sqrt(dx * dx + dy * dy + dz * dz)) * kEv) * pop[B];
+      }
     }
   }
   // xor tree over the 32 partials: levels o >= G pair partials of one lane, o < G cross lanes
@@ -191,9 +210,13 @@ __device__ __forceinline__ void fock_atom_group(const FockGeometry &g, const Dev
   const int c0 = g.csr_start[A], c1 = g.csr_start[A + 1];
   for (int k = lane; k < npk; k += G) {
     double acc = 0.0;
-    for (int c = c0; c < c1; ++c) {
-      const NearPair q = g.np[g.csr[c].y];
-      acc += jbuf[(q.u == A ? q.eoff_u : q.eoff_v) + k];
+    if (g.csr_eoff) {  // one independent load per partner
+      for (int c = c0; c < c1; ++c) acc += jbuf[g.csr_eoff[c] + k];
+    } else {
+      for (int c = c0; c < c1; ++c) {
+        const NearPair q = g.np[g.csr[c].y];
+        acc += jbuf[(q.u == A ? q.eoff_u : q.eoff_v) + k];
+      }
     }
     jacc[k] = acc;
   }
@@ -340,6 +363,25 @@ void launch_b_fock(cudaStream_t st, const BatchList &Lmol, const BatchList &Lrow
       }
       note_launch();
     });
+}
+
+// Thread per (A, B): EV / r_AB for far pairs, 0 for A == B and near pairs. Grid (ceil(N/128), N).
+__global__ void k_far_coulomb(int n, const double *__restrict__ xyz, const unsigned char *__restrict__ near_mask,
+                              double *__restrict__ gfar) {
+  const int A = blockIdx.y, B = blockIdx.x * blockDim.x + threadIdx.x;
+  if (B >= n) return;
+  double v = 0.0;
+  if (A != B && !near_mask[(size_t)A * n + B]) {
+    const double dx = xyz[3 * B] - xyz[3 * A], dy = xyz[3 * B + 1] - xyz[3 * A + 1], dz = xyz[3 * B + 2] - xyz[3 * A + 2];
+    v = (1.0 / sqrt(dx * dx + dy * dy + dz * dz)) * kEv;
+  }
+  gfar[(size_t)A * n + B] = v;
+}
+
+void launch_far_coulomb(cudaStream_t st, int n, const double *xyz, const unsigned char *near_mask, double *gfar) {
+  if (n <= 0) return;
+  k_far_coulomb<<<dim3((n + 127) / 128, n), 128, 0, st>>>(n, xyz, near_mask, gfar);
+  note_launch();
 }
 
 void launch_atom_blocks(cudaStream_t st, int n_atoms, const int *aoff, const int *z, const DeviceParams &P, int nao,
