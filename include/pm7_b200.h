@@ -184,6 +184,15 @@ pm7_status pm7_gradient(const pm7_molecule *molecule, const pm7_params *params,
                         const pm7_options *options, pm7_result *result, double *gradient,
                         double *max_gradient);
 
+/* pm7_run_batch (below) with each molecule's nuclear gradient, as pm7_gradient returns it:
+ * gradients[i] points to 3 * molecules[i].n_atoms doubles, filled when statuses[i] is PM7_OK.
+ * No counterpart in pm7-rs, whose optimiser and MD loops call closed_form_gradient one
+ * molecule at a time (src/optimizer.rs:318). Batched molecules get their gradient at the
+ * density the batch converged to; the others go through pm7_gradient. */
+pm7_status pm7_run_batch_gradient(int32_t n_molecules, const pm7_molecule *molecules,
+                                  const pm7_params *params, const pm7_options *options,
+                                  pm7_result *results, pm7_status *statuses, double *const *gradients);
+
 /* Replaces `fixed_density_gradient_with` (src/gradient.rs:638-700) and, with a spin
  * density, `fixed_density_gradient_uhf_with` (:1263-1350): core-core plus electronic
  * gradient at a given density, no corrections. `p_total` (nao^2, row-major) is the total

@@ -30,6 +30,7 @@
 
 #include "batch.hpp"
 #include "common.cuh"
+#include "gradient.cuh"
 #include "engine_internal.hpp"
 
 namespace pm7 {
@@ -936,6 +937,9 @@ struct BatchMol {
   std::string error;
   pm7_result result{};
   double t_admit = 0.0;
+  double *grad_out = nullptr;  // caller's 3 n_atoms doubles: the nuclear gradient at retirement
+  pm7_status grad_status = PM7_OK;
+  std::string grad_error;
 };
 
 static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -1842,6 +1846,33 @@ class BatchRunner {
       }
       CUDA_OK(cudaStreamSynchronize(st_));
     }
+    // nuclear gradients of the converged molecules that asked for one, at their final density,
+    // before their device memory goes (closed_form_gradient, src/gradient.rs:500-561)
+    for (int m = 0; m < n; ++m) {
+      BatchMol &b = *R[m];
+      const double *o = host + off[m];
+      if (!b.grad_out || o[2] == 0.0) continue;
+      GradGeometry g{};
+      g.n_atoms = b.d.g.n_atoms;
+      g.nao = b.d.g.nao;
+      g.n_near = b.d.g.n_near;
+      g.z = b.d.g.z;
+      g.aoff = b.d.g.aoff;
+      g.xyz = b.d.g.xyz;
+      g.near_mask = b.d.g.near_mask;
+      g.np = b.d.g.np;
+      g.Pt = ((int)o[0] % 2 == 0) ? b.d.P : b.d.Pn;  // P and P' swap every iteration
+      g.Ps = nullptr;
+      try {
+        const std::vector<double> gr =
+            geometry_gradient(st_, *P_, g, b.dframe, method_, b.o.smooth_dispersion, true,
+                              std::find(b.m.z.begin(), b.m.z.end(), 14) != b.m.z.end());
+        std::memcpy(b.grad_out, gr.data(), sizeof(double) * gr.size());
+      } catch (const Failure &f) {
+        b.grad_status = f.code;
+        b.grad_error = f.msg;
+      }
+    }
     parallel_for(n, [&](int m) {
       BatchMol &b = *R[m];
       const double *o = host + off[m];
@@ -1871,7 +1902,8 @@ class BatchRunner {
             for (int k = 0; k < nao; ++k) Cm[(size_t)i * nao + k] = V[m][(size_t)k * nao + i];
           b.result.mo_coeff = host_vec(Cm);
         }
-        b.status = PM7_OK;
+        b.status = b.grad_status;
+        b.error = b.grad_error;
       } catch (const Failure &f) {
         b.status = f.code;
         b.error = f.msg;
@@ -1949,7 +1981,7 @@ static size_t batch_budget(int64_t mb) {
 // Runs a closed batch: molecules are admitted as memory allows and iterated together;
 // open-shell requests take the single-molecule path.
 static void run_batch_impl(int n, const pm7_molecule *mols, const pm7_params *params, const pm7_options *opts,
-                           pm7_result *results, pm7_status *status) {
+                           pm7_result *results, pm7_status *status, double *const *gradients = nullptr) {
   if (n < 0 || (n > 0 && (!mols || !opts || !results || !status || !params)))
     throw Failure{PM7_ERR_INVALID_INPUT, "null argument"};
   if (n == 0) return;
@@ -1975,10 +2007,12 @@ static void run_batch_impl(int n, const pm7_molecule *mols, const pm7_params *pa
     status[i] = prep[i];
     if (!items[i]) continue;
     if (!BatchRunner::batchable(*items[i])) {
-      status[i] = pm7_run(&mols[i], params, &opts[i], &results[i]);
+      status[i] = gradients ? pm7_gradient(&mols[i], params, &opts[i], &results[i], gradients[i], nullptr)
+                            : pm7_run(&mols[i], params, &opts[i], &results[i]);
       items[i].reset();
       continue;
     }
+    if (gradients) items[i]->grad_out = gradients[i];
     pending.push_back(items[i].get());
   }
   const auto t_prep = std::chrono::steady_clock::now();
@@ -2109,6 +2143,25 @@ pm7_status pm7_run_batch(int32_t n_molecules, const pm7_molecule *molecules, con
                          const pm7_options *options, pm7_result *results, pm7_status *statuses) {
   try {
     run_batch_impl(n_molecules, molecules, params, options, results, statuses);
+    g_last_error.clear();
+    return PM7_OK;
+  } catch (const Failure &f) {
+    g_last_error = f.msg;
+    return f.code;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return PM7_ERR_INVALID_INPUT;
+  }
+}
+
+pm7_status pm7_run_batch_gradient(int32_t n_molecules, const pm7_molecule *molecules, const pm7_params *params,
+                                  const pm7_options *options, pm7_result *results, pm7_status *statuses,
+                                  double *const *gradients) {
+  try {
+    if (n_molecules > 0 && !gradients) throw Failure{PM7_ERR_INVALID_INPUT, "null gradient array"};
+    for (int i = 0; i < n_molecules; ++i)
+      if (!gradients[i]) throw Failure{PM7_ERR_INVALID_INPUT, "null gradient buffer for molecule " + std::to_string(i)};
+    run_batch_impl(n_molecules, molecules, params, options, results, statuses, gradients);
     g_last_error.clear();
     return PM7_OK;
   } catch (const Failure &f) {

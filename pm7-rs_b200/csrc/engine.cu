@@ -1151,13 +1151,14 @@ static int correction_copies(int n, int smooth) {
   return (int)std::max<size_t>(1, std::min<size_t>({(size_t)kStencil * n + 1, (size_t)65535, ((size_t)1 << 27) / per}));
 }
 
-// Nuclear gradient (eV/Bohr) at the density Pt (total) / Ps (spin, null for a closed shell) of
-// the built device molecule D: core-core + electronic pair terms (src/gradient.rs:654-700,
-// 1082-1247) and, with `corrections`, the post-SCF correction gradient (:208-261).
-static std::vector<double> device_gradient(cudaStream_t st, const DeviceParams &P, const DeviceMolecule &D, bool dpath,
-                                           const double *Pt, const double *Ps, int method, int smooth,
-                                           bool corrections, bool any_si) {
-  const int n = D.n;
+// Nuclear gradient (eV/Bohr) of a molecule on the device at the density g.Pt (total) / g.Ps
+// (spin, null for a closed shell): core-core + electronic pair terms (src/gradient.rs:654-700,
+// 1082-1247) and, with `corrections`, the post-SCF correction gradient (:208-261). g's atoms,
+// AO offsets, coordinates, near mask and near pairs are the molecule's; g.E and g.status are set
+// here.
+std::vector<double> geometry_gradient(cudaStream_t st, const DeviceParams &P, GradGeometry g, bool dpath, int method,
+                                      int smooth, bool corrections, bool any_si) {
+  const int n = g.n_atoms;
   std::vector<double> grad(3 * (size_t)n, 0.0);
   if (n == 0) return grad;
   const size_t npairs = (size_t)n * (size_t)(n - 1) / 2;
@@ -1167,17 +1168,6 @@ static std::vector<double> device_gradient(cudaStream_t st, const DeviceParams &
   G.alloc(3 * (size_t)n, st);
   status.alloc(1, st);
   CUDA_OK(cudaMemsetAsync(status.p, 0, sizeof(int), st));
-  GradGeometry g;
-  g.n_atoms = n;
-  g.nao = D.nao;
-  g.n_near = D.n_near;
-  g.z = D.z.p;
-  g.aoff = D.aoff.p;
-  g.xyz = D.xyz.p;
-  g.near_mask = D.mask.p;
-  g.np = D.near.p;
-  g.Pt = Pt;
-  g.Ps = Ps;
   g.E = E.p;
   g.status = status.p;
   {
@@ -1198,7 +1188,7 @@ static std::vector<double> device_gradient(cudaStream_t st, const DeviceParams &
     work.alloc(corrections_gradient_work(n, copies, smooth), st);
     energies.alloc((size_t)kStencil * n + 1, st);
     cg.alloc(3 * (size_t)n, st);
-    launch_corrections_gradient(st, n, D.z.p, D.xyz.p, method, smooth, any_si, copies, work.p, energies.p, cg.p);
+    launch_corrections_gradient(st, n, g.z, g.xyz, method, smooth, any_si, copies, work.p, energies.p, cg.p);
     launch_grad_add(st, n, kKcalToEv, cg.p, G.p);
   }
   int bad = 0;
@@ -1209,6 +1199,24 @@ static std::vector<double> device_gradient(cudaStream_t st, const DeviceParams &
   if (bad & 1) throw Failure{PM7_ERR_UNSUPPORTED, "gradient: a shell pair without an overlap formula"};
   if (bad & 2) throw Failure{PM7_ERR_INVALID_INPUT, "gradient: d-shell pair in the sp frame"};
   return grad;
+}
+
+// The same for the built single-molecule device state D.
+static std::vector<double> device_gradient(cudaStream_t st, const DeviceParams &P, const DeviceMolecule &D, bool dpath,
+                                           const double *Pt, const double *Ps, int method, int smooth,
+                                           bool corrections, bool any_si) {
+  GradGeometry g{};
+  g.n_atoms = D.n;
+  g.nao = D.nao;
+  g.n_near = D.n_near;
+  g.z = D.z.p;
+  g.aoff = D.aoff.p;
+  g.xyz = D.xyz.p;
+  g.near_mask = D.mask.p;
+  g.np = D.near.p;
+  g.Pt = Pt;
+  g.Ps = Ps;
+  return geometry_gradient(st, P, g, dpath, method, smooth, corrections, any_si);
 }
 
 // Host-side phase times of one pm7_run on stderr (PM7_HOST_TRACE set): where the wall time

@@ -249,4 +249,10 @@ inline void upload(DevBuf<T> &b, const std::vector<T> &v, cudaStream_t st) {
 }
 
 // Core Hamiltonian and stored pair integrals on the device (hamiltonian.rs:310-638).
+
+// Nuclear gradient (eV/Bohr, 3 per atom) of a molecule on the device at the density g.Pt / g.Ps
+// (engine.cu); g.E and g.status are provided by the call.
+struct GradGeometry;
+std::vector<double> geometry_gradient(cudaStream_t st, const DeviceParams &P, GradGeometry g, bool dpath, int method,
+                                      int smooth, bool corrections, bool any_si);
 }  // namespace pm7

@@ -24,7 +24,7 @@ EXPORTED = [
     "pm7_stage_corrections", "pm7_run_batch", "pm7_engine_config_default", "pm7_engine_create", "pm7_engine_submit",
     "pm7_engine_poll", "pm7_engine_destroy", "pm7_batch_partition", "pm7_stage_eigenvalues",
     "pm7_stage_product_tf32", "pm7_autotune_report", "pm7_gradient", "pm7_fixed_density_gradient",
-    "pm7_correction_gradient",
+    "pm7_correction_gradient", "pm7_run_batch_gradient",
 ]
 
 
@@ -69,6 +69,8 @@ def lib():
                                abi.DP, abi.DP]
     L.pm7_fixed_density_gradient.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, C.c_int32, abi.DP, abi.DP, abi.DP]
     L.pm7_correction_gradient.argtypes = [C.POINTER(abi.Molecule), C.c_int32, C.c_int32, abi.DP]
+    L.pm7_run_batch_gradient.argtypes = [C.c_int32, C.POINTER(abi.Molecule), C.c_void_p, C.POINTER(abi.Options),
+                                         C.POINTER(abi.Result), C.POINTER(C.c_int32), C.POINTER(abi.DP)]
     L.pm7_stage_eigenvalues.argtypes = [C.c_int32, C.POINTER(C.c_int32), abi.DP, abi.DP, C.c_int32]
     L.pm7_engine_config_default.argtypes = [C.POINTER(abi.EngineConfig)]
     L.pm7_engine_create.argtypes = [C.POINTER(abi.EngineConfig), C.POINTER(C.c_void_p)]
@@ -326,6 +328,43 @@ def run_batch(molecules, options=None, **common):
     for i in range(n):
         if st[i] == 0:
             out.append(result_to_dict(res[i]))
+        else:
+            out.append(Pm7Error(st[i], "batched solve failed"))
+        lib().pm7_result_free(C.byref(res[i]))
+    return out
+
+
+def run_batch_gradient(molecules, options=None, **common):
+    """`run_batch` with every molecule's nuclear gradient (`pm7_run_batch_gradient`).
+
+    Returns one entry per molecule: the dict of `closed_form_gradient` (scf, energy_ev,
+    gradient (N x 3, eV/Bohr), forces, max_gradient), or the `Pm7Error` for it.
+    """
+    n = len(molecules)
+    mols = [_Mol(z, x) for z, x in molecules]
+    keep = []
+    opts = (abi.Options * max(n, 1))()
+    for i in range(n):
+        o = dict(common)
+        if options is not None:
+            o.update(options[i])
+        opts[i] = _options_with_arrays(o, keep)
+    ms = (abi.Molecule * max(n, 1))(*[m.s for m in mols])
+    res = (abi.Result * max(n, 1))()
+    st = (C.c_int32 * max(n, 1))()
+    grads = [np.zeros((len(m.z), 3)) for m in mols]
+    gp = (abi.DP * max(n, 1))(*[g.ctypes.data_as(abi.DP) for g in grads])
+    h = params(opts[0].method if n else 0)
+    code = lib().pm7_run_batch_gradient(n, ms, h, opts, res, st, gp)
+    if code != 0:
+        raise Pm7Error(code, lib().pm7_last_error_message().decode())
+    out = []
+    for i in range(n):
+        if st[i] == 0:
+            scf = result_to_dict(res[i])
+            g = grads[i]
+            out.append({"scf": scf, "energy_ev": scf["total_ev"], "gradient": g, "forces": -g,
+                        "max_gradient": float(np.max(np.abs(g))) if g.size else 0.0})
         else:
             out.append(Pm7Error(st[i], "batched solve failed"))
         lib().pm7_result_free(C.byref(res[i]))

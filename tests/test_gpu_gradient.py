@@ -197,3 +197,20 @@ def test_correction_gradient_across_an_hbond_switch_3000_atoms():
     assert abs(g[a, 0] - ref) < FIXED_TOL, (g[a, 0], ref)
     assert abs(g[a, 0]) < 1.0
     assert np.max(np.abs(g.sum(axis=0))) < 1.0e-6
+
+
+def test_batched_gradients_match_single():
+    # pm7_run_batch_gradient: closed-shell molecules through the batch engine (gradient at the
+    # density the batch converged to), the UHF radical through pm7_gradient; each must match
+    # the single-molecule gradient to the SCF's convergence
+    mols = [G.alkane(3, seed=1), G.water_cluster(6, seed=2), chain_with_s_cl(6, seed=8)]
+    z, x, _ = small("methyl")
+    mols.append((z, x))
+    opts = [{}, {}, {}, {"multiplicity": 2}]
+    out = api.run_batch_gradient(mols, options=opts)
+    for (zz, xx), o, r in zip(mols, opts, out):
+        assert not isinstance(r, Exception), r
+        single = api.closed_form_gradient(zz, xx, **o)
+        assert abs(r["scf"]["heat_of_formation_kcal"] - single["scf"]["heat_of_formation_kcal"]) < 1.0e-5
+        assert np.max(np.abs(r["gradient"] - single["gradient"])) < SCF_TOL, np.max(np.abs(r["gradient"] - single["gradient"]))
+        assert np.array_equal(r["forces"], -r["gradient"])
