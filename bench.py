@@ -495,6 +495,14 @@ def run_batch_bench(args, world, rank, local):
     api.run_batch(mols, **opts)
     prof = api.profile_read()
     api.profile_enable(False)
+    # the same batch with every molecule's nuclear gradient (pm7_run_batch_gradient), one pass
+    grad = None
+    if not args.no_gradient:
+        t = time.perf_counter()
+        gres = api.run_batch_gradient(mols, **opts)
+        gw = allreduce_max(time.perf_counter() - t, world)
+        grad = {"value": len(every) / gw, "unit": "SCF+gradient/s (pm7_run_batch_gradient, host buffers)",
+                "wall_s": gw, "failed_rank0": sum(1 for r in gres if isinstance(r, Exception))}
     if rank != 0:
         return
     failed = sum(1 for r in res if isinstance(r, Exception))
@@ -527,6 +535,7 @@ def run_batch_bench(args, world, rank, local):
         "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu, "autotune": api.autotune_report(),
         "stages": {k: {"ms_total": round(v[0], 3), "calls": v[1]} for k, v in prof.items()},
         "stages_note": "one extra untimed batch with stage events",
+        "gradient": grad,
     }
     print(json.dumps(line), flush=True)
 
