@@ -214,3 +214,28 @@ def test_batched_gradients_match_single():
         assert abs(r["scf"]["heat_of_formation_kcal"] - single["scf"]["heat_of_formation_kcal"]) < 1.0e-5
         assert np.max(np.abs(r["gradient"] - single["gradient"])) < SCF_TOL, np.max(np.abs(r["gradient"] - single["gradient"]))
         assert np.array_equal(r["forces"], -r["gradient"])
+
+
+TM_CASES = ["ferrocene", "titanocene_dichloride", "chromyl_chloride", "permanganate", "tetrachloroplatinate",
+            "copper_chloride", "nickel_tetracarbonyl"]
+
+
+@pytest.mark.parametrize("name", TM_CASES)
+def test_fixed_density_gradient_transition_metals(golden, name):
+    # d-shell metals (PM7 d balance, 45x45 one-centre blocks) in the MNDO/d frame, at the
+    # oracle's converged density for the reference's golden geometries
+    case = golden[name]
+    z, x = H.parse_lines(case["atoms"])
+    r = H.run(z, x, charge=float(case["charge"]), multiplicity=case["multiplicity"], want_matrices=1)
+    ps = r["spin_density"] if r["unrestricted"] else None
+    ref = H.fixed_density_gradient(z, x, r["density"], ps)
+    got = api.fixed_density_gradient(z, x, r["density"], ps)
+    assert np.max(np.abs(got - ref)) < FIXED_TOL, (name, np.max(np.abs(got - ref)))
+
+
+def test_closed_form_gradient_ferrocene(golden):
+    case = golden["ferrocene"]
+    z, x = H.parse_lines(case["atoms"])
+    out = api.closed_form_gradient(z, x, charge=float(case["charge"]))
+    _, ref = H.gradient(z, x, charge=float(case["charge"]))
+    assert np.max(np.abs(out["gradient"] - ref)) < SCF_TOL
