@@ -1185,6 +1185,14 @@ class BatchRunner {
 
   size_t bytes_in_use() const { return bytes_in_use_; }
   long long sp2_fallbacks() const { return sp2_fallbacks_; }
+  // Host wall time of each phase of iterate() so far (seconds), for PM7_BATCH_TRACE.
+  static constexpr int kPhases = 7;
+  static const char *phase_name(int k) {
+    static const char *names[kPhases] = {"queue", "mixed_sync", "sp2", "eigensolve", "converge", "retire_end",
+                                         "retire"};
+    return names[k];
+  }
+  double phase_seconds(int k) const { return phase_s_[k]; }
   int active_count() const { return (int)active_.size(); }
 
   // Allocate, upload and build the integrals of the given molecules (one launch per
@@ -1277,6 +1285,12 @@ class BatchRunner {
   std::vector<BatchMol *> iterate() {
     std::vector<BatchMol *> finished;
     CUDA_OK(cudaSetDevice(ctx_.device));
+    auto t_last = std::chrono::steady_clock::now();
+    auto mark = [&](int k) {
+      const auto now = std::chrono::steady_clock::now();
+      phase_s_[k] += std::chrono::duration<double>(now - t_last).count();
+      t_last = now;
+    };
     if (active_.empty()) return retiring_.empty() ? finished : retire_end();
     Lists A = lists(active_, false);
     const int n = A.mol.n;
@@ -1305,11 +1319,13 @@ class BatchRunner {
     // which molecules take an fp32 cycle (decided on the device from their DIIS error)
     bool any_mixed = false;
     for (const BatchMol *b : active_) any_mixed = any_mixed || b->mixed;
+    mark(0);
     if (any_mixed) {
       CUDA_OK(cudaMemcpyAsync(flags_h_ + 2 * (size_t)cap_, flags_d_ + 2 * (size_t)cap_, n, cudaMemcpyDeviceToHost,
                               st_));
       CUDA_OK(cudaStreamSynchronize(st_));
     }
+    mark(1);
     // density: SP2 purification on the tensor cores for the larger molecules (fp32 cycles
     // on tcgen05, fp64 cycles on DMMA), the batched eigensolver for the small ones (where
     // it is as fast) and for what SP2 leaves
@@ -1404,6 +1420,7 @@ class BatchRunner {
         if (bad) throw Failure{PM7_ERR_CUDA, "tcgen05 squaring: a pipeline wait expired"};
       }
     }
+    mark(2);
     if (!fallback.empty()) {
       Stage s_(st_, "batch_eigensolve");
       Lists B = lists(fallback, true, &up_fallback_);
@@ -1412,6 +1429,7 @@ class BatchRunner {
       eigensolve(B);
       launch_b_gemm(st_, B.glow, desc_, ctl_, B.eig, 1);
     }
+    mark(3);
     {
       Stage s_(st_, "batch_converge");
       k_b_sqdiff_c<<<A.chunks.total, RB, 0, st_>>>(A.chunks, desc_);
@@ -1425,8 +1443,10 @@ class BatchRunner {
     for (int m = 0; m < n; ++m) (flags_h_[m] ? finished : keep).push_back(active_[m]);
     active_.swap(keep);
     // the previous iteration's retirement (its eigensolves ran alongside this step)
+    mark(4);
     std::vector<BatchMol *> done;
     if (!retiring_.empty()) done = retire_end();
+    mark(5);
     if (!finished.empty()) {
       bool vectors = false;
       for (const BatchMol *b : finished) vectors = vectors || b->o.want_matrices;
@@ -1437,6 +1457,7 @@ class BatchRunner {
         retire_begin(finished);
       }
     }
+    mark(6);
     return done;
   }
 
@@ -1968,6 +1989,7 @@ class BatchRunner {
   unsigned char *flags_h_ = nullptr, *flags_d_ = nullptr;
   int sp2_min_nao_ = 96;  // SP2 from this many basis functions up
   long long sp2_fallbacks_ = 0;
+  double phase_s_[kPhases] = {0};
 };
 
 // HBM budget for a batch: the caller's max_memory_mb when given, else 80% of free memory.
@@ -2036,10 +2058,15 @@ static void run_batch_impl(int n, const pm7_molecule *mols, const pm7_params *pa
     t_iter += std::chrono::duration<double>(a2 - a1).count();
     ++n_iter;
   }
-  if (std::getenv("PM7_BATCH_TRACE"))
+  if (std::getenv("PM7_BATCH_TRACE")) {
     std::fprintf(stderr, "batch: %d molecules, prepare %.3f s, admit %.3f s, %d iterations %.3f s, sp2 fallbacks %lld\n",
                  n, std::chrono::duration<double>(t_prep - t_start).count(), t_admit, n_iter, t_iter,
                  runner.sp2_fallbacks());
+    std::fprintf(stderr, "batch iterations (host wall, s):");
+    for (int k = 0; k < BatchRunner::kPhases; ++k)
+      std::fprintf(stderr, " %s %.3f", BatchRunner::phase_name(k), runner.phase_seconds(k));
+    std::fprintf(stderr, "\n");
+  }
   for (int i = 0; i < n; ++i)
     if (items[i]) {
       results[i] = items[i]->result;
