@@ -707,8 +707,29 @@ __device__ int lz_count(const double *a, const double *b, int m, double x) {
   }
   return c;
 }
+// One warp: 32-point multisection on the Sturm count (lanes evaluate 32 interior points, a
+// ballot keeps the sub-interval holding the wanted eigenvalue; 12 rounds shrink the Gershgorin
+// interval of T by 33^12, to the rounding floor).
+__device__ double lz_extreme(const double *a, const double *b, int m, double lo, double hi, int target, int lane) {
+  for (int it = 0; it < 12; ++it) {
+    const double x = lo + (hi - lo) * (double)(lane + 1) / 33.0;
+    const unsigned hit = __ballot_sync(0xffffffffu, lz_count(a, b, m, x) >= target);
+    const double xl = __shfl_sync(0xffffffffu, x, hit ? __ffs(hit) - 1 : 31);
+    if (hit) {
+      const int f = __ffs(hit) - 1;
+      const double xp = __shfl_sync(0xffffffffu, x, f > 0 ? f - 1 : 0);
+      hi = xl;
+      if (f > 0) lo = xp;
+    } else {
+      lo = xl;
+    }
+  }
+  return hi;
+}
+
 __global__ void k_lz_bounds(int n, const double *__restrict__ lz, double *__restrict__ bounds) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (blockIdx.x != 0) return;
+  const int lane = threadIdx.x & 31;
   const double *a = lz + 4 * (size_t)n, *b = a + kLzSteps;
   const int m = kLzSteps;
   double g_lo = 1.0e300, g_hi = -1.0e300;
@@ -717,21 +738,9 @@ __global__ void k_lz_bounds(int n, const double *__restrict__ lz, double *__rest
     g_lo = fmin(g_lo, a[i] - r);
     g_hi = fmax(g_hi, a[i] + r);
   }
-  double lo = g_lo, hi = g_hi, tmin, tmax;
-  for (int it = 0; it < 100; ++it) {  // smallest: count(x) >= 1
-    const double mid = 0.5 * (lo + hi);
-    if (lz_count(a, b, m, mid) >= 1) hi = mid;
-    else lo = mid;
-  }
-  tmin = hi;
-  lo = g_lo;
-  hi = g_hi;
-  for (int it = 0; it < 100; ++it) {  // largest: count(x) >= m
-    const double mid = 0.5 * (lo + hi);
-    if (lz_count(a, b, m, mid) >= m) hi = mid;
-    else lo = mid;
-  }
-  tmax = hi;
+  const double tmin = lz_extreme(a, b, m, g_lo, g_hi, 1, lane);  // smallest: count(x) >= 1
+  const double tmax = lz_extreme(a, b, m, g_lo, g_hi, m, lane);  // largest: count(x) >= m
+  if (lane != 0) return;
   const double R = tmax - tmin;
   if (!(R > 0.0) || !isfinite(R)) return;  // keep the Gershgorin interval
   double elo = fmax(tmin - 0.02 * R, bounds[0]), ehi = fmin(tmax + 0.04 * R, bounds[1]);
