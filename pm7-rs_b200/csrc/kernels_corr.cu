@@ -10,6 +10,7 @@
 
 #include "common.cuh"
 #include "batch.hpp"
+#include "engine_internal.hpp"
 #include "gradient.cuh"
 #include "kernels.hpp"
 
@@ -988,6 +989,25 @@ size_t corr_copy_stride(int n, int smooth) {
 
 }  // namespace
 
+// Temporary device buffers of one call, freed on the stream however the call ends.
+struct StreamTemps {
+  cudaStream_t st;
+  std::vector<void *> ptrs;
+  explicit StreamTemps(cudaStream_t s) : st(s) {}
+  StreamTemps(const StreamTemps &) = delete;
+  StreamTemps &operator=(const StreamTemps &) = delete;
+  template <class T>
+  T *alloc(size_t count) {
+    void *p = nullptr;
+    CUDA_OK(cudaMallocAsync(&p, sizeof(T) * (count > 0 ? count : 1), st));
+    ptrs.push_back(p);
+    return static_cast<T *>(p);
+  }
+  ~StreamTemps() {
+    for (void *p : ptrs) cudaFreeAsync(p, st);
+  }
+};
+
 size_t corrections_gradient_work(int n_atoms, int copies, int smooth) {
   return corr_base_doubles(n_atoms) + (size_t)copies * corr_copy_stride(n_atoms, smooth);
 }
@@ -996,7 +1016,7 @@ void launch_corrections_gradient(cudaStream_t st, int n, const int *z, const dou
                                  int any_si, int copies, double *work, double *energies, double *grad) {
   if (n <= 0) return;
   if (method == 3) {  // PM7-minus carries no post-SCF corrections
-    cudaMemsetAsync(grad, 0, 3 * sizeof(double) * (size_t)n, st);
+    CUDA_OK(cudaMemsetAsync(grad, 0, 3 * sizeof(double) * (size_t)n, st));
     return;
   }
   const int hh = method == 4;
@@ -1027,16 +1047,16 @@ void launch_corrections_gradient(cudaStream_t st, int n, const int *z, const dou
   k_hb_neighbours_warp<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, nbr, nbc);
   if (any_si) k_sioh<<<ga, 128, 0, st>>>(n, z, xyz, esioh0);  // without Si the term is zero
   k_corr_pair_grad<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, c6, hh, grad);
-  cudaMemsetAsync(energies + total, 0, sizeof(double), st);  // the local path holds changes
+  CUDA_OK(cudaMemsetAsync(energies + total, 0, sizeof(double), st));  // the local path holds changes
   note_launch(any_si ? 4 : 3);
   // the H-bond triples at the base geometry, their dependency atoms, and each atom's triples
   std::vector<int> cnt(n), off(n + 1, 0);
-  int *d_cnt = nullptr;
-  cudaMallocAsync((void **)&d_cnt, sizeof(int) * (n + 1), st);
+  StreamTemps tmp(st);
+  int *d_cnt = tmp.alloc<int>(n + 1);
   k_hb_tcount<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, d_cnt);
   note_launch();
-  cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
-  cudaStreamSynchronize(st);
+  CUDA_OK(cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
   for (int j = 0; j < n; ++j) off[j + 1] = off[j] + cnt[j];
   const int T = off[n];
   int4 *d_tri = nullptr;
@@ -1044,20 +1064,20 @@ void launch_corrections_gradient(cudaStream_t st, int n, const int *z, const dou
   int *d_deps = nullptr, *d_flag = nullptr, *d_list_off = nullptr, *d_list = nullptr;
   bool by_triple = true;
   if (T > 0) {
-    cudaMallocAsync((void **)&d_tri, sizeof(int4) * T, st);
-    cudaMallocAsync((void **)&d_e0, sizeof(double) * T, st);
-    cudaMallocAsync((void **)&d_deps, sizeof(int) * (size_t)T * kHbDeps, st);
-    cudaMallocAsync((void **)&d_flag, sizeof(int), st);
-    cudaMemsetAsync(d_flag, 0, sizeof(int), st);
-    cudaMemcpyAsync(d_cnt, off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st);
+    d_tri = tmp.alloc<int4>(T);
+    d_e0 = tmp.alloc<double>(T);
+    d_deps = tmp.alloc<int>((size_t)T * kHbDeps);
+    d_flag = tmp.alloc<int>(1);
+    CUDA_OK(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
+    CUDA_OK(cudaMemcpyAsync(d_cnt, off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
     k_hb_tfill<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, nbr, nbc, d_cnt, d_tri, d_e0);
     k_hb_tdeps<<<(T + 127) / 128, 128, 0, st>>>(T, n, z, xyz, nbr, nbc, d_tri, d_deps, d_flag);
     note_launch(2);
     std::vector<int> deps((size_t)T * kHbDeps);
     int flag = 0;
-    cudaMemcpyAsync(deps.data(), d_deps, sizeof(int) * deps.size(), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
+    CUDA_OK(cudaMemcpyAsync(deps.data(), d_deps, sizeof(int) * deps.size(), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
     by_triple = flag == 0;
     if (!by_triple) {  // the fallback's inputs: base H-bond energy per hydrogen, each atom's reach
       k_hbonds<<<(n + 3) / 4, 128, 0, st>>>(n, z, xyz, nbr, nbc, ehb0);
@@ -1075,18 +1095,19 @@ void launch_corrections_gradient(cudaStream_t st, int n, const int *z, const dou
           const int a = deps[(size_t)t * kHbDeps + p];
           if (a >= 0) list[fill[a]++] = t;
         }
-      cudaMallocAsync((void **)&d_list_off, sizeof(int) * (n + 1), st);
-      cudaMallocAsync((void **)&d_list, sizeof(int) * (list.empty() ? 1 : list.size()), st);
-      cudaMemcpyAsync(d_list_off, loff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st);
-      if (!list.empty()) cudaMemcpyAsync(d_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, st);
-      cudaStreamSynchronize(st);  // the host vectors are about to go
+      d_list_off = tmp.alloc<int>(n + 1);
+      d_list = tmp.alloc<int>(list.size());
+      CUDA_OK(cudaMemcpyAsync(d_list_off, loff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
+      if (!list.empty())
+        CUDA_OK(cudaMemcpyAsync(d_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, st));
+      CUDA_OK(cudaStreamSynchronize(st));  // the host vectors are about to go
     }
   }
   for (int s0 = 0; s0 < total; s0 += copies) {
     const int c = copies < total - s0 ? copies : total - s0;
     k_fd_displace<<<dim3((3 * n + 127) / 128, c), 128, 0, st>>>(n, xyz, s0, stride, copy0);
     if (T == 0) {
-      cudaMemsetAsync(energies + s0, 0, sizeof(double) * c, st);
+      CUDA_OK(cudaMemsetAsync(energies + s0, 0, sizeof(double) * c, st));
     } else if (by_triple) {
       k_fd_hb_triples<<<(c + 3) / 4, 128, 0, st>>>(n, z, nbr, nbc, d_tri, d_e0, d_list_off, d_list, s0, c, copy0, stride,
                                                    energies);
@@ -1102,9 +1123,7 @@ void launch_corrections_gradient(cudaStream_t st, int n, const int *z, const dou
     }
     note_launch(T > 0 && by_triple ? 2 : 1);
   }
-  for (void *p : {(void *)d_cnt, (void *)d_tri, (void *)d_e0, (void *)d_deps, (void *)d_flag, (void *)d_list_off,
-                  (void *)d_list})
-    if (p) cudaFreeAsync(p, st);
+  CUDA_OK(cudaGetLastError());
   k_fd_grad<<<(3 * n + 127) / 128, 128, 0, st>>>(n, energies, 1, grad);
   note_launch();
 }
