@@ -1036,13 +1036,21 @@ static void five_point_gradient(const Molecule &mol, double h, Energy energy, do
 // energies at -2h, -h, 0, +h, +2h, the five-point formula when both third differences stay
 // below `tol` (one smooth curve), else the second-order one-sided formula of the side whose
 // second difference is the smaller -- the side without the break, i.e. the derivative of the
-// branch the geometry is on, which is what the reference's analytic gradient gives there.
+// branch the geometry is on, which is what the reference's analytic gradient gives there. A
+// break at the geometry itself (both outer second differences below 1% of the middle one, as
+// at a symmetric tie) has no branch of its own: the right-hand one is taken; breaks on both
+// sides leave the central difference on +-h. A side counts as the cleaner one only when its
+// second difference is under half the other's, so rounding does not tip the choice.
 static double break_aware_derivative(double em2, double em1, double e0, double ep1, double ep2, double h, double tol) {
   const double d0 = em1 - em2, d1 = e0 - em1, d2 = ep1 - e0, d3 = ep2 - ep1;
   const double t1 = (d2 - d1) - (d1 - d0), t2 = (d3 - d2) - (d2 - d1);
   if (std::fabs(t1) <= tol && std::fabs(t2) <= tol) return (8.0 * (ep1 - em1) - (ep2 - em2)) / (12.0 * h);
-  if (std::fabs(d3 - d2) <= std::fabs(d1 - d0)) return (-3.0 * e0 + 4.0 * ep1 - ep2) / (2.0 * h);
-  return (3.0 * e0 - 4.0 * em1 + em2) / (2.0 * h);
+  const double sl = std::fabs(d1 - d0), sr = std::fabs(d3 - d2), sm = std::fabs(d2 - d1);
+  const double left = (3.0 * e0 - 4.0 * em1 + em2) / (2.0 * h), right = (-3.0 * e0 + 4.0 * ep1 - ep2) / (2.0 * h);
+  if (std::max(sl, sr) < 0.01 * sm) return right;  // the break is at the geometry
+  if (sl < 0.5 * sr) return left;
+  if (sr < 0.5 * sl) return right;
+  return (ep1 - em1) / (2.0 * h);
 }
 
 extern "C" {

@@ -44,16 +44,23 @@ __host__ __device__ inline double stencil_derivative(const double *e4, double h)
 // Derivative at 0 from energies at -2h, -h, 0, +h, +2h that may hold a jump or kink (the
 // post-SCF corrections' hard switches): with all four one-step differences on one smooth curve
 // (both third differences below `tol`, about h^3 times the third derivative for a smooth f)
-// the five-point formula; else the second-order one-sided formula of the side whose second
-// difference is the smaller, which holds no break and so gives the derivative of the branch
-// that 0 lies on.
+// the five-point formula; else a second-order formula on points free of the break: the
+// one-sided formula of a side whose second difference is under half the other's (the side the
+// break is not on, giving the derivative of the branch 0 lies on); for a break at 0 itself
+// (both outer second differences below 1% of the middle one: a switch the geometry sits on,
+// as at a symmetric tie) the right-hand branch; otherwise (breaks on both sides) the central
+// difference on +-h. The factor-2 margins keep rounding from tipping a choice.
 __host__ __device__ inline double robust_derivative(double em2, double em1, double e0, double ep1, double ep2, double h,
                                                     double tol) {
   const double d0 = em1 - em2, d1 = e0 - em1, d2 = ep1 - e0, d3 = ep2 - ep1;
   const double t1 = (d2 - d1) - (d1 - d0), t2 = (d3 - d2) - (d2 - d1);
   if (fabs(t1) <= tol && fabs(t2) <= tol) return (8.0 * (ep1 - em1) - (ep2 - em2)) / (12.0 * h);
-  if (fabs(d3 - d2) <= fabs(d1 - d0)) return (-3.0 * e0 + 4.0 * ep1 - ep2) / (2.0 * h);
-  return (3.0 * e0 - 4.0 * em1 + em2) / (2.0 * h);
+  const double sl = fabs(d1 - d0), sr = fabs(d3 - d2), sm = fabs(d2 - d1);
+  const double left = (3.0 * e0 - 4.0 * em1 + em2) / (2.0 * h), right = (-3.0 * e0 + 4.0 * ep1 - ep2) / (2.0 * h);
+  if (fmax(sl, sr) < 0.01 * sm) return right;  // the break is at 0
+  if (sl < 0.5 * sr) return left;
+  if (sr < 0.5 * sl) return right;
+  return (ep1 - em1) / (2.0 * h);
 }
 
 // Index of the pair u < v in the row-major upper triangle of an n-atom molecule.

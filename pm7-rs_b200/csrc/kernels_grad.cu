@@ -58,13 +58,20 @@ __global__ void k_grad_near_sp(GradGeometry g, DeviceParams P) {
   const int oa = g.aoff[q.a], ob = g.aoff[q.b];
   const double r = q.r, inv = 1.0 / r;
   const bool ha = ea.n_orb >= 4, hb = eb.n_orb >= 4;
+  // a sparkle (no orbitals; b, the lighter side, when there is one) holds no density: only its
+  // core's attraction on a's electrons (e1b) remains, and its density block is never read
+  const bool a_orb = ea.n_orb > 0, b_orb = eb.n_orb > 0;
   double E = 0.0;
   if (!ha && !hb) {
     const double aee = (ea.rho0 + eb.rho0) * (ea.rho0 + eb.rho0);
     double cf, pt;
     d_feather(r, cf, pt);
     const double ee = (1.0 / sqrt(r * r + aee)) * kEv * cf + pt * (1.0 - cf);
-    E = ee * (two_e_coef(g, oa, ob, 0, 0, 0, 0) - eb.core * ecore_coef(g, oa, 0, 0) - ea.core * ecore_coef(g, ob, 0, 0));
+    double c = 0.0;
+    if (a_orb && b_orb) c += two_e_coef(g, oa, ob, 0, 0, 0, 0);
+    if (a_orb) c -= eb.core * ecore_coef(g, oa, 0, 0);
+    if (b_orb) c -= ea.core * ecore_coef(g, ob, 0, 0);
+    E = ee * c;
   } else {
     double rot[3][3];
     d_rotation_to_x(-(q.d[0] * inv), -(q.d[1] * inv), -(q.d[2] * inv), rot);
@@ -79,8 +86,8 @@ __global__ void k_grad_near_sp(GradGeometry g, DeviceParams P) {
           else
             val = ri[2] * (rot[0][mu - 1] * rot[0][nu - 1]) +
                   ri[3] * (rot[1][mu - 1] * rot[1][nu - 1] + rot[2][mu - 1] * rot[2][nu - 1]);
-          double c = two_e_coef(g, oa, ob, mu, nu, 0, 0) - eb.core * ecore_coef(g, oa, mu, nu);
-          if (mu == 0) c -= ea.core * ecore_coef(g, ob, 0, 0);
+          double c = (b_orb ? two_e_coef(g, oa, ob, mu, nu, 0, 0) : 0.0) - eb.core * ecore_coef(g, oa, mu, nu);
+          if (mu == 0 && b_orb) c -= ea.core * ecore_coef(g, ob, 0, 0);
           E += c * val;
         }
     } else {

@@ -174,9 +174,15 @@ def _break_aware(e, h):
     t1, t2 = (d[2] - d[1]) - (d[1] - d[0]), (d[3] - d[2]) - (d[2] - d[1])
     if abs(t1) <= 1e-9 and abs(t2) <= 1e-9:
         return (8 * (ep1 - em1) - (ep2 - em2)) / (12 * h)
-    if abs(d[3] - d[2]) <= abs(d[1] - d[0]):
-        return (-3 * e0 + 4 * ep1 - ep2) / (2 * h)
-    return (3 * e0 - 4 * em1 + em2) / (2 * h)
+    sl, sr, sm = abs(d[1] - d[0]), abs(d[3] - d[2]), abs(d[2] - d[1])
+    left, right = (3 * e0 - 4 * em1 + em2) / (2 * h), (-3 * e0 + 4 * ep1 - ep2) / (2 * h)
+    if max(sl, sr) < 0.01 * sm:  # the break is at the point
+        return right
+    if sl < 0.5 * sr:
+        return left
+    if sr < 0.5 * sl:
+        return right
+    return (ep1 - em1) / (2 * h)
 
 
 def test_correction_gradient_across_an_hbond_switch_3000_atoms():
