@@ -1162,6 +1162,16 @@ std::vector<double> geometry_gradient(cudaStream_t st, const DeviceParams &P, Gr
   std::vector<double> grad(3 * (size_t)n, 0.0);
   if (n == 0) return grad;
   const size_t npairs = (size_t)n * (size_t)(n - 1) / 2;
+  {
+    // the stencil energies (12 per atom pair) are the gradient's one large buffer
+    size_t free_b = 0, total_b = 0;
+    CUDA_OK(cudaMemGetInfo(&free_b, &total_b));
+    const size_t need = npairs * kStencil * sizeof(double);
+    if (need > free_b)
+      throw Failure{PM7_ERR_INSUFFICIENT_MEMORY, "gradient needs " + std::to_string(need >> 20) +
+                                                     " MB of stencil energies, " + std::to_string(free_b >> 20) +
+                                                     " MB free on the device"};
+  }
   DevBuf<double> E, G;
   DevBuf<int> status;
   E.alloc(npairs * kStencil, st);
