@@ -360,6 +360,13 @@ pm7_status pm7_engine_create(const pm7_engine_config *config, pm7_engine **out);
 /* Queues one request; *ticket identifies it. Invalid input is reported by poll. */
 pm7_status pm7_engine_submit(pm7_engine *engine, const pm7_molecule *molecule, const pm7_options *options,
                              uint64_t *ticket);
+/* pm7_engine_submit with the request's nuclear gradient (eV/Bohr, as pm7_gradient returns
+ * it): the engine writes 3 * n_atoms doubles to `gradient` before the request is done, so the
+ * buffer must stay valid until pm7_engine_poll reports done. No counterpart in pm7-rs; its
+ * force callers (src/optimizer.rs:318) call closed_form_gradient per molecule. */
+pm7_status pm7_engine_submit_gradient(pm7_engine *engine, const pm7_molecule *molecule,
+                                      const pm7_options *options, double *gradient, uint64_t *ticket);
+
 /* *done = 1 when the request finished; the return value is then its pm7_run status,
  * *result is filled (caller frees) and *latency_ms is submit-to-finish time. With
  * wait != 0 the call blocks until the request finishes. A finished ticket is

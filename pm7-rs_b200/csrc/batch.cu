@@ -2273,8 +2273,8 @@ pm7_status pm7_engine_create(const pm7_engine_config *config, pm7_engine **out) 
   }
 }
 
-pm7_status pm7_engine_submit(pm7_engine *E, const pm7_molecule *molecule, const pm7_options *options,
-                             uint64_t *ticket) {
+static pm7_status engine_submit(pm7_engine *E, const pm7_molecule *molecule, const pm7_options *options,
+                                double *gradient, uint64_t *ticket) {
   if (!E || !molecule || !options || !ticket) return PM7_ERR_INVALID_INPUT;
   try {
     auto r = std::make_unique<EngineRequest>();
@@ -2296,6 +2296,7 @@ pm7_status pm7_engine_submit(pm7_engine *E, const pm7_molecule *molecule, const 
       r->mol = E->runner->prepare(to_molecule(molecule), *options);
       if (!BatchRunner::batchable(*r->mol))
         throw Failure{PM7_ERR_UNSUPPORTED, "the serving engine runs closed-shell RHF requests; use pm7_run"};
+      r->mol->grad_out = gradient;
       E->queue.push_back(raw);
     } catch (const Failure &f) {
       raw->status = f.code;
@@ -2310,6 +2311,20 @@ pm7_status pm7_engine_submit(pm7_engine *E, const pm7_molecule *molecule, const 
     g_last_error = f.msg;
     return f.code;
   }
+}
+
+pm7_status pm7_engine_submit(pm7_engine *E, const pm7_molecule *molecule, const pm7_options *options,
+                             uint64_t *ticket) {
+  return engine_submit(E, molecule, options, nullptr, ticket);
+}
+
+pm7_status pm7_engine_submit_gradient(pm7_engine *E, const pm7_molecule *molecule, const pm7_options *options,
+                                      double *gradient, uint64_t *ticket) {
+  if (!gradient) {
+    g_last_error = "null gradient buffer";
+    return PM7_ERR_INVALID_INPUT;
+  }
+  return engine_submit(E, molecule, options, gradient, ticket);
 }
 
 pm7_status pm7_engine_poll(pm7_engine *E, uint64_t ticket, int32_t wait, int32_t *done, pm7_result *result,

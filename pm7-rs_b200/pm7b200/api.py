@@ -24,7 +24,7 @@ EXPORTED = [
     "pm7_stage_corrections", "pm7_run_batch", "pm7_engine_config_default", "pm7_engine_create", "pm7_engine_submit",
     "pm7_engine_poll", "pm7_engine_destroy", "pm7_batch_partition", "pm7_stage_eigenvalues",
     "pm7_stage_product_tf32", "pm7_autotune_report", "pm7_gradient", "pm7_fixed_density_gradient",
-    "pm7_correction_gradient", "pm7_run_batch_gradient",
+    "pm7_correction_gradient", "pm7_run_batch_gradient", "pm7_engine_submit_gradient",
 ]
 
 
@@ -69,6 +69,8 @@ def lib():
                                abi.DP, abi.DP]
     L.pm7_fixed_density_gradient.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, C.c_int32, abi.DP, abi.DP, abi.DP]
     L.pm7_correction_gradient.argtypes = [C.POINTER(abi.Molecule), C.c_int32, C.c_int32, abi.DP]
+    L.pm7_engine_submit_gradient.argtypes = [C.c_void_p, C.POINTER(abi.Molecule), C.POINTER(abi.Options), abi.DP,
+                                             C.POINTER(C.c_uint64)]
     L.pm7_run_batch_gradient.argtypes = [C.c_int32, C.POINTER(abi.Molecule), C.c_void_p, C.POINTER(abi.Options),
                                          C.POINTER(abi.Result), C.POINTER(C.c_int32), C.POINTER(abi.DP)]
     L.pm7_stage_eigenvalues.argtypes = [C.c_int32, C.POINTER(C.c_int32), abi.DP, abi.DP, C.c_int32]
@@ -404,14 +406,23 @@ class Engine:
         self.method = method
         self._keep = {}
 
-    def submit(self, z, xyz_bohr, **options):
+    def submit(self, z, xyz_bohr, gradient=False, **options):
+        """Queue a request; with gradient=True the finished result also carries "gradient"
+        (N x 3, eV/Bohr) and "forces" (`pm7_engine_submit_gradient`)."""
         m = _Mol(z, xyz_bohr)
         keep = [m]
         options.setdefault("method", self.method)
         o = _options_with_arrays(options, keep)
         t = C.c_uint64()
-        _check(lib().pm7_engine_submit(self._h, C.byref(m.s), C.byref(o), C.byref(t)))
-        self._keep[t.value] = keep
+        if gradient:
+            g = np.zeros((len(m.z), 3))
+            keep.append(g)
+            _check(lib().pm7_engine_submit_gradient(self._h, C.byref(m.s), C.byref(o), g.ctypes.data_as(abi.DP),
+                                                    C.byref(t)))
+        else:
+            g = None
+            _check(lib().pm7_engine_submit(self._h, C.byref(m.s), C.byref(o), C.byref(t)))
+        self._keep[t.value] = (keep, g)
         return t.value
 
     def poll(self, ticket, wait=False):
@@ -424,7 +435,7 @@ class Engine:
             if code != 0:
                 raise Pm7Error(code, lib().pm7_last_error_message().decode())
             return False, None
-        self._keep.pop(ticket, None)
+        _, g = self._keep.pop(ticket, (None, None))
         if code != 0:
             lib().pm7_result_free(C.byref(r))
             return True, Pm7Error(code, lib().pm7_last_error_message().decode())
@@ -433,6 +444,9 @@ class Engine:
         finally:
             lib().pm7_result_free(C.byref(r))
         d["latency_ms"] = lat.value
+        if g is not None:
+            d["gradient"] = g
+            d["forces"] = -g
         return True, d
 
     def close(self):

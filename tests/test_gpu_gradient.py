@@ -245,3 +245,17 @@ def test_closed_form_gradient_ferrocene(golden):
     out = api.closed_form_gradient(z, x, charge=float(case["charge"]))
     _, ref = H.gradient(z, x, charge=float(case["charge"]))
     assert np.max(np.abs(out["gradient"] - ref)) < SCF_TOL
+
+
+def test_served_gradients_match_single():
+    # pm7_engine_submit_gradient: requests with and without a gradient in one serving engine
+    mols = [G.alkane(4, seed=3), G.water_cluster(5, seed=4), chain_with_s_cl(5, seed=9)]
+    with api.Engine() as eng:
+        tickets = [eng.submit(z, x, gradient=True) for z, x in mols] + [eng.submit(*mols[0])]
+        out = [eng.poll(t, wait=True)[1] for t in tickets]
+    for (z, x), r in zip(mols, out[:3]):
+        assert not isinstance(r, Exception), r
+        single = api.closed_form_gradient(z, x)
+        assert np.max(np.abs(r["gradient"] - single["gradient"])) < SCF_TOL
+        assert np.array_equal(r["forces"], -r["gradient"])
+    assert "gradient" not in out[3]
