@@ -376,6 +376,46 @@ pm7_status pm7_engine_poll(pm7_engine *engine, uint64_t ticket, int32_t wait, in
 /* Finishes every submitted request, then stops the worker. */
 pm7_status pm7_engine_destroy(pm7_engine *engine);
 
+/* ---- divide-and-conquer SCF --------------------------------------------------------
+ * `DandcOptions` (src/dandc/mod.rs:62-99); defaults from pm7_dandc_options_default. */
+typedef struct pm7_dandc_options {
+  double buffer;         /* buffer radius, Bohr (15.0) */
+  int32_t core_size;     /* target atoms per core (12) */
+  double fermi_width_ev; /* Fermi smearing of the common chemical potential (0.1) */
+  int32_t max_scf;       /* (200) */
+  double p_tol;          /* RMS density change over the stored blocks (1e-6) */
+  double mixing;         /* linear density mixing factor in (0, 1] (0.4) */
+} pm7_dandc_options;
+
+void pm7_dandc_options_default(pm7_dandc_options *options);
+
+/* `DandcResult` (src/dandc/mod.rs:121-140) with `DandcDerivatives` (:438-443). The global
+ * density is returned dense (nao x nao, row-major) with zeros outside the stored atom-pair
+ * pattern; the caller frees the arrays with pm7_dandc_result_free. */
+typedef struct pm7_dandc_result {
+  int32_t n_atoms, nao;
+  int32_t converged, iterations, subsystems, largest_subsystem, unrestricted;
+  double fermi_ev, electronic_ev, density_error;
+  double core_core_ev, correction_ev;
+  double energy_ev;                 /* electronic + core-core + corrections (dandc_derivatives) */
+  int64_t stored_density_elements;  /* SparseDensity::stored_elements */
+  double *charges;                  /* n_atoms Mulliken net charges (src/dandc/mod.rs:819-829) */
+  double *gradient;                 /* 3 n_atoms eV/Bohr when requested, else NULL */
+  double *density;                  /* nao x nao when options->want_matrices, else NULL */
+  double *spin_density;             /* nao x nao, unrestricted and options->want_matrices */
+} pm7_dandc_result;
+
+/* Replaces `run_dandc` (src/dandc/mod.rs:143-428) and, with want_gradient != 0,
+ * `dandc_derivatives` (:446-506) for a molecule: subsystem cores by recursive median
+ * bisection with a buffer shell, one Fock build and eigendecomposition per subsystem on the
+ * device, one global Fermi level, Dixon-Merz weights normalised per atom pair, linear mixing.
+ * A run that reaches max_scf returns PM7_OK with converged = 0, as the reference does.
+ * Option errors and a largest subsystem beyond the memory budget are PM7_ERR_INVALID_INPUT. */
+pm7_status pm7_run_dandc(const pm7_molecule *molecule, const pm7_params *params,
+                         const pm7_options *options, const pm7_dandc_options *dandc,
+                         int32_t want_gradient, pm7_dandc_result *result);
+void pm7_dandc_result_free(pm7_dandc_result *result);
+
 #ifdef __cplusplus
 }
 #endif

@@ -61,6 +61,9 @@ def lib():
     L.pm7_oracle_element.argtypes = [C.c_int, C.c_int, abi.DP]
     L.pm7_oracle_fixed_density_gradient.argtypes = [C.POINTER(abi.Molecule), C.c_int, C.c_int, abi.DP, abi.DP,
                                                     C.c_double, abi.DP]
+    L.pm7_oracle_run_dandc.argtypes = [C.POINTER(abi.Molecule), C.POINTER(abi.Options), C.POINTER(abi.DandcOptions),
+                                       C.POINTER(abi.DandcResult)]
+    L.pm7_oracle_dandc_result_free.argtypes = [C.POINTER(abi.DandcResult)]
     L.pm7_oracle_correction_gradient.argtypes = [C.POINTER(abi.Molecule), C.c_int, C.c_int, C.c_double, abi.DP]
     libs = sorted(glob.glob(os.path.join(os.path.dirname(np.__file__) + ".libs", "libscipy_openblas64_*.so")))
     if libs:
@@ -230,6 +233,42 @@ def gradient(z, xyz_bohr, step=1.0e-3, corr_step=1.0e-5, **options):
     g = g + correction_gradient(z, xyz_bohr, method=method, smooth=options.get("smooth_dispersion", False),
                                 step=corr_step)
     return r, g
+
+
+def run_dandc(z, xyz_bohr, dandc=None, gradient=False, step=1.0e-3, corr_step=1.0e-5, **options):
+    """Oracle `run_dandc` (src/dandc/mod.rs:143-428): the result fields as a dict (the dense
+    global density under want_matrices). With `gradient`, `dandc_derivatives`' gradient
+    (:462-481): the RHF fixed-density gradient of the total density plus the correction
+    gradient."""
+    m = _Mol(z, xyz_bohr)
+    want = gradient or options.get("want_matrices", 1)
+    options = dict(options, want_matrices=int(bool(want)))
+    o = abi.default_options(**options)
+    d = abi.default_dandc_options(**(dandc or {}))
+    r = abi.DandcResult()
+    code = lib().pm7_oracle_run_dandc(C.byref(m.s), C.byref(o), C.byref(d), C.byref(r))
+    if code != 0:
+        raise OracleError(code, lib().pm7_oracle_last_error().decode())
+    try:
+        n, nao = r.n_atoms, r.nao
+        out = {k: getattr(r, k) for k in ("n_atoms", "nao", "converged", "iterations", "subsystems",
+                                           "largest_subsystem", "unrestricted", "fermi_ev", "electronic_ev",
+                                           "density_error", "core_core_ev", "correction_ev", "energy_ev",
+                                           "stored_density_elements")}
+        out["converged"] = bool(out["converged"])
+        out["unrestricted"] = bool(out["unrestricted"])
+        out["charges"] = _arr(r.charges, n)
+        for k in ("density", "spin_density"):
+            a = _arr(getattr(r, k), nao * nao)
+            out[k] = None if a is None else a.reshape(nao, nao)
+    finally:
+        lib().pm7_oracle_dandc_result_free(C.byref(r))
+    if gradient:
+        method = options.get("method", 0)
+        g = fixed_density_gradient(z, xyz_bohr, out["density"], None, method=method, step=step)
+        out["gradient"] = g + correction_gradient(z, xyz_bohr, method=method,
+                                                  smooth=options.get("smooth_dispersion", False), step=corr_step)
+    return out
 
 
 def numerical_gradient(z, xyz_bohr, step=1.0e-4, **options):

@@ -184,4 +184,12 @@ void matmul(const Mat &a, const Mat &b, Mat &c);
 // P = w * V_occ^T V_occ from the first n_occ rows of vt.
 void density_from_vectors(const std::vector<double> &vt, int n, int n_occ, double w, Mat &p);
 
+// Shared by the divide-and-conquer restatement (dandc.cpp).
+Molecule to_molecule(const pm7_molecule *m);
+void validate_input(const Molecule &mol, const pm7_options &o);                    // src/scf.rs:937-1040
+void memory_guard(int nao, size_t n_pairs, bool has_d, int64_t explicit_mb);       // src/memory.rs:95-118
+Mat sad_density(const Molecule &mol, const Basis &basis, const Params &p, double n_electrons);  // scf.rs:1050-1114
+double correction_energy(const Molecule &mol, const pm7_options &o, double parts[5]);  // src/scf.rs:907-932
+extern thread_local std::string g_error;
+
 }  // namespace oracle

@@ -292,7 +292,7 @@ static double frob(const Mat &a, const Mat &b) {
 }
 
 // sad_density (src/scf.rs:1050-1114).
-static Mat sad_density(const Molecule &mol, const Basis &basis, const Params &p, double n_electrons) {
+Mat sad_density(const Molecule &mol, const Basis &basis, const Params &p, double n_electrons) {
   int nao = basis.nao;
   Mat P(nao);
   double total_tore = 0.0;
@@ -718,7 +718,7 @@ static ScfState uhf_loop(const Molecule &mol, const Basis &basis, const Params &
 
 // ---- input validation and memory guard ----------------------------------
 
-static void validate_input(const Molecule &mol, const pm7_options &o) {  // src/scf.rs:937-1040
+void validate_input(const Molecule &mol, const pm7_options &o) {  // src/scf.rs:937-1040
   auto bad = [](const std::string &m) { throw Error(PM7_ERR_INVALID_INPUT, m); };
   if (mol.size() == 0) bad("a PM7 calculation needs at least one atom");
   if (!std::isfinite(o.charge)) bad("charge must be finite");
@@ -768,7 +768,7 @@ static uint64_t available_memory_bytes() {
   return 0;
 }
 
-static void memory_guard(int nao, size_t n_pairs, bool has_d, int64_t explicit_mb) {  // src/memory.rs:95-118
+void memory_guard(int nao, size_t n_pairs, bool has_d, int64_t explicit_mb) {  // src/memory.rs:95-118
   uint64_t budget = 0;
   bool have = false;
   if (explicit_mb >= 0) {
@@ -800,7 +800,7 @@ static void memory_guard(int nao, size_t n_pairs, bool has_d, int64_t explicit_m
 
 // ---- post-SCF quantities -------------------------------------------------
 
-static double correction_energy(const Molecule &mol, const pm7_options &o, double parts[5]) {
+double correction_energy(const Molecule &mol, const pm7_options &o, double parts[5]) {
   for (int k = 0; k < 5; ++k) parts[k] = 0.0;
   if (o.method == PM7_METHOD_PM7_MINUS) return 0.0;  // src/method.rs:35-37
   parts[0] = o.smooth_dispersion ? dispersion_energy_smooth(mol) : dispersion_energy(mol);
@@ -977,7 +977,7 @@ static void run(const Molecule &mol, const pm7_options &o, pm7_result *r) {
   }
 }
 
-static Molecule to_molecule(const pm7_molecule *m) {
+Molecule to_molecule(const pm7_molecule *m) {
   Molecule mol;
   if (!m || m->n_atoms < 0) throw Error(PM7_ERR_INVALID_INPUT, "null molecule");
   for (int i = 0; i < m->n_atoms; ++i) {
@@ -987,7 +987,7 @@ static Molecule to_molecule(const pm7_molecule *m) {
   return mol;
 }
 
-static thread_local std::string g_error;
+thread_local std::string g_error;
 
 template <class F>
 static pm7_status guarded(F f) {

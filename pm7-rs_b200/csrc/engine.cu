@@ -258,36 +258,6 @@ Layout build_layout(const Molecule &m, const ParamSet &ps) {
   return L;
 }
 
-struct DeviceMolecule {
-  cudaStream_t st;
-  int n = 0, nao = 0, n_near = 0;
-  DevBuf<int> z, aoff, ao_atom, csr_start, csr_eoff;
-  DevBuf<double> xyz, H, w, ecore, jbuf, pop, cc_partial, scal, gfar;
-  DevBuf<NearPair> near;
-  DevBuf<int2> csr;
-  DevBuf<unsigned char> mask;
-  DevBuf<int> status;
-  double core_core_ev = 0.0;
-
-  FockGeometry geometry() const {
-    FockGeometry g;
-    g.n_atoms = n;
-    g.nao = nao;
-    g.n_near = n_near;
-    g.z = z.p;
-    g.aoff = aoff.p;
-    g.ao_atom = ao_atom.p;
-    g.xyz = xyz.p;
-    g.near_mask = mask.p;
-    g.np = near.p;
-    g.csr_start = csr_start.p;
-    g.csr = csr.p;
-    g.csr_eoff = csr_eoff.p;
-    g.w = w.p;
-    g.gfar = gfar.p;
-    return g;
-  }
-};
 
 __global__ void k_fill_mask(int n_near, int n_atoms, const NearPair *np, unsigned char *mask) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -298,7 +268,7 @@ __global__ void k_fill_mask(int n_near, int n_atoms, const NearPair *np, unsigne
 
 // `dpath`: the molecule has a d-shell atom (or the caller forced it), so every pair is
 // evaluated in the MNDO/d frame (hamiltonian.rs:346-355).
-static void build_device_molecule(DeviceMolecule &D, const Molecule &m, const Layout &L, const DeviceParams &P,
+void build_device_molecule(DeviceMolecule &D, const Molecule &m, const Layout &L, const DeviceParams &P,
                                   bool dpath, cudaStream_t st) {
   D.st = st;
   D.n = m.n;

@@ -250,6 +250,42 @@ inline void upload(DevBuf<T> &b, const std::vector<T> &v, cudaStream_t st) {
 
 // Core Hamiltonian and stored pair integrals on the device (hamiltonian.rs:310-638).
 
+// One molecule's geometry, integrals and core Hamiltonian on the device (engine.cu).
+struct DeviceMolecule {
+  cudaStream_t st;
+  int n = 0, nao = 0, n_near = 0;
+  DevBuf<int> z, aoff, ao_atom, csr_start, csr_eoff;
+  DevBuf<double> xyz, H, w, ecore, jbuf, pop, cc_partial, scal, gfar;
+  DevBuf<NearPair> near;
+  DevBuf<int2> csr;
+  DevBuf<unsigned char> mask;
+  DevBuf<int> status;
+  double core_core_ev = 0.0;
+
+  FockGeometry geometry() const {
+    FockGeometry g;
+    g.n_atoms = n;
+    g.nao = nao;
+    g.n_near = n_near;
+    g.z = z.p;
+    g.aoff = aoff.p;
+    g.ao_atom = ao_atom.p;
+    g.xyz = xyz.p;
+    g.near_mask = mask.p;
+    g.np = near.p;
+    g.csr_start = csr_start.p;
+    g.csr = csr.p;
+    g.csr_eoff = csr_eoff.p;
+    g.w = w.p;
+    g.gfar = gfar.p;
+    return g;
+  }
+};
+// Uploads m / L and evaluates every pair's integrals, H_core and the core-core energy;
+// `dpath` selects the MNDO/d frame for every pair (hamiltonian.rs:346-355).
+void build_device_molecule(DeviceMolecule &D, const Molecule &m, const Layout &L, const DeviceParams &P, bool dpath,
+                           cudaStream_t st);
+
 // Nuclear gradient (eV/Bohr, 3 per atom) of a molecule on the device at the density g.Pt / g.Ps
 // (engine.cu); g.E and g.status are provided by the call.
 struct GradGeometry;

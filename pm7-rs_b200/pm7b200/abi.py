@@ -107,6 +107,56 @@ class Result(C.Structure):
     ]
 
 
+ANGSTROM_TO_BOHR = 1.0 / 0.529177210903  # src/constants.rs:21
+EV_TO_HARTREE = 1.0 / 27.211386245988     # src/constants.rs:19
+
+
+class DandcOptions(C.Structure):
+    """`DandcOptions` (pm7-rs src/dandc/mod.rs:62-81)."""
+    _fields_ = [
+        ("buffer", C.c_double),
+        ("core_size", C.c_int32),
+        ("fermi_width_ev", C.c_double),
+        ("max_scf", C.c_int32),
+        ("p_tol", C.c_double),
+        ("mixing", C.c_double),
+    ]
+
+
+class DandcResult(C.Structure):
+    """`DandcResult` with the energy of `DandcDerivatives` (src/dandc/mod.rs:121-140, 438-443)."""
+    _fields_ = [
+        ("n_atoms", C.c_int32),
+        ("nao", C.c_int32),
+        ("converged", C.c_int32),
+        ("iterations", C.c_int32),
+        ("subsystems", C.c_int32),
+        ("largest_subsystem", C.c_int32),
+        ("unrestricted", C.c_int32),
+        ("fermi_ev", C.c_double),
+        ("electronic_ev", C.c_double),
+        ("density_error", C.c_double),
+        ("core_core_ev", C.c_double),
+        ("correction_ev", C.c_double),
+        ("energy_ev", C.c_double),
+        ("stored_density_elements", C.c_int64),
+        ("charges", DP),
+        ("gradient", DP),
+        ("density", DP),
+        ("spin_density", DP),
+    ]
+
+
+def default_dandc_options(**kw):
+    """`DandcOptions::default()` (src/dandc/mod.rs:70-81): buffer in Bohr."""
+    d = DandcOptions(15.0, 12, 0.1, 200, 1.0e-6, 0.4)
+    for k, v in kw.items():
+        if not hasattr(d, k):
+            raise TypeError(f"unknown divide-and-conquer option {k!r}")
+        setattr(d, k, v)
+    return d
+
+
 def default_options(**kw):
     """`Pm7Options::default()` (pm7-rs src/scf.rs:207-233) as an Options struct."""
     o = Options()

@@ -25,6 +25,7 @@ EXPORTED = [
     "pm7_engine_poll", "pm7_engine_destroy", "pm7_batch_partition", "pm7_stage_eigenvalues",
     "pm7_stage_product_tf32", "pm7_autotune_report", "pm7_gradient", "pm7_fixed_density_gradient",
     "pm7_correction_gradient", "pm7_run_batch_gradient", "pm7_engine_submit_gradient",
+    "pm7_dandc_options_default", "pm7_run_dandc", "pm7_dandc_result_free",
 ]
 
 
@@ -73,6 +74,10 @@ def lib():
                                              C.POINTER(C.c_uint64)]
     L.pm7_run_batch_gradient.argtypes = [C.c_int32, C.POINTER(abi.Molecule), C.c_void_p, C.POINTER(abi.Options),
                                          C.POINTER(abi.Result), C.POINTER(C.c_int32), C.POINTER(abi.DP)]
+    L.pm7_dandc_options_default.argtypes = [C.POINTER(abi.DandcOptions)]
+    L.pm7_run_dandc.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, C.POINTER(abi.Options),
+                                C.POINTER(abi.DandcOptions), C.c_int32, C.POINTER(abi.DandcResult)]
+    L.pm7_dandc_result_free.argtypes = [C.POINTER(abi.DandcResult)]
     L.pm7_stage_eigenvalues.argtypes = [C.c_int32, C.POINTER(C.c_int32), abi.DP, abi.DP, C.c_int32]
     L.pm7_engine_config_default.argtypes = [C.POINTER(abi.EngineConfig)]
     L.pm7_engine_create.argtypes = [C.POINTER(abi.EngineConfig), C.POINTER(C.c_void_p)]
@@ -184,6 +189,65 @@ def closed_form_gradient(z, xyz_bohr, **options):
     finally:
         lib().pm7_result_free(C.byref(r))
     return {"scf": scf, "energy_ev": scf["total_ev"], "gradient": g, "forces": -g, "max_gradient": mx.value}
+
+
+def dandc_result_to_dict(r):
+    n, nao = r.n_atoms, r.nao
+    d = {k: getattr(r, k) for k in ("n_atoms", "nao", "converged", "iterations", "subsystems", "largest_subsystem",
+                                     "unrestricted", "fermi_ev", "electronic_ev", "density_error", "core_core_ev",
+                                     "correction_ev", "energy_ev", "stored_density_elements")}
+    d["converged"] = bool(d["converged"])
+    d["unrestricted"] = bool(d["unrestricted"])
+    d["charges"] = _arr(r.charges, n)
+    g = _arr(r.gradient, 3 * n)
+    d["gradient"] = None if g is None else g.reshape(n, 3)
+    for k in ("density", "spin_density"):
+        a = _arr(getattr(r, k), nao * nao)
+        d[k] = None if a is None else a.reshape(nao, nao)
+    return d
+
+
+def run_dandc(z, xyz_bohr, dandc=None, gradient=True, **options):
+    """`run_dandc` (src/dandc/mod.rs:143-428) and, with `gradient`, `dandc_derivatives`
+    (:446-506) on the device. `dandc` holds `DandcOptions` fields (buffer in Bohr, core_size,
+    fermi_width_ev, max_scf, p_tol, mixing); `options` the `Pm7Options` fields. Returns the
+    `DandcResult` fields plus energy_ev, charges, the gradient (N x 3, eV/Bohr) and, when
+    want_matrices is set, the dense global density (zeros outside the stored pattern). A run
+    that reaches max_scf returns converged = False, as the reference does."""
+    m = _Mol(z, xyz_bohr)
+    o = abi.default_options(**options)
+    d = abi.default_dandc_options(**(dandc or {}))
+    r = abi.DandcResult()
+    code = lib().pm7_run_dandc(C.byref(m.s), params(o.method), C.byref(o), C.byref(d), int(bool(gradient)),
+                               C.byref(r))
+    if code != 0:
+        raise Pm7Error(code, lib().pm7_last_error_message().decode())
+    try:
+        return dandc_result_to_dict(r)
+    finally:
+        lib().pm7_dandc_result_free(C.byref(r))
+
+
+def dandc(z, xyz_bohr, buffer_angstrom=8.0, core_size=12, method="pm7", charge=0.0, multiplicity=1,
+          reference="auto", scf_tolerance=None, max_scf=None):
+    """The reference's Python `dandc` binding (src/python.rs:1409-1494): buffer in Angstrom
+    (positions stay in Bohr, as everywhere in this API),
+    raises when the SCF does not converge; returns energy_ev, energy_hartree,
+    forces_ev_per_angstrom, fermi_ev, subsystems, largest_subsystem, iterations, unrestricted,
+    stored_density_elements."""
+    dc = {"buffer": buffer_angstrom * abi.ANGSTROM_TO_BOHR, "core_size": int(core_size),
+          "max_scf": 200 if max_scf is None else int(max_scf),
+          "p_tol": 1.0e-6 if scf_tolerance is None else float(scf_tolerance)}
+    r = run_dandc(z, xyz_bohr, dandc=dc, gradient=True, method=method, charge=charge, multiplicity=multiplicity,
+                  reference=reference, want_matrices=0)
+    if not r["converged"]:
+        raise ValueError(f"the divide-and-conquer SCF did not converge after {r['iterations']} iterations "
+                         f"(error={r['density_error']:.3e})")
+    return {"energy_ev": r["energy_ev"], "energy_hartree": r["energy_ev"] * abi.EV_TO_HARTREE,
+            "forces_ev_per_angstrom": -r["gradient"] * abi.ANGSTROM_TO_BOHR, "fermi_ev": r["fermi_ev"],
+            "subsystems": r["subsystems"], "largest_subsystem": r["largest_subsystem"],
+            "iterations": r["iterations"], "unrestricted": r["unrestricted"],
+            "stored_density_elements": r["stored_density_elements"]}
 
 
 def fixed_density_gradient(z, xyz_bohr, p_total, p_spin=None, method=0, force_dpath=False):

@@ -12,6 +12,8 @@
   becomes S with probability 0.1 (C-S 1.82 A) and each H becomes Cl with probability 0.1
   (C-Cl 1.77 A); `stream(count, seed)` - molecules of log-uniform size in 3..500 atoms,
   half such chains and half water clusters.
+* `flat_alkane(n)` - the flat zig-zag C_nH_(2n+2) chain (no jitter) of the divide-and-
+  conquer workload.
 All draws use numpy.random.default_rng(seed).
 """
 import math
@@ -199,3 +201,20 @@ def stream(count, seed=0, lo=3, hi=500):
             k = max(1, int(round(target / 3.0)))
             mols.append(water_cluster(k, centre_jitter=0.1, rng=rng))
     return mols
+
+
+def flat_alkane(n):
+    """C_nH_{2n+2} as a flat all-anti zig-zag (1.26 Angstrom along x, 0.44 across y, CH2
+    hydrogens at z = +-0.89, caps 1.09 Angstrom out along x): the one-dimensional chain of
+    pm7-rs tests/dandc.rs:95-127, on which the divide-and-conquer subsystem count grows with
+    n while the subsystem size does not. Returns (z, xyz in Bohr)."""
+    dx, dy = 1.26, 0.44
+    z, x = [], []
+    for i in range(n):
+        xx, yy = i * dx, (0.0 if i % 2 == 0 else dy)
+        s = -0.5 if i % 2 == 0 else 0.5
+        z += [6, 1, 1]
+        x += [(xx, yy, 0.0), (xx, yy + s, 0.89), (xx, yy + s, -0.89)]
+    z += [1, 1]
+    x += [(-1.09, 0.0, 0.0), ((n - 1) * dx + 1.09, 0.0 if (n - 1) % 2 == 0 else dy, 0.0)]
+    return np.array(z, dtype=np.uint8), np.array(x) * ANG
