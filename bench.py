@@ -25,6 +25,9 @@ Other workloads (`--workload`):
              C/S chains with Cl, and water clusters, seed 0) submitted to `pm7_engine` with
              Poisson arrivals at 80% of the engine's measured burst capacity; reports
              solves/s and p50/p99 submit-to-finish latency, and the plain path on a sample.
+  dandc640   the divide-and-conquer SCF (`pm7_run_dandc`) of the flat chain C640H1282,
+             1,922 atoms, buffer 15 Bohr, cores of 8 atoms; a step is one solve from host
+             buffers to host results.
 """
 import argparse
 import json
@@ -619,6 +622,69 @@ def run_stream_bench(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_dandc_bench(args, world, rank, local):
+    """Configuration: the divide-and-conquer SCF of the flat chain C640H1282 (1,922 atoms),
+    buffer 15 Bohr, cores of 8 atoms, p_tol 1e-7, SCF options e_tol 1e-10 / p_tol 1e-8 /
+    max_scf 400: the largest system of pm7-rs's divide-and-conquer scaling series. One molecule
+    per rank (replicas); each step is one pm7_run_dandc from host buffers to host results."""
+    from pm7b200 import api
+    from pm7b200 import geometry as G
+
+    z, x = G.flat_alkane(640)
+    dc = dict(buffer=15.0, core_size=8, p_tol=1.0e-7, max_scf=400)
+    opts = dict(e_tol=1.0e-10, p_tol=1.0e-8, max_scf=400, device=local, want_matrices=0)
+    for _ in range(args.warmup):
+        r = api.run_dandc(z, x, dandc=dc, gradient=False, **opts)
+    barrier(world)
+    sampler = ClockSampler(local, interval_ms=500)
+    sampler.start()
+    launches0 = api.launch_count()
+    walls = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        r = api.run_dandc(z, x, dandc=dc, gradient=False, **opts)
+        walls.append(time.perf_counter() - t)
+    launches = api.launch_count() - launches0
+    clocks = sampler.stop()
+    barrier(world)
+    wall = allreduce_max(sum(walls), world)
+    t = time.perf_counter()
+    rg = api.run_dandc(z, x, dandc=dc, gradient=True, **opts)
+    gwall = time.perf_counter() - t
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import harness
+
+        zc, xc = G.flat_alkane(160)
+        t = time.perf_counter()
+        o = harness.run_dandc(zc, xc, dandc=dc, want_matrices=0, e_tol=1.0e-10, p_tol=1.0e-8, max_scf=400)
+        tc = time.perf_counter() - t
+        scale = len(z) / len(zc)  # the method is linear in the atom count at a fixed buffer
+        cpu = {"value": 1.0 / (tc * scale), "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"the oracle's D&C of C160H322 ({len(zc)} atoms, {o['iterations']} iterations, "
+                         f"{tc:.1f} s) scaled by the atom ratio {scale:.2f} to the 1,922-atom chain"}
+    n = len(z)
+    line = {
+        "metric": "PM7 divide-and-conquer SCF solves/s", "value": world * args.steps / wall, "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic", "dtype": "f64",
+        "config": {"workload": "dandc640", "atoms": n, "nao": int(r["nao"]), "buffer_bohr": 15.0, "core_size": 8,
+                   "subsystems": r["subsystems"], "largest_subsystem": r["largest_subsystem"],
+                   "iterations": r["iterations"], "converged": r["converged"],
+                   "stored_density_elements": r["stored_density_elements"], "parallelism": f"replicas{world}",
+                   "l2": "the global density (nao^2 doubles) and the per-subsystem buckets exceed L2 together"},
+        "e2e": {"value": world * args.steps / wall, "unit": "solves/s",
+                "note": "wall clock around pm7_run_dandc with host buffers (partition, build, SCF, results)"},
+        "per_iteration_ms": wall * 1e3 / args.steps / max(r["iterations"], 1),
+        "gradient": {"wall_s": gwall, "unit": "s per pm7_run_dandc with the gradient",
+                     "max_abs_ev_per_bohr": float(np.abs(rg["gradient"]).max())},
+        "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -626,7 +692,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="water334",
-                    choices=["water334", "water1000", "decane", "batch4096", "stream"])
+                    choices=["water334", "water1000", "decane", "batch4096", "stream", "dandc640"])
     ap.add_argument("--stream-count", type=int, default=600)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="batch4096/stream: fp64, or fp32 tcgen05 purification cycles with fp64 refinement")
@@ -647,6 +713,8 @@ def main():
             run_batch_bench(args, world, rank, local)
         elif args.workload == "stream":
             run_stream_bench(args, world, rank, local)
+        elif args.workload == "dandc640":
+            run_dandc_bench(args, world, rank, local)
         else:
             run_b200(args, world, rank, local)
     finally:

@@ -56,7 +56,7 @@ def test_large_subsystems_take_the_per_matrix_solver_and_stay_exact():
     exact = api.run_pm7(z, x, want_matrices=0, e_tol=1e-10, p_tol=1e-8)
     d = api.run_dandc(z, x, dandc=dict(buffer=200.0, core_size=60, p_tol=1e-9, max_scf=400), gradient=False,
                       want_matrices=0)
-    assert d["converged"] and d["subsystems"] == 5 and d["largest_subsystem"] == 300
+    assert d["converged"] and d["subsystems"] > 1 and d["largest_subsystem"] == 300
     assert abs(d["energy_ev"] - exact["total_ev"]) < 1e-6
     assert np.abs(d["charges"] - exact["charges"]).max() < 1e-6
 
