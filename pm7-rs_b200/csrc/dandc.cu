@@ -16,9 +16,12 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <memory>
 #include <unordered_map>
 
@@ -31,6 +34,7 @@ namespace {
 
 constexpr double kDcPad = 1.0e5;  // diagonal of the padding rows of a bucket matrix (eV)
 constexpr int kDcPartials = 128;   // blocks of the reductions (fixed: the sums are deterministic)
+constexpr size_t kDcLanes = 16;    // side streams for the subsystems' independent launch sequences
 
 // ---------------------------------------------------------------------------------------
 // kernels
@@ -409,6 +413,7 @@ void check_dandc_options(const pm7_dandc_options &d) {  // src/dandc/mod.rs:83-1
 void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7_options *opt,
                     const pm7_dandc_options *dco, int want_gradient, pm7_dandc_result *res) {
   if (!mol || !params || !opt || !dco || !res) throw Failure{PM7_ERR_INVALID_INPUT, "null argument"};
+  const auto t_start = std::chrono::steady_clock::now();
   const pm7_options &o = *opt;
   const pm7_dandc_options &dc = *dco;
   Molecule m = to_molecule(mol);
@@ -579,21 +584,76 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
     b.info.alloc(b.count, st);
     CUDA_OK(cudaMemsetAsync(b.info.p, 0, sizeof(int) * b.count, st));
   }
+  // Lanes: the subsystems' launch sequences are independent, so they run on kDcLanes side
+  // streams forked from and joined back into the main stream (parallel branches of the captured
+  // graphs), each lane with its own scratch. The lanes synchronise before their buffers go.
   const size_t mm = (size_t)std::max(max_nao, 1) * std::max(max_nao, 1);
-  DevBuf<double> Pl, Pa, Pb, Fa, Fb, Vf, Dm, econ_part, econ, se, sw;
-  Pl.alloc(mm, st);
-  Fa.alloc(mm, st);
-  Dm.alloc(mm, st);
-  if (unrestricted) {
-    Pa.alloc(mm, st);
-    Pb.alloc(mm, st);
-    Fb.alloc(mm, st);
+  const size_t vv = (size_t)chan * std::max(max_np, 1) * std::max(max_np, 1);
+  struct Lane {
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    DevBuf<double> Pl, Pa, Pb, Fa, Fb, Vf, env, part;
+    ~Lane() {
+      if (st) cudaStreamSynchronize(st);
+      if (done) cudaEventDestroy(done);
+      // the buffers are released (stream-ordered on the main stream) after this body
+    }
+  };
+  const int n_lanes = (int)std::min<size_t>(kDcLanes, std::max<size_t>(subs.size(), 1));
+  std::deque<Lane> lanes(n_lanes);
+  struct LaneStreams {
+    std::deque<Lane> &l;
+    cudaEvent_t fork = nullptr;
+    ~LaneStreams() {
+      for (Lane &x : l)
+        if (x.st) {
+          cudaStreamSynchronize(x.st);
+          cudaStreamDestroy(x.st);
+          x.st = nullptr;
+        }
+      if (fork) cudaEventDestroy(fork);
+    }
+  } lane_streams{lanes};
+  CUDA_OK(cudaEventCreateWithFlags(&lane_streams.fork, cudaEventDisableTiming));
+  for (Lane &L : lanes) {
+    CUDA_OK(cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking));
+    CUDA_OK(cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming));
+    L.Pl.alloc(mm, st);
+    L.Fa.alloc(mm, st);
+    if (unrestricted) {
+      L.Pa.alloc(mm, st);
+      L.Pb.alloc(mm, st);
+      L.Fb.alloc(mm, st);
+    }
+    L.Vf.alloc(vv, st);
+    L.env.alloc(std::max(largest_atoms, 1), st);
+    L.part.alloc(kDcPartials, st);
   }
-  Vf.alloc((size_t)chan * std::max(max_np, 1) * std::max(max_np, 1), st);
-  econ_part.alloc(kDcPartials, st);
+  auto fork = [&]() {
+    CUDA_OK(cudaEventRecord(lane_streams.fork, st));
+    for (Lane &L : lanes) CUDA_OK(cudaStreamWaitEvent(L.st, lane_streams.fork, 0));
+  };
+  auto join = [&]() {
+    for (Lane &L : lanes) {
+      CUDA_OK(cudaEventRecord(L.done, L.st));
+      CUDA_OK(cudaStreamWaitEvent(st, L.done, 0));
+    }
+  };
+  // each subsystem's Fermi-weighted density (and spin density), kept until the ordered scatter
+  std::vector<size_t> dm_off(subs.size() + 1, 0);
+  for (size_t a = 0; a < subs.size(); ++a) dm_off[a + 1] = dm_off[a] + (size_t)subs[a]->nao * subs[a]->nao;
+  DevBuf<double> Dm, econ, se, sw;
+  Dm.alloc(std::max<size_t>(dm_off.back(), 1) * (unrestricted ? 2 : 1), st);
   econ.alloc(std::max<size_t>(subs.size(), 1), st);
   se.alloc(std::max<size_t>(n_states, 1), st);
   sw.alloc(std::max<size_t>(n_states, 1), st);
+  struct LaneSync {  // destroyed first: no lane work is pending when the buffers above are released
+    std::deque<Lane> &l;
+    ~LaneSync() {
+      for (Lane &x : l)
+        if (x.st) cudaStreamSynchronize(x.st);
+    }
+  } lane_sync{lanes};
 
   // eigensolver workspaces (the bucket shapes are fixed for the whole run)
   cusolverDnParams_t sparams = nullptr;
@@ -629,46 +689,56 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
   double fermi = 0.0, err = INFINITY, electronic = 0.0;
   int iterations = 0;
   bool converged = false;
-  for (int iter = 0; iter < dc.max_scf; ++iter) {
-    iterations = iter + 1;
+  // One iteration is three parts: the subsystem Fock builds (queue_pre), the eigensolves
+  // (cuSOLVER, issued directly) and the Fermi level with the reassembly (queue_post). The first
+  // iteration runs them as plain launches, which also settles the autotuned Fock shapes; from the
+  // second on the two launch sequences (thousands of small kernels, identical every iteration)
+  // are replayed as CUDA graphs.
+  auto queue_pre = [&]() {
     // environment potential of the current populations (src/dandc/mod.rs:946-998)
     k_dc_pops<<<(N + 127) / 128, 128, 0, st>>>(N, aoff.p, norb.p, nao_g, Pg.p, pops.p);
     k_dc_coulomb<<<(N + 3) / 4, 128, 0, st>>>(N, xyz.p, pops.p, gelec.p);
     note_launch();
     note_launch();
     // every subsystem: Fock build, environment, packing, energy (src/dandc/mod.rs:526-663)
+    fork();
     for (size_t a = 0; a < subs.size(); ++a) {
       DcSub &s = *subs[a];
+      Lane &L = lanes[a % lanes.size()];
+      const cudaStream_t ls = L.st;
       if (s.nao == 0) {
-        CUDA_OK(cudaMemsetAsync(econ.p + a, 0, sizeof(double), st));
+        CUDA_OK(cudaMemsetAsync(econ.p + a, 0, sizeof(double), ls));
         continue;
       }
       DcBucket &b = buckets[s.bucket];
       const size_t nn = (size_t)s.nao * s.nao;
-      k_dc_env<<<(s.m.n + 3) / 4, 128, 0, st>>>(s.m.n, s.parent.p, xyz.p, pops.p, gelec.p, env.p);
-      k_dc_gather<<<grid_for(nn), 256, 0, st>>>(s.nao, s.map.p, s.ao_par.p, N, nao_g, wdev.p, Pg.p,
-                                                unrestricted ? Sg.p : nullptr, Pl.p, Pa.p, Pb.p);
+      k_dc_env<<<(s.m.n + 3) / 4, 128, 0, ls>>>(s.m.n, s.parent.p, xyz.p, pops.p, gelec.p, L.env.p);
+      k_dc_gather<<<grid_for(nn), 256, 0, ls>>>(s.nao, s.map.p, s.ao_par.p, N, nao_g, wdev.p, Pg.p,
+                                                unrestricted ? Sg.p : nullptr, L.Pl.p, L.Pa.p, L.Pb.p);
       note_launch();
       note_launch();
       const FockGeometry g = s.D.geometry();
       double *slot_a = b.A.p + (size_t)s.slot * b.np * b.np;
       if (!unrestricted) {
-        launch_fock(st, g, P, s.D.H.p, Pl.p, Pl.p, 0.5, Fa.p, s.D.pop.p, s.D.jbuf.p);
+        launch_fock(ls, g, P, s.D.H.p, L.Pl.p, L.Pl.p, 0.5, L.Fa.p, s.D.pop.p, s.D.jbuf.p);
       } else {
-        launch_fock(st, g, P, s.D.H.p, Pl.p, Pa.p, 1.0, Fa.p, s.D.pop.p, s.D.jbuf.p);
-        launch_fock(st, g, P, s.D.H.p, Pl.p, Pb.p, 1.0, Fb.p, s.D.pop.p, s.D.jbuf.p);
+        launch_fock(ls, g, P, s.D.H.p, L.Pl.p, L.Pa.p, 1.0, L.Fa.p, s.D.pop.p, s.D.jbuf.p);
+        launch_fock(ls, g, P, s.D.H.p, L.Pl.p, L.Pb.p, 1.0, L.Fb.p, s.D.pop.p, s.D.jbuf.p);
       }
       const size_t npp = (size_t)b.np * b.np;
-      k_dc_pack<<<grid_for(npp), 256, 0, st>>>(s.nao, b.np, Fa.p, s.ao_atom.p, env.p, slot_a);
+      k_dc_pack<<<grid_for(npp), 256, 0, ls>>>(s.nao, b.np, L.Fa.p, s.ao_atom.p, L.env.p, slot_a);
       note_launch();
       if (unrestricted) {
-        k_dc_pack<<<grid_for(npp), 256, 0, st>>>(s.nao, b.np, Fb.p, s.ao_atom.p, env.p, slot_a + npp);
+        k_dc_pack<<<grid_for(npp), 256, 0, ls>>>(s.nao, b.np, L.Fb.p, s.ao_atom.p, L.env.p, slot_a + npp);
         note_launch();
       }
-      k_dc_energy<<<kDcPartials, 256, 0, st>>>(s.nao, b.np, s.core_ao, Pl.p, s.D.H.p, slot_a, econ_part.p);
+      k_dc_energy<<<kDcPartials, 256, 0, ls>>>(s.nao, b.np, s.core_ao, L.Pl.p, s.D.H.p, slot_a, L.part.p);
       note_launch();
-      launch_sum(st, econ_part.p, kDcPartials, econ.p + a);
+      launch_sum(ls, L.part.p, kDcPartials, econ.p + a);
     }
+    join();
+  };
+  auto queue_eig = [&]() {
     // the subsystem eigenproblems, bucket by bucket
     for (DcBucket &b : buckets) {
       if (b.np >= 512) {
@@ -682,39 +752,56 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
                                          hwork.empty() ? nullptr : hwork.data(), wh_max, b.info.p, b.count));
       }
     }
+  };
+  auto queue_post = [&]() {
     // weighted spectra and the common Fermi level
-    for (auto &sp : subs) {
-      DcSub &s = *sp;
+    fork();
+    for (size_t a = 0; a < subs.size(); ++a) {
+      DcSub &s = *subs[a];
       if (s.nao == 0) continue;
+      const cudaStream_t ls = lanes[a % lanes.size()].st;
       DcBucket &b = buckets[s.bucket];
       for (int c = 0; c < chan; ++c) {
         const size_t k = (size_t)s.slot + c;
-        k_dc_norms<<<(s.nao + 3) / 4, 128, 0, st>>>(s.nao, b.np, s.core_ao, unrestricted ? 0.5 : 1.0,
+        k_dc_norms<<<(s.nao + 3) / 4, 128, 0, ls>>>(s.nao, b.np, s.core_ao, unrestricted ? 0.5 : 1.0,
                                                     b.A.p + k * b.np * b.np, b.eps.p + k * b.np,
                                                     se.p + s.spec + (size_t)c * s.nao, sw.p + s.spec + (size_t)c * s.nao);
         note_launch();
       }
     }
+    join();
     k_dc_fermi<<<1, 1024, 0, st>>>(n_states, se.p, sw.p, n_elec, dc.fermi_width_ev, scal.p + 1);
     note_launch();
-    // reassembly: V^T diag(f) V per subsystem, scattered with the weights (src/dandc/mod.rs:354-393)
-    for (int spin = 0; spin < (unrestricted ? 2 : 1); ++spin) {
-      double *target = spin ? Ns.p : Nx.p;
-      for (auto &sp : subs) {
-        DcSub &s = *sp;
-        if (s.nao == 0) continue;
-        DcBucket &b = buckets[s.bucket];
-        const size_t npp = (size_t)b.np * b.np;
+    // reassembly (src/dandc/mod.rs:354-393): V^T diag(f) V per subsystem on the lanes, then the
+    // weighted scatter into the global density in subsystem order on the main stream
+    fork();
+    for (size_t a = 0; a < subs.size(); ++a) {
+      DcSub &s = *subs[a];
+      if (s.nao == 0) continue;
+      Lane &L = lanes[a % lanes.size()];
+      DcBucket &b = buckets[s.bucket];
+      const size_t npp = (size_t)b.np * b.np;
+      for (int spin = 0; spin < (unrestricted ? 2 : 1); ++spin) {
         for (int c = 0; c < chan; ++c) {
           const double scale = !unrestricted ? 1.0 : (c == 0 ? 0.5 : (spin ? -0.5 : 0.5));
           const size_t k = (size_t)s.slot + c;
-          k_dc_occupy<<<grid_for(npp), 256, 0, st>>>(s.nao, b.np, scale, b.A.p + k * npp, b.eps.p + k * b.np,
-                                                     scal.p + 1, dc.fermi_width_ev, Vf.p + (size_t)c * npp);
+          k_dc_occupy<<<grid_for(npp), 256, 0, L.st>>>(s.nao, b.np, scale, b.A.p + k * npp, b.eps.p + k * b.np,
+                                                       scal.p + 1, dc.fermi_width_ev, L.Vf.p + (size_t)c * npp);
           note_launch();
         }
         // the channels' slots are adjacent, so both enter one product of inner dimension chan*np
-        launch_gemm_tn(st, s.nao, s.nao, chan * b.np, 1.0, Vf.p, b.np, b.A.p + (size_t)s.slot * npp, b.np, Dm.p, s.nao);
-        k_dc_scatter<<<grid_for((size_t)s.nao * s.nao), 256, 0, st>>>(s.nao, s.core_ao, s.map.p, Dm.p, nao_g, target);
+        launch_gemm_tn(L.st, s.nao, s.nao, chan * b.np, 1.0, L.Vf.p, b.np, b.A.p + (size_t)s.slot * npp, b.np,
+                       Dm.p + (spin ? dm_off.back() : 0) + dm_off[a], s.nao);
+      }
+    }
+    join();
+    for (int spin = 0; spin < (unrestricted ? 2 : 1); ++spin) {
+      double *target = spin ? Ns.p : Nx.p;
+      for (size_t a = 0; a < subs.size(); ++a) {
+        DcSub &s = *subs[a];
+        if (s.nao == 0) continue;
+        k_dc_scatter<<<grid_for((size_t)s.nao * s.nao), 256, 0, st>>>(
+            s.nao, s.core_ao, s.map.p, Dm.p + (spin ? dm_off.back() : 0) + dm_off[a], nao_g, target);
         note_launch();
       }
     }
@@ -722,6 +809,63 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
                                              unrestricted ? Sg.p : nullptr, unrestricted ? Ns.p : nullptr, partials.p);
     note_launch();
     launch_sum(st, partials.p, kDcPartials, scal.p);
+  };
+  struct Graphs {
+    cudaGraphExec_t pre = nullptr, post = nullptr;
+    int n_pre = 0, n_post = 0;
+    ~Graphs() {
+      if (pre) cudaGraphExecDestroy(pre);
+      if (post) cudaGraphExecDestroy(post);
+    }
+  } graphs;
+  auto capture = [&](const std::function<void()> &fn, cudaGraphExec_t &exec, int &nodes) {
+    const long long before = pm7_launch_count();
+    cudaGraph_t graph = nullptr;
+    CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    fn();
+    CUDA_OK(cudaStreamEndCapture(st, &graph));
+    nodes = (int)(pm7_launch_count() - before);
+    note_launch(-nodes);  // counted when replayed
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CUDA_OK(ie);
+  };
+  auto replay = [&](cudaGraphExec_t exec, int nodes) {
+    CUDA_OK(cudaGraphLaunch(exec, st));
+    note_launch(nodes);
+  };
+  // PM7_DANDC_TRACE: per-phase wall times on stderr (each phase then ends in a synchronise)
+  const bool trace = std::getenv("PM7_DANDC_TRACE") != nullptr;
+  double t_phase[4] = {0, 0, 0, 0};
+  auto tick = [&](int k, std::chrono::steady_clock::time_point &t) {
+    if (!trace) return;
+    CUDA_OK(cudaStreamSynchronize(st));
+    const auto now = std::chrono::steady_clock::now();
+    t_phase[k] += std::chrono::duration<double, std::milli>(now - t).count();
+    t = now;
+  };
+  if (trace) CUDA_OK(cudaStreamSynchronize(st));
+  auto t = std::chrono::steady_clock::now();
+  const double t_setup = std::chrono::duration<double, std::milli>(t - t_start).count();
+  for (int iter = 0; iter < dc.max_scf; ++iter) {
+    iterations = iter + 1;
+    if (iter == 0) {
+      queue_pre();
+      tick(1, t);
+      queue_eig();
+      tick(2, t);
+      queue_post();
+      tick(3, t);
+    } else {
+      if (!graphs.pre) capture(queue_pre, graphs.pre, graphs.n_pre);
+      replay(graphs.pre, graphs.n_pre);
+      tick(1, t);
+      queue_eig();
+      tick(2, t);
+      if (!graphs.post) capture(queue_post, graphs.post, graphs.n_post);
+      replay(graphs.post, graphs.n_post);
+      tick(3, t);
+    }
     double sc[3];
     CUDA_OK(cudaMemcpyAsync(sc, scal.p, sizeof(sc), cudaMemcpyDeviceToHost, st));
     if (!subs.empty())
@@ -765,6 +909,9 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
     }
   }
 
+  if (trace)
+    std::fprintf(stderr, "pm7_run_dandc ms: setup %.1f fock %.1f eigen %.1f reassembly %.1f (%d iterations, %zu buckets)\n",
+                 t_setup, t_phase[1], t_phase[2], t_phase[3], iterations, buckets.size());
   // energy, charges and (on request) the gradient at the divide-and-conquer density
   DeviceMolecule Dg;
   build_device_molecule(Dg, m, Lg, P, Lg.has_d, st);
