@@ -35,6 +35,7 @@ namespace {
 constexpr double kDcPad = 1.0e5;  // diagonal of the padding rows of a bucket matrix (eV)
 constexpr int kDcPartials = 128;   // blocks of the reductions (fixed: the sums are deterministic)
 constexpr size_t kDcLanes = 16;    // side streams for the subsystems' independent launch sequences
+constexpr int kDcAssembleBlocks = 148 * 8;  // grid of the global assembly (8 blocks per SM)
 
 // ---------------------------------------------------------------------------------------
 // kernels
@@ -255,46 +256,52 @@ __global__ void k_dc_occupy(int nao, int np, double scale, const double *__restr
   }
 }
 
-// Adds the weighted subsystem density into the global next density (SparseDensity::accumulate):
-// out[map k, map l] += w_kl D_kl over the pairs with w > 0.
-__global__ void k_dc_scatter(int nao, int core_ao, const int *__restrict__ map, const double *__restrict__ D,
-                             int nao_glob, double *__restrict__ out) {
-  const size_t nn = (size_t)nao * nao;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nn; e += (size_t)gridDim.x * blockDim.x) {
-    const int k = (int)(e / nao), l = (int)(e % nao);
-    const bool ck = k < core_ao, cl = l < core_ao;
-    if (!ck && !cl) continue;
-    const double w = (ck && cl) ? 1.0 : 0.5;
-    out[(size_t)map[k] * nao_glob + map[l]] += w * D[e];
-  }
-}
+// One stored atom pair's contributions to the next global density: at most two subsystems
+// weight it, the one whose core holds A and the one whose core holds B (a pair with both atoms
+// in one core has a single contribution of weight 1). Per contribution: the offset of that
+// subsystem's density in the product buffer, its order, A's and B's local AO offsets, the weight.
+struct DcPairSrc {
+  long long off[2];
+  int nao[2], la[2], lb[2];
+  double w[2];
+  int n;
+};
 
-// Normalises the next density by the realised weight total of each stored pair
-// (src/dandc/mod.rs:236-258), sums (P - next)^2 (rms_diff), mixes P <- (1 - m) P + m next
-// (sparse.rs mix) and clears next; the spin density likewise, without the error.
-__global__ void k_dc_finish(int nao, int n_glob, const int *__restrict__ ao_atom, const unsigned char *__restrict__ wcnt,
-                            double mixing, double *__restrict__ P, double *__restrict__ Nx, double *__restrict__ S,
-                            double *__restrict__ Ns, double *__restrict__ partials) {
+// The next global density assembled from the subsystem densities (scatter_density +
+// SparseDensity::accumulate, src/dandc/mod.rs:770-814, in the fixed order above), normalised by
+// the realised weight total (:236-258), its RMS difference to P (rms_diff) and the mixing
+// P <- (1 - m) P + m next (sparse.rs mix); the spin density likewise, without the error.
+// Thread per global element; partial sums of (P - next)^2 per block.
+__global__ void k_dc_assemble(int nao, int n_glob, const int *__restrict__ ao_atom, const int *__restrict__ aoff,
+                              const int *__restrict__ pair_rec, const DcPairSrc *__restrict__ recs,
+                              const double *__restrict__ D, const double *__restrict__ Ds, double mixing,
+                              double *__restrict__ P, double *__restrict__ S, double *__restrict__ partials) {
   __shared__ double sh[32];
   const size_t nn = (size_t)nao * nao;
-  double s = 0.0;
+  double acc = 0.0;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nn; e += (size_t)gridDim.x * blockDim.x) {
     const int k = (int)(e / nao), l = (int)(e % nao);
-    const int c = wcnt[(size_t)ao_atom[k] * n_glob + ao_atom[l]];
-    if (c == 0) continue;
-    const double norm = 1.0 / (0.5 * c);
-    const double nx = Nx[e] * norm;
-    const double d = P[e] - nx;
-    s += d * d;
-    P[e] = (1.0 - mixing) * P[e] + mixing * nx;
-    Nx[e] = 0.0;
-    if (S) {
-      S[e] = (1.0 - mixing) * S[e] + mixing * (Ns[e] * norm);
-      Ns[e] = 0.0;
+    const int A = ao_atom[k], B = ao_atom[l];
+    const int r = pair_rec[(size_t)A * n_glob + B];
+    if (r < 0) continue;
+    const DcPairSrc &q = recs[r];
+    const int mu = k - aoff[A], nu = l - aoff[B];
+    double t = 0.0, wt = 0.0, ts = 0.0;
+    for (int c = 0; c < q.n; ++c) {
+      const size_t i = (size_t)q.off[c] + (size_t)(q.la[c] + mu) * q.nao[c] + q.lb[c] + nu;
+      t += q.w[c] * D[i];
+      if (Ds) ts += q.w[c] * Ds[i];
+      wt += q.w[c];
     }
+    const double norm = 1.0 / wt;
+    const double nx = t * norm;
+    const double d = P[e] - nx;
+    acc += d * d;
+    P[e] = (1.0 - mixing) * P[e] + mixing * nx;
+    if (S) S[e] = (1.0 - mixing) * S[e] + mixing * (ts * norm);
   }
-  s = block_sum(s, sh);
-  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
 }
 
 unsigned grid_for(size_t items) { return (unsigned)std::max<size_t>(1, std::min<size_t>((items + 255) / 256, 4096)); }
@@ -502,7 +509,7 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
 
   // global arrays
   const size_t nng = (size_t)nao_g * nao_g;
-  DevBuf<double> xyz, q, gnuc, gelec, pops, Pg, Nx, Sg, Ns, partials, scal;
+  DevBuf<double> xyz, q, gnuc, gelec, pops, Pg, Sg, partials, scal;
   DevBuf<int> aoff, norb, ao_atom;
   DevBuf<unsigned char> wdev;
   upload(xyz, m.xyz, st);
@@ -514,7 +521,7 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
   gnuc.alloc(N, st);
   gelec.alloc(N, st);
   pops.alloc(N, st);
-  partials.alloc(kDcPartials, st);
+  partials.alloc(kDcAssembleBlocks, st);
   scal.alloc(4, st);  // [0] error^2 sum, [1] Fermi level, [2] Fermi status
   {
     // atomic-density start on the diagonal blocks (src/dandc/mod.rs:289-301); the spin density
@@ -528,12 +535,6 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
       for (int k = 0; k < nao_g; ++k) h[(size_t)k * nao_g + k] = scale * diag[k];
       upload(Sg, h, st);
     }
-  }
-  Nx.alloc(nng, st);
-  CUDA_OK(cudaMemsetAsync(Nx.p, 0, sizeof(double) * nng, st));
-  if (unrestricted) {
-    Ns.alloc(nng, st);
-    CUDA_OK(cudaMemsetAsync(Ns.p, 0, sizeof(double) * nng, st));
   }
   if (N > 0) k_dc_coulomb<<<(N + 3) / 4, 128, 0, st>>>(N, xyz.p, q.p, gnuc.p);
   note_launch();
@@ -647,6 +648,50 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
   econ.alloc(std::max<size_t>(subs.size(), 1), st);
   se.alloc(std::max<size_t>(n_states, 1), st);
   sw.alloc(std::max<size_t>(n_states, 1), st);
+  // the contributions of every stored atom pair (see DcPairSrc), indexed by an N x N table
+  DevBuf<int> pair_rec_d;
+  DevBuf<DcPairSrc> recs_d;
+  {
+    std::vector<int> core_of(N, -1), local(N, -1);
+    for (size_t a = 0; a < subs.size(); ++a)
+      for (int i = 0; i < subs[a]->part.n_core; ++i) core_of[subs[a]->part.parent[i]] = (int)a;
+    // local atom index of every parent atom, per subsystem, filled on demand below
+    std::vector<std::vector<int>> where(subs.size());
+    auto local_of = [&](int a, int atom) {
+      std::vector<int> &w = where[a];
+      if (w.empty()) {
+        w.assign(N, -1);
+        for (int i = 0; i < subs[a]->m.n; ++i) w[subs[a]->part.parent[i]] = i;
+      }
+      return w[atom];
+    };
+    std::vector<int> rec((size_t)N * N, -1);
+    std::vector<DcPairSrc> recs;
+    for (int A = 0; A < N; ++A)
+      for (int B = 0; B < N; ++B) {
+        if (!wcnt[(size_t)A * N + B]) continue;
+        DcPairSrc q{};
+        const int sa = core_of[A], sb = core_of[B];
+        for (int sub : {sa, sb}) {
+          if (q.n == 1 && sub == sa) break;  // both atoms in one core: one contribution
+          const int ia = local_of(sub, A), ib = local_of(sub, B);
+          if (ia < 0 || ib < 0) continue;
+          const DcSub &x = *subs[sub];
+          const bool ca = ia < x.part.n_core, cb = ib < x.part.n_core;
+          if (!ca && !cb) continue;
+          q.off[q.n] = (long long)dm_off[sub];
+          q.nao[q.n] = x.nao;
+          q.la[q.n] = x.L.aoff[ia];
+          q.lb[q.n] = x.L.aoff[ib];
+          q.w[q.n] = (ca && cb) ? 1.0 : 0.5;
+          ++q.n;
+        }
+        rec[(size_t)A * N + B] = (int)recs.size();
+        recs.push_back(q);
+      }
+    upload(pair_rec_d, rec, st);
+    upload(recs_d, recs, st);
+  }
   struct LaneSync {  // destroyed first: no lane work is pending when the buffers above are released
     std::deque<Lane> &l;
     ~LaneSync() {
@@ -772,8 +817,8 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
     join();
     k_dc_fermi<<<1, 1024, 0, st>>>(n_states, se.p, sw.p, n_elec, dc.fermi_width_ev, scal.p + 1);
     note_launch();
-    // reassembly (src/dandc/mod.rs:354-393): V^T diag(f) V per subsystem on the lanes, then the
-    // weighted scatter into the global density in subsystem order on the main stream
+    // reassembly (src/dandc/mod.rs:354-393): V^T diag(f) V per subsystem on the lanes, then every
+    // stored element of the global density gathers its (at most two) weighted contributions
     fork();
     for (size_t a = 0; a < subs.size(); ++a) {
       DcSub &s = *subs[a];
@@ -795,20 +840,11 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
       }
     }
     join();
-    for (int spin = 0; spin < (unrestricted ? 2 : 1); ++spin) {
-      double *target = spin ? Ns.p : Nx.p;
-      for (size_t a = 0; a < subs.size(); ++a) {
-        DcSub &s = *subs[a];
-        if (s.nao == 0) continue;
-        k_dc_scatter<<<grid_for((size_t)s.nao * s.nao), 256, 0, st>>>(
-            s.nao, s.core_ao, s.map.p, Dm.p + (spin ? dm_off.back() : 0) + dm_off[a], nao_g, target);
-        note_launch();
-      }
-    }
-    k_dc_finish<<<kDcPartials, 256, 0, st>>>(nao_g, N, ao_atom.p, wdev.p, dc.mixing, Pg.p, Nx.p,
-                                             unrestricted ? Sg.p : nullptr, unrestricted ? Ns.p : nullptr, partials.p);
+    k_dc_assemble<<<kDcAssembleBlocks, 256, 0, st>>>(nao_g, N, ao_atom.p, aoff.p, pair_rec_d.p, recs_d.p, Dm.p,
+                                               unrestricted ? Dm.p + dm_off.back() : nullptr, dc.mixing, Pg.p,
+                                               unrestricted ? Sg.p : nullptr, partials.p);
     note_launch();
-    launch_sum(st, partials.p, kDcPartials, scal.p);
+    launch_sum(st, partials.p, kDcAssembleBlocks, scal.p);
   };
   struct Graphs {
     cudaGraphExec_t pre = nullptr, post = nullptr;
