@@ -630,7 +630,7 @@ def run_dandc_bench(args, world, rank, local):
     from pm7b200 import api
     from pm7b200 import geometry as G
 
-    z, x = G.flat_alkane(640)
+    z, x = G.flat_alkane(args.dandc_carbons)
     dc = dict(buffer=15.0, core_size=8, p_tol=1.0e-7, max_scf=400)
     opts = dict(e_tol=1.0e-10, p_tol=1.0e-8, max_scf=400, device=local, want_matrices=0)
     for _ in range(args.warmup):
@@ -664,13 +664,13 @@ def run_dandc_bench(args, world, rank, local):
         scale = len(z) / len(zc)  # the method is linear in the atom count at a fixed buffer
         cpu = {"value": 1.0 / (tc * scale), "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"the oracle's D&C of C160H322 ({len(zc)} atoms, {o['iterations']} iterations, "
-                         f"{tc:.1f} s) scaled by the atom ratio {scale:.2f} to the 1,922-atom chain"}
+                         f"{tc:.1f} s) scaled by the atom ratio {scale:.2f} to the {len(z)}-atom chain"}
     n = len(z)
     line = {
         "metric": "PM7 divide-and-conquer SCF solves/s", "value": world * args.steps / wall, "unit": "solves/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic", "dtype": "f64",
-        "config": {"workload": "dandc640", "atoms": n, "nao": int(r["nao"]), "buffer_bohr": 15.0, "core_size": 8,
+        "config": {"workload": f"dandc{args.dandc_carbons}", "atoms": n, "nao": int(r["nao"]), "buffer_bohr": 15.0, "core_size": 8,
                    "subsystems": r["subsystems"], "largest_subsystem": r["largest_subsystem"],
                    "iterations": r["iterations"], "converged": r["converged"],
                    "stored_density_elements": r["stored_density_elements"], "parallelism": f"replicas{world}",
@@ -694,6 +694,7 @@ def main():
     ap.add_argument("--workload", default="water334",
                     choices=["water334", "water1000", "decane", "batch4096", "stream", "dandc640"])
     ap.add_argument("--stream-count", type=int, default=600)
+    ap.add_argument("--dandc-carbons", type=int, default=640, help="dandc640: chain length (small cases for profiles)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="batch4096/stream: fp64, or fp32 tcgen05 purification cycles with fp64 refinement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
