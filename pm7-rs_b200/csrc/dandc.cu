@@ -547,7 +547,7 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
   env.alloc(std::max(largest_atoms, 1), st);
   for (auto &sp : subs) {
     DcSub &s = *sp;
-    build_device_molecule(s.D, s.m, s.L, P, s.L.has_d, st);
+    build_device_molecule(s.D, s.m, s.L, P, s.L.has_d, st, false);
     std::vector<int> map(s.nao), par(s.nao);
     for (int i = 0; i < s.m.n; ++i)
       for (int mu = 0; mu < s.L.norb[i]; ++mu) {
@@ -578,6 +578,16 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
     s.bucket = (int)(it - buckets.begin());
     s.slot = it->count;
     it->count += chan;
+  }
+  {
+    // the builds were queued without waiting: one synchronisation for all their statuses
+    std::vector<int> status(subs.size(), 0);
+    for (size_t a = 0; a < subs.size(); ++a)
+      CUDA_OK(cudaMemcpyAsync(&status[a], subs[a]->D.status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaGetLastError());
+    for (int x : status)
+      if (x != 0) throw Failure{PM7_ERR_UNSUPPORTED, "a pair's shells are outside the sp-frame integral kernels"};
   }
   for (DcBucket &b : buckets) {
     b.A.alloc((size_t)b.count * b.np * b.np, st);

@@ -269,7 +269,7 @@ __global__ void k_fill_mask(int n_near, int n_atoms, const NearPair *np, unsigne
 // `dpath`: the molecule has a d-shell atom (or the caller forced it), so every pair is
 // evaluated in the MNDO/d frame (hamiltonian.rs:346-355).
 void build_device_molecule(DeviceMolecule &D, const Molecule &m, const Layout &L, const DeviceParams &P,
-                                  bool dpath, cudaStream_t st) {
+                                  bool dpath, cudaStream_t st, bool wait) {
   D.st = st;
   D.n = m.n;
   D.nao = L.nao;
@@ -310,6 +310,7 @@ void build_device_molecule(DeviceMolecule &D, const Molecule &m, const Layout &L
                     L.nao, D.H.p);
   if (m.n >= 2) launch_sum_partials(st, D.cc_partial.p, np, D.scal.p);
   else CUDA_OK(cudaMemsetAsync(D.scal.p, 0, sizeof(double), st));
+  if (!wait) return;  // the caller reads D.status and D.scal[0] itself
   int status = 0;
   double cc = 0.0;
   CUDA_OK(cudaMemcpyAsync(&status, D.status.p, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -282,9 +282,11 @@ struct DeviceMolecule {
   }
 };
 // Uploads m / L and evaluates every pair's integrals, H_core and the core-core energy;
-// `dpath` selects the MNDO/d frame for every pair (hamiltonian.rs:346-355).
+// `dpath` selects the MNDO/d frame for every pair (hamiltonian.rs:346-355). With `wait` false
+// the call only queues the work: D.status (nonzero: a pair outside the sp-frame kernels) and
+// D.scal[0] (the core-core energy) are then the caller's to read.
 void build_device_molecule(DeviceMolecule &D, const Molecule &m, const Layout &L, const DeviceParams &P, bool dpath,
-                           cudaStream_t st);
+                           cudaStream_t st, bool wait = true);
 
 // Nuclear gradient (eV/Bohr, 3 per atom) of a molecule on the device at the density g.Pt / g.Ps
 // (engine.cu); g.E and g.status are provided by the call.
