@@ -22,7 +22,9 @@
 #include <cstring>
 #include <deque>
 #include <functional>
+#include <exception>
 #include <memory>
+#include <thread>
 #include <unordered_map>
 
 #include "common.cuh"
@@ -421,6 +423,20 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
                     const pm7_dandc_options *dco, int want_gradient, pm7_dandc_result *res) {
   if (!mol || !params || !opt || !dco || !res) throw Failure{PM7_ERR_INVALID_INPUT, "null argument"};
   const auto t_start = std::chrono::steady_clock::now();
+  // PM7_DANDC_TRACE: setup sub-phases and per-phase iteration times on stderr (phases then end
+  // in a synchronise)
+  const bool trace = std::getenv("PM7_DANDC_TRACE") != nullptr;
+  std::string setup_marks;
+  auto t_mark = t_start;
+  auto mark = [&](const char *what, cudaStream_t sync_st) {
+    if (!trace) return;
+    if (sync_st) cudaStreamSynchronize(sync_st);
+    const auto now = std::chrono::steady_clock::now();
+    char buf[64];
+    std::snprintf(buf, sizeof buf, " %s %.1f", what, std::chrono::duration<double, std::milli>(now - t_mark).count());
+    setup_marks += buf;
+    t_mark = now;
+  };
   const pm7_options &o = *opt;
   const pm7_dandc_options &dc = *dco;
   Molecule m = to_molecule(mol);
@@ -445,13 +461,32 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
       s->m.z.push_back(m.z[a]);
       for (int k = 0; k < 3; ++k) s->m.xyz.push_back(m.xyz[3 * a + k]);
     }
-    s->L = build_layout(s->m, ps);
+    subs.push_back(std::move(s));
+  }
+  {
+    // the subsystems' layouts (pair lists, AO offsets) are independent host work: a few threads
+    const int workers = (int)std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 16);
+    std::vector<std::exception_ptr> errs(workers);
+    std::vector<std::thread> pool;
+    for (int w = 0; w < workers; ++w)
+      pool.emplace_back([&, w] {
+        try {
+          for (size_t a = (size_t)w; a < subs.size(); a += (size_t)workers) subs[a]->L = build_layout(subs[a]->m, ps);
+        } catch (...) {
+          errs[w] = std::current_exception();
+        }
+      });
+    for (std::thread &t : pool) t.join();
+    for (auto &e : errs)
+      if (e) std::rethrow_exception(e);
+  }
+  for (auto &sp : subs) {
+    DcSub *s = sp.get();
     s->nao = s->L.nao;
     s->core_ao = s->part.n_core < s->m.n ? s->L.aoff[s->part.n_core] : s->nao;
     s->np = dc_bucket(s->nao);
     largest_atoms = std::max(largest_atoms, s->m.n);
     largest_nao = std::max(largest_nao, s->nao);
-    subs.push_back(std::move(s));
   }
   const bool unrestricted =
       o.reference == PM7_REF_UNRESTRICTED || (o.reference == PM7_REF_AUTO && o.multiplicity > 1);
@@ -476,6 +511,7 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
                         " orbitals. Reduce the buffer, or drop divide and conquer and use the exact SCF."};
   }
 
+  mark("layouts", nullptr);
   // the stored pattern and the realised weight totals, in half units (0, 1 or 2: a pair is
   // weighted only by the subsystems whose core holds one of its atoms)
   std::vector<unsigned char> wcnt((size_t)N * N, 0);
@@ -501,6 +537,7 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
     throw Failure{PM7_ERR_INVALID_INPUT, "the divide-and-conquer driver was given a system with negative electron count"};
   const double n_beta_extra = (o.multiplicity - 1) * 0.5;
 
+  mark("pattern", nullptr);
   DeviceContext &ctx = context_for(o.device);
   std::lock_guard<std::mutex> lock(ctx.run_mutex);
   CUDA_OK(cudaSetDevice(ctx.device));
@@ -527,18 +564,23 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
     // atomic-density start on the diagonal blocks (src/dandc/mod.rs:289-301); the spin density
     // starts as a scaled copy of the total's diagonal (:302-323)
     std::vector<double> diag = sad_diag(m, Lg, ps, n_elec);
-    std::vector<double> h(nng, 0.0);
-    for (int k = 0; k < nao_g; ++k) h[(size_t)k * nao_g + k] = diag[k];
-    upload(Pg, h, st);
+    DevBuf<double> dd;
+    upload(dd, diag, st);
+    Pg.alloc(nng, st);
+    launch_set_diag(st, nao_g, dd.p, Pg.p);  // zero, then the diagonal
     if (unrestricted) {
       const double scale = core_e > 0.0 ? 2.0 * n_beta_extra / core_e : 0.0;
-      for (int k = 0; k < nao_g; ++k) h[(size_t)k * nao_g + k] = scale * diag[k];
-      upload(Sg, h, st);
+      for (double &v : diag) v *= scale;
+      DevBuf<double> ds;
+      upload(ds, diag, st);
+      Sg.alloc(nng, st);
+      launch_set_diag(st, nao_g, ds.p, Sg.p);
     }
   }
   if (N > 0) k_dc_coulomb<<<(N + 3) / 4, 128, 0, st>>>(N, xyz.p, q.p, gnuc.p);
   note_launch();
 
+  mark("globals", st);
   // subsystems: device molecules, AO maps, the nuclear environment folded into H once
   int max_nao = 0, max_np = 0;
   size_t n_states = 0;
@@ -580,6 +622,7 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
     it->count += chan;
   }
   {
+    mark("builds_queued", nullptr);
     // the builds were queued without waiting: one synchronisation for all their statuses
     std::vector<int> status(subs.size(), 0);
     for (size_t a = 0; a < subs.size(); ++a)
@@ -658,6 +701,7 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
   econ.alloc(std::max<size_t>(subs.size(), 1), st);
   se.alloc(std::max<size_t>(n_states, 1), st);
   sw.alloc(std::max<size_t>(n_states, 1), st);
+  mark("builds_done+lanes", st);
   // the contributions of every stored atom pair (see DcPairSrc), indexed by an N x N table
   DevBuf<int> pair_rec_d;
   DevBuf<DcPairSrc> recs_d;
@@ -677,9 +721,20 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
     };
     std::vector<int> rec((size_t)N * N, -1);
     std::vector<DcPairSrc> recs;
-    for (int A = 0; A < N; ++A)
-      for (int B = 0; B < N; ++B) {
-        if (!wcnt[(size_t)A * N + B]) continue;
+    // the stored pairs are exactly the (core, member) pairs of the subsystems, both ways round
+    std::vector<std::pair<int, int>> stored_pairs;
+    for (const auto &sp : subs) {
+      const auto &par = sp->part.parent;
+      for (int i = 0; i < sp->part.n_core; ++i)
+        for (int j = 0; j < (int)par.size(); ++j) {
+          stored_pairs.emplace_back(par[i], par[j]);
+          stored_pairs.emplace_back(par[j], par[i]);
+        }
+    }
+    for (const auto &ab : stored_pairs) {
+      const int A = ab.first, B = ab.second;
+      if (rec[(size_t)A * N + B] >= 0) continue;
+      {
         DcPairSrc q{};
         const int sa = core_of[A], sb = core_of[B];
         for (int sub : {sa, sb}) {
@@ -699,9 +754,11 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
         rec[(size_t)A * N + B] = (int)recs.size();
         recs.push_back(q);
       }
+    }
     upload(pair_rec_d, rec, st);
     upload(recs_d, recs, st);
   }
+  mark("pair_table", st);
   struct LaneSync {  // destroyed first: no lane work is pending when the buffers above are released
     std::deque<Lane> &l;
     ~LaneSync() {
@@ -881,7 +938,6 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
     note_launch(nodes);
   };
   // PM7_DANDC_TRACE: per-phase wall times on stderr (each phase then ends in a synchronise)
-  const bool trace = std::getenv("PM7_DANDC_TRACE") != nullptr;
   double t_phase[4] = {0, 0, 0, 0};
   auto tick = [&](int k, std::chrono::steady_clock::time_point &t) {
     if (!trace) return;
@@ -956,8 +1012,9 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
   }
 
   if (trace)
-    std::fprintf(stderr, "pm7_run_dandc ms: setup %.1f fock %.1f eigen %.1f reassembly %.1f (%d iterations, %zu buckets)\n",
-                 t_setup, t_phase[1], t_phase[2], t_phase[3], iterations, buckets.size());
+    std::fprintf(stderr,
+                 "pm7_run_dandc ms: setup %.1f (%s) fock %.1f eigen %.1f reassembly %.1f (%d iterations, %zu buckets)\n",
+                 t_setup, setup_marks.c_str(), t_phase[1], t_phase[2], t_phase[3], iterations, buckets.size());
   // energy, charges and (on request) the gradient at the divide-and-conquer density
   DeviceMolecule Dg;
   build_device_molecule(Dg, m, Lg, P, Lg.has_d, st);
