@@ -61,6 +61,25 @@ def test_large_subsystems_take_the_per_matrix_solver_and_stay_exact():
     assert np.abs(d["charges"] - exact["charges"]).max() < 1e-6
 
 
+@pytest.mark.parametrize("method", [1, 3, 4])
+def test_method_variants_match_the_oracle(method):
+    # PM7-TS, PM7-minus (no corrections), PM7-HH (its H-H repulsion term)
+    z, x = G.flat_alkane(8)
+    dc = dict(buffer=10.0, core_size=6, p_tol=1e-8, max_scf=400)
+    d = api.run_dandc(z, x, dandc=dc, gradient=False, method=method, **OPTS)
+    o = harness.run_dandc(z, x, dandc=dc, method=method, **OPTS)
+    _compare(d, o)
+
+
+def test_smooth_dispersion_matches_the_oracle():
+    z, x = G.water_cluster(12, seed=4)
+    dc = dict(buffer=9.0, core_size=9, p_tol=1e-8, max_scf=400)
+    d = api.run_dandc(z, x, dandc=dc, gradient=True, smooth_dispersion=1, **OPTS)
+    o = harness.run_dandc(z, x, dandc=dc, gradient=True, smooth_dispersion=1, **OPTS)
+    _compare(d, o)
+    assert np.abs(d["gradient"] - o["gradient"]).max() < 1e-5 + 1e-6 * np.abs(o["gradient"]).max()
+
+
 def test_water_cluster_matches_the_oracle():
     z, x = G.water_cluster(40, seed=1)
     dc = dict(buffer=10.0, core_size=12, p_tol=1e-8, max_scf=400)
