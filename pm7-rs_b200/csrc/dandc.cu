@@ -6,8 +6,10 @@
 // small device molecule of its own: its pair integrals and core Hamiltonian are built once by
 // the engine's build kernels, and every iteration runs one Fock build on it (the engine's Fock
 // kernel on the global density restricted to the subsystem). The subsystem Fock matrices are
-// padded into size buckets and diagonalised together (cuSOLVER XsyevBatched below order 512,
-// dsyevd above). One Fermi level for the whole molecule is found by bisection in a single
+// padded into size buckets and diagonalised together: up to order 112 by a shared-memory Jacobi
+// kernel (one block per matrix, warm-started from the previous iteration's eigenvectors), above
+// that by cuSOLVER (XsyevBatched below order 512, dsyevd above). One Fermi level for the whole
+// molecule is found by bisection in a single
 // thread block; each subsystem's Fermi-weighted density (V^T diag(f) V on the FP64 tensor
 // cores) is scattered with the Dixon-Merz weights into a global density kept dense in HBM
 // (zeros outside the stored atom-pair pattern: a 180 GB device holds it at any size this
