@@ -167,3 +167,21 @@ def test_memory_budget_names_the_buffer():
     with pytest.raises(api.Pm7Error) as e:
         api.run_dandc(z, x, dandc=dict(buffer=30.0, core_size=6), max_memory_mb=1)
     assert e.value.code == 1 and "buffer" in e.value.message
+
+
+def test_no_chemical_potential_is_an_error_naming_the_spectrum():
+    z = np.array([1, 1], dtype=np.uint8)
+    x = np.array([[0.0, 0.0, 0.0], [1.4, 0.0, 0.0]])
+    with pytest.raises(api.Pm7Error) as e:
+        api.run_dandc(z, x, dandc=dict(buffer=10.0, core_size=1), charge=-10.0)
+    assert e.value.code == 1 and "no chemical potential" in e.value.message and "spectra span" in e.value.message
+
+
+def test_single_atom_and_sparkle_free_edge_cases():
+    z = np.array([8], dtype=np.uint8)
+    x = np.zeros((1, 3))
+    dc = dict(buffer=10.0, core_size=4, p_tol=1e-8, max_scf=400)
+    d = api.run_dandc(z, x, dandc=dc, gradient=True, charge=-2.0, **OPTS)
+    o = harness.run_dandc(z, x, dandc=dc, charge=-2.0, **OPTS)
+    _compare(d, o)
+    assert d["subsystems"] == 1 and np.abs(d["gradient"]).max() < 1e-12

@@ -118,3 +118,12 @@ def test_invalid_options_are_refused(bad, text):
     with pytest.raises(harness.OracleError) as e:
         harness.run_dandc(z, x, dandc=bad)
     assert text in str(e.value)
+
+
+def test_no_chemical_potential_is_an_error_naming_the_spectrum():
+    # src/dandc/mod.rs:741-757: more electrons than the subsystem states hold
+    z = np.array([1, 1], dtype=np.uint8)
+    x = np.array([[0.0, 0.0, 0.0], [1.4, 0.0, 0.0]])
+    with pytest.raises(harness.OracleError) as e:
+        harness.run_dandc(z, x, dandc=dict(buffer=10.0, core_size=1), charge=-10.0)
+    assert "no chemical potential" in str(e.value) and "spectra span" in str(e.value)
