@@ -416,6 +416,14 @@ pm7_status pm7_run_dandc(const pm7_molecule *molecule, const pm7_params *params,
                          int32_t want_gradient, pm7_dandc_result *result);
 void pm7_dandc_result_free(pm7_dandc_result *result);
 
+/* The subsystem partition of pm7_run_dandc alone (host only, no device), for parity tests of
+ * `partition` (src/dandc/partition.rs): core_of[atom] = the subsystem whose core holds the atom,
+ * sizes[s] = atoms of subsystem s (core and buffer; sizes holds n_atoms entries), the count of
+ * subsystems and of stored atom pairs (ordered, the diagonal included). */
+pm7_status pm7_stage_dandc_partition(const pm7_molecule *molecule, int32_t core_size, double buffer,
+                                     int32_t *core_of, int32_t *sizes, int32_t *n_subsystems,
+                                     int64_t *stored_pairs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -438,6 +438,36 @@ pm7_status pm7_oracle_run_dandc(const pm7_molecule *m, const pm7_options *o, con
   }
 }
 
+// The oracle's partition, in the layout of pm7_stage_dandc_partition.
+pm7_status pm7_oracle_dandc_partition(const pm7_molecule *m, int32_t core_size, double buffer, int32_t *core_of,
+                                      int32_t *sizes, int32_t *n_subsystems, int64_t *stored_pairs) {
+  try {
+    const Molecule mol = to_molecule(m);
+    const std::vector<Part> parts = partition(mol, core_size, buffer);
+    const int n = mol.size();
+    std::vector<unsigned char> seen((size_t)n * n, 0);
+    int64_t pairs = 0;
+    for (size_t a = 0; a < parts.size(); ++a) {
+      const Part &p = parts[a];
+      sizes[a] = (int32_t)p.parent.size();
+      for (int i = 0; i < p.n_core; ++i) core_of[p.parent[i]] = (int32_t)a;
+      for (int i = 0; i < (int)p.parent.size(); ++i)
+        for (int j = 0; j < (int)p.parent.size(); ++j)
+          if (p.weight(i, j) > 0.0) {
+            unsigned char &v = seen[(size_t)p.parent[i] * n + p.parent[j]];
+            pairs += v == 0;
+            v = 1;
+          }
+    }
+    *n_subsystems = (int32_t)parts.size();
+    *stored_pairs = pairs;
+    return PM7_OK;
+  } catch (const std::exception &e) {
+    g_error = e.what();
+    return PM7_ERR_INVALID_INPUT;
+  }
+}
+
 void pm7_oracle_dandc_result_free(pm7_dandc_result *r) {
   if (!r) return;
   std::free(r->charges);

@@ -64,6 +64,8 @@ def lib():
     L.pm7_oracle_run_dandc.argtypes = [C.POINTER(abi.Molecule), C.POINTER(abi.Options), C.POINTER(abi.DandcOptions),
                                        C.POINTER(abi.DandcResult)]
     L.pm7_oracle_dandc_result_free.argtypes = [C.POINTER(abi.DandcResult)]
+    L.pm7_oracle_dandc_partition.argtypes = [C.POINTER(abi.Molecule), C.c_int32, C.c_double, C.POINTER(C.c_int32),
+                                             C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
     L.pm7_oracle_correction_gradient.argtypes = [C.POINTER(abi.Molecule), C.c_int, C.c_int, C.c_double, abi.DP]
     libs = sorted(glob.glob(os.path.join(os.path.dirname(np.__file__) + ".libs", "libscipy_openblas64_*.so")))
     if libs:
@@ -233,6 +235,22 @@ def gradient(z, xyz_bohr, step=1.0e-3, corr_step=1.0e-5, **options):
     g = g + correction_gradient(z, xyz_bohr, method=method, smooth=options.get("smooth_dispersion", False),
                                 step=corr_step)
     return r, g
+
+
+def dandc_partition(z, xyz_bohr, core_size=12, buffer=15.0):
+    """The oracle's divide-and-conquer partition (src/dandc/partition.rs): (core_of, sizes,
+    stored atom pairs), in the layout of the engine's pm7_stage_dandc_partition."""
+    m = _Mol(z, xyz_bohr)
+    n = len(m.z)
+    core_of = np.zeros(n, dtype=np.int32)
+    sizes = np.zeros(max(n, 1), dtype=np.int32)
+    count = C.c_int32()
+    pairs = C.c_int64()
+    _check(lib().pm7_oracle_dandc_partition(C.byref(m.s), int(core_size), float(buffer),
+                                            core_of.ctypes.data_as(C.POINTER(C.c_int32)),
+                                            sizes.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(count),
+                                            C.byref(pairs)))
+    return core_of, sizes[:count.value].copy(), pairs.value
 
 
 def run_dandc(z, xyz_bohr, dandc=None, gradient=False, step=1.0e-3, corr_step=1.0e-5, **options):

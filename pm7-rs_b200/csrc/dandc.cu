@@ -1300,6 +1300,41 @@ pm7_status pm7_run_dandc(const pm7_molecule *molecule, const pm7_params *params,
   }
 }
 
+pm7_status pm7_stage_dandc_partition(const pm7_molecule *molecule, int32_t core_size, double buffer, int32_t *core_of,
+                                     int32_t *sizes, int32_t *n_subsystems, int64_t *stored_pairs) {
+  try {
+    if (!molecule || !core_of || !sizes || !n_subsystems || !stored_pairs)
+      throw Failure{PM7_ERR_INVALID_INPUT, "null argument"};
+    if (core_size <= 0 || !(buffer > 0.0)) throw Failure{PM7_ERR_INVALID_INPUT, "invalid core size or buffer"};
+    const Molecule m = to_molecule(molecule);
+    const std::vector<DcPart> parts = dc_partition(m, core_size, buffer);
+    std::vector<unsigned char> seen((size_t)m.n * m.n, 0);
+    int64_t pairs = 0;
+    for (size_t a = 0; a < parts.size(); ++a) {
+      const DcPart &p = parts[a];
+      sizes[a] = (int32_t)p.parent.size();
+      for (int i = 0; i < p.n_core; ++i) core_of[p.parent[i]] = (int32_t)a;
+      for (int i = 0; i < (int)p.parent.size(); ++i)
+        for (int j = 0; j < (int)p.parent.size(); ++j) {
+          if (i >= p.n_core && j >= p.n_core) continue;
+          unsigned char &v = seen[(size_t)p.parent[i] * m.n + p.parent[j]];
+          pairs += v == 0;
+          v = 1;
+        }
+    }
+    *n_subsystems = (int32_t)parts.size();
+    *stored_pairs = pairs;
+    g_last_error.clear();
+    return PM7_OK;
+  } catch (const Failure &f) {
+    g_last_error = f.msg;
+    return f.code;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return PM7_ERR_INVALID_INPUT;
+  }
+}
+
 void pm7_dandc_result_free(pm7_dandc_result *r) {
   if (!r) return;
   std::free(r->charges);

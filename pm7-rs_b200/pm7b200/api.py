@@ -25,7 +25,7 @@ EXPORTED = [
     "pm7_engine_poll", "pm7_engine_destroy", "pm7_batch_partition", "pm7_stage_eigenvalues",
     "pm7_stage_product_tf32", "pm7_autotune_report", "pm7_gradient", "pm7_fixed_density_gradient",
     "pm7_correction_gradient", "pm7_run_batch_gradient", "pm7_engine_submit_gradient",
-    "pm7_dandc_options_default", "pm7_run_dandc", "pm7_dandc_result_free",
+    "pm7_dandc_options_default", "pm7_run_dandc", "pm7_dandc_result_free", "pm7_stage_dandc_partition",
 ]
 
 
@@ -78,6 +78,8 @@ def lib():
     L.pm7_run_dandc.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, C.POINTER(abi.Options),
                                 C.POINTER(abi.DandcOptions), C.c_int32, C.POINTER(abi.DandcResult)]
     L.pm7_dandc_result_free.argtypes = [C.POINTER(abi.DandcResult)]
+    L.pm7_stage_dandc_partition.argtypes = [C.POINTER(abi.Molecule), C.c_int32, C.c_double, C.POINTER(C.c_int32),
+                                            C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
     L.pm7_stage_eigenvalues.argtypes = [C.c_int32, C.POINTER(C.c_int32), abi.DP, abi.DP, C.c_int32]
     L.pm7_engine_config_default.argtypes = [C.POINTER(abi.EngineConfig)]
     L.pm7_engine_create.argtypes = [C.POINTER(abi.EngineConfig), C.POINTER(C.c_void_p)]
@@ -226,6 +228,22 @@ def run_dandc(z, xyz_bohr, dandc=None, gradient=True, **options):
         return dandc_result_to_dict(r)
     finally:
         lib().pm7_dandc_result_free(C.byref(r))
+
+
+def dandc_partition(z, xyz_bohr, core_size=12, buffer=15.0):
+    """The subsystem partition `pm7_run_dandc` uses (host only): (core_of per atom, sizes per
+    subsystem, stored atom pairs)."""
+    m = _Mol(z, xyz_bohr)
+    n = len(m.z)
+    core_of = np.zeros(n, dtype=np.int32)
+    sizes = np.zeros(max(n, 1), dtype=np.int32)
+    count = C.c_int32()
+    pairs = C.c_int64()
+    _check(lib().pm7_stage_dandc_partition(C.byref(m.s), int(core_size), float(buffer),
+                                           core_of.ctypes.data_as(C.POINTER(C.c_int32)),
+                                           sizes.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(count),
+                                           C.byref(pairs)))
+    return core_of, sizes[:count.value].copy(), pairs.value
 
 
 def dandc(z, xyz_bohr, buffer_angstrom=8.0, core_size=12, method="pm7", charge=0.0, multiplicity=1,
