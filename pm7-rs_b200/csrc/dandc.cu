@@ -885,15 +885,17 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
     std::vector<int> core_of(N, -1), local(N, -1);
     for (size_t a = 0; a < subs.size(); ++a)
       for (int i = 0; i < subs[a]->part.n_core; ++i) core_of[subs[a]->part.parent[i]] = (int)a;
-    // local atom index of every parent atom, per subsystem, filled on demand below
-    std::vector<std::vector<int>> where(subs.size());
+    // local atom index of a parent atom in a subsystem: (atom, local) sorted per subsystem, built
+    // on demand (memory in proportion to the subsystems' sizes, not to N per subsystem)
+    std::vector<std::vector<std::pair<int, int>>> where(subs.size());
     auto local_of = [&](int a, int atom) {
-      std::vector<int> &w = where[a];
+      std::vector<std::pair<int, int>> &w = where[a];
       if (w.empty()) {
-        w.assign(N, -1);
-        for (int i = 0; i < subs[a]->m.n; ++i) w[subs[a]->part.parent[i]] = i;
+        for (int i = 0; i < subs[a]->m.n; ++i) w.emplace_back(subs[a]->part.parent[i], i);
+        std::sort(w.begin(), w.end());
       }
-      return w[atom];
+      const auto it = std::lower_bound(w.begin(), w.end(), std::make_pair(atom, -1));
+      return (it != w.end() && it->first == atom) ? it->second : -1;
     };
     std::vector<int> rec((size_t)N * N, -1);
     std::vector<DcPairSrc> recs;
