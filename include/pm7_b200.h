@@ -388,6 +388,8 @@ typedef struct pm7_dandc_options {
 } pm7_dandc_options;
 
 void pm7_dandc_options_default(pm7_dandc_options *options);
+/* sizeof(pm7_dandc_options), sizeof(pm7_dandc_result): bindings check their mirrors. */
+void pm7_dandc_abi_sizes(int64_t out[2]);
 
 /* `DandcResult` (src/dandc/mod.rs:121-140) with `DandcDerivatives` (:438-443). The global
  * density is returned dense (nao x nao, row-major) with zeros outside the stored atom-pair

@@ -1274,6 +1274,11 @@ using namespace pm7;
 
 extern "C" {
 
+void pm7_dandc_abi_sizes(int64_t out[2]) {
+  out[0] = (int64_t)sizeof(pm7_dandc_options);
+  out[1] = (int64_t)sizeof(pm7_dandc_result);
+}
+
 void pm7_dandc_options_default(pm7_dandc_options *d) {  // src/dandc/mod.rs:70-81
   if (!d) return;
   d->buffer = 15.0;

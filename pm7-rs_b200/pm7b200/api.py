@@ -26,6 +26,7 @@ EXPORTED = [
     "pm7_stage_product_tf32", "pm7_autotune_report", "pm7_gradient", "pm7_fixed_density_gradient",
     "pm7_correction_gradient", "pm7_run_batch_gradient", "pm7_engine_submit_gradient",
     "pm7_dandc_options_default", "pm7_run_dandc", "pm7_dandc_result_free", "pm7_stage_dandc_partition",
+    "pm7_dandc_abi_sizes",
 ]
 
 
@@ -339,6 +340,12 @@ def corrections(z, xyz_bohr, method=0, smooth=False):
 def abi_sizes():
     out = (C.c_int64 * 3)()
     lib().pm7_abi_sizes(out)
+    return tuple(out)
+
+
+def dandc_abi_sizes():
+    out = (C.c_int64 * 2)()
+    lib().pm7_dandc_abi_sizes(out)
     return tuple(out)
 
 

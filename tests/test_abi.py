@@ -34,6 +34,23 @@ def test_struct_layouts_match_the_header():
     assert sizes == (C.sizeof(abi.Molecule), C.sizeof(abi.Options), C.sizeof(abi.Result))
 
 
+def test_dandc_struct_layouts_match_the_header():
+    import ctypes as C
+
+    assert api.dandc_abi_sizes() == (C.sizeof(abi.DandcOptions), C.sizeof(abi.DandcResult))
+
+
+def test_dandc_options_default_matches_reference_defaults():
+    import ctypes as C
+
+    d = abi.DandcOptions()
+    api.lib().pm7_dandc_options_default(C.byref(d))
+    ref = abi.default_dandc_options()
+    for name, _ in abi.DandcOptions._fields_:
+        assert getattr(d, name) == getattr(ref, name), name
+    assert (d.buffer, d.core_size, d.fermi_width_ev, d.max_scf, d.p_tol, d.mixing) == (15.0, 12, 0.1, 200, 1.0e-6, 0.4)
+
+
 def test_options_default_matches_reference_defaults():
     import ctypes as C
 
