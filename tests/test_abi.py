@@ -81,3 +81,26 @@ def test_invalid_molecule_is_rejected_before_any_device_work():
         api.run_pm7(np.array([1, 1], dtype=np.uint8), np.zeros((2, 3)))
     assert info.value.code == 1
     assert "same position" in api.lib().pm7_last_error_message().decode()
+
+
+def test_divide_and_conquer_refuses_bad_options_before_any_device_work():
+    # option checks (src/dandc/mod.rs:83-110) come before the device is touched
+    from pm7b200 import geometry as G
+
+    z, x = G.flat_alkane(2)
+    with pytest.raises(api.Pm7Error) as e:
+        api.run_dandc(z, x, dandc=dict(buffer=-1.0))
+    assert e.value.code == 1 and "buffer" in e.value.message
+
+
+def test_without_a_device_the_divide_and_conquer_call_fails_loudly():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    from pm7b200 import geometry as G
+
+    z, x = G.flat_alkane(2)
+    with pytest.raises(api.Pm7Error) as e:
+        api.run_dandc(z, x)
+    assert e.value.code == 9  # PM7_ERR_CUDA: no CPU fallback
