@@ -264,6 +264,14 @@ pm7_status pm7_stage_eigenvalues(int32_t count, const int32_t *orders, const dou
 pm7_status pm7_stage_core_core(const pm7_molecule *molecule, const pm7_params *params,
                                double *energy_ev);
 
+/* The left-to-right f64 sum of n terms, t_i = a[i] (b NULL) or t_i = a[i] * b[i] (each
+ * product rounded, then added), computed on `device` and returned in *out with the exact
+ * bits of a serial loop. This is how the engine evaluates the reference's energy folds
+ * (`Matrix::frobenius_dot`, src/linalg.rs:138-141; the pair-order sum of
+ * `core_core_energy`, src/repulsion.rs:16-36); exposed as a stage for bit-exact tests.
+ * Host buffers. */
+pm7_status pm7_stage_seqsum(int64_t n, const double *a, const double *b, double *out, int32_t device);
+
 /* Post-SCF corrections in kcal/mol (`correction_energy`, src/scf.rs:907-932):
  * out[0] dispersion, out[1] H-bond, out[2] C#C, out[3] Si-O-H, out[4] PM7-HH. */
 pm7_status pm7_stage_corrections(const pm7_molecule *molecule, int32_t method,

@@ -268,6 +268,36 @@ double pair_core_energy(const Element &ei, const Element &ej, int zi, int zj, do
   return enuc + corr;
 }
 
+// Diagnostic only: PM7_ORACLE_EXACT_SUMS=1 replaces the reference's plain sequential sums of
+// the energy (Frobenius products, core-core) by Neumaier's compensated summation, which shows
+// how much of a large system's energy is the rounding of those sums.
+static bool exact_sums() {
+  static const bool on = std::getenv("PM7_ORACLE_EXACT_SUMS") != nullptr;
+  return on;
+}
+
+static double neumaier(const double *t, size_t n) {
+  double s = 0.0, c = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    double x = t[i], u = s + x;
+    c += std::fabs(s) >= std::fabs(x) ? (s - u) + x : (x - u) + s;
+    s = u;
+  }
+  return s + c;
+}
+
+// `Matrix::frobenius_dot` (src/linalg.rs:138-141): a plain left-to-right fold.
+static double frob(const Mat &a, const Mat &b) {
+  if (exact_sums()) {
+    std::vector<double> t(a.a.size());
+    for (size_t i = 0; i < t.size(); ++i) t[i] = a.a[i] * b.a[i];
+    return neumaier(t.data(), t.size());
+  }
+  double s = 0.0;
+  for (size_t i = 0; i < a.a.size(); ++i) s += a.a[i] * b.a[i];
+  return s;
+}
+
 double core_core_energy(const Molecule &mol, const Params &p) {
   int n = mol.size();
   std::vector<double> terms((size_t)n * (n > 0 ? n - 1 : 0) / 2);
@@ -278,6 +308,7 @@ double core_core_energy(const Molecule &mol, const Params &p) {
       terms[base + (j - i - 1)] = pair_core_energy(p.element(mol.z[i]), p.element(mol.z[j]), mol.z[i], mol.z[j],
                                                     (mol.pos[j] - mol.pos[i]).norm(), p);
   }
+  if (exact_sums()) return neumaier(terms.data(), terms.size());
   double s = 0.0;
   for (double t : terms) s += t;
   return s;
@@ -285,11 +316,7 @@ double core_core_energy(const Molecule &mol, const Params &p) {
 
 // ---- SCF helpers (src/scf.rs) ------------------------------------------
 
-static double frob(const Mat &a, const Mat &b) {
-  double s = 0.0;
-  for (size_t i = 0; i < a.a.size(); ++i) s += a.a[i] * b.a[i];
-  return s;
-}
+
 
 // sad_density (src/scf.rs:1050-1114).
 Mat sad_density(const Molecule &mol, const Basis &basis, const Params &p, double n_electrons) {

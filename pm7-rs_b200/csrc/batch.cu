@@ -86,15 +86,25 @@ __global__ void __launch_bounds__(RB) k_b_init(BatchList L, const MolDesc *__res
   }
 }
 
-// Core-core energy of each molecule: its pair-sweep partials in fixed order.
-__global__ void __launch_bounds__(RB) k_b_cc_sum(BatchList L, const MolDesc *__restrict__ D, MolCtl *__restrict__ C) {
-  const int slot = L.slot[blockIdx.x];
-  const MolDesc &d = D[slot];
-  const size_t np = (size_t)d.g.n_atoms * d.cc_nx;
-  double v[1] = {0.0};
-  for (size_t i = threadIdx.x; i < np; i += RB) v[0] += d.cc_partial[i];
-  block_sum_n<1>(v);
-  if (threadIdx.x == 0) C[slot].core_core = d.g.n_atoms >= 2 ? v[0] : 0.0;
+// The two fold jobs of each finished molecule, <P, H> and <P, F> (F = the final Fock in X),
+// from the device descriptors: P and Pn swap on the device, so only D knows the density.
+__global__ void k_b_fold_jobs(int n, const int *__restrict__ slots, const MolDesc *__restrict__ D,
+                              MolCtl *__restrict__ C, SeqSumJob *__restrict__ jobs) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  const MolDesc &d = D[slots[m]];
+  MolCtl &c = C[slots[m]];
+  const size_t nn = (size_t)d.g.nao * d.g.nao;
+  jobs[2 * m] = {d.P, d.H, nn, &c.e_fold[0]};
+  jobs[2 * m + 1] = {d.P, d.X, nn, &c.e_fold[1]};
+}
+
+// e_final = 1/2 (<P, H> + <P, F>) from the two folds of the final density (scf.rs:1297-1298).
+__global__ void k_b_fold_energy(int n, const int *__restrict__ slots, MolCtl *__restrict__ C) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  MolCtl &c = C[slots[m]];
+  c.e_final = 0.5 * (c.e_fold[0] + c.e_fold[1]);
 }
 
 // Make room in the DIIS ring (HistoryHost::push).
@@ -987,7 +997,6 @@ static size_t mol_layout(BatchMol &b, char *base) {
   d.ecore = (double *)take(8 * (size_t)L.e_len);
   d.jbuf = (double *)take(8 * (size_t)L.e_len);
   d.pop = (double *)take(8 * (size_t)n);
-  d.cc_partial = (double *)take(8 * (size_t)n * gx);
   d.eps_out = (double *)take(8 * (size_t)nao);
   d.V_out = b.o.want_matrices ? (double *)take(8 * nn) : nullptr;
   d.atom_out = (double *)take(8 * (size_t)kAtomOut * n);
@@ -1028,6 +1037,7 @@ static size_t mol_layout(BatchMol &b, char *base) {
   d.n_occ = b.n_occ;
   d.dframe = b.dframe;
   d.cc_nx = gx;
+  d.cc_terms = d.X;  // n (n - 1) / 2 <= nao^2 doubles, free until the first SCF step
   d.want_matrices = b.o.want_matrices;
   d.smooth_dispersion = b.o.smooth_dispersion;
   (void)sad;
@@ -1114,6 +1124,7 @@ class BatchRunner {
     cudaStreamSynchronize(eig_st_);
     cudaStreamSynchronize(st_);
     if (rarena_) cudaFree(rarena_);
+    if (fold_scr_) cudaFree(fold_scr_);
     if (desc_) cudaFree(desc_);
     if (ctl_) cudaFree(ctl_);
     if (arena_) cudaFree(arena_);
@@ -1272,8 +1283,13 @@ class BatchRunner {
       if (A.sp_near.total) launch_b_near_integrals(st_, A.sp_near, desc_, *P_);
       if (A.d_near.total) launch_b_near_integrals_d(st_, A.d_near, desc_, *P_);
       launch_b_hcore_diag(st_, A.atoms, desc_, *P_);
-      k_b_cc_sum<<<A.mol.n, RB, 0, st_>>>(A.mol, desc_, ctl_);
-      note_launch();
+      // core-core energies: the pair-order fold of each molecule (repulsion.rs:16-36)
+      std::vector<SeqSumJob> jobs;
+      for (BatchMol *b : in) {
+        const size_t np = (size_t)b->m.n * (b->m.n > 0 ? b->m.n - 1 : 0) / 2;
+        jobs.push_back({b->d.cc_terms, nullptr, np, &ctl_[b->slot].core_core});
+      }
+      queue_folds(jobs, fold_build_up_);
     }
     CUDA_OK(cudaStreamSynchronize(st_));
     CUDA_OK(cudaGetLastError());
@@ -1522,6 +1538,36 @@ class BatchRunner {
     map_stage_.resize(256 * (size_t)cap);
   }
 
+  // Reference-order sums (launch_seqsum_table) of `jobs` on the main stream; the job table
+  // and its chunk offsets go up through `up` (one set in flight per upload buffer).
+  // `fill`, when given, writes the device job table itself (after the upload, before the sums).
+  void queue_folds(const std::vector<SeqSumJob> &jobs, ListUpload &up,
+                   const std::function<void(SeqSumJob *)> &fill = nullptr) {
+    if (jobs.empty()) return;
+    const int count = (int)jobs.size();
+    up.begin();
+    size_t off_jobs, off_first;
+    SeqSumJob *hj = (SeqSumJob *)up.add(sizeof(SeqSumJob) * count, off_jobs);
+    std::memcpy(hj, jobs.data(), sizeof(SeqSumJob) * count);
+    long long *hf = (long long *)up.add(sizeof(long long) * (count + 1), off_first);
+    long long total = 0;
+    for (int j = 0; j < count; ++j) {
+      hf[j] = total;
+      total += (long long)seqsum_chunks(jobs[j].n);
+    }
+    hf[count] = total;
+    char *dev = up.commit(st_);
+    if (fill) fill((SeqSumJob *)(dev + off_jobs));
+    const size_t need = seqsum_table_scratch_bytes(total);
+    if (need > fold_cap_) {
+      if (fold_scr_) CUDA_OK(cudaFreeAsync(fold_scr_, st_));
+      fold_cap_ = need + need / 4;
+      CUDA_OK(cudaMallocAsync(&fold_scr_, fold_cap_, st_));
+    }
+    launch_seqsum_table(st_, (const SeqSumJob *)(dev + off_jobs), (const long long *)(dev + off_first), count,
+                        total, fold_scr_);
+  }
+
   void release(BatchMol &b) {
     if (b.base) cudaFreeAsync(b.base, st_);
     b.base = nullptr;
@@ -1723,7 +1769,7 @@ class BatchRunner {
     const int n = A.mol.n;
     bool vectors = false;
     for (const BatchMol *b : R) vectors = vectors || b->o.want_matrices;
-    finish_scf(A);
+    finish_scf(A, R);
     {
       // reported orbitals: eigenvectors of the last extrapolated Fock, or of the final
       // Fock when a level shift was active (scf.rs:1299-1305)
@@ -1751,13 +1797,24 @@ class BatchRunner {
 
   // Final Fock and energy, corrections and per-atom outputs (the SCF's last step of the
   // finished molecules), on the main stream.
-  void finish_scf(const Lists &A) {
+  void finish_scf(const Lists &A, const std::vector<BatchMol *> &R) {
     const int n = A.mol.n;
     Stage s_(st_, "batch_finish");
     launch_b_fock(st_, A.mol, A.rows, A.near, A.atoms, desc_, ctl_, *P_, 1);
-    k_b_energy_c<<<A.chunks.total, RB, 0, st_>>>(A.chunks, desc_, ctl_, 1);
-    k_b_reduce<<<(n + 127) / 128, 128, 0, st_>>>(n, A.mol.slot, desc_, ctl_, 1);
-    note_launch(2);
+    // the final electronic energy as the reference's two folds (the final Fock is in X); the
+    // job table is filled on the device (the density pointer lives there)
+    std::vector<SeqSumJob> jobs;
+    for (const BatchMol *b : R) {
+      const size_t nn = (size_t)b->L.nao * b->L.nao;
+      jobs.push_back({nullptr, nullptr, nn, nullptr});
+      jobs.push_back({nullptr, nullptr, nn, nullptr});
+    }
+    queue_folds(jobs, fold_retire_up_, [&](SeqSumJob *dev_jobs) {
+      k_b_fold_jobs<<<(n + 127) / 128, 128, 0, st_>>>(n, A.mol.slot, desc_, ctl_, dev_jobs);
+      note_launch();
+    });
+    k_b_fold_energy<<<(n + 127) / 128, 128, 0, st_>>>(n, A.mol.slot, ctl_);
+    note_launch();
     launch_b_corrections(st_, A.mol, A.pairs, desc_, ctl_, method_, A.max_atoms);
     k_b_atom_out<<<n, 128, 0, st_>>>(A.mol, desc_, *P_);
     note_launch();
@@ -1771,7 +1828,7 @@ class BatchRunner {
   void retire_begin(std::vector<BatchMol *> &R) {
     Lists A = lists(R, true, nullptr, true);
     const int n = A.mol.n;
-    finish_scf(A);
+    finish_scf(A, R);
     {
       Stage s_(st_, "batch_orbitals");
       k_b_to_bucket<<<dim3(n, kBucketBlocks), RB, 0, st_>>>(A.mol, desc_, ctl_, A.eig, 2);
@@ -1949,7 +2006,9 @@ class BatchRunner {
   std::vector<int> free_slots_;
   std::vector<BatchMol *> active_;
   size_t bytes_in_use_ = 0;
-  ListUpload up_, up_fallback_, up_sp2_, up_sp32_, ptr_up_;
+  ListUpload up_, up_fallback_, up_sp2_, up_sp32_, ptr_up_, fold_build_up_, fold_retire_up_;
+  void *fold_scr_ = nullptr;  // records of the reference-order sums
+  size_t fold_cap_ = 0;
   char *pin_ = nullptr;
   size_t pin_cap_ = 0;
   double *out_d_ = nullptr;

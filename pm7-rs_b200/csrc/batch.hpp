@@ -23,7 +23,8 @@ struct MolDesc {
   FockGeometry g;            // atoms, AO layout, near pairs, w store, near mask
   int n_occ, dframe, cc_nx;  // cc_nx: column blocks of the core-core sweep (ceil(N/128))
   int want_matrices, smooth_dispersion;
-  double *H, *w, *ecore, *jbuf, *pop, *cc_partial;  // w: writable alias of g.w
+  double *H, *w, *ecore, *jbuf, *pop;  // w: writable alias of g.w
+  double *cc_terms;          // build only: pair core-core energies in pair order (aliases X)
   double *P, *Pn, *X;        // density, next density, scratch (nao^2 each; P/Pn swap on device)
   double *hist;              // kHist x {F, E = FP - PF, D} blocks of nao^2
   double *eps_out, *V_out;   // reported orbital energies (nao) and vectors (nao^2, optional)
@@ -59,6 +60,7 @@ struct MolCtl {
   double sp2_err[3], sp2_emin, sp2_emax;
   // results
   double core_core, e_final, corr[5];
+  double e_fold[2];  // <P, H> and <P, F> of the final density, as the reference's folds
 };
 
 // Where this iteration's eigensolve of a molecule lives (bucket buffers, row k of V =

@@ -297,19 +297,24 @@ void build_device_molecule(DeviceMolecule &D, const Molecule &m, const Layout &L
   D.scal.alloc(8, st);
   D.status.alloc(1, st);
   CUDA_OK(cudaMemsetAsync(D.status.p, 0, sizeof(int), st));
-  const size_t np = pairs_all_partials(m.n);
-  D.cc_partial.alloc(np, st);
+  // the pair energies in pair order, summed as the reference's fold (repulsion.rs:16-36)
+  const size_t npairs = (size_t)m.n * (m.n > 0 ? m.n - 1 : 0) / 2;
+  D.cc_terms.alloc(npairs, st);
+  DevBuf<unsigned char> ss_scratch;
+  ss_scratch.alloc(seqsum_scratch_bytes(npairs, 1), st);
   if (dpath) {
-    launch_pairs_all_d(st, m.n, D.z.p, D.xyz.p, D.aoff.p, L.nao, P, D.H.p, D.cc_partial.p);
+    launch_pairs_all_d(st, m.n, D.z.p, D.xyz.p, D.aoff.p, L.nao, P, D.H.p, D.cc_terms.p);
     launch_near_integrals_d(st, D.n_near, D.z.p, D.xyz.p, D.near.p, P, D.w.p, D.ecore.p);
   } else {
-    launch_pairs_all(st, m.n, D.z.p, D.xyz.p, D.aoff.p, L.nao, P, D.H.p, D.cc_partial.p, D.status.p);
+    launch_pairs_all(st, m.n, D.z.p, D.xyz.p, D.aoff.p, L.nao, P, D.H.p, D.cc_terms.p, D.status.p);
     launch_near_integrals(st, D.n_near, D.z.p, D.xyz.p, D.near.p, P, D.w.p, D.ecore.p, D.status.p);
   }
   launch_hcore_diag(st, m.n, D.z.p, D.xyz.p, D.aoff.p, D.csr_start.p, D.csr.p, D.near.p, D.ecore.p, D.mask.p, P,
                     L.nao, D.H.p);
-  if (m.n >= 2) launch_sum_partials(st, D.cc_partial.p, np, D.scal.p);
-  else CUDA_OK(cudaMemsetAsync(D.scal.p, 0, sizeof(double), st));
+  SeqSumBatch fold{};
+  fold.job[0] = {D.cc_terms.p, nullptr, npairs, D.scal.p};
+  fold.count = 1;
+  launch_seqsum(st, fold, ss_scratch.p);
   if (!wait) return;  // the caller reads D.status and D.scal[0] itself
   int status = 0;
   double cc = 0.0;
@@ -518,6 +523,18 @@ static double host_sum(const DevBuf<double> &partials, size_t count, double *dsc
   return *v;
 }
 
+// The reference's energy folds on the device (scf.rs:1237,1297-1298,1405,1503-1504): one
+// reference-order sum per (density, matrix) pair, d[i] = fold of a[i] * b[i] over nn
+// elements, queued on st. The host adds them left to right, as the reference's
+// expression does.
+static void queue_energy_folds(cudaStream_t st, size_t nn, int count, const double *const *a,
+                               const double *const *b, double *d, void *scratch) {
+  SeqSumBatch B{};
+  for (int i = 0; i < count; ++i) B.job[i] = {a[i], b[i], nn, d + i};
+  B.count = count;
+  launch_seqsum(st, B, scratch);
+}
+
 struct ScfOut {
   bool converged = false;
   int iterations = 0;
@@ -582,6 +599,8 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   const bool accel_on = o.use_diis && o.accelerator != PM7_ACCEL_NONE;
   partials.alloc(std::max<size_t>(((size_t)(n + 31) / 32) * ((n + 31) / 32), 4096), st);
   dscal.alloc(8, st);
+  DevBuf<unsigned char> folds;
+  folds.alloc(seqsum_scratch_bytes(nn, 2), st);
   coef.alloc(kmax + 1, st);
   const int dot_blocks = 296;
   dots.alloc((size_t)dot_blocks * 32, st);
@@ -620,8 +639,15 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     }
     double *Fk = hF[slot].p;
     { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, out.P.p, out.P.p, 0.5, Fk, D.pop.p, D.jbuf.p); }
-    size_t ne = launch_energy(st, nn, out.P.p, D.H.p, Fk, partials.p);
-    launch_sum(st, partials.p, ne, dscal.p + 0);
+    {
+      // <P, H> into dscal[0], <P, F> into dscal[3] (dscal[1], dscal[2] hold the error and step)
+      SeqSumBatch B{};
+      B.job[0] = {out.P.p, D.H.p, nn, dscal.p + 0};
+      B.job[1] = {out.P.p, Fk, nn, dscal.p + 3};
+      B.count = 2;
+      Stage s_(st, "energy_folds");
+      launch_seqsum(st, B, folds.p);
+    }
     CUDA_OK(cudaMemcpyAsync(hD[slot].p, out.P.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
     // DIIS error e = F P - P F = F P - (F P)^T
     if (phase32) {
@@ -657,10 +683,10 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
       launch_reduce_rows(st, dots.p, dot_blocks, k, dotout.p + 32);
     }
     double *sc = reinterpret_cast<double *>(ctx.pinned), *dh = sc + 8;
-    CUDA_OK(cudaMemcpyAsync(sc, dscal.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(sc, dscal.p, sizeof(double) * 4, cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaMemcpyAsync(dh, dotout.p, sizeof(double) * 48, cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
-    const double e_elec = 0.5 * sc[0];
+    const double e_elec = 0.5 * (sc[0] + sc[3]);
     const double err_norm = std::sqrt(sc[1]);
     hist.record(std::vector<double>(dh, dh + k + 1), std::vector<double>(dh + 16, dh + 16 + k + 1),
                 std::vector<double>(dh + 32, dh + 32 + k));
@@ -726,8 +752,14 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   }
   // final Fock and energy at the converged density
   { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, out.P.p, out.P.p, 0.5, F.p, D.pop.p, D.jbuf.p); }
-  size_t ne = launch_energy(st, nn, out.P.p, D.H.p, F.p, partials.p);
-  out.electronic_ev = 0.5 * host_sum(partials, ne, dscal.p, st);
+  {
+    const double *fa[2] = {out.P.p, out.P.p}, *fb[2] = {D.H.p, F.p};
+    queue_energy_folds(st, nn, 2, fa, fb, dscal.p, folds.p);
+    double *sc = reinterpret_cast<double *>(ctx.pinned);
+    CUDA_OK(cudaMemcpyAsync(sc, dscal.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    out.electronic_ev = 0.5 * (sc[0] + sc[1]);
+  }
   // Reported orbitals: the eigenvectors of the last extrapolated Fock, or of the real
   // Fock when a level shift was active (scf.rs:1299-1305); their energies alone when no
   // matrices are returned.
@@ -835,6 +867,8 @@ static void run_uhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   for (DevBuf<double> *b : {&Pa, &Pb, &Pt, &Fa, &Fb, &X, &E, &Ua, &Ub, &Pan, &Pbn}) b->alloc(nn, st);
   partials.alloc(std::max<size_t>(((size_t)(n + 31) / 32) * ((n + 31) / 32), 4096), st);
   dscal.alloc(8, st);
+  DevBuf<unsigned char> folds;
+  folds.alloc(seqsum_scratch_bytes(nn, 3), st);
   const double ntot = std::max(n_alpha + n_beta, 1);
   {
     DevBuf<double> total;
@@ -869,13 +903,11 @@ static void run_uhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   StallGuardHost guard(o.level_shift);
   const bool trace = std::getenv("PM7_SCF_TRACE") != nullptr;
   double e_old = 0.0;
+  // <Pt, H>, <Pa, Fa>, <Pb, Fb> into dscal[0..3), as the reference's folds
   auto energy = [&](const double *pt, const double *pa, const double *fa, const double *pb, const double *fb) {
-    size_t c1 = launch_dot(st, nn, pt, D.H.p, partials.p);
-    launch_sum(st, partials.p, c1, dscal.p + 0);
-    c1 = launch_dot(st, nn, pa, fa, partials.p);
-    launch_sum(st, partials.p, c1, dscal.p + 1);
-    c1 = launch_dot(st, nn, pb, fb, partials.p);
-    launch_sum(st, partials.p, c1, dscal.p + 2);
+    const double *xa[3] = {pt, pa, pb}, *xb[3] = {D.H.p, fa, fb};
+    Stage s_(st, "energy_folds");
+    queue_energy_folds(st, nn, 3, xa, xb, dscal.p, folds.p);
   };
   for (int iter = 0; iter < o.max_scf; ++iter) {
     out.iterations = iter + 1;
@@ -1743,6 +1775,33 @@ pm7_status pm7_stage_core_core(const pm7_molecule *molecule, const pm7_params *p
     DeviceMolecule D;
     build_device_molecule(D, m, L, P, L.has_d, ctx.stream);
     *energy_ev = D.core_core_ev;
+  });
+}
+
+pm7_status pm7_stage_seqsum(int64_t n, const double *a, const double *b, double *out, int32_t device) {
+  return guarded([&] {
+    if (n < 0 || !out || (n > 0 && !a)) throw Failure{PM7_ERR_INVALID_INPUT, "seqsum: bad length or null arrays"};
+    DeviceContext &ctx = context_for(device);
+    std::lock_guard<std::mutex> lock(ctx.run_mutex);
+    CUDA_OK(cudaSetDevice(ctx.device));
+    cudaStream_t st = ctx.stream;
+    DevBuf<double> A, B, R;
+    DevBuf<unsigned char> scratch;
+    A.alloc((size_t)n, st);
+    if (n > 0) CUDA_OK(cudaMemcpyAsync(A.p, a, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    if (b) {
+      B.alloc((size_t)n, st);
+      if (n > 0) CUDA_OK(cudaMemcpyAsync(B.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    }
+    R.alloc(1, st);
+    scratch.alloc(seqsum_scratch_bytes((size_t)n, 1), st);
+    SeqSumBatch job{};
+    job.job[0] = {A.p, b ? B.p : nullptr, (size_t)n, R.p};
+    job.count = 1;
+    launch_seqsum(st, job, scratch.p);
+    CUDA_OK(cudaMemcpyAsync(out, R.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaGetLastError());
   });
 }
 

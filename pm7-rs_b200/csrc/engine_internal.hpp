@@ -255,7 +255,7 @@ struct DeviceMolecule {
   cudaStream_t st;
   int n = 0, nao = 0, n_near = 0;
   DevBuf<int> z, aoff, ao_atom, csr_start, csr_eoff;
-  DevBuf<double> xyz, H, w, ecore, jbuf, pop, cc_partial, scal, gfar;
+  DevBuf<double> xyz, H, w, ecore, jbuf, pop, cc_terms, scal, gfar;  // cc_terms: pair energies in pair order
   DevBuf<NearPair> near;
   DevBuf<int2> csr;
   DevBuf<unsigned char> mask;

@@ -24,20 +24,24 @@ struct NearPair {
 };
 
 // ---- build (kernels_build.cu) ----
+// cc_terms: the N(N-1)/2 pair core-core energies in pair order (u < v, row by row), for
+// the reference-order sum.
 void launch_pairs_all(cudaStream_t st, int n_atoms, const int *z, const double *xyz, const int *aoff, int nao,
-                      const DeviceParams &P, double *H, double *cc_partial, int *status);
-size_t pairs_all_partials(int n_atoms);
+                      const DeviceParams &P, double *H, double *cc_terms, int *status);
+// Position of pair (u, v), u < v, in the pair order of `core_core_energy` (src/repulsion.rs:19-22).
+__host__ __device__ inline size_t pair_index(int n, int u, int v) {
+  return (size_t)u * (2 * (size_t)n - u - 1) / 2 + (size_t)(v - u - 1);
+}
 void launch_near_integrals(cudaStream_t st, int n_near, const int *z, const double *xyz, const NearPair *np,
                            const DeviceParams &P, double *w, double *ecore, int *status);
 void launch_hcore_diag(cudaStream_t st, int n_atoms, const int *z, const double *xyz, const int *aoff,
                        const int *csr_start, const int2 *csr, const NearPair *np, const double *ecore,
                        const unsigned char *near_mask, const DeviceParams &P, int nao, double *H);
-void launch_sum_partials(cudaStream_t st, const double *in, size_t n, double *out);
 
 // ---- MNDO/d frame (kernels_d.cu): used for every pair of a molecule with a d-shell atom ----
 // beta*S blocks from the general Slater overlaps, plus core-core partials (as launch_pairs_all).
 void launch_pairs_all_d(cudaStream_t st, int n_atoms, const int *z, const double *xyz, const int *aoff, int nao,
-                        const DeviceParams &P, double *H, double *cc_partial);
+                        const DeviceParams &P, double *H, double *cc_terms);
 // Near-pair w blocks and packed electron-core blocks (as launch_near_integrals), one warp per pair.
 void launch_near_integrals_d(cudaStream_t st, int n_near, const int *z, const double *xyz, const NearPair *np,
                              const DeviceParams &P, double *w, double *ecore);
@@ -101,6 +105,28 @@ void launch_atom_pop(cudaStream_t st, int n_atoms, const int *aoff, const int *z
 // out[81 a + 9 i + j] = Pm of atom a's diagonal block (i, j < n_orb; 0 elsewhere).
 void launch_atom_blocks(cudaStream_t st, int n_atoms, const int *aoff, const int *z, const DeviceParams &P, int nao,
                         const double *Pm, double *out);
+
+// ---- reference-order sums (kernels_seqsum.cu) ----
+// The exact value of the left-to-right fold s = ((-0 + t_0) + t_1) + ... over t_i = a[i]
+// (b null) or t_i = fl(a[i] * b[i]) (no fused multiply-add), written to *out: bit for
+// bit what a serial loop gives, computed in parallel. Up to four sums per launch.
+struct SeqSumJob {
+  const double *a, *b;
+  size_t n;
+  double *out;  // device
+};
+struct SeqSumBatch {
+  SeqSumJob job[4];
+  int count;
+};
+size_t seqsum_chunks(size_t n);  // work units of one sum of n terms
+size_t seqsum_scratch_bytes(size_t n_max, int jobs);
+void launch_seqsum(cudaStream_t st, const SeqSumBatch &B, void *scratch);
+// Many sums from a device table: first[j] = sum over earlier jobs of seqsum_chunks(n),
+// first[count] = total_chunks (device array of count + 1).
+size_t seqsum_table_scratch_bytes(long long total_chunks);
+void launch_seqsum_table(cudaStream_t st, const SeqSumJob *jobs, const long long *first, int count,
+                         long long total_chunks, void *scratch);
 
 // ---- corrections (kernels_corr.cu) ----
 // out[0] dispersion, out[1] H-bond, out[2] C#C, out[3] Si-O-H, out[4] PM7-HH (kcal/mol).

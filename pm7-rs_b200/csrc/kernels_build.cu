@@ -54,29 +54,28 @@ __device__ __forceinline__ double pair_sp_elem(int n_atoms, const int *__restric
   return ecc;
 }
 
-// All pairs u < v: beta*S off-diagonal blocks of H and the core-core energy.
-// Grid: (ceil(N/128), N), block 128; blockIdx.y = u. Energies are reduced per
-// block into `cc_partial[blockIdx.y * gridDim.x + blockIdx.x]`.
+// All pairs u < v: beta*S off-diagonal blocks of H and the core-core energy of each pair,
+// written to cc_terms[pair_index(u, v)] (pair order, for the reference-order sum).
+// Grid: (ceil(N/128), N), block 128; blockIdx.y = u.
 __global__ void k_pairs_all(int n_atoms, const int *__restrict__ z, const double *__restrict__ xyz,
                             const int *__restrict__ aoff, int nao, DeviceParams P, double *__restrict__ H,
-                            double *__restrict__ cc_partial, int *__restrict__ status) {
-  const double ecc = pair_sp_elem(n_atoms, z, xyz, aoff, nao, P, H, status, blockIdx.y,
-                                  blockIdx.x * blockDim.x + threadIdx.x);
-  const double s = block_sum<128>(ecc);
-  if (threadIdx.x == 0) cc_partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+                            double *__restrict__ cc_terms, int *__restrict__ status) {
+  const int u = blockIdx.y, v = blockIdx.x * blockDim.x + threadIdx.x;
+  const double ecc = pair_sp_elem(n_atoms, z, xyz, aoff, nao, P, H, status, u, v);
+  if (v > u && v < n_atoms) cc_terms[pair_index(n_atoms, u, v)] = ecc;
 }
 
-// Batched: item = (atom u, column block) of one molecule; partial u * cc_nx + block.
+// Batched: item = (atom u, column block) of one molecule; each pair's core-core energy to
+// cc_terms in pair order.
 __global__ void k_b_pairs_all(BatchList L, const MolDesc *__restrict__ D, DeviceParams P) {
   const int item = blockIdx.x;
   const int m = batch_find(L, item);
   const MolDesc &d = D[L.slot[m]];
   const int local = item - L.prefix[m];
   const int u = local / d.cc_nx, bx = local - u * d.cc_nx;
-  const double ecc = pair_sp_elem(d.g.n_atoms, d.g.z, d.g.xyz, d.g.aoff, d.g.nao, P, d.H, nullptr, u,
-                                  bx * blockDim.x + threadIdx.x);
-  const double s = block_sum<128>(ecc);
-  if (threadIdx.x == 0) d.cc_partial[(size_t)u * d.cc_nx + bx] = s;
+  const int v = bx * blockDim.x + threadIdx.x;
+  const double ecc = pair_sp_elem(d.g.n_atoms, d.g.z, d.g.xyz, d.g.aoff, d.g.nao, P, d.H, nullptr, u, v);
+  if (v > u && v < d.g.n_atoms) d.cc_terms[pair_index(d.g.n_atoms, u, v)] = ecc;
 }
 
 // Near pairs: store w in (u,v) orientation and the packed electron-core blocks of
@@ -238,24 +237,16 @@ __global__ void __launch_bounds__(HDIAG_THREADS) k_b_hcore_diag(BatchList L, con
                    d.ecore, d.g.near_mask, P, d.g.nao, d.H);
 }
 
-__global__ void k_sum_partials(const double *__restrict__ in, size_t n, double *__restrict__ out) {
-  double s = 0.0;
-  for (size_t i = threadIdx.x; i < n; i += blockDim.x) s += in[i];
-  s = block_sum<256>(s);
-  if (threadIdx.x == 0) *out = s;
-}
-
 // ---- host launchers ------------------------------------------------------
 
 void launch_pairs_all(cudaStream_t st, int n_atoms, const int *z, const double *xyz, const int *aoff, int nao,
-                      const DeviceParams &P, double *H, double *cc_partial, int *status) {
+                      const DeviceParams &P, double *H, double *cc_terms, int *status) {
   if (n_atoms < 2) return;
   dim3 grid((n_atoms + 127) / 128, n_atoms);
-  k_pairs_all<<<grid, 128, 0, st>>>(n_atoms, z, xyz, aoff, nao, P, H, cc_partial, status);
+  k_pairs_all<<<grid, 128, 0, st>>>(n_atoms, z, xyz, aoff, nao, P, H, cc_terms, status);
   note_launch();
 }
 
-size_t pairs_all_partials(int n_atoms) { return (size_t)((n_atoms + 127) / 128) * (size_t)n_atoms; }
 
 void launch_near_integrals(cudaStream_t st, int n_near, const int *z, const double *xyz, const NearPair *np,
                            const DeviceParams &P, double *w, double *ecore, int *status) {
@@ -287,11 +278,6 @@ void launch_b_near_integrals(cudaStream_t st, const BatchList &L, const MolDesc 
 void launch_b_hcore_diag(cudaStream_t st, const BatchList &L, const MolDesc *D, const DeviceParams &P) {
   if (L.total <= 0) return;
   k_b_hcore_diag<<<L.total, HDIAG_THREADS, 0, st>>>(L, D, P);
-  note_launch();
-}
-
-void launch_sum_partials(cudaStream_t st, const double *in, size_t n, double *out) {
-  k_sum_partials<<<1, 256, 0, st>>>(in, n, out);
   note_launch();
 }
 

@@ -1036,26 +1036,26 @@ __device__ __forceinline__ double pair_d_elem(int n_atoms, const int *__restrict
   return pair_core_energy(P, eu, ev, sqrt(ex * ex + ey * ey + ez * ez));
 }
 
-// All pairs u < v in the MNDO/d frame: beta*S blocks of H and the core-core energy
-// partials. Grid (ceil(N/128), N), block 128, blockIdx.y = u.
+// All pairs u < v in the MNDO/d frame: beta*S blocks of H and each pair's core-core
+// energy in pair order. Grid (ceil(N/128), N), block 128, blockIdx.y = u.
 __global__ void k_pairs_all_d(int n_atoms, const int *__restrict__ z, const double *__restrict__ xyz,
                               const int *__restrict__ aoff, int nao, DeviceParams P, double *__restrict__ H,
-                              double *__restrict__ cc_partial) {
-  const double ecc = pair_d_elem(n_atoms, z, xyz, aoff, nao, P, H, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
-  const double s = block_sum<128>(ecc);
-  if (threadIdx.x == 0) cc_partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+                              double *__restrict__ cc_terms) {
+  const int u = blockIdx.y, v = blockIdx.x * blockDim.x + threadIdx.x;
+  const double ecc = pair_d_elem(n_atoms, z, xyz, aoff, nao, P, H, u, v);
+  if (v > u && v < n_atoms) cc_terms[pair_index(n_atoms, u, v)] = ecc;
 }
 
-// Batched: item = (atom u, column block) of one molecule.
+// Batched: item = (atom u, column block) of one molecule; pair energies to cc_terms.
 __global__ void k_b_pairs_all_d(BatchList L, const MolDesc *__restrict__ D, DeviceParams P) {
   const int item = blockIdx.x;
   const int m = batch_find(L, item);
   const MolDesc &d = D[L.slot[m]];
   const int local = item - L.prefix[m];
   const int u = local / d.cc_nx, bx = local - u * d.cc_nx;
-  const double ecc = pair_d_elem(d.g.n_atoms, d.g.z, d.g.xyz, d.g.aoff, d.g.nao, P, d.H, u, bx * blockDim.x + threadIdx.x);
-  const double s = block_sum<128>(ecc);
-  if (threadIdx.x == 0) d.cc_partial[(size_t)u * d.cc_nx + bx] = s;
+  const int v = bx * blockDim.x + threadIdx.x;
+  const double ecc = pair_d_elem(d.g.n_atoms, d.g.z, d.g.xyz, d.g.aoff, d.g.nao, P, d.H, u, v);
+  if (v > u && v < d.g.n_atoms) d.cc_terms[pair_index(d.g.n_atoms, u, v)] = ecc;
 }
 
 // One pair for the stage entry point: w (npair_a x npair_b), e1b/e2a and S (9x9 each).
@@ -1161,10 +1161,10 @@ void ensure_smem(const void *fn, size_t bytes) {
 // ---- host launchers ------------------------------------------------------
 
 void launch_pairs_all_d(cudaStream_t st, int n_atoms, const int *z, const double *xyz, const int *aoff, int nao,
-                        const DeviceParams &P, double *H, double *cc_partial) {
+                        const DeviceParams &P, double *H, double *cc_terms) {
   if (n_atoms < 2) return;
   dim3 grid((n_atoms + 127) / 128, n_atoms);
-  k_pairs_all_d<<<grid, 128, 0, st>>>(n_atoms, z, xyz, aoff, nao, P, H, cc_partial);
+  k_pairs_all_d<<<grid, 128, 0, st>>>(n_atoms, z, xyz, aoff, nao, P, H, cc_terms);
   note_launch();
 }
 

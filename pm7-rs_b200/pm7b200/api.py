@@ -26,7 +26,7 @@ EXPORTED = [
     "pm7_stage_product_tf32", "pm7_autotune_report", "pm7_gradient", "pm7_fixed_density_gradient",
     "pm7_correction_gradient", "pm7_run_batch_gradient", "pm7_engine_submit_gradient",
     "pm7_dandc_options_default", "pm7_run_dandc", "pm7_dandc_result_free", "pm7_stage_dandc_partition",
-    "pm7_dandc_abi_sizes",
+    "pm7_dandc_abi_sizes", "pm7_stage_seqsum",
 ]
 
 
@@ -82,6 +82,7 @@ def lib():
     L.pm7_stage_dandc_partition.argtypes = [C.POINTER(abi.Molecule), C.c_int32, C.c_double, C.POINTER(C.c_int32),
                                             C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
     L.pm7_stage_eigenvalues.argtypes = [C.c_int32, C.POINTER(C.c_int32), abi.DP, abi.DP, C.c_int32]
+    L.pm7_stage_seqsum.argtypes = [C.c_int64, abi.DP, abi.DP, abi.DP, C.c_int32]
     L.pm7_engine_config_default.argtypes = [C.POINTER(abi.EngineConfig)]
     L.pm7_engine_create.argtypes = [C.POINTER(abi.EngineConfig), C.POINTER(C.c_void_p)]
     L.pm7_engine_submit.argtypes = [C.c_void_p, C.POINTER(abi.Molecule), C.POINTER(abi.Options),
@@ -328,6 +329,20 @@ def core_core(z, xyz_bohr, method=0):
     e = C.c_double()
     _check(lib().pm7_stage_core_core(C.byref(m.s), params(method), C.byref(e)))
     return e.value
+
+
+def seqsum(a, b=None, device=0):
+    """The left-to-right f64 sum of a (or of the rounded products a*b), evaluated on the
+    device with the exact bits of a serial loop: the fold the reference's energies use
+    (`Matrix::frobenius_dot`, src/linalg.rs:138-141)."""
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+    bb = None if b is None else np.ascontiguousarray(b, dtype=np.float64).reshape(-1)
+    if bb is not None and bb.size != a.size:
+        raise ValueError("seqsum: a and b differ in length")
+    out = C.c_double()
+    _check(lib().pm7_stage_seqsum(a.size, a.ctypes.data_as(abi.DP), None if bb is None else bb.ctypes.data_as(abi.DP),
+                                  C.byref(out), int(device)))
+    return out.value
 
 
 def corrections(z, xyz_bohr, method=0, smooth=False):
