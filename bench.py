@@ -225,8 +225,21 @@ def barrier(world):
         dist.barrier()
 
 
+def bench_config(args, desc, z, world):
+    """The `config` both arms print for the single-molecule workloads (identical dicts)."""
+    nao = nao_of(z)
+    return {"workload": args.workload, "description": desc, "seed": 0, "n_atoms": len(z), "nao": nao,
+            "parallelism": f"replicas{world}",
+            "l2": f"inputs larger than L2 (H, F, P and DIIS history are {8 * nao * nao / 1e6:.0f} MB each at nao={nao})"}
+
+
 def run_reference(args, world, rank):
-    """CPU restatement of the reference (oracle/) on the host cores; rank 0 only."""
+    """CPU restatement of the reference (oracle/) on the host cores; rank 0 only.
+
+    Every step, warm-up included, is one complete `run_pm7` solve of the workload (core
+    Hamiltonian, SCF to the default tolerances, core-core, corrections, charges, dipole) on
+    all host cores: OpenMP over pairs, atoms and rows as the reference's rayon pool, and the
+    OpenBLAS bundled with numpy for the eigensolver."""
     if rank != 0:
         return
     from oracle import harness
@@ -234,27 +247,26 @@ def run_reference(args, world, rank):
     z, x, desc = workload(args.workload)
     cores = os.cpu_count() or 1
     harness.set_threads(cores)
-    # untimed probe: the iteration count of the complete solve (deterministic for this input)
-    probe_t, n_full = cpu_sample_full(z, x)
-    n_sample = min(3, n_full)
     for _ in range(args.warmup):
-        harness.sample(z, x, n_sample, want_matrices=0)
-    totals = []
+        harness.run(z, x, want_matrices=0)
+    times, r = [], None
     for _ in range(args.steps):
-        tb, ti, tp, it = harness.sample(z, x, n_sample, want_matrices=0)
-        per_iter = ti / max(it, 1)
-        totals.append(tb + tp + per_iter * n_full)
-    solve_s = sum(totals) / len(totals)
+        t = time.perf_counter()
+        r = harness.run(z, x, want_matrices=0)
+        times.append(time.perf_counter() - t)
+    solve_s = sum(times) / len(times)
     value = 1.0 / solve_s
-    sample = (f"per step: core build + {n_sample} of the {n_full} SCF iterations + post-SCF terms of the {desc}, "
-              f"scaled to one complete solve (untimed full-solve probe: {probe_t:.1f} s)")
+    sample = (f"{args.steps} complete solves of the {desc} ({r['iterations']} SCF iterations each), "
+              f"{min(times):.2f}-{max(times):.2f} s per solve")
     line = {
         "impl": "reference", "metric": "PM7 SCF solves/s (RHF single point)", "value": value, "unit": "solves/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": solve_s * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "description": desc, "seed": 0, "scf_iterations": n_full},
+        "config": bench_config(args, desc, z, world),
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "result": {"heat_of_formation_kcal": r["heat_of_formation_kcal"], "total_ev": r["total_ev"],
+                   "scf_iterations": r["iterations"]},
     }
     print(json.dumps(line), flush=True)
 
@@ -407,6 +419,23 @@ def run_b200(args, world, rank, local):
                      "achieved": achieved_gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                      "frac": achieved_gbs / peaks.get("hbm_gbs", 6650.0), "traffic": read_traffic("fock"),
                      "algorithmic_per_launch": f"{nbytes:.4g} B", "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+    # whole-solve roofline: iterations x (Fock bytes / HBM + dense flops / FP64 peak), the
+    # dense flops per iteration being an eigensolve (10/3 n^3), the density (n^2 n_occ) and the
+    # commutator (2 n^3); the pair integrals (the build stage, ~0.3% of a solve) are not counted
+    whole = None
+    if dgemm and fock_calls:
+        n_occ = int(r0["n_occ"])
+        its = r0["iterations"]
+        fock_b = 8.0 * (near_w_doubles(z, x) + 3.0 * nao * nao)
+        dense = 10.0 / 3.0 * nao ** 3 + float(nao) ** 2 * n_occ + 2.0 * nao ** 3
+        t_roof = its * (fock_b / (peaks.get("hbm_gbs", 6650.0) * 1e9) + dense / (dgemm * 1e12))
+        t_meas = dev_s / args.steps
+        whole = {"roofline_ms": t_roof * 1e3, "measured_ms": t_meas * 1e3, "frac": t_roof / t_meas,
+                 "iterations": its, "dense_flops_per_iteration": dense, "fock_bytes_per_iteration": fock_b,
+                 "note": "roofline time of the solve over its measured device time; pair integrals not counted"}
+    extras = None
+    if world == 1 and not args.no_extras and args.workload == "water334" and args.precision == "fp64":
+        extras = default_extras(args, local)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         t_cpu, it_cpu = cpu_sample_full(z, x)
@@ -419,9 +448,7 @@ def run_b200(args, world, rank, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
         "dtype": "f64" if args.precision == "fp64" else "f32 (tcgen05 3xTF32) + f64 refinement",
-        "config": {"workload": args.workload, "description": desc, "seed": 0, "n_atoms": n_atoms, "nao": nao,
-                   "scf_iterations": r0["iterations"], "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (H, F, P and DIIS history are 32 MB each at nao=2004)"},
+        "config": bench_config(args, desc, z, world),
         "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
@@ -431,13 +458,45 @@ def run_b200(args, world, rank, local):
         "pair_integrals": pair_rate,
         "autotune": api.autotune_report(),
         "mixed_precision": mixed,
+        "whole_solve_roofline": whole,
+        "served_and_batched": extras,
         "gradient": grad,
         "stages": stages,
         "clocks": clocks,
         "cpu_baseline": cpu,
-        "result": {"heat_of_formation_kcal": r0["heat_of_formation_kcal"], "total_ev": r0["total_ev"]},
+        "result": {"heat_of_formation_kcal": r0["heat_of_formation_kcal"], "total_ev": r0["total_ev"],
+                   "scf_iterations": r0["iterations"]},
     }
     print(json.dumps(line), flush=True)
+
+
+def default_extras(args, local):
+    """The served stream (FP64 and mixed precision) and the 4,096-molecule batch, one pass
+    each, for the default line: what the served/batched engine sustains against the plain
+    path on the same requests."""
+    sub = argparse.Namespace(**vars(args))
+    sub.steps, sub.warmup, sub.no_gradient, sub.no_cpu_baseline = 1, 1, True, True
+    out = {}
+    for prec in ("fp64", "mixed"):
+        sub.precision = prec
+        ln = run_stream_bench(sub, 1, 0, local, oracle_check=True)
+        out[f"stream_{prec}"] = {
+            "solves_per_s": ln["value"], "latency_ms": ln["latency_ms"], "requests": ln["config"]["requests"],
+            "rate_per_s": ln["config"]["rate_per_s"], "capacity_per_s": ln["config"]["capacity_per_s"],
+            "plain_fp64_solves_per_s": ln["plain_path"]["value"],
+            "served_over_plain": ln["plain_path"]["served_over_plain"],
+            "max_dhf_diff_vs_plain_kcal": ln["plain_path"]["max_dhf_diff_kcal"],
+            "oracle_check": ln.get("oracle_check"), "failed": ln["config"]["failed"], "clocks": ln["clocks"]}
+    for prec in ("fp64", "mixed"):
+        sub.precision = prec
+        ln = run_batch_bench(sub, 1, 0, local)
+        out[f"batch4096_{prec}"] = {
+            "solves_per_s": ln["value"], "wall_s": ln["ms_per_step"] / 1e3,
+            "plain_fp64_solves_per_s": ln["plain_path"]["value"],
+            "batched_over_plain": ln["plain_path"]["batched_over_plain"],
+            "max_dhf_diff_vs_plain_kcal": ln["plain_path"]["max_dhf_diff_kcal"],
+            "failed": ln["config"]["failed_rank0"], "clocks": ln["clocks"]}
+    return out
 
 
 def _percentiles(v):
@@ -540,10 +599,10 @@ def run_batch_bench(args, world, rank, local):
         "stages_note": "one extra untimed batch with stage events",
         "gradient": grad,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
-def run_stream_bench(args, world, rank, local):
+def run_stream_bench(args, world, rank, local, oracle_check=False):
     """Configuration: a served stream with Poisson arrivals at ~80% of capacity."""
     from pm7b200 import api
     from pm7b200 import geometry as G
@@ -619,7 +678,15 @@ def run_stream_bench(args, world, rank, local):
         "stages": {k: {"ms_total": round(v[0], 3), "calls": v[1]} for k, v in prof.items()},
         "stages_note": f"one more untimed burst of {len(burst)} requests with stage events",
     }
-    print(json.dumps(line), flush=True)
+    if oracle_check:
+        # the served results against the FP64 oracle on the stream's smaller requests
+        small = [i for i in range(count) if len(mols[i][0]) <= 120 and not isinstance(res[i], Exception)][:8]
+        _, ores = _oracle_sample(mols, small)
+        line["oracle_check"] = {
+            "requests": len(small), "max_dhf_err_kcal": max(abs(res[i]["heat_of_formation_kcal"] -
+                                                                ores[i]["heat_of_formation_kcal"]) for i in small),
+            "max_charge_err": max(float(np.max(np.abs(res[i]["charges"] - ores[i]["charges"]))) for i in small)}
+    return line
 
 
 def run_dandc_bench(args, world, rank, local):
@@ -701,6 +768,8 @@ def main():
     ap.add_argument("--no-fp64-peak", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision solve of the default workload")
     ap.add_argument("--no-gradient", action="store_true", help="skip the nuclear-gradient figure of the default workload")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload: skip the served-stream and batch figures added to its line")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU only: rank 0 runs, the other ranks exit without joining a process group
@@ -711,9 +780,13 @@ def main():
         if args.impl == "reference":
             run_reference(args, world, rank)
         elif args.workload == "batch4096":
-            run_batch_bench(args, world, rank, local)
+            line = run_batch_bench(args, world, rank, local)
+            if line:
+                print(json.dumps(line), flush=True)
         elif args.workload == "stream":
-            run_stream_bench(args, world, rank, local)
+            line = run_stream_bench(args, world, rank, local, oracle_check=not args.no_cpu_baseline)
+            if line:
+                print(json.dumps(line), flush=True)
         elif args.workload == "dandc640":
             run_dandc_bench(args, world, rank, local)
         else:

@@ -251,6 +251,13 @@ pm7_status pm7_stage_square_tf32(int32_t n, const double *x, double *c_out);
  * Replaces, in those cycles, the product of `commutator_into` (src/scf.rs:1148-1156). */
 pm7_status pm7_stage_product_tf32(int32_t n, const double *a, const double *b, double *c_out);
 
+/* Failure drill of the bounded device waits (no counterpart in pm7-rs): runs the tcgen05
+ * squaring of an n x n zero matrix (1 <= n <= 4096) with its copy producer withholding
+ * every copy, so the pipeline's mbarrier waits never complete. Each wait gives up after its
+ * time limit (1 s), the kernel frees its tensor memory and returns, and the call returns
+ * PM7_ERR_TIMEOUT, as pm7_run does when a wait expires; the CUDA context stays usable. */
+pm7_status pm7_stage_tf32_wait_drill(int32_t n);
+
 /* Eigenvalues (ascending, no eigenvectors) of `count` symmetric matrices, the stage that
  * gives the reported MO energies when no orbitals are returned. Replaces the eigenvalue
  * half of `symmetric_eigen` (src/linalg.rs:231-278, faer self_adjoint_eigen) as used by
@@ -381,6 +388,10 @@ pm7_status pm7_engine_submit_gradient(pm7_engine *engine, const pm7_molecule *mo
  * forgotten after it is polled. */
 pm7_status pm7_engine_poll(pm7_engine *engine, uint64_t ticket, int32_t wait, int32_t *done, pm7_result *result,
                            double *latency_ms);
+/* Admission record of the engine so far: out[0] requests admitted, out[1] the most
+ * requests resident on the device at once, out[2] the most device bytes they held at once
+ * (their footprints), out[3] the HBM budget in bytes. No counterpart in pm7-rs. */
+pm7_status pm7_engine_stats(pm7_engine *engine, int64_t out[4]);
 /* Finishes every submitted request, then stops the worker. */
 pm7_status pm7_engine_destroy(pm7_engine *engine);
 

@@ -1433,7 +1433,7 @@ class BatchRunner {
         int bad = 0;
         CUDA_OK(cudaMemcpyAsync(&bad, err32_, sizeof(int), cudaMemcpyDeviceToHost, st_));
         CUDA_OK(cudaStreamSynchronize(st_));
-        if (bad) throw Failure{PM7_ERR_CUDA, "tcgen05 squaring: a pipeline wait expired"};
+        if (bad) throw Failure{PM7_ERR_TIMEOUT, "tcgen05 squaring: a pipeline wait expired"};
       }
     }
     mark(2);
@@ -2159,6 +2159,8 @@ struct pm7_engine {
   std::unordered_map<uint64_t, std::unique_ptr<pm7::EngineRequest>> requests;
   std::unordered_map<pm7::BatchMol *, pm7::EngineRequest *> by_mol;
   uint64_t next_ticket = 1;
+  // admission record: requests admitted, most requests resident at once, most bytes resident
+  int64_t admitted = 0, peak_active = 0, peak_bytes = 0;
   bool stop = false;
   std::string worker_error;
   std::thread worker;
@@ -2188,6 +2190,9 @@ static void engine_loop(pm7_engine *E) {
           admit.push_back(r->mol.get());
           E->by_mol[r->mol.get()] = r;
         }
+        E->admitted += (int64_t)admit.size();
+        E->peak_active = std::max<int64_t>(E->peak_active, active);
+        E->peak_bytes = std::max<int64_t>(E->peak_bytes, (int64_t)used);
       }
       E->runner->admit(admit);
       std::vector<BatchMol *> fin = E->runner->iterate();
@@ -2407,6 +2412,16 @@ pm7_status pm7_engine_poll(pm7_engine *E, uint64_t ticket, int32_t wait, int32_t
   g_last_error = r->error;
   E->requests.erase(it);
   return s;
+}
+
+pm7_status pm7_engine_stats(pm7_engine *E, int64_t out[4]) {
+  if (!E || !out) return PM7_ERR_INVALID_INPUT;
+  std::lock_guard<std::mutex> lk(E->mu);
+  out[0] = E->admitted;
+  out[1] = E->peak_active;
+  out[2] = E->peak_bytes;
+  out[3] = (int64_t)E->budget;
+  return PM7_OK;
 }
 
 pm7_status pm7_engine_destroy(pm7_engine *E) {

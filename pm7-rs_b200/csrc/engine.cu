@@ -453,7 +453,7 @@ struct Purifier {
     int bad = 0;
     CUDA_OK(cudaMemcpyAsync(&bad, err32.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
-    if (bad) throw Failure{PM7_ERR_CUDA, "tcgen05 squaring: a pipeline wait expired"};
+    if (bad) throw Failure{PM7_ERR_TIMEOUT, "tcgen05 squaring: a pipeline wait expired"};
     if (!ok) return false;
     launch_sp2_density32(st, n, ld, X32.p, w, P);
     return true;
@@ -1689,7 +1689,36 @@ pm7_status pm7_stage_square_tf32(int32_t n, const double *x, double *c_out) {
     CUDA_OK(cudaMemcpyAsync(c_out, C.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
     CUDA_OK(cudaGetLastError());
-    if (e) throw Failure{PM7_ERR_CUDA, "tcgen05 squaring: a pipeline wait expired"};
+    if (e) throw Failure{PM7_ERR_TIMEOUT, "tcgen05 squaring: a pipeline wait expired"};
+  });
+}
+
+pm7_status pm7_stage_tf32_wait_drill(int32_t n) {
+  return guarded([&] {
+    if (n < 1 || n > 4096) throw Failure{PM7_ERR_INVALID_INPUT, "wait drill needs 1 <= n <= 4096"};
+    DeviceContext &ctx = context_for(0);
+    std::lock_guard<std::mutex> lock(ctx.run_mutex);
+    CUDA_OK(cudaSetDevice(ctx.device));
+    cudaStream_t st = ctx.stream;
+    const int ld = ((n + 31) / 32) * 32;
+    const size_t ll = (size_t)ld * ld;
+    DevBuf<float> hi, lo, C32;
+    DevBuf<int> err;
+    for (DevBuf<float> *b : {&hi, &lo, &C32}) {
+      b->alloc(ll, st);
+      CUDA_OK(cudaMemsetAsync(b->p, 0, sizeof(float) * ll, st));
+    }
+    err.alloc(1, st);
+    CUDA_OK(cudaMemsetAsync(err.p, 0, sizeof(int), st));
+    alignas(64) unsigned char map_hi[128], map_lo[128];
+    if (!make_square_map(hi.p, ld, map_hi) || !make_square_map(lo.p, ld, map_lo))
+      throw Failure{PM7_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
+    launch_square_tf32x3(st, n, ld, map_hi, map_lo, C32.p, err.p, nullptr, 0, 1);
+    int e = 0;
+    CUDA_OK(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaGetLastError());
+    if (e) throw Failure{PM7_ERR_TIMEOUT, "tcgen05 squaring: a pipeline wait expired (drill)"};
   });
 }
 
@@ -1724,7 +1753,7 @@ pm7_status pm7_stage_product_tf32(int32_t n, const double *a, const double *b, d
     CUDA_OK(cudaMemcpyAsync(c_out, Cm.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
     CUDA_OK(cudaGetLastError());
-    if (e) throw Failure{PM7_ERR_CUDA, "tcgen05 product: a pipeline wait expired"};
+    if (e) throw Failure{PM7_ERR_TIMEOUT, "tcgen05 product: a pipeline wait expired"};
   });
 }
 

@@ -169,9 +169,11 @@ bool make_square_map(const float *base, int ld, void *map_out);
 // Sets the tcgen05 kernels' shared-memory attributes on the current device (idempotent).
 void prepare_tf32_kernels();
 size_t square_tf32x3_smem();
-// state/step: as the fp64 SP2 steps (state may be null: always runs).
+// state/step: as the fp64 SP2 steps (state may be null: always runs). drill != 0: the failure
+// drill, the copy producer withholds every copy so each pipeline wait runs out its time limit
+// and the kernel sets *error and returns.
 void launch_square_tf32x3(cudaStream_t st, int n, int ld, const void *map_hi, const void *map_lo, float *C,
-                          int *error, const double *state = nullptr, int step = 0);
+                          int *error, const double *state = nullptr, int step = 0, int drill = 0);
 // C = A B for symmetric A, B given as split tensor maps (all 128x128 tiles, no mirror).
 void launch_product_tf32x3(cudaStream_t st, int n, int ld, const void *a_hi, const void *a_lo, const void *b_hi,
                            const void *b_lo, float *C, int *error);

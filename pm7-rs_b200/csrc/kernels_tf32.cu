@@ -12,7 +12,7 @@
 // multicast); warp 1 lane 0 issues tcgen05.mma (M=128, N=128, K=8) into a 128-column TMEM
 // accumulator and releases each stage with tcgen05.commit; all four warps read the
 // accumulator back with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = tile rows) and
-// store it. Every mbarrier wait has an iteration limit; on expiry the CTA records an error,
+// store it. Every mbarrier wait has a time limit (1 s); on expiry the CTA records an error,
 // stops issuing, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -30,7 +30,7 @@ constexpr int TM = 128, TN = 128, TK = 32, STAGES = 3;
 constexpr int TILE_BYTES = TM * TK * 4;            // 16 KB: 128 rows x 32 fp32 (128 B per row)
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;        // Ahi, Alo, Bhi, Blo
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;  // + alignment slack + barriers
-constexpr uint32_t kWaitLimit = 1u << 26;          // try_wait polls before giving up
+constexpr unsigned long long kWaitNs = 1000000000ull;  // a pipeline wait gives up after 1 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -44,11 +44,18 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
-// Bounded wait for phase `parity` of an mbarrier; false when the limit expired or the
-// CTA aborted.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for phase `parity` of an mbarrier; false when the time limit expired (the
+// CTA's abort flag is then set) or another thread of the CTA already aborted.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
   const uint32_t addr = smem_u32(bar);
-  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+  unsigned long long t0 = 0;
+  for (uint32_t it = 0; it < (1u << 30); ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -58,7 +65,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
         : "r"(addr), "r"(parity)
         : "memory");
     if (done) return true;
-    if ((it & 255) == 255 && *abort_flag) return false;
+    if ((it & 15) == 15) {
+      if (*abort_flag) return false;
+      const unsigned long long t = global_ns();
+      if (it == 15) t0 = t;
+      else if (t - t0 > kWaitNs) break;
+    }
   }
   *abort_flag = 1;
   return false;
@@ -112,7 +124,7 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
 __device__ __forceinline__ void product_tile(int bm, int bn, const CUtensorMap *a_hi, const CUtensorMap *a_lo,
                                              const CUtensorMap *b_hi, const CUtensorMap *b_lo, bool mirror, int n,
                                              int ld, float *__restrict__ C, int *__restrict__ error,
-                                             unsigned char *smem_raw) {
+                                             unsigned char *smem_raw, bool withhold_copies = false) {
   // stage buffers on a 1024-byte boundary (128-byte swizzle atoms)
   unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
@@ -151,6 +163,7 @@ __device__ __forceinline__ void product_tile(int bm, int bn, const CUtensorMap *
       if (kt >= STAGES && !mbar_wait(&empty[s], (uint32_t)((kt / STAGES - 1) & 1), abort_flag)) break;
       unsigned char *st = smem + s * STAGE_BYTES;
       mbar_expect_tx(&full[s], STAGE_BYTES);
+      if (withhold_copies) continue;  // failure drill: the stage never fills, every wait runs out
       const int k0 = kt * TK;
       tma_load_2d(st + 0 * TILE_BYTES, a_hi, &full[s], k0, m0);
       tma_load_2d(st + 1 * TILE_BYTES, a_lo, &full[s], k0, m0);
@@ -232,14 +245,14 @@ __device__ __forceinline__ void lower_tile(int t, int &bm, int &bn) {
 __global__ void __launch_bounds__(128) k_square_tf32x3(const __grid_constant__ CUtensorMap map_hi,
                                                        const __grid_constant__ CUtensorMap map_lo, int n, int ld,
                                                        float *__restrict__ C, int *__restrict__ error,
-                                                       const double *__restrict__ sp2, int step) {
+                                                       const double *__restrict__ sp2, int step, int drill) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // an SP2 step after the purification stopped: the whole CTA leaves before any barrier,
   // tensor-memory or copy set-up
   if (!sp2_active(sp2, step)) return;
   int bm, bn;
   lower_tile(blockIdx.x, bm, bn);
-  product_tile(bm, bn, &map_hi, &map_lo, &map_hi, &map_lo, true, n, ld, C, error, smem_raw);
+  product_tile(bm, bn, &map_hi, &map_lo, &map_hi, &map_lo, true, n, ld, C, error, smem_raw, drill != 0);
 }
 
 // C = A B of two symmetric split operands, every 128x128 tile (the DIIS commutator F P of
@@ -301,12 +314,12 @@ void launch_product_tf32x3(cudaStream_t st, int n, int ld, const void *a_hi, con
 }
 
 void launch_square_tf32x3(cudaStream_t st, int n, int ld, const void *map_hi, const void *map_lo, float *C,
-                          int *error, const double *state, int step) {
+                          int *error, const double *state, int step, int drill) {
   prepare_tf32_kernels();
   const int t = (n + TM - 1) / TM;
   k_square_tf32x3<<<t * (t + 1) / 2, 128, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap *>(map_hi),
                                                             *reinterpret_cast<const CUtensorMap *>(map_lo), n, ld, C,
-                                                            error, state, step);
+                                                            error, state, step, drill);
   note_launch();
 }
 

@@ -26,7 +26,8 @@ EXPORTED = [
     "pm7_stage_product_tf32", "pm7_autotune_report", "pm7_gradient", "pm7_fixed_density_gradient",
     "pm7_correction_gradient", "pm7_run_batch_gradient", "pm7_engine_submit_gradient",
     "pm7_dandc_options_default", "pm7_run_dandc", "pm7_dandc_result_free", "pm7_stage_dandc_partition",
-    "pm7_dandc_abi_sizes", "pm7_stage_seqsum",
+    "pm7_dandc_abi_sizes", "pm7_stage_seqsum", "pm7_stage_tf32_wait_drill",
+    "pm7_engine_stats",
 ]
 
 
@@ -83,6 +84,7 @@ def lib():
                                             C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
     L.pm7_stage_eigenvalues.argtypes = [C.c_int32, C.POINTER(C.c_int32), abi.DP, abi.DP, C.c_int32]
     L.pm7_stage_seqsum.argtypes = [C.c_int64, abi.DP, abi.DP, abi.DP, C.c_int32]
+    L.pm7_stage_tf32_wait_drill.argtypes = [C.c_int32]
     L.pm7_engine_config_default.argtypes = [C.POINTER(abi.EngineConfig)]
     L.pm7_engine_create.argtypes = [C.POINTER(abi.EngineConfig), C.POINTER(C.c_void_p)]
     L.pm7_engine_submit.argtypes = [C.c_void_p, C.POINTER(abi.Molecule), C.POINTER(abi.Options),
@@ -90,6 +92,7 @@ def lib():
     L.pm7_engine_poll.argtypes = [C.c_void_p, C.c_uint64, C.c_int32, C.POINTER(C.c_int32), C.POINTER(abi.Result),
                                   C.POINTER(C.c_double)]
     L.pm7_engine_destroy.argtypes = [C.c_void_p]
+    L.pm7_engine_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
     _lib = L
     return L
 
@@ -331,6 +334,12 @@ def core_core(z, xyz_bohr, method=0):
     return e.value
 
 
+def tf32_wait_drill(n=128):
+    """Status code of the bounded-wait drill (pm7_stage_tf32_wait_drill): the tcgen05
+    squaring with its copies withheld; 10 (PM7_ERR_TIMEOUT) when every wait gave up."""
+    return int(lib().pm7_stage_tf32_wait_drill(int(n)))
+
+
 def seqsum(a, b=None, device=0):
     """The left-to-right f64 sum of a (or of the rounded products a*b), evaluated on the
     device with the exact bits of a serial loop: the fold the reference's energies use
@@ -528,6 +537,13 @@ class Engine:
             _check(lib().pm7_engine_submit(self._h, C.byref(m.s), C.byref(o), C.byref(t)))
         self._keep[t.value] = (keep, g)
         return t.value
+
+    def stats(self):
+        """Admission record: requests admitted, the most resident at once, the most device
+        bytes they held at once, and the HBM budget in bytes (`pm7_engine_stats`)."""
+        out = (C.c_int64 * 4)()
+        _check(lib().pm7_engine_stats(self._h, out))
+        return {"admitted": out[0], "peak_active": out[1], "peak_bytes": out[2], "budget_bytes": out[3]}
 
     def poll(self, ticket, wait=False):
         """(done, result): result is the run_pm7 dict plus "latency_ms", or a Pm7Error."""
