@@ -86,17 +86,18 @@ __global__ void __launch_bounds__(RB) k_b_init(BatchList L, const MolDesc *__res
   }
 }
 
-// The two fold jobs of each finished molecule, <P, H> and <P, F> (F = the final Fock in X),
-// from the device descriptors: P and Pn swap on the device, so only D knows the density.
+// The two energy fold jobs of each listed molecule, <P, H> and <P, F> (F: this iteration's
+// Fock in the history ring, or with final_pass the final Fock in X), from the device
+// descriptors: P and Pn swap on the device, so only D knows the density.
 __global__ void k_b_fold_jobs(int n, const int *__restrict__ slots, const MolDesc *__restrict__ D,
-                              MolCtl *__restrict__ C, SeqSumJob *__restrict__ jobs) {
+                              MolCtl *__restrict__ C, SeqSumJob *__restrict__ jobs, int final_pass) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= n) return;
   const MolDesc &d = D[slots[m]];
   MolCtl &c = C[slots[m]];
   const size_t nn = (size_t)d.g.nao * d.g.nao;
   jobs[2 * m] = {d.P, d.H, nn, &c.e_fold[0]};
-  jobs[2 * m + 1] = {d.P, d.X, nn, &c.e_fold[1]};
+  jobs[2 * m + 1] = {d.P, final_pass ? d.X : hist_F(d, c.slot), nn, &c.e_fold[1]};
 }
 
 // e_final = 1/2 (<P, H> + <P, F>) from the two folds of the final density (scf.rs:1297-1298).
@@ -197,10 +198,11 @@ __global__ void __launch_bounds__(RB) k_b_dots_c(BatchList L, const MolDesc *__r
     for (int i = 0; i < 3 * kHist + 2; ++i) d.part[(size_t)r.q * kPart + 2 + i] = v[i];
 }
 
-// Per molecule: the chunk partials summed in chunk order. what 0: E_el, |E|^2 and the
-// DIIS inner products; what 1: the final E_el.
+// Per molecule: the chunk partials summed in chunk order: E_el of the iteration (for the
+// convergence test; the reported energy is the reference's fold, k_b_fold_energy), |E|^2
+// and the DIIS inner products.
 __global__ void k_b_reduce(int n, const int *__restrict__ slots, const MolDesc *__restrict__ D,
-                           MolCtl *__restrict__ C, int what) {
+                           MolCtl *__restrict__ C) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= n) return;
   const MolDesc &d = D[slots[m]];
@@ -208,10 +210,6 @@ __global__ void k_b_reduce(int n, const int *__restrict__ slots, const MolDesc *
   const int nc = items_chunks(d.g.nao);
   double e = 0.0;
   for (int q = 0; q < nc; ++q) e += d.part[(size_t)q * kPart + 0];
-  if (what == 1) {
-    c.e_final = 0.5 * e;
-    return;
-  }
   c.e_elec = 0.5 * e;
   double err2 = 0.0;
   for (int q = 0; q < nc; ++q) err2 += d.part[(size_t)q * kPart + 1];
@@ -1328,7 +1326,7 @@ class BatchRunner {
     {
       Stage s_(st_, "batch_diis");
       k_b_dots_c<<<A.chunks.total, RB, 0, st_>>>(A.chunks, desc_, ctl_);
-      k_b_reduce<<<nb, 128, 0, st_>>>(n, A.mol.slot, desc_, ctl_, 0);
+      k_b_reduce<<<nb, 128, 0, st_>>>(n, A.mol.slot, desc_, ctl_);
       k_b_control<<<(n + 63) / 64, 64, 0, st_>>>(n, A.mol.slot, ctl_, flags_d_ + 2 * (size_t)cap_);
       note_launch(3);
     }
@@ -1540,6 +1538,22 @@ class BatchRunner {
 
   // Reference-order sums (launch_seqsum_table) of `jobs` on the main stream; the job table
   // and its chunk offsets go up through `up` (one set in flight per upload buffer).
+  // <P, H> and <P, F> of every molecule of the list into its MolCtl::e_fold; the job table is
+  // filled on the device (the density pointer lives there).
+  void queue_energy_folds(const Lists &A, const std::vector<BatchMol *> &mols, ListUpload &up, int final_pass) {
+    const int n = A.mol.n;
+    std::vector<SeqSumJob> jobs;
+    for (const BatchMol *b : mols) {
+      const size_t nn = (size_t)b->L.nao * b->L.nao;
+      jobs.push_back({nullptr, nullptr, nn, nullptr});
+      jobs.push_back({nullptr, nullptr, nn, nullptr});
+    }
+    queue_folds(jobs, up, [&](SeqSumJob *dev_jobs) {
+      k_b_fold_jobs<<<(n + 127) / 128, 128, 0, st_>>>(n, A.mol.slot, desc_, ctl_, dev_jobs, final_pass);
+      note_launch();
+    });
+  }
+
   // `fill`, when given, writes the device job table itself (after the upload, before the sums).
   void queue_folds(const std::vector<SeqSumJob> &jobs, ListUpload &up,
                    const std::function<void(SeqSumJob *)> &fill = nullptr) {
@@ -1801,18 +1815,8 @@ class BatchRunner {
     const int n = A.mol.n;
     Stage s_(st_, "batch_finish");
     launch_b_fock(st_, A.mol, A.rows, A.near, A.atoms, desc_, ctl_, *P_, 1);
-    // the final electronic energy as the reference's two folds (the final Fock is in X); the
-    // job table is filled on the device (the density pointer lives there)
-    std::vector<SeqSumJob> jobs;
-    for (const BatchMol *b : R) {
-      const size_t nn = (size_t)b->L.nao * b->L.nao;
-      jobs.push_back({nullptr, nullptr, nn, nullptr});
-      jobs.push_back({nullptr, nullptr, nn, nullptr});
-    }
-    queue_folds(jobs, fold_retire_up_, [&](SeqSumJob *dev_jobs) {
-      k_b_fold_jobs<<<(n + 127) / 128, 128, 0, st_>>>(n, A.mol.slot, desc_, ctl_, dev_jobs);
-      note_launch();
-    });
+    // the final electronic energy as the reference's two folds (the final Fock is in X)
+    queue_energy_folds(A, R, fold_retire_up_, 1);
     k_b_fold_energy<<<(n + 127) / 128, 128, 0, st_>>>(n, A.mol.slot, ctl_);
     note_launch();
     launch_b_corrections(st_, A.mol, A.pairs, desc_, ctl_, method_, A.max_atoms);

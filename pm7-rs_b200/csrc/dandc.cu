@@ -327,6 +327,8 @@ struct DcJacJob {
   double *slot;   // np x np: the Fock matrix in, the eigenvectors (rows) out
   double *eps;    // np eigenvalues out
   double *basis;  // np x np: the previous eigenvectors (rows), updated
+  int *info;      // 0 solved; 1 off-diagonal part still above 1e-12 of the diagonal after the
+                  // last sweep; 2 non-finite (read with the bucket's eigensolver status)
   int n, np;
 };
 
@@ -427,6 +429,19 @@ __global__ void __launch_bounds__(kJacThreads) k_dc_jacobi(const DcJacJob *__res
       }
       __syncthreads();
     }
+  }
+  {
+    // convergence and finiteness of what is handed on
+    double off = 0.0, dia = 0.0;
+    for (int e = tid; e < n * n; e += nt) {
+      const int i = e / n, j = e % n;
+      const double v = A[i * ld + j];
+      if (i == j) dia += v * v;
+      else off += v * v;
+    }
+    off = block_sum(off, red);
+    dia = block_sum(dia, red);
+    if (tid == 0) *jb.info = !(isfinite(off) && isfinite(dia)) ? 2 : (off > 1.0e-24 * dia ? 1 : 0);
   }
   for (int i = tid; i < n; i += nt) {  // a total order (NaN last), so the ranks are a permutation
     const double vi = A[i * ld + i], v = vi == vi ? vi : INFINITY;
@@ -641,7 +656,9 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
       o.reference == PM7_REF_UNRESTRICTED || (o.reference == PM7_REF_AUTO && o.multiplicity > 1);
   const int chan = unrestricted ? 2 : 1;
   {
-    uint64_t need = (uint64_t)nao_g * nao_g * 8 * (unrestricted ? 4 : 2) + (uint64_t)N * N;
+    // global density (and spin channels), the stored-pair mask (N^2 bytes) and the int32
+    // atom-pair table of the reassembly (4 N^2 bytes)
+    uint64_t need = (uint64_t)nao_g * nao_g * 8 * (unrestricted ? 4 : 2) + (uint64_t)N * N * 5;
     for (const auto &s : subs) {
       const uint64_t pairs = (uint64_t)s->m.n * (s->m.n > 0 ? s->m.n - 1 : 0) / 2;
       need += (uint64_t)s->np * s->np * 8 * chan + (uint64_t)s->m.n * s->m.n * 9 + (uint64_t)s->nao * s->nao * 8 +
@@ -805,7 +822,7 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
       const size_t npp = (size_t)b.np * b.np;
       for (int c = 0; c < chan; ++c) {
         const size_t k = (size_t)sp->slot + c;
-        jac.push_back(DcJacJob{b.A.p + k * npp, b.eps.p + k * b.np, jac_basis.p + off, sp->nao, b.np});
+        jac.push_back(DcJacJob{b.A.p + k * npp, b.eps.p + k * b.np, jac_basis.p + off, b.info.p + k, sp->nao, b.np});
         off += npp;
       }
       jac_n = std::max(jac_n, sp->nao);
@@ -1169,7 +1186,8 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
     CUDA_OK(cudaGetLastError());
     for (const auto &v : infos)
       for (int x : v)
-        if (x != 0) throw Failure{PM7_ERR_LINEAR_ALGEBRA, "subsystem eigendecomposition failed (info " + std::to_string(x) + ")"};
+        if (x != 0)
+          throw Failure{PM7_ERR_LINEAR_ALGEBRA, "subsystem eigendecomposition failed (info " + std::to_string(x) + ")"};
     if (sc[2] != 0.0) {
       // the message of src/dandc/mod.rs:743-757: the span of the subsystems' (alpha) spectra
       std::vector<double> eh(n_states);
@@ -1312,23 +1330,27 @@ pm7_status pm7_stage_dandc_partition(const pm7_molecule *molecule, int32_t core_
   try {
     if (!molecule || !core_of || !sizes || !n_subsystems || !stored_pairs)
       throw Failure{PM7_ERR_INVALID_INPUT, "null argument"};
-    if (core_size <= 0 || !(buffer > 0.0)) throw Failure{PM7_ERR_INVALID_INPUT, "invalid core size or buffer"};
+    // the same option checks as the solve (src/dandc/mod.rs:83-110)
+    pm7_dandc_options d;
+    pm7_dandc_options_default(&d);
+    d.core_size = core_size;
+    d.buffer = buffer;
+    check_dandc_options(d);
     const Molecule m = to_molecule(molecule);
     const std::vector<DcPart> parts = dc_partition(m, core_size, buffer);
-    std::vector<unsigned char> seen((size_t)m.n * m.n, 0);
-    int64_t pairs = 0;
+    // stored (ordered) atom pairs: those with at least one atom in some subsystem's core,
+    // counted as sorted unique keys over the subsystems (memory linear in their sizes)
+    std::vector<int64_t> keys;
     for (size_t a = 0; a < parts.size(); ++a) {
       const DcPart &p = parts[a];
       sizes[a] = (int32_t)p.parent.size();
       for (int i = 0; i < p.n_core; ++i) core_of[p.parent[i]] = (int32_t)a;
       for (int i = 0; i < (int)p.parent.size(); ++i)
-        for (int j = 0; j < (int)p.parent.size(); ++j) {
-          if (i >= p.n_core && j >= p.n_core) continue;
-          unsigned char &v = seen[(size_t)p.parent[i] * m.n + p.parent[j]];
-          pairs += v == 0;
-          v = 1;
-        }
+        for (int j = 0; j < (int)p.parent.size(); ++j)
+          if (i < p.n_core || j < p.n_core) keys.push_back((int64_t)p.parent[i] * m.n + p.parent[j]);
     }
+    std::sort(keys.begin(), keys.end());
+    const int64_t pairs = (int64_t)(std::unique(keys.begin(), keys.end()) - keys.begin());
     *n_subsystems = (int32_t)parts.size();
     *stored_pairs = pairs;
     g_last_error.clear();

