@@ -2436,6 +2436,13 @@ pm7_status pm7_engine_destroy(pm7_engine *E) {
     E->cv.notify_all();
   }
   if (E->worker.joinable()) E->worker.join();
+  if (std::getenv("PM7_BATCH_TRACE") && E->runner) {
+    std::fprintf(stderr, "engine: %lld requests, peak %lld resident; iterations (host wall, s):", (long long)E->admitted,
+                 (long long)E->peak_active);
+    for (int k = 0; k < pm7::BatchRunner::kPhases; ++k)
+      std::fprintf(stderr, " %s %.3f", pm7::BatchRunner::phase_name(k), E->runner->phase_seconds(k));
+    std::fprintf(stderr, "\n");
+  }
   for (auto &kv : E->requests) pm7_result_free(&kv.second->result);
   E->runner.reset();
   delete E;

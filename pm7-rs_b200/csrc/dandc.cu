@@ -308,166 +308,6 @@ __global__ void k_dc_assemble(int nao, int n_glob, const int *__restrict__ ao_at
   if (threadIdx.x == 0) partials[blockIdx.x] = acc;
 }
 
-// ---- subsystem eigensolver: cyclic Jacobi in shared memory, one block per matrix ----------
-//
-// A subsystem's Fock matrix changes little from one iteration to the next, so the previous
-// iteration's eigenvectors W nearly diagonalise it: the kernel forms W F W^T and runs parallel
-// cyclic Jacobi sweeps (round-robin pairing, n'/2 disjoint rotations per round, the classical
-// rotation of Golub & Van Loan, sym.schur2) on that, which converges in a few sweeps, and
-// accumulates the rotations into W. The first iteration starts from the identity. Sweeps stop
-// when the off-diagonal part falls below 1e-15 of the diagonal (Frobenius norms), or after
-// kJacSweeps. Eigenvalues are sorted ascending (ties by index) and the eigenvectors written as
-// rows of the np x np slot (zero padding, padding eigenvalues kDcPad), as the batched
-// eigensolver leaves them.
-constexpr int kJacMax = 112;       // largest order: two n x (n + 1) tiles fit in shared memory
-constexpr int kJacSweeps = 24;
-constexpr int kJacThreads = 512;
-
-struct DcJacJob {
-  double *slot;   // np x np: the Fock matrix in, the eigenvectors (rows) out
-  double *eps;    // np eigenvalues out
-  double *basis;  // np x np: the previous eigenvectors (rows), updated
-  int *info;      // 0 solved; 1 off-diagonal part still above 1e-12 of the diagonal after the
-                  // last sweep; 2 non-finite (read with the bucket's eigensolver status)
-  int n, np;
-};
-
-__global__ void __launch_bounds__(kJacThreads) k_dc_jacobi(const DcJacJob *__restrict__ jobs, int warm) {
-  extern __shared__ double jsm[];
-  __shared__ double cc[kJacMax / 2 + 1], ss[kJacMax / 2 + 1], red[32];
-  __shared__ int pp[kJacMax / 2 + 1], qq[kJacMax / 2 + 1], rk[kJacMax], inv[kJacMax];
-  __shared__ int done;
-  const DcJacJob jb = jobs[blockIdx.x];
-  const int n = jb.n, np = jb.np, ld = n + 1;
-  if (n <= 0 || n > kJacMax) return;
-  double *A = jsm, *W = jsm + (size_t)n * ld;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int e = tid; e < n * n; e += nt) {
-    const int i = e / n, k = e % n;
-    W[i * ld + k] = warm ? jb.basis[(size_t)i * np + k] : (i == k ? 1.0 : 0.0);
-  }
-  __syncthreads();
-  if (warm) {
-    // T = F W^T (F read from the slot) into A, then W T back into the slot
-    for (int e = tid; e < n * n; e += nt) {
-      const int k = e / n, j = e % n;
-      const double *f = jb.slot + (size_t)k * np;
-      double t = 0.0;
-      for (int l = 0; l < n; ++l) t += f[l] * W[j * ld + l];
-      A[k * ld + j] = t;
-    }
-    __syncthreads();
-    for (int e = tid; e < n * n; e += nt) {
-      const int i = e / n, j = e % n;
-      double t = 0.0;
-      for (int k = 0; k < n; ++k) t += W[i * ld + k] * A[k * ld + j];
-      jb.slot[(size_t)i * np + j] = t;
-    }
-    __syncthreads();
-  }
-  for (int e = tid; e < n * n; e += nt) {  // symmetric part
-    const int i = e / n, j = e % n;
-    A[i * ld + j] = 0.5 * (jb.slot[(size_t)i * np + j] + jb.slot[(size_t)j * np + i]);
-  }
-  __syncthreads();
-  const int m = (n % 2 == 0) ? n - 1 : n;  // rotating indices 1..m around the fixed index 0
-  const int half = (m + 1) / 2;            // rotations per round
-  for (int sweep = 0; sweep < kJacSweeps; ++sweep) {
-    double off = 0.0, dia = 0.0;
-    for (int e = tid; e < n * n; e += nt) {
-      const int i = e / n, j = e % n;
-      const double v = A[i * ld + j];
-      if (i == j) dia += v * v;
-      else off += v * v;
-    }
-    off = block_sum(off, red);
-    dia = block_sum(dia, red);
-    if (tid == 0) done = !(off > 1.0e-30 * dia);
-    __syncthreads();
-    if (done) break;
-    for (int r = 0; r < m; ++r) {
-      for (int k = tid; k < half; k += nt) {
-        int p = k == 0 ? 0 : (r + k) % m + 1, q = k == 0 ? r + 1 : (r - k + m) % m + 1;
-        if (p > q) {
-          const int t = p;
-          p = q;
-          q = t;
-        }
-        double c = 1.0, s = 0.0;
-        if (q < n) {  // index n is the odd order's idle slot
-          const double apq = A[p * ld + q];
-          if (apq != 0.0) {
-            const double tau = (A[q * ld + q] - A[p * ld + p]) / (2.0 * apq);
-            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-            c = 1.0 / sqrt(1.0 + t * t);
-            s = t * c;
-          }
-        }
-        pp[k] = p;
-        qq[k] = q;
-        cc[k] = c;
-        ss[k] = s;
-      }
-      __syncthreads();
-      for (int e = tid; e < half * n; e += nt) {  // A <- A J
-        const int k = e / n, i = e % n, p = pp[k], q = qq[k];
-        if (q >= n) continue;
-        const double ap = A[i * ld + p], aq = A[i * ld + q];
-        A[i * ld + p] = cc[k] * ap - ss[k] * aq;
-        A[i * ld + q] = ss[k] * ap + cc[k] * aq;
-      }
-      __syncthreads();
-      for (int e = tid; e < half * n; e += nt) {  // A <- J^T A, W <- J^T W
-        const int k = e / n, j = e % n, p = pp[k], q = qq[k];
-        if (q >= n) continue;
-        const double ap = A[p * ld + j], aq = A[q * ld + j];
-        A[p * ld + j] = cc[k] * ap - ss[k] * aq;
-        A[q * ld + j] = ss[k] * ap + cc[k] * aq;
-        const double wp = W[p * ld + j], wq = W[q * ld + j];
-        W[p * ld + j] = cc[k] * wp - ss[k] * wq;
-        W[q * ld + j] = ss[k] * wp + cc[k] * wq;
-      }
-      __syncthreads();
-    }
-  }
-  {
-    // convergence and finiteness of what is handed on
-    double off = 0.0, dia = 0.0;
-    for (int e = tid; e < n * n; e += nt) {
-      const int i = e / n, j = e % n;
-      const double v = A[i * ld + j];
-      if (i == j) dia += v * v;
-      else off += v * v;
-    }
-    off = block_sum(off, red);
-    dia = block_sum(dia, red);
-    if (tid == 0) *jb.info = !(isfinite(off) && isfinite(dia)) ? 2 : (off > 1.0e-24 * dia ? 1 : 0);
-  }
-  for (int i = tid; i < n; i += nt) {  // a total order (NaN last), so the ranks are a permutation
-    const double vi = A[i * ld + i], v = vi == vi ? vi : INFINITY;
-    int r = 0;
-    for (int j = 0; j < n; ++j) {
-      const double uj = A[j * ld + j], u = uj == uj ? uj : INFINITY;
-      r += (u < v) || (u == v && j < i);
-    }
-    rk[i] = r;
-  }
-  __syncthreads();
-  for (int i = tid; i < n; i += nt) {
-    inv[rk[i]] = i;
-    jb.eps[rk[i]] = A[i * ld + i];
-  }
-  for (int i = n + tid; i < np; i += nt) jb.eps[i] = kDcPad;
-  __syncthreads();
-  for (int e = tid; e < np * np; e += nt) {
-    const int r = e / np, k = e % np;
-    const double v = (r < n && k < n) ? W[inv[r] * ld + k] : 0.0;
-    jb.slot[e] = v;
-    jb.basis[e] = v;
-  }
-}
-
-size_t jacobi_smem(int n) { return sizeof(double) * 2 * (size_t)n * (n + 1); }
 
 unsigned grid_for(size_t items) { return (unsigned)std::max<size_t>(1, std::min<size_t>((items + 255) / 256, 4096)); }
 
@@ -568,7 +408,7 @@ struct DcSub {
 
 struct DcBucket {
   int np = 0, count = 0;  // matrices (2 per subsystem when unrestricted)
-  bool jacobi = false;    // solved by k_dc_jacobi (np <= kJacMax), else by cuSOLVER
+  bool jacobi = false;    // solved by k_dc_jacobi (np <= kJacobiMax), else by cuSOLVER
   DevBuf<double> A, eps;
   DevBuf<int> info;
 };
@@ -803,12 +643,12 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
     b.eps.alloc((size_t)b.count * b.np, st);
     b.info.alloc(b.count, st);
     CUDA_OK(cudaMemsetAsync(b.info.p, 0, sizeof(int) * b.count, st));
-    b.jacobi = b.np <= kJacMax;
+    b.jacobi = b.np <= kJacobiMax;
   }
   // the Jacobi jobs (one block per matrix) and their kept eigenvector bases
-  std::vector<DcJacJob> jac;
+  std::vector<JacobiJob> jac;
   DevBuf<double> jac_basis;
-  DevBuf<DcJacJob> jac_d;
+  DevBuf<JacobiJob> jac_d;
   int jac_n = 0;
   {
     size_t basis_len = 0;
@@ -822,14 +662,14 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
       const size_t npp = (size_t)b.np * b.np;
       for (int c = 0; c < chan; ++c) {
         const size_t k = (size_t)sp->slot + c;
-        jac.push_back(DcJacJob{b.A.p + k * npp, b.eps.p + k * b.np, jac_basis.p + off, b.info.p + k, sp->nao, b.np});
+        jac.push_back(JacobiJob{b.A.p + k * npp, b.eps.p + k * b.np, jac_basis.p + off, b.info.p + k, sp->nao, b.np});
         off += npp;
       }
       jac_n = std::max(jac_n, sp->nao);
     }
     upload(jac_d, jac, st);
     if (!jac.empty())
-      CUDA_OK(cudaFuncSetAttribute(k_dc_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)jacobi_smem(jac_n)));
+      prepare_jacobi_eigen(jac_n);
   }
   // Lanes: the subsystems' launch sequences are independent, so they run on kDcLanes side
   // streams forked from and joined back into the main stream (parallel branches of the captured
@@ -1048,10 +888,10 @@ void run_dandc_impl(const pm7_molecule *mol, const pm7_params *params, const pm7
   };
   int jac_warm = 0;  // the Jacobi bases hold the previous iteration's eigenvectors
   auto queue_eig = [&]() {
-    // the subsystem eigenproblems: one Jacobi launch for every matrix of order <= kJacMax, the
+    // the subsystem eigenproblems: one Jacobi launch for every matrix of order <= kJacobiMax, the
     // larger buckets through cuSOLVER
     if (!jac.empty()) {
-      k_dc_jacobi<<<(unsigned)jac.size(), kJacThreads, jacobi_smem(jac_n), st>>>(jac_d.p, jac_warm);
+      launch_jacobi_eigen(st, jac_d.p, (int)jac.size(), jac_n, jac_warm, kDcPad);
       note_launch();
     }
     for (DcBucket &b : buckets) {

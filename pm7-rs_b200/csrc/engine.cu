@@ -18,6 +18,7 @@
 #include <functional>
 #include <limits>
 #include <map>
+#include <memory>
 #include <thread>
 #include <mutex>
 #include <string>
@@ -350,6 +351,82 @@ struct Eigen {
   }
 };
 
+// Eigendecomposition on the SCF path (`symmetric_eigen`, src/linalg.rs:231-278): cuSOLVER
+// dsyevd, or with PM7_DENSITY_SOLVER=jacobi the repo's Jacobi kernel for orders up to
+// kJacobiMax, warm-started from this object's previous eigenvectors (one object per spin
+// channel). Jacobi is not the default: measured per solve it is no faster than dsyevd at
+// ~60 orbitals and slower from ~100 (40 against 28 ms at 108), and on exactly degenerate
+// frontier levels (the reference's O2++ triplet and Cl- cases) its choice of vectors inside
+// the degenerate space leads the SCF to another state than the reference's. In place: A
+// becomes the eigenvectors, one per row (row-major), eigenvalues ascending in eps(). A Jacobi
+// solve that ends unconverged or non-finite raises PM7_ERR_LINEAR_ALGEBRA at the next
+// check(), which the caller makes after a stream synchronisation.
+static bool use_jacobi(int n) {
+  const char *env = std::getenv("PM7_DENSITY_SOLVER");
+  return env && std::strcmp(env, "jacobi") == 0 && n <= kJacobiMax;
+}
+
+constexpr int kOwnEigvalsMax = 511;  // eigenvalues alone: the cluster tridiagonalisation up to here
+
+struct Diag {
+  DeviceContext &ctx;
+  cudaStream_t st;
+  int n;
+  bool jac;
+  std::unique_ptr<Eigen> lib;
+  DevBuf<double> basis, ev;
+  DevBuf<int> info;
+  DevBuf<JacobiJob> job;
+  double *slot = nullptr;
+  bool warm = false, pending = false;
+  int *pin;  // pinned copy of the Jacobi status
+  Diag(DeviceContext &ctx, int n_, double *probe, int *pinned_info)
+      : ctx(ctx), st(ctx.stream), n(n_), jac(use_jacobi(n_)), pin(pinned_info) {
+    if (jac) {
+      basis.alloc((size_t)n * n, st);
+      ev.alloc(n, st);
+      info.alloc(1, st);
+      prepare_jacobi_eigen(n);
+    } else {
+      lib = std::make_unique<Eigen>(ctx, n, probe);
+    }
+  }
+  void solve(double *A, bool vectors = true) {
+    if (!jac) {
+      lib->solve(A, vectors);
+      return;
+    }
+    if (A != slot) {
+      upload(job, std::vector<JacobiJob>{JacobiJob{A, ev.p, basis.p, info.p, n, n}}, st);
+      slot = A;
+    }
+    launch_jacobi_eigen(st, job.p, 1, n, warm ? 1 : 0, 0.0);
+    warm = true;
+    CUDA_OK(cudaMemcpyAsync(pin, info.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    pending = true;
+  }
+  // Eigenvalues of A into eps(); A keeps its contents unless the solver is Jacobi or
+  // cuSOLVER (which leave eigenvectors). Up to kOwnEigvalsMax the values come from the
+  // repo's cluster tridiagonalisation and Sturm multisection.
+  void values(double *A) {
+    const char *env = std::getenv("PM7_DENSITY_SOLVER");
+    const bool library_only = env && std::strcmp(env, "syevd") == 0;
+    if (jac || library_only || n > kOwnEigvalsMax) {
+      solve(A, false);
+      return;
+    }
+    eigvals_device(st, {EigvalsRequest{A, n, n, lib->eps.p}}, ctx.eig_scratch);
+  }
+  void check() {
+    if (!pending) return;
+    pending = false;
+    if (*pin != 0)
+      throw Failure{PM7_ERR_LINEAR_ALGEBRA, *pin == 1 ? "Jacobi eigensolver did not converge"
+                                                      : "Jacobi eigensolver: non-finite matrix"};
+  }
+  const double *eps() const { return jac ? ev.p : lib->eps.p; }
+};
+
 // Density from F by SP2 purification: P = w X with X the aufbau projector onto the
 // n_occ lowest eigenvectors of F. Returns false when the iteration does not settle on
 // an idempotent X (degenerate frontier levels), so the caller diagonalises instead.
@@ -498,18 +575,19 @@ struct Purifier {
   }
 };
 
-// Density solver for the SCF loop: SP2 for large systems (tensor-core squarings), the
-// cuSOLVER eigendecomposition for small ones or when SP2 cannot settle. The choice can
-// be forced with PM7_DENSITY_SOLVER=sp2|syevd.
+// Density solver for the SCF loop: SP2 above kJacobiMax orbitals (tensor-core squarings;
+// 16 against 37 ms per solve at 240 orbitals), the eigendecomposition (Diag) up to it and
+// when SP2 cannot settle. PM7_DENSITY_SOLVER=sp2|jacobi|syevd forces one (jacobi and syevd
+// turn SP2 off; syevd also keeps the final eigenvalues on cuSOLVER).
 // DIIS error below which the mixed-precision SCF switches to fp64 densities.
 static constexpr double kMixedSwitch = 1.0e-3;
 static constexpr double kMixedSwitchStep = 1.0e-6;  // rms density step that also ends the fp32 phase
 
 static bool use_sp2(int n) {
   const char *env = std::getenv("PM7_DENSITY_SOLVER");
-  if (env && std::strcmp(env, "syevd") == 0) return false;
+  if (env && (std::strcmp(env, "syevd") == 0 || std::strcmp(env, "jacobi") == 0)) return false;
   if (env && std::strcmp(env, "sp2") == 0) return true;
-  return n >= 256;
+  return n > kJacobiMax;
 }
 
 static thread_local double *t_pinned_scalar = nullptr;  // set per solve from the context
@@ -618,7 +696,7 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     launch_set_diag(st, n, dd.p, out.P.p);
     CUDA_OK(cudaStreamSynchronize(st));
   }
-  Eigen eig(ctx, n, Fuse.p);
+  Diag eig(ctx, n, Fuse.p, reinterpret_cast<int *>(ctx.pinned + 8192));
   const bool sp2 = use_sp2(n);
   Purifier pur(st, sp2 ? n : 1, reinterpret_cast<double *>(ctx.pinned + 4096));
   bool diagonalised = false;  // whether Fuse holds the eigenvectors of the last iteration
@@ -732,6 +810,7 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     }
     size_t nd = launch_sqdiff(st, nn, Pnew.p, out.P.p, partials.p);
     const double dp = std::sqrt(host_sum(partials, nd, dscal.p + 2, st) / (double)std::max<size_t>(nn, 1));
+    eig.check();
     out.density_error = dp;
     const double de = std::fabs(e_elec - e_old);
     std::swap(out.P.p, Pnew.p);
@@ -762,17 +841,22 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   const bool vectors = o.want_matrices != 0;
   if (guard.shift > 0.0) {
     CUDA_OK(cudaMemcpyAsync(Fuse.p, F.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
-    { Stage s_(st, "eigensolve"); eig.solve(Fuse.p, vectors); }
+    Stage s_(st, "eigensolve");
+    if (vectors) eig.solve(Fuse.p, true);
+    else eig.values(Fuse.p);
   } else if (!diagonalised) {
-    { Stage s_(st, "eigensolve"); eig.solve(Fuse.p, vectors); }
+    Stage s_(st, "eigensolve");
+    if (vectors) eig.solve(Fuse.p, true);
+    else eig.values(Fuse.p);
   }
   if (vectors) {
     out.Va.alloc(nn, st);
     CUDA_OK(cudaMemcpyAsync(out.Va.p, Fuse.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
   }
   out.eps_a.resize(n);
-  CUDA_OK(cudaMemcpyAsync(out.eps_a.data(), eig.eps.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(out.eps_a.data(), eig.eps(), sizeof(double) * n, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaStreamSynchronize(st));
+  eig.check();
   out.n_occ = n_occ;
 }
 
@@ -890,7 +974,8 @@ static void run_uhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     }
     CUDA_OK(cudaStreamSynchronize(st));
   }
-  Eigen eig(ctx, n, Ua.p);
+  Diag eig(ctx, n, Ua.p, reinterpret_cast<int *>(ctx.pinned + 8192));
+  Diag eig_b(ctx, n, Ub.p, reinterpret_cast<int *>(ctx.pinned + 8192 + 64));
   const bool sp2 = use_sp2(n);
   Purifier pur(st, sp2 ? n : 1, reinterpret_cast<double *>(ctx.pinned + 4096));
   bool diag_a = false;  // whether Ua holds the alpha eigenvectors of the last iteration
@@ -952,16 +1037,18 @@ static void run_uhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     if (!pa_ok) {
       { Stage s_(st, "eigensolve"); eig.solve(Ua.p); }
       { Stage s_(st, "density_gemm"); launch_density(st, n, n_alpha, 1.0, Ua.p, n, Pan.p); }
-      CUDA_OK(cudaMemcpyAsync(ea.data(), eig.eps.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaMemcpyAsync(ea.data(), eig.eps(), sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     }
     if (!pb_ok) {
-      { Stage s_(st, "eigensolve"); eig.solve(Ub.p); }
+      { Stage s_(st, "eigensolve"); eig_b.solve(Ub.p); }
       { Stage s_(st, "density_gemm"); launch_density(st, n, n_beta, 1.0, Ub.p, n, Pbn.p); }
     }
     size_t c2 = launch_sqdiff(st, nn, Pan.p, Pa.p, partials.p);
     const double dpa = std::sqrt(host_sum(partials, c2, dscal.p + 5, st) / (double)nn);
     c2 = launch_sqdiff(st, nn, Pbn.p, Pb.p, partials.p);
     const double dpb = std::sqrt(host_sum(partials, c2, dscal.p + 5, st) / (double)nn);
+    eig.check();
+    eig_b.check();
     const double dp = dpa + dpb;
     out.density_error = dp;
     out.eps_a = ea;
@@ -996,19 +1083,21 @@ static void run_uhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     CUDA_OK(cudaMemcpyAsync(Ua.p, Fa.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
     { Stage s_(st, "eigensolve"); eig.solve(Ua.p); }
     out.eps_a.resize(n);
-    CUDA_OK(cudaMemcpyAsync(out.eps_a.data(), eig.eps.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(out.eps_a.data(), eig.eps(), sizeof(double) * n, cudaMemcpyDeviceToHost, st));
   } else if (!diag_a) {
     { Stage s_(st, "eigensolve"); eig.solve(Ua.p); }
     out.eps_a.resize(n);
-    CUDA_OK(cudaMemcpyAsync(out.eps_a.data(), eig.eps.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(out.eps_a.data(), eig.eps(), sizeof(double) * n, cudaMemcpyDeviceToHost, st));
   }
   CUDA_OK(cudaMemcpyAsync(out.Va.p, Ua.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
   CUDA_OK(cudaMemcpyAsync(Ub.p, Fb.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
-  { Stage s_(st, "eigensolve"); eig.solve(Ub.p); }
+  { Stage s_(st, "eigensolve"); eig_b.solve(Ub.p); }
   CUDA_OK(cudaMemcpyAsync(out.Vb.p, Ub.p, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
   out.eps_b.resize(n);
-  CUDA_OK(cudaMemcpyAsync(out.eps_b.data(), eig.eps.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(out.eps_b.data(), eig_b.eps(), sizeof(double) * n, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaStreamSynchronize(st));
+  eig.check();
+  eig_b.check();
   out.unrestricted = true;
   out.n_occ = n_alpha;
   out.n_occ_beta = n_beta;

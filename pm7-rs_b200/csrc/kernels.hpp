@@ -128,6 +128,21 @@ size_t seqsum_table_scratch_bytes(long long total_chunks);
 void launch_seqsum_table(cudaStream_t st, const SeqSumJob *jobs, const long long *first, int count,
                          long long total_chunks, void *scratch);
 
+// ---- Jacobi eigensolver (kernels_jacobi.cu): one block per matrix of order <= kJacobiMax ----
+constexpr int kJacobiMax = 112;  // largest order: two n x (n + 1) tiles fit in shared memory
+constexpr int kJacobiThreads = 512;
+struct JacobiJob {
+  double *slot;   // np x np: the symmetric matrix in, its eigenvectors (rows, ascending) out
+  double *eps;    // np eigenvalues out (padding rows get `pad`)
+  double *basis;  // np x np: the previous eigenvectors (rows), used when warm, updated
+  int *info;      // 0 solved; 1 off-diagonal part still above 1e-12 of the diagonal after the
+                  // last sweep; 2 non-finite
+  int n, np;
+};
+size_t jacobi_smem(int n);
+void prepare_jacobi_eigen(int max_n);  // shared-memory attribute on the current device
+void launch_jacobi_eigen(cudaStream_t st, const JacobiJob *jobs, int count, int max_n, int warm, double pad);
+
 // ---- corrections (kernels_corr.cu) ----
 // out[0] dispersion, out[1] H-bond, out[2] C#C, out[3] Si-O-H, out[4] PM7-HH (kcal/mol).
 void launch_corrections(cudaStream_t st, int n_atoms, const int *z, const double *xyz, int method, int smooth,

@@ -246,3 +246,17 @@ def test_sp2_uhf():
     a = _with_solver("sp2", lambda: api.run_pm7(z, x, reference="uhf"))
     o = harness.run(z, x, reference="uhf")
     _compare_runs("sp2-uhf", a, o, len(z))
+
+
+def test_jacobi_eigensolver_matches_the_library_one():
+    # the Jacobi kernel (orders <= 112, warm-started from the previous iteration's vectors)
+    # and cuSOLVER's dsyevd take the same SCF path to the same state, RHF and UHF
+    for z, x, kw in ((*G.decane(3), {}), (*_cluster(15, 4), {}), (*_cluster(10, 2), {"reference": "uhf"})):
+        a = _with_solver("jacobi", lambda: api.run_pm7(z, x, **kw))
+        b = _with_solver("syevd", lambda: api.run_pm7(z, x, **kw))
+        o = harness.run(z, x, **kw)
+        assert a["iterations"] == b["iterations"]
+        assert abs(a["heat_of_formation_kcal"] - b["heat_of_formation_kcal"]) < 1e-7
+        assert np.max(np.abs(a["density"] - b["density"])) < 1e-8
+        np.testing.assert_allclose(a["mo_energies"], b["mo_energies"], rtol=0, atol=1e-8)
+        _compare_runs("jacobi", a, o, len(z))

@@ -20,7 +20,8 @@ def fold(a, b=None):
     """Serial left-to-right sum (numpy's accumulate adds one element at a time)."""
     t = np.asarray(a, np.float64) if b is None else np.asarray(a, np.float64) * np.asarray(b, np.float64)
     t = t.reshape(-1)
-    return -0.0 if t.size == 0 else float(np.add.accumulate(t)[-1])
+    with np.errstate(over="ignore", invalid="ignore"):
+        return -0.0 if t.size == 0 else float(np.add.accumulate(t)[-1])
 
 
 def bits(x):
