@@ -433,7 +433,7 @@ struct Diag {
 struct Purifier {
   cudaStream_t st;
   int n;
-  DevBuf<double> X, X2, scratch, bounds, state;
+  DevBuf<double> X, X2, scratch, bounds, state, parts;
   int last_iterations = 0;
   double *pin = nullptr;  // kSp2Len pinned doubles for the purification state
   Purifier(cudaStream_t s, int n_, double *pinned_state) : st(s), n(n_), pin(pinned_state) {
@@ -551,21 +551,24 @@ struct Purifier {
       }
       launch_sp2_init(st, n, F, bounds.p, X.p);
       const Sp2Rule rule{1.0e-13 * std::max(1, n_occ), 1.0e-6, kMaxSteps};
+      // Fused steps on the ping-pong pair (X, X2): step s reads the iterate from one and
+      // writes the next, already updated, to the other; its traces come from the previous
+      // step's epilogue (the first from k_sp2_norms).
+      if (!parts.p) parts.alloc(sp2_parts_doubles(n), st);
       last_iterations = run_chunks(
           [&](int s) {
-            {
-              Stage g_(st, "sp2_square_gemm");
-              launch_sp2_square(st, n, X.p, X2.p, state.p, s);
-            }
-            launch_sp2_trace(st, n, X.p, X2.p, (double)n_occ, state.p, s, rule);
-            launch_sp2_update(st, n, X.p, X2.p, state.p, s);
+            if (s == 0) launch_sp2_norms(st, n, X.p, state.p, parts.p);
+            launch_sp2_decide(st, (double)n_occ, state.p, parts.p, s, rule);
+            Stage g_(st, "sp2_square_gemm");
+            launch_sp2_step(st, n, s % 2 == 0 ? X.p : X2.p, s % 2 == 0 ? X2.p : X.p, state.p, parts.p, s);
           },
           "sp2_square_gemm", hint64);
       bool ok = pin[kSp2Ok] != 0.0;
       // an idempotent X whose trace is not n_occ is a wrong projector (degenerate frontier)
       if (ok && std::fabs(pin[kSp2TrX] - (double)n_occ) > 1.0e-3) ok = false;
       if (ok) {
-        launch_scale(st, (size_t)n * n, w, X.p, P);
+        const int stop = (int)pin[kSp2Stop];  // the iterate after the last step is in its output
+        launch_scale(st, (size_t)n * n, w, stop % 2 == 0 ? X2.p : X.p, P);
         return true;
       }
       if (!refine) return false;

@@ -165,6 +165,7 @@ enum Sp2State {
   kSp2Stop = 4,                                            // step at which it stopped (1e9: running)
   kSp2Ok = 5,                                              // 1: converged, 0: failed
   kSp2Ring = 6,                                            // errors of the last three steps
+  kSp2Parts = 9,                                           // trace partials of the current iterate
   kSp2Len = 12
 };
 // Stopping rule of one purification: converged when |err| <= tol_done, or at the rounding
@@ -219,6 +220,15 @@ void launch_sp2_square(cudaStream_t st, int n, const double *X, double *X2, cons
 void launch_sp2_trace(cudaStream_t st, int n, const double *X, const double *X2, double n_occ, double *state, int step,
                       Sp2Rule rule);
 void launch_sp2_update(cudaStream_t st, int n, double *X, const double *X2, const double *state, int step);
+// The fused SP2 iteration on a ping-pong pair: launch_sp2_norms gives the starting iterate's
+// trace partials; per step, launch_sp2_decide turns the current partials into the branch and
+// the stopping rule, and launch_sp2_step writes the next iterate Y = X^2 or 2X - X^2 (the
+// squaring's epilogue applies the branch) with its own partials. `parts` holds
+// sp2_parts_doubles(n) doubles.
+size_t sp2_parts_doubles(int n);
+void launch_sp2_norms(cudaStream_t st, int n, const double *X, double *state, double *parts);
+void launch_sp2_decide(cudaStream_t st, double n_occ, double *state, const double *parts, int step, Sp2Rule rule);
+void launch_sp2_step(cudaStream_t st, int n, const double *X, double *Y, double *state, double *parts, int step);
 }
 
 namespace pm7 {

@@ -29,15 +29,16 @@ namespace {
 constexpr int BK = 16, STAGES = 3;
 constexpr int BM = 64, BN = 64;  // full-product tile (also the batched kernel's)
 
-template <int TBM, int TBN>
+template <int TBM, int TBN, int TBK = BK, int TST = STAGES>
 struct GemmShape {
   static constexpr int LA = TBM + 4, LB = TBN + 4;
-  static constexpr int STAGE = BK * (LA + LB);          // doubles per stage
-  static constexpr int SMEM = STAGES * STAGE * 8;       // bytes
+  static constexpr int STAGE = TBK * (LA + LB);         // doubles per stage
+  static constexpr int SMEM = TST * STAGE * 8;          // bytes
 };
 constexpr int GEMM_SMEM = GemmShape<64, 64>::SMEM;       // 52,224 bytes
 constexpr int SYM_BM = 128, SYM_BN = 64;
 constexpr int SYM_SMEM = GemmShape<SYM_BM, SYM_BN>::SMEM;  // 76,800 bytes
+constexpr int SYM_SMEM_K32 = GemmShape<SYM_BM, SYM_BN, 32, 2>::SMEM;  // 102,400 bytes: 32-deep slabs, two stages
 
 __device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -65,35 +66,35 @@ __device__ __forceinline__ void dmma16x8x8(double *d, const double *a, const dou
                : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-// One k-slab (16 rows) of the A and B tiles into shared memory, 128 threads.
-template <int TBM, int TBN, bool VEC>
+// One k-slab (TBK rows) of the A and B tiles into shared memory, 128 threads.
+template <int TBM, int TBN, bool VEC, int TBK = BK, int TST = STAGES>
 __device__ __forceinline__ void load_stage(double *sA, double *sB, int k0, int m0, int n0, int M, int N, int K,
                                            const double *__restrict__ A, int lda, const double *__restrict__ B,
                                            int ldb) {
-  using S = GemmShape<TBM, TBN>;
+  using S = GemmShape<TBM, TBN, TBK, TST>;
   const int tid = threadIdx.x;
   if (VEC) {
 #pragma unroll
-    for (int e = tid; e < BK * TBM / 2; e += 128) {
+    for (int e = tid; e < TBK * TBM / 2; e += 128) {
       const int row = e / (TBM / 2), col = (e % (TBM / 2)) * 2, kr = k0 + row;
       const int r = kr < K ? min(max(M - (m0 + col), 0), 2) * 8 : 0;
       cp_async16(sA + row * S::LA + col, r ? A + (size_t)kr * lda + m0 + col : A, r);
     }
 #pragma unroll
-    for (int e = tid; e < BK * TBN / 2; e += 128) {
+    for (int e = tid; e < TBK * TBN / 2; e += 128) {
       const int row = e / (TBN / 2), col = (e % (TBN / 2)) * 2, kr = k0 + row;
       const int r = kr < K ? min(max(N - (n0 + col), 0), 2) * 8 : 0;
       cp_async16(sB + row * S::LB + col, r ? B + (size_t)kr * ldb + n0 + col : B, r);
     }
   } else {
 #pragma unroll
-    for (int e = tid; e < BK * TBM; e += 128) {
+    for (int e = tid; e < TBK * TBM; e += 128) {
       const int row = e / TBM, col = e % TBM, kr = k0 + row;
       const bool p = kr < K && (m0 + col) < M;
       cp_async8(sA + row * S::LA + col, p ? A + (size_t)kr * lda + m0 + col : A, p);
     }
 #pragma unroll
-    for (int e = tid; e < BK * TBN; e += 128) {
+    for (int e = tid; e < TBK * TBN; e += 128) {
       const int row = e / TBN, col = e % TBN, kr = k0 + row;
       const bool p = kr < K && (n0 + col) < N;
       cp_async8(sB + row * S::LB + col, p ? B + (size_t)kr * ldb + n0 + col : B, p);
@@ -102,14 +103,29 @@ __device__ __forceinline__ void load_stage(double *sA, double *sB, int k0, int m
 }
 }  // namespace
 
+// The fused SP2 step in a symmetric product's epilogue: with `x` (the squared matrix
+// itself, row stride lda), each written element becomes y = X^2 (square) or 2X - X^2, and
+// tr Y and |Y|_F^2 (off-diagonal elements counted twice: Y is symmetric) are summed per
+// 64 x 64 block (R, C), R >= C, of the lower triangle into parts[2 b], parts[2 b + 1],
+// b = R (R + 1) / 2 + C. The order of those sums depends on the element coordinates alone
+// (per row over its 32-column warp span in fragment order, the four lanes of a row by a
+// fixed shuffle tree, the two spans, then the block's rows in ascending order), so every
+// tile shape gives the same bits.
+struct Sp2Fuse {
+  const double *x;  // null: a plain product
+  bool square;
+  double *parts;
+};
+
 // One TBM x TBN tile, 4 warps as 2 x 2 of (TBM/2) x (TBN/2). sym != 0: only elements
 // with m >= n are written, each also mirrored to (n, m), so the output is exactly
 // symmetric (P = w V^T V and X X).
-template <int TBM, int TBN, bool VEC>
+template <int TBM, int TBN, bool VEC, int TBK = BK, int TST = STAGES>
 __device__ __forceinline__ void gemm_tile_impl(double *smem, int bm, int bn, int M, int N, int K, double alpha,
                                                const double *__restrict__ A, int lda, const double *__restrict__ B,
-                                               int ldb, double *__restrict__ C, int ldc, int sym) {
-  using S = GemmShape<TBM, TBN>;
+                                               int ldb, double *__restrict__ C, int ldc, int sym,
+                                               const Sp2Fuse &fuse = Sp2Fuse{nullptr, false, nullptr}) {
+  using S = GemmShape<TBM, TBN, TBK, TST>;
   constexpr int TM = TBM / 2, TN = TBN / 2, FM = TM / 16, FN = TN / 8;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
@@ -123,28 +139,28 @@ __device__ __forceinline__ void gemm_tile_impl(double *smem, int bm, int bn, int
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
 
-  const int ktiles = (K + BK - 1) / BK;
+  const int ktiles = (K + TBK - 1) / TBK;
 #pragma unroll
-  for (int s = 0; s < STAGES - 1; ++s) {
+  for (int s = 0; s < TST - 1; ++s) {
     if (s < ktiles) {
       double *st = smem + s * S::STAGE;
-      load_stage<TBM, TBN, VEC>(st, st + BK * S::LA, s * BK, m0, n0, M, N, K, A, lda, B, ldb);
+      load_stage<TBM, TBN, VEC, TBK, TST>(st, st + TBK * S::LA, s * TBK, m0, n0, M, N, K, A, lda, B, ldb);
     }
     cp_async_commit();
   }
   for (int kt = 0; kt < ktiles; ++kt) {
-    cp_async_wait<STAGES - 2>();  // tile kt has landed (this thread's copies)
-    __syncthreads();              // ... everyone's, and stage (kt - 1) % STAGES is free
-    const int pf = kt + STAGES - 1;
+    cp_async_wait<TST - 2>();  // tile kt has landed (this thread's copies)
+    __syncthreads();           // ... everyone's, and stage (kt - 1) % TST is free
+    const int pf = kt + TST - 1;
     if (pf < ktiles) {
-      double *st = smem + (pf % STAGES) * S::STAGE;
-      load_stage<TBM, TBN, VEC>(st, st + BK * S::LA, pf * BK, m0, n0, M, N, K, A, lda, B, ldb);
+      double *st = smem + (pf % TST) * S::STAGE;
+      load_stage<TBM, TBN, VEC, TBK, TST>(st, st + TBK * S::LA, pf * TBK, m0, n0, M, N, K, A, lda, B, ldb);
     }
     cp_async_commit();
-    const double *sA = smem + (kt % STAGES) * S::STAGE;
-    const double *sB = sA + BK * S::LA;
+    const double *sA = smem + (kt % TST) * S::STAGE;
+    const double *sB = sA + TBK * S::LA;
 #pragma unroll
-    for (int kk = 0; kk < BK; kk += 8) {
+    for (int kk = 0; kk < TBK; kk += 8) {
       double a[FM][4], b[FN][2];
 #pragma unroll
       for (int i = 0; i < FM; ++i) {
@@ -167,6 +183,9 @@ __device__ __forceinline__ void gemm_tile_impl(double *smem, int bm, int bn, int
     }
   }
   cp_async_wait<0>();
+  double rtr[FM][2], rsq[FM][2];  // fused step: this thread's part of each of its rows
+#pragma unroll
+  for (int i = 0; i < FM; ++i) rtr[i][0] = rtr[i][1] = rsq[i][0] = rsq[i][1] = 0.0;
 #pragma unroll
   for (int i = 0; i < FM; ++i)
 #pragma unroll
@@ -176,28 +195,77 @@ __device__ __forceinline__ void gemm_tile_impl(double *smem, int bm, int bn, int
         const int m = m0 + wm * TM + i * 16 + g + (q >> 1) * 8;
         const int n = n0 + wn * TN + j * 8 + 2 * t + (q & 1);
         if (m >= M || n >= N) continue;
-        const double v = alpha * acc[i][j][q];
+        double v = alpha * acc[i][j][q];
         if (!sym) {
           C[(size_t)m * ldc + n] = v;
         } else if (m >= n) {
+          if (fuse.x) {
+            if (!fuse.square) v = 2.0 * fuse.x[(size_t)m * lda + n] - v;
+            if (m == n) {
+              rtr[i][q >> 1] += v;
+              rsq[i][q >> 1] += v * v;
+            } else {
+              rsq[i][q >> 1] += 2.0 * (v * v);
+            }
+          }
           C[(size_t)m * ldc + n] = v;
           C[(size_t)n * ldc + m] = v;
         }
       }
+  if (fuse.x) {
+    static_assert(TN == 32 && TBN == 64, "the fused SP2 sums assume 32-column warp spans of 64-column tiles");
+    // the four lanes of a row (t = 0..3) by a fixed tree
+#pragma unroll
+    for (int i = 0; i < FM; ++i)
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int o = 1; o <= 2; o <<= 1) {
+          rtr[i][h] += __shfl_xor_sync(0xffffffffu, rtr[i][h], o);
+          rsq[i][h] += __shfl_xor_sync(0xffffffffu, rsq[i][h], o);
+        }
+    __syncthreads();  // the pipeline's shared memory is free again
+    double *row_tr = smem, *row_sq = smem + 2 * TBM;  // [span][row of the tile]
+    if (t == 0)
+#pragma unroll
+      for (int i = 0; i < FM; ++i)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = wm * TM + i * 16 + g + 8 * h;
+          row_tr[wn * TBM + r] = rtr[i][h];
+          row_sq[wn * TBM + r] = rsq[i][h];
+        }
+    __syncthreads();
+    constexpr int NB = TBM / 64;
+    if (tid < NB) {
+      const int R = m0 / 64 + tid, Cb = n0 / 64;
+      if (R >= Cb) {
+        double a = 0.0, b = 0.0;
+        for (int r = 64 * tid; r < 64 * tid + 64; ++r) {
+          a += row_tr[r] + row_tr[TBM + r];
+          b += row_sq[r] + row_sq[TBM + r];
+        }
+        const size_t blk = (size_t)R * (R + 1) / 2 + Cb;
+        fuse.parts[2 * blk] = a;
+        fuse.parts[2 * blk + 1] = b;
+      }
+    }
+  }
 }
 
 __device__ __forceinline__ bool gemm_vec_ok(const double *A, int lda, const double *B, int ldb) {
   return ((lda | ldb) & 1) == 0 && ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) == 0;
 }
 
-template <int TBM, int TBN>
+template <int TBM, int TBN, int TBK = BK, int TST = STAGES>
 __device__ __forceinline__ void gemm_tile_t(double *smem, int bm, int bn, int M, int N, int K, double alpha,
                                             const double *__restrict__ A, int lda, const double *__restrict__ B,
-                                            int ldb, double *__restrict__ C, int ldc, int sym) {
+                                            int ldb, double *__restrict__ C, int ldc, int sym,
+                                            const Sp2Fuse &fuse = Sp2Fuse{nullptr, false, nullptr}) {
   if (gemm_vec_ok(A, lda, B, ldb))
-    gemm_tile_impl<TBM, TBN, true>(smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym);
+    gemm_tile_impl<TBM, TBN, true, TBK, TST>(smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym, fuse);
   else
-    gemm_tile_impl<TBM, TBN, false>(smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym);
+    gemm_tile_impl<TBM, TBN, false, TBK, TST>(smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym, fuse);
 }
 
 __device__ __forceinline__ void gemm_tile(double *smem, int bm, int bn, int M, int N, int K, double alpha,
@@ -221,25 +289,39 @@ static inline int sym_tiles(int n) {
   return t;
 }
 
+// The fused SP2 step of a symmetric n x n product (launch_sp2_step): parts != null makes
+// the tiles apply the update chosen in state[kSp2Square] and write the 64 x 64 block trace
+// partials; the first CTA records their count in state[kSp2Parts].
+__device__ __forceinline__ Sp2Fuse sp2_fuse(int n, const double *x, double *state, double *parts) {
+  if (!parts) return Sp2Fuse{nullptr, false, nullptr};
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const int t64 = (n + 63) / 64;
+    state[kSp2Parts] = (double)(t64 * (t64 + 1) / 2);
+  }
+  return Sp2Fuse{x, state[kSp2Square] != 0.0, parts};
+}
+
 // Symmetric n x n product on 64x64 tiles of the lower triangle (four CTAs per SM): more,
 // smaller tiles than k_gemm_sym, the faster shape when 128x64 tiles leave SMs idle.
 __global__ void __launch_bounds__(128, 4) k_gemm_sym64(int n, int K, double alpha, const double *__restrict__ A,
                                                        int lda, const double *__restrict__ B, int ldb,
-                                                       double *__restrict__ C, int ldc, const double *__restrict__ sp2,
-                                                       int step) {
+                                                       double *__restrict__ C, int ldc, double *__restrict__ sp2,
+                                                       int step, double *__restrict__ parts) {
   extern __shared__ __align__(16) double gemm_smem[];
   if (!sp2_active(sp2, step)) return;
   int t = blockIdx.x, r = 0;
   while ((r + 1) * (r + 2) / 2 <= t) ++r;
-  gemm_tile_t<BM, BN>(gemm_smem, r, t - r * (r + 1) / 2, n, n, K, alpha, A, lda, B, ldb, C, ldc, 1);
+  gemm_tile_t<BM, BN>(gemm_smem, r, t - r * (r + 1) / 2, n, n, K, alpha, A, lda, B, ldb, C, ldc, 1,
+                      sp2_fuse(n, A, sp2, parts));
 }
 
 // Symmetric n x n product over the enumerated lower-triangle tiles (row block r holds
-// column blocks 0 .. ceil((r+1) SYM_BM / SYM_BN) - 1).
+// column blocks 0 .. ceil((r+1) SYM_BM / SYM_BN) - 1); K slabs of TBK rows, TST stages.
+template <int TBK, int TST>
 __global__ void __launch_bounds__(128, 2) k_gemm_sym(int n, int K, double alpha, const double *__restrict__ A,
                                                      int lda, const double *__restrict__ B, int ldb,
-                                                     double *__restrict__ C, int ldc, const double *__restrict__ sp2,
-                                                     int step) {
+                                                     double *__restrict__ C, int ldc, double *__restrict__ sp2,
+                                                     int step, double *__restrict__ parts) {
   extern __shared__ __align__(16) double gemm_smem[];
   if (!sp2_active(sp2, step)) return;  // an SP2 step after the purification stopped
   const int cols = (n + SYM_BN - 1) / SYM_BN;
@@ -249,7 +331,8 @@ __global__ void __launch_bounds__(128, 2) k_gemm_sym(int n, int K, double alpha,
     if (t < nc) break;
     t -= nc;
   }
-  gemm_tile_t<SYM_BM, SYM_BN>(gemm_smem, r, t, n, n, K, alpha, A, lda, B, ldb, C, ldc, 1);
+  gemm_tile_t<SYM_BM, SYM_BN, TBK, TST>(gemm_smem, r, t, n, n, K, alpha, A, lda, B, ldb, C, ldc, 1,
+                                        sp2_fuse(n, A, sp2, parts));
 }
 
 // Grouped over molecules: item = one 64x64 tile of one molecule's product.
@@ -283,7 +366,8 @@ static void gemm_smem_attr() {
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64 || done[dev]) return;
   cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
-  cudaFuncSetAttribute(k_gemm_sym, cudaFuncAttributeMaxDynamicSharedMemorySize, SYM_SMEM);
+  cudaFuncSetAttribute(k_gemm_sym<BK, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, SYM_SMEM);
+  cudaFuncSetAttribute(k_gemm_sym<32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SYM_SMEM_K32);
   cudaFuncSetAttribute(k_gemm_sym64, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
   cudaFuncSetAttribute(k_b_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
   done[dev] = true;
@@ -307,20 +391,32 @@ void launch_gemm_tn(cudaStream_t st, int M, int N, int K, double alpha, const do
 }
 
 // Symmetric product C = alpha A^T B (n x n, inner dimension K) on the tile shape the
-// autotuner picked for this size: 0 = 128x64 (k_gemm_sym), 1 = 64x64 (k_gemm_sym64).
+// autotuner picked for this size: 0 = 128x64 (k_gemm_sym, 16-deep slabs, three stages),
+// 1 = 64x64 (k_gemm_sym64), 2 = 128x64 with 32-deep slabs in two stages. All give the same
+// bits: every element is the same chain of DMMA steps over k in the same order. With
+// `parts` the product is the fused SP2 step (sp2_fuse).
 static void launch_sym(cudaStream_t st, const char *what, int n, int K, double alpha, const double *A, int lda,
-                       const double *B, int ldb, double *C, int ldc, const double *sp2, int step) {
+                       const double *B, int ldb, double *C, int ldc, double *sp2, int step, double *parts = nullptr) {
   gemm_smem_attr();
   const int bucket = ((n + 255) / 256) * 256;
-  autotune(st, std::string(what) + "|n" + std::to_string(bucket), 2, [&](int v) {
+  autotune(st, std::string(what) + "|n" + std::to_string(bucket), 3, [&](int v) {
     if (v == 0) {
-      k_gemm_sym<<<sym_tiles(n), 128, SYM_SMEM, st>>>(n, K, alpha, A, lda, B, ldb, C, ldc, sp2, step);
-    } else {
+      k_gemm_sym<BK, STAGES><<<sym_tiles(n), 128, SYM_SMEM, st>>>(n, K, alpha, A, lda, B, ldb, C, ldc, sp2, step,
+                                                                  parts);
+    } else if (v == 1) {
       const int t = (n + BM - 1) / BM;
-      k_gemm_sym64<<<t * (t + 1) / 2, 128, GEMM_SMEM, st>>>(n, K, alpha, A, lda, B, ldb, C, ldc, sp2, step);
+      k_gemm_sym64<<<t * (t + 1) / 2, 128, GEMM_SMEM, st>>>(n, K, alpha, A, lda, B, ldb, C, ldc, sp2, step, parts);
+    } else {
+      k_gemm_sym<32, 2><<<sym_tiles(n), 128, SYM_SMEM_K32, st>>>(n, K, alpha, A, lda, B, ldb, C, ldc, sp2, step,
+                                                                  parts);
     }
     note_launch();
   });
+}
+
+size_t sp2_parts_doubles(int n) {
+  const int t = (n + BM - 1) / BM;
+  return 2 * (size_t)std::max(std::max(sym_tiles(n), t * (t + 1) / 2), 296) + 8;
 }
 
 void launch_density(cudaStream_t st, int n, int k, double w, const double *V, int ldv, double *P) {
@@ -792,6 +888,49 @@ __global__ void k_sp2_update(size_t len, double *__restrict__ X, const double *_
     X[e] = square ? X2[e] : 2.0 * X[e] - X2[e];
 }
 
+// tr X and |X|_F^2 (= tr X^2 for symmetric X) of the starting iterate, per-block partials in
+// the layout of the fused step's (parts[2 b], parts[2 b + 1]); the count to state[kSp2Parts].
+__global__ void k_sp2_norms(int n, const double *__restrict__ X, double *__restrict__ state,
+                            double *__restrict__ parts) {
+  const size_t len = (size_t)n * n;
+  double tr = 0.0, sq = 0.0;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x) {
+    const double v = X[e];
+    sq += v * v;
+    if (e % (n + 1) == 0) tr += v;
+  }
+  tr = block_sum<256>(tr);
+  sq = block_sum<256>(sq);
+  if (threadIdx.x == 0) {
+    parts[2 * blockIdx.x] = tr;
+    parts[2 * blockIdx.x + 1] = sq;
+    if (blockIdx.x == 0) state[kSp2Parts] = (double)gridDim.x;
+  }
+}
+
+// The SP2 decision of step `step` from the current iterate's trace partials (the fused
+// step's epilogue, or k_sp2_norms for the first): tr X, tr X^2 = |X|_F^2, the branch
+// (square when it brings the trace closer to n_occ) and the stopping rule on tr X - tr X^2.
+__global__ void k_sp2_decide(double n_occ, double *__restrict__ state, const double *__restrict__ parts, int step,
+                             Sp2Rule rule) {
+  if (!sp2_active(state, step)) return;
+  const int count = (int)state[kSp2Parts];
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < count; i += blockDim.x) {
+    a += parts[2 * i];
+    b += parts[2 * i + 1];
+  }
+  a = block_sum<256>(a);
+  b = block_sum<256>(b);
+  if (threadIdx.x == 0) {
+    state[kSp2TrX] = a;
+    state[kSp2TrX2] = b;
+    state[kSp2Square] = fabs(b - n_occ) < fabs(2.0 * a - b - n_occ) ? 1.0 : 0.0;
+    state[kSp2Err] = a - b;
+    sp2_control(state, step, a - b, rule);
+  }
+}
+
 __global__ void k_sp2_reset(double *state) {
   const int i = threadIdx.x;
   if (i < kSp2Len) state[i] = i == kSp2Stop ? 1.0e9 : 0.0;
@@ -831,7 +970,21 @@ void launch_sp2_reset(cudaStream_t st, double *state) {
 }
 
 void launch_sp2_square(cudaStream_t st, int n, const double *X, double *X2, const double *state, int step) {
-  launch_sym(st, "sp2_square", n, n, 1.0, X, n, X, n, X2, n, state, step);
+  launch_sym(st, "sp2_square", n, n, 1.0, X, n, X, n, X2, n, const_cast<double *>(state), step);
+}
+
+void launch_sp2_step(cudaStream_t st, int n, const double *X, double *Y, double *state, double *parts, int step) {
+  launch_sym(st, "sp2_square", n, n, 1.0, X, n, X, n, Y, n, state, step, parts);
+}
+
+void launch_sp2_norms(cudaStream_t st, int n, const double *X, double *state, double *parts) {
+  k_sp2_norms<<<296, 256, 0, st>>>(n, X, state, parts);
+  note_launch();
+}
+
+void launch_sp2_decide(cudaStream_t st, double n_occ, double *state, const double *parts, int step, Sp2Rule rule) {
+  k_sp2_decide<<<1, 256, 0, st>>>(n_occ, state, parts, step, rule);
+  note_launch();
 }
 
 void launch_sp2_trace(cudaStream_t st, int n, const double *X, const double *X2, double n_occ, double *state, int step,
