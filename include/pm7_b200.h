@@ -73,9 +73,11 @@ typedef enum pm7_dipole_origin {
   PM7_DIPOLE_CENTRE_OF_CHARGE = 2
 } pm7_dipole_origin;
 
-/* Arithmetic of the SCF cycles. FP64 is the plain path; MIXED runs the early
- * cycles in FP32 (Fock build and density on tensor cores with FP32
- * accumulation) and re-converges in FP64 (engine knob; no reference analogue). */
+/* Arithmetic of the SCF cycles. FP64 is the plain path; MIXED computes the early
+ * cycles' densities (SP2 squarings) and, on the plain path, their DIIS commutator product
+ * at FP32 accuracy on the tcgen05 tensor cores (3xTF32, FP32 accumulation), keeps the Fock
+ * build in FP64, and re-converges in FP64 cycles, the only ones that may end the SCF
+ * (engine knob; no reference analogue). */
 typedef enum pm7_precision {
   PM7_PRECISION_FP64 = 0,
   PM7_PRECISION_MIXED = 1
