@@ -2043,7 +2043,10 @@ class BatchRunner {
   unsigned rside_ = 0;                // round robin over the side streams
   int side_used_ = 0;       // side streams with queued eigensolves not yet joined
   size_t lz_smem_ = 48 * 1024;  // dynamic shared memory k_b_lanczos is set up for
-  static constexpr int kLeanEig = 512;  // from this order the library solver, below the cluster one
+  // Eigenvalues alone at retirement: the cluster kernel for every order it takes (it runs
+  // asynchronously beside the next SCF step; cuSOLVER's dsyevd held the host thread for the
+  // whole solve of each large molecule, ~1 s per 600 requests of the served stream).
+  static constexpr int kLeanEig = kTriMaxN + 1;
   void *work_ = nullptr;
   size_t work_cap_ = 0;
   std::vector<char> host_work_;

@@ -189,7 +189,7 @@ def test_engine_without_matrices_retires_asynchronously_and_alone_equals_mixed()
     # without returned matrices a retirement's eigenvalue solves run beside the next SCF
     # step and its outputs are gathered one step later; results must not change
     target = G.water_cluster(14, seed=5)
-    big = G.water_cluster(180, seed=6)  # order >= 512: the library eigensolver on a side stream
+    big = G.water_cluster(180, seed=6)  # order 1,080: the cluster eigenvalue kernel beside the next step
     others = [G.alkane(n, seed=n) for n in (3, 11, 26)] + [G.water_cluster(k, seed=k) for k in (8, 40)] + [big]
     with api.Engine() as eng:
         t = eng.submit(*target, want_matrices=0)
