@@ -363,7 +363,9 @@ pm7_status pm7_batch_partition(int32_t n_molecules, const pm7_molecule *molecule
 /* A serving engine: a worker thread on one GPU admits submitted closed-shell RHF
  * requests as HBM (their device footprint against hbm_budget_mb, or 80% of free
  * memory when -1) and max_active (0 = unlimited) allow, advances all admitted
- * requests together one SCF iteration per step, and retires each as it converges. */
+ * requests together one SCF iteration per step, and retires each as it converges.
+ * Open-shell and forced-UHF requests run one at a time through the pm7_run path on a
+ * second worker thread, beside the batch. */
 typedef struct pm7_engine pm7_engine;
 typedef struct pm7_engine_config {
   int32_t device;

@@ -933,6 +933,7 @@ struct BatchMol {
   int n_occ = 0;
   bool dframe = false;
   std::vector<double> init_density;  // optional caller density
+  std::vector<double> init_spin;     // optional caller spin density (single-path requests)
   // device state
   int slot = -1;
   char *base = nullptr;
@@ -1175,10 +1176,9 @@ class BatchRunner {
     b->mixed = o.precision == PM7_PRECISION_MIXED && b->L.nao >= sp2_min_nao_;
     b->bytes = mol_layout(*b, nullptr);
     b->np = bucket_size(b->L.nao);
-    if (o.initial_density) {
-      const size_t nn = (size_t)b->L.nao * b->L.nao;
-      b->init_density.assign(o.initial_density, o.initial_density + nn);
-    }
+    const size_t nn = (size_t)b->L.nao * b->L.nao;
+    if (o.initial_density) b->init_density.assign(o.initial_density, o.initial_density + nn);
+    if (o.initial_spin_density) b->init_spin.assign(o.initial_spin_density, o.initial_spin_density + nn);
     b->o.initial_density = nullptr;
     b->o.initial_spin_density = nullptr;
     return b;
@@ -2163,6 +2163,7 @@ struct pm7_engine {
   std::mutex mu;
   std::condition_variable cv, done_cv;
   std::deque<pm7::EngineRequest *> queue;
+  std::deque<pm7::EngineRequest *> single;  // open-shell requests: the pm7_run path, own thread
   std::unordered_map<uint64_t, std::unique_ptr<pm7::EngineRequest>> requests;
   std::unordered_map<pm7::BatchMol *, pm7::EngineRequest *> by_mol;
   uint64_t next_ticket = 1;
@@ -2170,10 +2171,49 @@ struct pm7_engine {
   int64_t admitted = 0, peak_active = 0, peak_bytes = 0;
   bool stop = false;
   std::string worker_error;
-  std::thread worker;
+  std::thread worker, single_worker;
 };
 
 namespace pm7 {
+
+// Requests the batch does not take (open shells, forced UHF) run one at a time through
+// pm7_run / pm7_gradient on a second worker thread, on the device context's own stream, so
+// they proceed beside the batch's SCF steps instead of being refused.
+static void engine_single_loop(pm7_engine *E) {
+  const pm7_params *params = nullptr;
+  const pm7_status ps = pm7_params_load(E->method, &params);
+  for (;;) {
+    EngineRequest *r = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(E->mu);
+      E->cv.wait(lk, [&] { return E->stop || !E->single.empty(); });
+      if (E->single.empty()) break;  // stopping, nothing left
+      r = E->single.front();
+      E->single.pop_front();
+    }
+    BatchMol &b = *r->mol;
+    std::vector<uint8_t> z(b.m.z.begin(), b.m.z.end());
+    const pm7_molecule mol{b.m.n, z.data(), b.m.xyz.data()};
+    pm7_options o = b.o;
+    o.device = E->device;
+    o.initial_density = b.init_density.empty() ? nullptr : b.init_density.data();
+    o.initial_spin_density = b.init_spin.empty() ? nullptr : b.init_spin.data();
+    pm7_result res{};
+    pm7_status st = ps;
+    std::string err = ps == PM7_OK ? "" : g_last_error;
+    if (ps == PM7_OK) {
+      st = b.grad_out ? pm7_gradient(&mol, params, &o, &res, b.grad_out, nullptr) : pm7_run(&mol, params, &o, &res);
+      err = st == PM7_OK ? "" : g_last_error;
+    }
+    std::lock_guard<std::mutex> lk(E->mu);
+    r->status = st;
+    r->error = err;
+    r->result = res;
+    r->done = true;
+    r->t_done = std::chrono::steady_clock::now();
+    E->done_cv.notify_all();
+  }
+}
 
 static void engine_loop(pm7_engine *E) {
   try {
@@ -2335,6 +2375,7 @@ pm7_status pm7_engine_create(const pm7_engine_config *config, pm7_engine **out) 
     E->budget = batch_budget(config->hbm_budget_mb);
     E->max_active = config->max_active;
     E->worker = std::thread(engine_loop, E);
+    E->single_worker = std::thread(engine_single_loop, E);
     *out = E;
     g_last_error.clear();
     return PM7_OK;
@@ -2365,10 +2406,9 @@ static pm7_status engine_submit(pm7_engine *E, const pm7_molecule *molecule, con
     EngineRequest *raw = r.get();
     try {
       r->mol = E->runner->prepare(to_molecule(molecule), *options);
-      if (!BatchRunner::batchable(*r->mol))
-        throw Failure{PM7_ERR_UNSUPPORTED, "the serving engine runs closed-shell RHF requests; use pm7_run"};
       r->mol->grad_out = gradient;
-      E->queue.push_back(raw);
+      if (BatchRunner::batchable(*r->mol)) E->queue.push_back(raw);
+      else E->single.push_back(raw);
     } catch (const Failure &f) {
       raw->status = f.code;
       raw->error = f.msg;
@@ -2439,6 +2479,7 @@ pm7_status pm7_engine_destroy(pm7_engine *E) {
     E->cv.notify_all();
   }
   if (E->worker.joinable()) E->worker.join();
+  if (E->single_worker.joinable()) E->single_worker.join();
   if (std::getenv("PM7_BATCH_TRACE") && E->runner) {
     std::fprintf(stderr, "engine: %lld requests, peak %lld resident; iterations (host wall, s):", (long long)E->admitted,
                  (long long)E->peak_active);

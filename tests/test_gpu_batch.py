@@ -122,15 +122,31 @@ def test_engine_serves_and_alone_equals_mixed(golden):
     assert abs(mixed["heat_of_formation_kcal"] - o["heat_of_formation_kcal"]) < DHF_TOL
 
 
-def test_engine_rejects_open_shell_and_bad_input():
+def test_engine_serves_open_shells_beside_the_batch_and_rejects_bad_input():
+    # open-shell (UHF) requests run through the single-molecule path on the engine's second
+    # worker, beside closed-shell requests in the batch; results as run_pm7 / the oracle
+    methyl = (np.array([6, 1, 1, 1], np.uint8), np.array([[0, 0, 0], [2.0, 0, 0], [-1.0, 1.7, 0], [-1.0, -1.7, 0]]))
+    triplet_pair = (np.array([8, 8], np.uint8), np.array([[0, 0, 0], [1.21 / 0.529177210903, 0, 0]]))  # O2
+    closed = [G.water_cluster(k, seed=k) for k in (3, 9)]
     with api.Engine() as eng:
-        t = eng.submit(np.array([6, 1, 1, 1], np.uint8),
-                       np.array([[0, 0, 0], [2.0, 0, 0], [-1.0, 1.7, 0], [-1.0, -1.7, 0]]), multiplicity=2)
-        done, r = eng.poll(t, wait=True)
-        assert done and isinstance(r, api.Pm7Error) and r.code == 4
+        t1 = eng.submit(*methyl, multiplicity=2)
+        tc = [eng.submit(*m) for m in closed]
+        t2 = eng.submit(*triplet_pair, multiplicity=3)
+        t3 = eng.submit(*methyl, multiplicity=2, gradient=True)
+        r1, r2, r3 = (eng.poll(t, wait=True)[1] for t in (t1, t2, t3))
+        rc = [eng.poll(t, wait=True)[1] for t in tc]
         t = eng.submit(np.array([1, 1], np.uint8), np.zeros((2, 3)))
-        done, r = eng.poll(t, wait=True)
-        assert done and isinstance(r, api.Pm7Error) and r.code == 1
+        done, bad = eng.poll(t, wait=True)
+        assert done and isinstance(bad, api.Pm7Error) and bad.code == 1
+    for r, (z, x), mult in ((r1, methyl, 2), (r2, triplet_pair, 3), (r3, methyl, 2)):
+        assert not isinstance(r, Exception) and r["unrestricted"]
+        o = harness.run(z, x, multiplicity=mult)
+        assert abs(r["heat_of_formation_kcal"] - o["heat_of_formation_kcal"]) < DHF_TOL
+        assert np.max(np.abs(r["charges"] - o["charges"])) < Q_TOL
+    single = api.closed_form_gradient(*methyl, multiplicity=2)
+    np.testing.assert_allclose(r3["gradient"], single["gradient"], rtol=0, atol=1e-9)
+    for r, m in zip(rc, closed):
+        assert abs(r["heat_of_formation_kcal"] - harness.run(*m)["heat_of_formation_kcal"]) < DHF_TOL
 
 
 def test_batch_density_by_sp2_and_by_eigensolver_agree(monkeypatch):
