@@ -652,7 +652,9 @@ __global__ void __launch_bounds__(1024) k_b_lanczos(BatchList L, const MolDesc *
   c.sp2_emax = fmin(ehi + pad, c.sp2_emax);
 }
 
-// X <- (emax I - X) / (emax - emin): spectrum in [0, 1], occupied levels near 1. Item = a chunk.
+// X <- (emax I - X) / (emax - emin): spectrum in [0, 1], occupied levels near 1. Item = a
+// chunk; the chunk's tr X and |X|_F^2 go to part[q kPart + 0 / 1] (the first fused step's
+// decision).
 __global__ void __launch_bounds__(RB) k_b_sp2_x0(BatchList L, const MolDesc *__restrict__ D,
                                                  const MolCtl *__restrict__ C) {
   const ChunkRef r = chunk_ref(L, D, blockIdx.x);
@@ -660,19 +662,31 @@ __global__ void __launch_bounds__(RB) k_b_sp2_x0(BatchList L, const MolDesc *__r
   const MolCtl &c = C[r.slot];
   const int n = d.g.nao;
   const double emax = c.sp2_emax, inv = 1.0 / (c.sp2_emax - c.sp2_emin);
+  double v[2] = {0.0, 0.0};
   for (size_t e = r.e0 + threadIdx.x; e < r.e1; e += RB) {
     const size_t i = e / n, j = e - i * n;
-    d.X[e] = ((i == j ? emax : 0.0) - d.X[e]) * inv;
+    const double x = ((i == j ? emax : 0.0) - d.X[e]) * inv;
+    d.X[e] = x;
+    if (i == j) v[0] += x;
+    v[1] += x * x;
+  }
+  block_sum_n<2>(v);
+  if (threadIdx.x == 0) {
+    d.part[(size_t)r.q * kPart + 0] = v[0];
+    d.part[(size_t)r.q * kPart + 1] = v[1];
   }
 }
 
-// One SP2 decision after Pn = X X (block per molecule): the trace rule picks X <- X^2 or
-// 2X - X^2 (whichever moves tr X toward n_occ); the purification stops at idempotency
-// (tr X - tr X^2 at the rounding floor) with tr X = n_occ, or gives up (non-finite, 100
-// steps, or an idempotent X of the wrong trace) and leaves the molecule to the
-// eigensolver. flags[m]: 0 running, 1 done, 2 failed.
-__global__ void __launch_bounds__(RB) k_b_sp2_decide(BatchList L, const MolDesc *__restrict__ D,
-                                                     MolCtl *__restrict__ C, unsigned char *__restrict__ flags) {
+// The fused fp64 SP2 step's decision (block per molecule), before the squaring: tr X and
+// tr X^2 = |X|_F^2 of the current iterate from its partials (the first step: x0's chunk
+// partials; later: the previous squaring's 64 x 64 tile partials, both summed in a fixed
+// order), then the trace rule (X^2 or 2X - X^2, whichever moves tr X toward n_occ) and the
+// stopping rule: idempotency (tr X - tr X^2 at the rounding floor) with tr X = n_occ, or
+// failure (non-finite, 100 steps, or an idempotent X of the wrong trace), which leaves the
+// molecule to the eigensolver; flags[m]: 0 running, 1 done, 2 failed. sp2_apply marks the
+// molecules whose step runs now.
+__global__ void __launch_bounds__(RB) k_b_sp2_decide64(BatchList L, const MolDesc *__restrict__ D,
+                                                       MolCtl *__restrict__ C, unsigned char *__restrict__ flags) {
   const int m = blockIdx.x;
   const int slot = L.slot[m];
   const MolDesc &d = D[slot];
@@ -681,18 +695,20 @@ __global__ void __launch_bounds__(RB) k_b_sp2_decide(BatchList L, const MolDesc 
     if (threadIdx.x == 0) c.sp2_apply = 0;
     return;
   }
-  const int n = d.g.nao;
+  const int n = d.g.nao, k = c.sp2_steps;
+  const int t = (n + 63) / 64;
+  const int count = k == 0 ? items_chunks(n) : t * (t + 1) / 2;
+  const size_t stride = k == 0 ? kPart : 2;
   double v[2] = {0.0, 0.0};
-  for (int i = threadIdx.x; i < n; i += RB) {
-    v[0] += d.X[(size_t)i * n + i];
-    v[1] += d.Pn[(size_t)i * n + i];
+  for (int i = threadIdx.x; i < count; i += RB) {
+    v[0] += d.part[(size_t)i * stride + 0];
+    v[1] += d.part[(size_t)i * stride + 1];
   }
   block_sum_n<2>(v);
   if (threadIdx.x == 0) {
     const double a = v[0], b = v[1], nocc = (double)d.n_occ;
     c.sp2_square = fabs(b - nocc) < fabs(2.0 * a - b - nocc) ? 1 : 0;
     const double e = a - b;
-    const int k = c.sp2_steps;  // errors recorded before this one
     int state = 0;
     if (!isfinite(e)) {
       state = 2;
@@ -712,21 +728,15 @@ __global__ void __launch_bounds__(RB) k_b_sp2_decide(BatchList L, const MolDesc 
   }
 }
 
-// X <- X^2 or 2X - X^2 for the molecules decided this step; Pn = 2 X for those that
-// converged. Item = a chunk.
-__global__ void __launch_bounds__(RB) k_b_sp2_apply(BatchList L, const MolDesc *__restrict__ D,
-                                                    const MolCtl *__restrict__ C) {
+// After the fused steps: a converged molecule whose last iterate landed in X gets the
+// density Pn = 2 X (one landing in Pn was written doubled by the squaring). Item = a chunk.
+__global__ void __launch_bounds__(RB) k_b_sp2_final64(BatchList L, const MolDesc *__restrict__ D,
+                                                      const MolCtl *__restrict__ C) {
   const ChunkRef r = chunk_ref(L, D, blockIdx.x);
   const MolDesc &d = D[r.slot];
   const MolCtl &c = C[r.slot];
-  if (!c.sp2_apply) return;
-  const bool sq = c.sp2_square != 0, fin = c.sp2_state == 1;
-  for (size_t e = r.e0 + threadIdx.x; e < r.e1; e += RB) {
-    const double x2 = d.Pn[e];
-    const double x = sq ? x2 : 2.0 * d.X[e] - x2;
-    d.X[e] = x;
-    if (fin) d.Pn[e] = 2.0 * x;
-  }
+  if (c.sp2_state != 1 || (c.sp2_steps - 1) % 2 == 0) return;
+  for (size_t e = r.e0 + threadIdx.x; e < r.e1; e += RB) d.Pn[e] = 2.0 * d.X[e];
 }
 
 // Stall guard (StallGuardHost::update, scf.rs:1581-1656).
@@ -1372,11 +1382,10 @@ class BatchRunner {
       // attributes were set in the constructor, outside any capture).
       auto queue_chunk = [&](bool r64, bool r32) {
         for (int k = 0; k < chunk; ++k) {
-          if (r64) {
-            launch_b_gemm(st_, S.glow, desc_, ctl_, nullptr, 2);
-            k_b_sp2_decide<<<S.mol.n, RB, 0, st_>>>(S.mol, desc_, ctl_, f64);
-            k_b_sp2_apply<<<S.chunks.total, RB, 0, st_>>>(S.chunks, desc_, ctl_);
-            note_launch(2);
+          if (r64) {  // the fused step: decision, then the squaring that applies it
+            k_b_sp2_decide64<<<S.mol.n, RB, 0, st_>>>(S.mol, desc_, ctl_, f64);
+            note_launch();
+            launch_b_gemm(st_, S.glow, desc_, ctl_, nullptr, 3);
           }
           if (r32) {
             launch_b_square_tf32x3(st_, T.tiles, desc_, ctl_, maps_, err32_);
@@ -1417,6 +1426,10 @@ class BatchRunner {
         for (int m = 0; m < T.mol.n; ++m) run32 = run32 || flags_h_[cap_ + m] == 0;
       }
       if (exec) CUDA_OK(cudaGraphExecDestroy(exec));
+      if (S.mol.n) {
+        k_b_sp2_final64<<<S.chunks.total, RB, 0, st_>>>(S.chunks, desc_, ctl_);
+        note_launch();
+      }
       for (int m = 0; m < S.mol.n; ++m)
         if (flags_h_[m] != 1) {
           fallback.push_back(purify64[m]);

@@ -115,6 +115,7 @@ struct Sp2Fuse {
   const double *x;  // null: a plain product
   bool square;
   double *parts;
+  double scale;     // written elements are scale * y (2: the final iterate becomes the density)
 };
 
 // One TBM x TBN tile, 4 warps as 2 x 2 of (TBM/2) x (TBN/2). sym != 0: only elements
@@ -124,7 +125,7 @@ template <int TBM, int TBN, bool VEC, int TBK = BK, int TST = STAGES>
 __device__ __forceinline__ void gemm_tile_impl(double *smem, int bm, int bn, int M, int N, int K, double alpha,
                                                const double *__restrict__ A, int lda, const double *__restrict__ B,
                                                int ldb, double *__restrict__ C, int ldc, int sym,
-                                               const Sp2Fuse &fuse = Sp2Fuse{nullptr, false, nullptr}) {
+                                               const Sp2Fuse &fuse = Sp2Fuse{nullptr, false, nullptr, 1.0}) {
   using S = GemmShape<TBM, TBN, TBK, TST>;
   constexpr int TM = TBM / 2, TN = TBN / 2, FM = TM / 16, FN = TN / 8;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -208,6 +209,7 @@ __device__ __forceinline__ void gemm_tile_impl(double *smem, int bm, int bn, int
               rsq[i][q >> 1] += 2.0 * (v * v);
             }
           }
+          if (fuse.x) v *= fuse.scale;
           C[(size_t)m * ldc + n] = v;
           C[(size_t)n * ldc + m] = v;
         }
@@ -261,7 +263,7 @@ template <int TBM, int TBN, int TBK = BK, int TST = STAGES>
 __device__ __forceinline__ void gemm_tile_t(double *smem, int bm, int bn, int M, int N, int K, double alpha,
                                             const double *__restrict__ A, int lda, const double *__restrict__ B,
                                             int ldb, double *__restrict__ C, int ldc, int sym,
-                                            const Sp2Fuse &fuse = Sp2Fuse{nullptr, false, nullptr}) {
+                                            const Sp2Fuse &fuse = Sp2Fuse{nullptr, false, nullptr, 1.0}) {
   if (gemm_vec_ok(A, lda, B, ldb))
     gemm_tile_impl<TBM, TBN, true, TBK, TST>(smem, bm, bn, M, N, K, alpha, A, lda, B, ldb, C, ldc, sym, fuse);
   else
@@ -293,12 +295,12 @@ static inline int sym_tiles(int n) {
 // the tiles apply the update chosen in state[kSp2Square] and write the 64 x 64 block trace
 // partials; the first CTA records their count in state[kSp2Parts].
 __device__ __forceinline__ Sp2Fuse sp2_fuse(int n, const double *x, double *state, double *parts) {
-  if (!parts) return Sp2Fuse{nullptr, false, nullptr};
+  if (!parts) return Sp2Fuse{nullptr, false, nullptr, 1.0};
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     const int t64 = (n + 63) / 64;
     state[kSp2Parts] = (double)(t64 * (t64 + 1) / 2);
   }
-  return Sp2Fuse{x, state[kSp2Square] != 0.0, parts};
+  return Sp2Fuse{x, state[kSp2Square] != 0.0, parts, 1.0};
 }
 
 // Symmetric n x n product on 64x64 tiles of the lower triangle (four CTAs per SM): more,
@@ -354,8 +356,25 @@ __global__ void __launch_bounds__(128, 4) k_b_gemm(BatchList L, const MolDesc *_
     int bm = 0;
     while ((bm + 1) * (bm + 2) / 2 <= local) ++bm;
     const int bn = local - bm * (bm + 1) / 2;
-    if (op == 1) gemm_tile(gemm_smem, bm, bn, n, n, d.n_occ, 2.0, E[m].in, E[m].ldv, E[m].in, E[m].ldv, d.Pn, n, 1);
-    else if (Cc[slot].sp2_state == 0) gemm_tile(gemm_smem, bm, bn, n, n, n, 1.0, d.X, n, d.X, n, d.Pn, n, 1);
+    if (op == 1) {
+      gemm_tile(gemm_smem, bm, bn, n, n, d.n_occ, 2.0, E[m].in, E[m].ldv, E[m].in, E[m].ldv, d.Pn, n, 1);
+    } else if (op == 2) {
+      if (Cc[slot].sp2_state == 0) gemm_tile(gemm_smem, bm, bn, n, n, n, 1.0, d.X, n, d.X, n, d.Pn, n, 1);
+    } else {
+      // the fused SP2 step on the (X, Pn) ping-pong pair: step k (decided just before by
+      // k_b_sp2_decide64) reads its iterate from X for even k, from Pn for odd k, and writes
+      // the next one, updated, to the other; the 64 x 64 tiles' trace partials go to part.
+      // When the step is the last (converged), an iterate landing in Pn is written as the
+      // density 2 X right away (one landing in X is doubled into Pn after the steps).
+      const MolCtl &c = Cc[slot];
+      if (!c.sp2_apply) return;
+      const int k = c.sp2_steps - 1;
+      const double *cur = (k % 2 == 0) ? d.X : d.Pn;
+      double *dst = (k % 2 == 0) ? d.Pn : d.X;
+      const double scale = (c.sp2_state == 1 && dst == d.Pn) ? 2.0 : 1.0;
+      gemm_tile_t<BM, BN>(gemm_smem, bm, bn, n, n, n, 1.0, cur, n, cur, n, dst, n, 1,
+                          Sp2Fuse{cur, c.sp2_square != 0, d.part, scale});
+    }
   }
 }
 
