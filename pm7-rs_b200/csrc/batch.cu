@@ -2412,21 +2412,29 @@ static pm7_status engine_submit(pm7_engine *E, const pm7_molecule *molecule, con
       }
       std::this_thread::sleep_for(std::chrono::microseconds(100));
     }
-    std::lock_guard<std::mutex> g(E->mu);
-    if (!E->runner) throw Failure{PM7_ERR_CUDA, E->worker_error.empty() ? "engine not ready" : E->worker_error};
-    r->ticket = E->next_ticket++;
-    *ticket = r->ticket;
+    BatchRunner *runner = nullptr;
+    {
+      std::lock_guard<std::mutex> g(E->mu);
+      if (!E->runner) throw Failure{PM7_ERR_CUDA, E->worker_error.empty() ? "engine not ready" : E->worker_error};
+      runner = E->runner.get();
+    }
+    // host preparation (validation, layout, pair lists) outside the engine's lock: it reads
+    // only the runner's fixed parameters, and the worker keeps admitting and iterating meanwhile
     EngineRequest *raw = r.get();
+    bool batch = false;
     try {
-      r->mol = E->runner->prepare(to_molecule(molecule), *options);
+      r->mol = runner->prepare(to_molecule(molecule), *options);
       r->mol->grad_out = gradient;
-      if (BatchRunner::batchable(*r->mol)) E->queue.push_back(raw);
-      else E->single.push_back(raw);
+      batch = BatchRunner::batchable(*r->mol);
     } catch (const Failure &f) {
       raw->status = f.code;
       raw->error = f.msg;
       raw->done = true;
     }
+    std::lock_guard<std::mutex> g(E->mu);
+    r->ticket = E->next_ticket++;
+    *ticket = r->ticket;
+    if (!raw->done) (batch ? E->queue : E->single).push_back(raw);
     E->requests[raw->ticket] = std::move(r);
     E->cv.notify_all();
     g_last_error.clear();
