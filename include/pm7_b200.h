@@ -75,9 +75,9 @@ typedef enum pm7_dipole_origin {
 
 /* Arithmetic of the SCF cycles. FP64 is the plain path; MIXED computes the early
  * cycles' densities (SP2 squarings) and, on the plain path, their DIIS commutator product
- * at FP32 accuracy on the tcgen05 tensor cores (3xTF32, FP32 accumulation), keeps the Fock
- * build in FP64, and re-converges in FP64 cycles, the only ones that may end the SCF
- * (engine knob; no reference analogue). */
+ * at FP32 accuracy on the tcgen05 tensor cores (3xTF32, FP32 accumulation), builds their Fock
+ * matrices in FP32 while the DIIS error is above 10 eV, and re-converges in FP64 cycles, the
+ * only ones that may end the SCF (engine knob; no reference analogue). */
 typedef enum pm7_precision {
   PM7_PRECISION_FP64 = 0,
   PM7_PRECISION_MIXED = 1
@@ -234,6 +234,13 @@ pm7_status pm7_stage_core_hamiltonian(const pm7_molecule *molecule, const pm7_pa
 pm7_status pm7_stage_fock(const pm7_molecule *molecule, const pm7_params *params,
                           int32_t force_dpath, const double *p_tot, const double *p_spin,
                           double *f_out);
+
+/* The same Fock matrix from the FP32 build of the mixed-precision mode's early cycles: the
+ * densities and the stored pair integrals read as float and summed in FP32, the output in
+ * double (src/fock.rs:149-418 at FP32 accuracy); a stage for accuracy tests. */
+pm7_status pm7_stage_fock_fp32(const pm7_molecule *molecule, const pm7_params *params,
+                               int32_t force_dpath, const double *p_tot, const double *p_spin,
+                               double *f_out);
 
 /* Per-pair two-centre blocks for atoms (i, j) at displacement d = R_j - R_i
  * (Bohr): w (npair_i x npair_j), e1b/e2a (9x9) and the overlap (9x9), all in

@@ -810,7 +810,10 @@ __global__ void k_b_converge(int n, const int *__restrict__ slots, MolDesc *__re
   d.Pn = t;
   c.e_old = c.e_elec;
   const bool residual_ok = c.shift == 0.0 && sqrt(c.err2) < 1.0e-7;
-  if (!c.use32 && c.iter > 0 && de < c.e_tol && (dp < c.p_tol || residual_ok)) {  // only fp64 cycles end the SCF
+  bool hist64 = true;  // no Fock matrix of the DIIS history came from the FP32 build
+  for (int i = 0; i < c.n_ord; ++i) hist64 = hist64 && !((c.f32_slots >> c.ord[i]) & 1);
+  // only fp64 cycles end the SCF, and only from a history of FP64 Fock builds
+  if (!c.use32 && hist64 && c.iter > 0 && de < c.e_tol && (dp < c.p_tol || residual_ok)) {
     c.converged = 1;
     c.done = 1;
   } else {
@@ -1016,6 +1019,9 @@ static size_t mol_layout(BatchMol &b, char *base) {
   d.hi32 = b.mixed ? (float *)take(4 * l32) : nullptr;
   d.lo32 = b.mixed ? (float *)take(4 * l32) : nullptr;
   d.C32 = b.mixed ? (float *)take(4 * l32) : nullptr;
+  d.P32 = b.mixed ? (float *)take(4 * nn) : nullptr;
+  d.w32 = b.mixed ? (float *)take(4 * (size_t)L.w_len) : nullptr;
+  d.w_len = (size_t)L.w_len;
   d.corr_scratch = (double *)take(8 * corrections_scratch(n));
   // the uploaded tables, contiguous: xyz | sad | z | aoff | ao_atom | csr_start | csr | near | mask
   const size_t up0 = off;

@@ -31,6 +31,8 @@ struct MolDesc {
   double *atom_out;          // per atom: population and the hybrid-dipole density elements
   double *part;              // per-item partial sums of the chunked reductions (kPart each)
   float *X32, *hi32, *lo32, *C32;  // mixed precision: fp32 SP2 iterate, its tf32 split, X^2 (ld32^2)
+  float *P32, *w32;          // mixed precision: the density and the w store as float (FP32 Fock build)
+  size_t w_len;              // doubles in the w store
   int ld32;
   double *corr_scratch;      // post-SCF corrections scratch
 };
@@ -57,6 +59,7 @@ struct MolCtl {
   // SP2 purification of this iteration: state 0 running, 1 converged, 2 failed
   int sp2_state, sp2_steps, sp2_fallbacks, sp2_square, sp2_apply;
   int mixed, use32, fp32_iters;  // mixed precision: still in fp32 cycles, this cycle fp32, count
+  int f32_slots;                 // ring slots whose Fock matrix came from the FP32 build (bit mask)
   double sp2_err[3], sp2_emin, sp2_emax;
   // results
   double core_core, e_final, corr[5];
@@ -93,6 +96,14 @@ __device__ __forceinline__ size_t mol_nn(const MolDesc &d) { return (size_t)d.g.
 __device__ __forceinline__ double *hist_F(const MolDesc &d, int s) { return d.hist + (size_t)s * 3 * mol_nn(d); }
 __device__ __forceinline__ double *hist_E(const MolDesc &d, int s) { return hist_F(d, s) + mol_nn(d); }
 __device__ __forceinline__ double *hist_D(const MolDesc &d, int s) { return hist_F(d, s) + 2 * mol_nn(d); }
+
+// Whether this iteration's Fock build of a molecule runs in FP32: a mixed-precision molecule
+// in its fp32 cycles whose DIIS error is above kFock32Switch eV (the guess and the first A-DIIS
+// cycles). The SCF does not end while the DIIS history holds such a Fock matrix.
+constexpr double kFock32Switch = 10.0;
+__device__ __forceinline__ bool fock32_now(const MolDesc &d, const MolCtl &c) {
+  return d.P32 != nullptr && c.mixed && (c.iter == 0 || c.err2 > kFock32Switch * kFock32Switch);
+}
 
 // Chunk `item` of a chunk list: list position, slot and element range [e0, e1).
 struct ChunkRef {

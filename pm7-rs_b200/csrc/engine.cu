@@ -585,6 +585,13 @@ struct Purifier {
 // DIIS error below which the mixed-precision SCF switches to fp64 densities.
 static constexpr double kMixedSwitch = 1.0e-3;
 static constexpr double kMixedSwitchStep = 1.0e-6;  // rms density step that also ends the fp32 phase
+// DIIS error (eV) above which an fp32 cycle also builds its Fock matrix in FP32: the guess and
+// the first A-DIIS cycles. The FP32 build's ~1e-6 relative error stays in the DIIS history's
+// Fock matrices, so the SCF may not end while the history holds one: the reported orbitals come
+// from the last extrapolated Fock (on a 1,002-atom water cluster a switch at 0.1 took 20
+// iterations instead of 17, one at 1 shifted the HOMO by 1e-3 eV; at 10 the last FP32 build is
+// cycle 6 and the SCF still ends at 17 from a clean history).
+static constexpr double kFock32Switch = 10.0;
 
 static bool use_sp2(int n) {
   const char *env = std::getenv("PM7_DENSITY_SOLVER");
@@ -706,6 +713,10 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   // Mixed precision: fp32 (tcgen05) densities while the DIIS error is large, then fp64
   // refinement cycles; only an fp64 cycle may end the SCF.
   bool phase32 = sp2 && o.precision == PM7_PRECISION_MIXED;
+  DevBuf<float> P32, w32;  // float copies of the density and the w store for the FP32 Fock build
+  bool w32_ready = false;
+  double last_err = std::numeric_limits<double>::infinity();
+  std::vector<char> fock32_slot(kmax, 0);  // ring slots whose Fock matrix came from the FP32 build
   HistoryHost hist(kmax);
   StallGuardHost guard(o.level_shift);
   const bool trace = std::getenv("PM7_SCF_TRACE") != nullptr;
@@ -719,7 +730,21 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
       hD[slot].alloc(nn, st);
     }
     double *Fk = hF[slot].p;
-    { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, out.P.p, out.P.p, 0.5, Fk, D.pop.p, D.jbuf.p); }
+    fock32_slot[slot] = phase32 && last_err > kFock32Switch;
+    if (fock32_slot[slot]) {
+      Stage s_(st, "fock_fp32");
+      if (!w32_ready) {
+        P32.alloc(nn, st);
+        w32.alloc((size_t)L.w_len, st);
+        launch_to_float(st, (size_t)L.w_len, D.w.p, w32.p);
+        w32_ready = true;
+      }
+      launch_to_float(st, nn, out.P.p, P32.p);
+      launch_fock32(st, g, P, D.H.p, out.P.p, P32.p, P32.p, 0.5, Fk, D.pop.p, D.jbuf.p, w32.p);
+    } else {
+      Stage s_(st, "fock");
+      launch_fock(st, g, P, D.H.p, out.P.p, out.P.p, 0.5, Fk, D.pop.p, D.jbuf.p);
+    }
     // the iteration's energy for the convergence test, summed accurately: the reference's
     // folds carry ~1e-8 eV of rounding noise at a thousand atoms, the size of e_tol itself,
     // so they are kept for the reported energy only
@@ -765,6 +790,7 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     CUDA_OK(cudaStreamSynchronize(st));
     const double e_elec = 0.5 * sc[0];
     const double err_norm = std::sqrt(sc[1]);
+    last_err = err_norm;
     hist.record(std::vector<double>(dh, dh + k + 1), std::vector<double>(dh + 16, dh + 16 + k + 1),
                 std::vector<double>(dh + 32, dh + 32 + k));
     // extrapolation weights over the chronological history
@@ -819,14 +845,16 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
     std::swap(out.P.p, Pnew.p);
     e_old = e_elec;
     const bool residual_ok = guard.shift == 0.0 && err_norm < 1.0e-7;
-    if (!used32 && iter > 0 && de < o.e_tol && (dp < o.p_tol || residual_ok)) {
+    bool hist64 = true;  // no Fock matrix of the DIIS history came from the FP32 build
+    for (int e : hist.entries()) hist64 = hist64 && !fock32_slot[e];
+    if (!used32 && hist64 && iter > 0 && de < o.e_tol && (dp < o.p_tol || residual_ok)) {
       out.converged = true;
       break;
     }
     guard.update(dp, e_elec);
     if (trace)
-      std::fprintf(stderr, "scf %4d E %.10f dp %.3e err %.3e shift %.2f%s\n", out.iterations, e_elec, dp, err_norm,
-                   guard.shift, used32 ? " fp32" : "");
+      std::fprintf(stderr, "scf %4d E %.10f dp %.3e err %.3e shift %.2f%s%s\n", out.iterations, e_elec, dp, err_norm,
+                   guard.shift, used32 ? " fp32" : "", fock32_slot[slot] ? " fock32" : "");
   }
   // final Fock and energy at the converged density
   { Stage s_(st, "fock"); launch_fock(st, g, P, D.H.p, out.P.p, out.P.p, 0.5, F.p, D.pop.p, D.jbuf.p); }
@@ -1516,7 +1544,8 @@ static pm7_status guarded(Fn fn) {
 // ---- stage entry points ----------------------------------------------------
 
 static void stage_core(const pm7_molecule *mol, const pm7_params *params, int force_dpath, double *h_out,
-                       int32_t *nao_out, const double *p_tot, const double *p_spin, double *f_out) {
+                       int32_t *nao_out, const double *p_tot, const double *p_spin, double *f_out,
+                       bool fp32 = false) {
   Molecule m = to_molecule(mol);
   const int method = *reinterpret_cast<const int *>(params);
   const ParamSet &ps = param_set(method);
@@ -1537,6 +1566,19 @@ static void stage_core(const pm7_molecule *mol, const pm7_params *params, int fo
     upload(Pt, std::vector<double>(p_tot, p_tot + nn), st);
     upload(Ps, std::vector<double>(p_spin, p_spin + nn), st);
     F.alloc(nn, st);
+    if (fp32) {
+      DevBuf<float> Pt32, Ps32, w32;
+      Pt32.alloc(nn, st);
+      Ps32.alloc(nn, st);
+      w32.alloc(D.w.n, st);
+      launch_to_float(st, nn, Pt.p, Pt32.p);
+      launch_to_float(st, nn, Ps.p, Ps32.p);
+      launch_to_float(st, D.w.n, D.w.p, w32.p);
+      launch_fock32(st, D.geometry(), P, D.H.p, Pt.p, Pt32.p, Ps32.p, 1.0, F.p, D.pop.p, D.jbuf.p, w32.p);
+      CUDA_OK(cudaMemcpyAsync(f_out, F.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaStreamSynchronize(st));
+      return;
+    }
     launch_fock(st, D.geometry(), P, D.H.p, Pt.p, Ps.p, 1.0, F.p, D.pop.p, D.jbuf.p);
     CUDA_OK(cudaMemcpyAsync(f_out, F.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
@@ -1713,6 +1755,11 @@ pm7_status pm7_stage_core_hamiltonian(const pm7_molecule *molecule, const pm7_pa
 pm7_status pm7_stage_fock(const pm7_molecule *molecule, const pm7_params *params, int32_t force_dpath,
                           const double *p_tot, const double *p_spin, double *f_out) {
   return guarded([&] { stage_core(molecule, params, force_dpath, nullptr, nullptr, p_tot, p_spin, f_out); });
+}
+
+pm7_status pm7_stage_fock_fp32(const pm7_molecule *molecule, const pm7_params *params, int32_t force_dpath,
+                               const double *p_tot, const double *p_spin, double *f_out) {
+  return guarded([&] { stage_core(molecule, params, force_dpath, nullptr, nullptr, p_tot, p_spin, f_out, true); });
 }
 
 pm7_status pm7_stage_pair(const pm7_params *params, int32_t z_i, int32_t z_j, const double d[3], int32_t force_dpath,

@@ -70,6 +70,13 @@ void launch_far_coulomb(cudaStream_t st, int n_atoms, const double *xyz, const u
 // F = H + J(Pt) - K(s * Ps). `pop` (n_atoms) and `jbuf` (packed, like ecore) are scratch.
 void launch_fock(cudaStream_t st, const FockGeometry &g, const DeviceParams &P, const double *H, const double *Pt,
                  const double *Ps, double s_scale, double *F, double *pop, double *jbuf);
+// The same F with the density and the stored integrals read as float (Pt, Ps, w: float copies)
+// and summed in FP32; populations from the double density Pt64. For early mixed-precision cycles.
+void launch_fock32(cudaStream_t st, const FockGeometry &g, const DeviceParams &P, const double *H,
+                   const double *Pt64, const float *Pt, const float *Ps, double s_scale, double *F, double *pop,
+                   double *jbuf, const float *w);
+// dst[i] = (float)src[i], i < n.
+void launch_to_float(cudaStream_t st, size_t n, const double *src, float *dst);
 
 // ---- dense algebra (kernels_dense.cu) ----
 // C[M x N] = alpha * A^T B, A: K x M row-major (lda), B: K x N row-major (ldb), C row-major (ldc). FP64 DMMA.

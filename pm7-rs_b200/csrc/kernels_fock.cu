@@ -10,6 +10,9 @@
 //                    plus each pair's packed Coulomb contributions to both atoms;
 //   * k_fock_atom  - diagonal atom blocks: one-centre terms, the near Coulomb
 //                    contributions in partner order, and the far point-charge Coulomb.
+// The kernels are templated on R, the type of the density and the stored integrals they read
+// and of their sums: double for every FP64 cycle, float for the early cycles of the mixed
+// precision mode (the output F, H, the far potential and the populations stay double).
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -42,8 +45,9 @@ __global__ void k_atom_blocks(int n_atoms, const int *__restrict__ aoff, const i
   }
 }
 
+template <typename R>
 __device__ __forceinline__ void fock_far_elem(const FockGeometry &g, const double *__restrict__ H,
-                                              const double *__restrict__ Ps, double s_scale, double *__restrict__ F,
+                                              const R *__restrict__ Ps, double s_scale, double *__restrict__ F,
                                               int i, int j) {
   const int A = g.ao_atom[i], B = g.ao_atom[j];
   if (A == B || g.near_mask[(size_t)A * g.n_atoms + B]) return;
@@ -56,41 +60,44 @@ __device__ __forceinline__ void fock_far_elem(const FockGeometry &g, const doubl
     v = (1.0 / sqrt(dx * dx + dy * dy + dz * dz)) * kEv;
   }
   const size_t ij = (size_t)i * g.nao + j;
-  F[ij] = H[ij] - s_scale * Ps[ij] * v;
+  F[ij] = H[ij] - (double)((R)s_scale * Ps[ij] * (R)v);
 }
 
-__global__ void k_fock_far(FockGeometry g, const double *__restrict__ H, const double *__restrict__ Ps,
+template <typename R>
+__global__ void k_fock_far(FockGeometry g, const double *__restrict__ H, const R *__restrict__ Ps,
                            double s_scale, double *__restrict__ F) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= g.nao || j >= g.nao) return;
-  fock_far_elem(g, H, Ps, s_scale, F, i, j);
+  fock_far_elem<R>(g, H, Ps, s_scale, F, i, j);
 }
 
 // One near pair's Fock terms, a group of G lanes per pair: lanes over the pair's outputs —
 // the exchange block F_uv (n_u x n_v elements), then the packed Coulomb partials of u from
 // P_vv and of v from P_uu (summed per atom by the atom kernel). Every output is one lane's
-// sum in a fixed order, so the result does not depend on G or the block size.
-template <int G>
+// sum in a fixed order, so the result does not depend on G or the block size. `wstore` is the
+// w store in type R (g.w itself for double).
+template <int G, typename R = double>
 __device__ __forceinline__ void fock_near_pair(const FockGeometry &g, const DeviceParams &P,
-                                               const double *__restrict__ H, const double *__restrict__ Pt,
-                                               const double *__restrict__ Ps, double s_scale,
-                                               double *__restrict__ F, double *__restrict__ jbuf, int p, int lane) {
+                                               const double *__restrict__ H, const R *__restrict__ Pt,
+                                               const R *__restrict__ Ps, double s_scale,
+                                               double *__restrict__ F, double *__restrict__ jbuf, int p, int lane,
+                                               const R *__restrict__ wstore) {
   const NearPair q = g.np[p];
   const int nu_ = P.elements[g.z[q.u]].n_orb, nv = P.elements[g.z[q.v]].n_orb;
   const int ou = g.aoff[q.u], ov = g.aoff[q.v], nao = g.nao;
   const int npv = nv * (nv + 1) / 2, npu = nu_ * (nu_ + 1) / 2;
-  const double *w = g.w + q.woff;
+  const R *w = wstore + q.woff;
   const int nx = nu_ * nv, total = nx + npu + npv;
   for (int t = lane; t < total; t += G) {
     if (t < nx) {  // exchange element (mu, la)
       const int mu = t / nv, la = t - mu * nv;
-      double acc = 0.0;
+      R acc = 0;
       for (int nu = 0; nu < nu_; ++nu) {
-        const double *row = w + dpack(mu, nu) * npv;
+        const R *row = w + dpack(mu, nu) * npv;
         for (int si = 0; si < nv; ++si) acc += Ps[(size_t)(ou + nu) * nao + ov + si] * row[dpack(la, si)];
       }
-      const double kv = -acc * s_scale;
+      const double kv = -(double)(acc * (R)s_scale);
       const size_t e1 = (size_t)(ou + mu) * nao + ov + la, e2 = (size_t)(ov + la) * nao + ou + mu;
       F[e1] = H[e1] + kv;
       F[e2] = H[e2] + kv;
@@ -98,17 +105,17 @@ __device__ __forceinline__ void fock_near_pair(const FockGeometry &g, const Devi
       const int k = t - nx;
       int mu = 0;
       while ((mu + 1) * (mu + 2) / 2 <= k) ++mu;
-      const double *row = w + k * npv;
-      double acc = 0.0;
+      const R *row = w + k * npv;
+      R acc = 0;
       for (int la = 0; la < nv; ++la)
         for (int si = 0; si < nv; ++si) acc += Pt[(size_t)(ov + la) * nao + ov + si] * row[dpack(la, si)];
-      jbuf[q.eoff_u + k] = acc;
+      jbuf[q.eoff_u + k] = (double)acc;
     } else {  // Coulomb on v from P_uu, packed element col
       const int col = t - nx - npu;
-      double acc = 0.0;
+      R acc = 0;
       for (int mu = 0; mu < nu_; ++mu)
         for (int nu = 0; nu < nu_; ++nu) acc += Pt[(size_t)(ou + mu) * nao + ou + nu] * w[dpack(mu, nu) * npv + col];
-      jbuf[q.eoff_v + col] = acc;
+      jbuf[q.eoff_v + col] = (double)acc;
     }
   }
 }
@@ -117,17 +124,17 @@ __device__ __forceinline__ void fock_near_pair(const FockGeometry &g, const Devi
 // that take a pair at a time. (G, T) is an autotuned launch shape with identical results:
 // whole warps suit the 9-orbital pairs, narrow groups the hydrogen-rich sp pairs (3 to 36
 // outputs each).
-template <int G, int T>
+template <int G, int T, typename R = double>
 __global__ void __launch_bounds__(T, 1) k_fock_near(FockGeometry g, DeviceParams P, const double *__restrict__ H,
-                                                    const double *__restrict__ Pt, const double *__restrict__ Ps,
+                                                    const R *__restrict__ Pt, const R *__restrict__ Ps,
                                                     double s_scale, double *__restrict__ F,
-                                                    double *__restrict__ jbuf) {
+                                                    double *__restrict__ jbuf, const R *__restrict__ w) {
   constexpr int NG = T / G;
   static_assert(128 % NG == 0, "groups per block must divide 128");
   const int lane = threadIdx.x % G, grp = threadIdx.x / G;
   for (int r = 0; r < 128 / NG; ++r) {
     const int p = blockIdx.x * 128 + grp + NG * r;
-    if (p < g.n_near) fock_near_pair<G>(g, P, H, Pt, Ps, s_scale, F, jbuf, p, lane);
+    if (p < g.n_near) fock_near_pair<G, R>(g, P, H, Pt, Ps, s_scale, F, jbuf, p, lane, w);
   }
 }
 
@@ -155,10 +162,10 @@ __device__ __forceinline__ double oc_sp(int a, int b, int c, int d, const Elemen
 // one-centre terms and the assembly of the atom's diagonal block (lanes over its elements).
 // `jacc` is the group's 45 doubles of shared memory; `gmask` the group's lanes. No block-wide
 // barrier.
-template <int G>
+template <int G, typename R = double>
 __device__ __forceinline__ void fock_atom_group(const FockGeometry &g, const DeviceParams &P,
-                                                const double *__restrict__ H, const double *__restrict__ Pt,
-                                                const double *__restrict__ Ps, double s_scale,
+                                                const double *__restrict__ H, const R *__restrict__ Pt,
+                                                const R *__restrict__ Ps, double s_scale,
                                                 const double *__restrict__ pop, const double *__restrict__ jbuf,
                                                 double *__restrict__ F, int A, double *jacc, int lane,
                                                 unsigned gmask) {
@@ -224,20 +231,20 @@ __device__ __forceinline__ void fock_atom_group(const FockGeometry &g, const Dev
   const double *oc = (no == 9 && e.onecenter_slot >= 0) ? P.onecenter + (size_t)e.onecenter_slot * 2025 : nullptr;
   for (int idx = lane; idx < no * no; idx += G) {
     const int mu = idx / no, nu = idx - mu * no;
-    double acc = 0.0;
+    R acc = 0;
     for (int la = 0; la < no; ++la)
       for (int si = 0; si < no; ++si) {
-        const double pt = Pt[(size_t)(off + la) * nao + off + si];
-        const double ps = s_scale * Ps[(size_t)(off + la) * nao + off + si];
+        const R pt = Pt[(size_t)(off + la) * nao + off + si];
+        const R ps = (R)s_scale * Ps[(size_t)(off + la) * nao + off + si];
         if (oc) {
-          acc += pt * oc[dpack(mu, nu) * 45 + dpack(la, si)];
-          acc -= ps * oc[dpack(mu, la) * 45 + dpack(nu, si)];
+          acc += pt * (R)oc[dpack(mu, nu) * 45 + dpack(la, si)];
+          acc -= ps * (R)oc[dpack(mu, la) * 45 + dpack(nu, si)];
         } else {
-          acc += pt * oc_sp(mu, nu, la, si, e);
-          acc -= ps * oc_sp(mu, la, nu, si, e);
+          acc += pt * (R)oc_sp(mu, nu, la, si, e);
+          acc -= ps * (R)oc_sp(mu, la, nu, si, e);
         }
       }
-    double v = acc + jacc[dpack(mu, nu)];
+    double v = (double)acc + jacc[dpack(mu, nu)];
     if (mu == nu) v += far;
     const size_t ij = (size_t)(off + mu) * nao + off + nu;
     F[ij] = H[ij] + v;
@@ -252,9 +259,9 @@ __device__ __forceinline__ unsigned group_mask() {
 }
 
 // A block of T threads, T/G atoms (a group of G lanes each).
-template <int G, int T>
+template <int G, int T, typename R = double>
 __global__ void __launch_bounds__(T) k_fock_atom(FockGeometry g, DeviceParams P, const double *__restrict__ H,
-                                                 const double *__restrict__ Pt, const double *__restrict__ Ps,
+                                                 const R *__restrict__ Pt, const R *__restrict__ Ps,
                                                  double s_scale, const double *__restrict__ pop,
                                                  const double *__restrict__ jbuf, double *__restrict__ F) {
   constexpr int NG = T / G;
@@ -262,7 +269,7 @@ __global__ void __launch_bounds__(T) k_fock_atom(FockGeometry g, DeviceParams P,
   const int grp = threadIdx.x / G;
   const int A = blockIdx.x * NG + grp;
   if (A < g.n_atoms)
-    fock_atom_group<G>(g, P, H, Pt, Ps, s_scale, pop, jbuf, F, A, jacc[grp], threadIdx.x % G, group_mask<G>());
+    fock_atom_group<G, R>(g, P, H, Pt, Ps, s_scale, pop, jbuf, F, A, jacc[grp], threadIdx.x % G, group_mask<G>());
 }
 
 // The atom launch shapes, X(variant, G lanes per atom, T threads per block).
@@ -286,6 +293,32 @@ __global__ void k_b_atom_pop(BatchList L, const MolDesc *__restrict__ D, DeviceP
   }
 }
 
+// The FP32 build's inputs, item = 8 rows of one molecule (the far kernel's items): rows of the
+// density as float and a 1/items share of the w store (on the guess iteration only, whose
+// build is always FP32 in mixed precision); item 0 marks the ring slot this iteration's Fock
+// matrix goes to as built in FP32 or not.
+__global__ void __launch_bounds__(256) k_b_fock32_inputs(BatchList L, const MolDesc *__restrict__ D,
+                                                         MolCtl *__restrict__ C) {
+  const int item = blockIdx.x;
+  const int m = batch_find(L, item);
+  const int slot = L.slot[m];
+  const MolDesc &d = D[slot];
+  MolCtl &c = C[slot];
+  const int q = item - L.prefix[m], nq = L.prefix[m + 1] - L.prefix[m];
+  const bool f32 = fock32_now(d, c);
+  if (q == 0 && threadIdx.x == 0) {  // nothing in this launch reads f32_slots
+    if (f32) c.f32_slots |= 1 << c.slot;
+    else c.f32_slots &= ~(1 << c.slot);
+  }
+  if (!f32) return;
+  const size_t n = d.g.nao, e0 = (size_t)q * 8 * n, e1 = min(e0 + 8 * n, n * n);
+  for (size_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) d.P32[e] = (float)d.P[e];
+  if (c.iter == 0) {
+    const size_t w0 = d.w_len * q / nq, w1 = d.w_len * (q + 1) / nq;
+    for (size_t e = w0 + threadIdx.x; e < w1; e += blockDim.x) d.w32[e] = (float)d.g.w[e];
+  }
+}
+
 // Item = 8 rows of one molecule's matrix (warp per row, lanes over columns).
 __global__ void __launch_bounds__(256) k_b_fock_far(BatchList L, const MolDesc *__restrict__ D,
                                                     const MolCtl *__restrict__ C, int final_pass) {
@@ -296,7 +329,11 @@ __global__ void __launch_bounds__(256) k_b_fock_far(BatchList L, const MolDesc *
   const int i = (item - L.prefix[m]) * 8 + (threadIdx.x >> 5);
   if (i >= d.g.nao) return;
   double *F = fock_target(d, C[slot], final_pass);
-  for (int j = threadIdx.x & 31; j < d.g.nao; j += 32) fock_far_elem(d.g, d.H, d.P, 0.5, F, i, j);
+  if (!final_pass && fock32_now(d, C[slot])) {
+    for (int j = threadIdx.x & 31; j < d.g.nao; j += 32) fock_far_elem<float>(d.g, d.H, d.P32, 0.5, F, i, j);
+  } else {
+    for (int j = threadIdx.x & 31; j < d.g.nao; j += 32) fock_far_elem<double>(d.g, d.H, d.P, 0.5, F, i, j);
+  }
 }
 
 // Item = 128 near pairs of one molecule (groups of G lanes, a pair per group at a time).
@@ -311,9 +348,12 @@ __global__ void __launch_bounds__(T, 1) k_b_fock_near(BatchList L, const MolDesc
   const MolDesc &d = D[slot];
   const int lane = threadIdx.x % G, grp = threadIdx.x / G;
   double *F = fock_target(d, C[slot], final_pass);
+  const bool f32 = !final_pass && fock32_now(d, C[slot]);
   for (int r = 0; r < 128 / NG; ++r) {
     const int p = (item - L.prefix[m]) * 128 + grp + NG * r;
-    if (p < d.g.n_near) fock_near_pair<G>(d.g, P, d.H, d.P, d.P, 0.5, F, d.jbuf, p, lane);
+    if (p >= d.g.n_near) continue;
+    if (f32) fock_near_pair<G, float>(d.g, P, d.H, d.P32, d.P32, 0.5, F, d.jbuf, p, lane, d.w32);
+    else fock_near_pair<G>(d.g, P, d.H, d.P, d.P, 0.5, F, d.jbuf, p, lane, d.g.w);
   }
 }
 
@@ -329,8 +369,13 @@ __global__ void __launch_bounds__(T) k_b_fock_atom(BatchList L, const MolDesc *_
   const int m = batch_find(L, item);
   const int slot = L.slot[m];
   const MolDesc &d = D[slot];
-  fock_atom_group<G>(d.g, P, d.H, d.P, d.P, 0.5, d.pop, d.jbuf, fock_target(d, C[slot], final_pass),
-                     item - L.prefix[m], jacc[grp], threadIdx.x % G, group_mask<G>());
+  double *F = fock_target(d, C[slot], final_pass);
+  if (!final_pass && fock32_now(d, C[slot]))
+    fock_atom_group<G, float>(d.g, P, d.H, d.P32, d.P32, 0.5, d.pop, d.jbuf, F, item - L.prefix[m], jacc[grp],
+                              threadIdx.x % G, group_mask<G>());
+  else
+    fock_atom_group<G>(d.g, P, d.H, d.P, d.P, 0.5, d.pop, d.jbuf, F, item - L.prefix[m], jacc[grp],
+                       threadIdx.x % G, group_mask<G>());
 }
 
 // Size bucket of an autotune key: the next power of two above n.
@@ -341,6 +386,10 @@ void launch_b_fock(cudaStream_t st, const BatchList &Lmol, const BatchList &Lrow
   if (Lmol.n <= 0) return;
   k_b_atom_pop<<<Lmol.n, 128, 0, st>>>(Lmol, D, P);
   note_launch();
+  if (!final_pass && Lrows.total > 0) {
+    k_b_fock32_inputs<<<Lrows.total, 256, 0, st>>>(Lrows, D, const_cast<MolCtl *>(C));
+    note_launch();
+  }
   if (Lrows.total > 0) k_b_fock_far<<<Lrows.total, 256, 0, st>>>(Lrows, D, C, final_pass);
   note_launch();
   if (Lnear.total > 0)
@@ -401,14 +450,14 @@ void launch_fock(cudaStream_t st, const FockGeometry &g, const DeviceParams &P, 
                  const double *Ps, double s_scale, double *F, double *pop, double *jbuf) {
   launch_atom_pop(st, g.n_atoms, g.aoff, g.z, P, g.nao, Pt, pop);
   dim3 blk(32, 8), grd((g.nao + 31) / 32, (g.nao + 7) / 8);
-  k_fock_far<<<grd, blk, 0, st>>>(g, H, Ps, s_scale, F);
+  k_fock_far<double><<<grd, blk, 0, st>>>(g, H, Ps, s_scale, F);
   note_launch();
   if (g.n_near > 0) {
     const int blocks = (g.n_near + 127) / 128;
     autotune(st, "fock_near|pairs" + std::to_string(pow2_bucket(g.n_near)), kNearVariants, [&](int v) {
       switch (v) {
 #define PM7_LAUNCH(i, G, T) \
-  case i: k_fock_near<G, T><<<blocks, T, 0, st>>>(g, P, H, Pt, Ps, s_scale, F, jbuf); break;
+  case i: k_fock_near<G, T><<<blocks, T, 0, st>>>(g, P, H, Pt, Ps, s_scale, F, jbuf, g.w); break;
         PM7_NEAR_SHAPES(PM7_LAUNCH)
 #undef PM7_LAUNCH
       }
@@ -424,6 +473,35 @@ void launch_fock(cudaStream_t st, const FockGeometry &g, const DeviceParams &P, 
     }
     note_launch();
   });
+}
+
+__global__ void k_to_float(size_t n, const double *__restrict__ src, float *__restrict__ dst) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    dst[e] = (float)src[e];
+}
+
+void launch_to_float(cudaStream_t st, size_t n, const double *src, float *dst) {
+  if (n == 0) return;
+  const size_t blocks = std::min<size_t>((n + 255) / 256, 148 * 8);
+  k_to_float<<<(unsigned)blocks, 256, 0, st>>>(n, src, dst);
+  note_launch();
+}
+
+// The FP32 build: one launch shape each (near pairs in groups of 8 lanes, atoms a warp each);
+// the populations come from the double density Pt64.
+void launch_fock32(cudaStream_t st, const FockGeometry &g, const DeviceParams &P, const double *H,
+                   const double *Pt64, const float *Pt, const float *Ps, double s_scale, double *F, double *pop,
+                   double *jbuf, const float *w) {
+  launch_atom_pop(st, g.n_atoms, g.aoff, g.z, P, g.nao, Pt64, pop);
+  dim3 blk(32, 8), grd((g.nao + 31) / 32, (g.nao + 7) / 8);
+  k_fock_far<float><<<grd, blk, 0, st>>>(g, H, Ps, s_scale, F);
+  note_launch();
+  if (g.n_near > 0) {
+    k_fock_near<8, 256, float><<<(g.n_near + 127) / 128, 256, 0, st>>>(g, P, H, Pt, Ps, s_scale, F, jbuf, w);
+    note_launch();
+  }
+  k_fock_atom<32, 256, float><<<(g.n_atoms + 7) / 8, 256, 0, st>>>(g, P, H, Pt, Ps, s_scale, pop, jbuf, F);
+  note_launch();
 }
 
 }  // namespace pm7

@@ -27,7 +27,7 @@ EXPORTED = [
     "pm7_correction_gradient", "pm7_run_batch_gradient", "pm7_engine_submit_gradient",
     "pm7_dandc_options_default", "pm7_run_dandc", "pm7_dandc_result_free", "pm7_stage_dandc_partition",
     "pm7_dandc_abi_sizes", "pm7_stage_seqsum", "pm7_stage_tf32_wait_drill",
-    "pm7_engine_stats",
+    "pm7_engine_stats", "pm7_stage_fock_fp32",
 ]
 
 
@@ -59,6 +59,7 @@ def lib():
     L.pm7_stage_core_hamiltonian.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, C.c_int32, abi.DP,
                                              C.POINTER(C.c_int32)]
     L.pm7_stage_fock.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, C.c_int32, abi.DP, abi.DP, abi.DP]
+    L.pm7_stage_fock_fp32.argtypes = L.pm7_stage_fock.argtypes
     L.pm7_stage_pair.argtypes = [C.c_void_p, C.c_int32, C.c_int32, abi.DP, C.c_int32, abi.DP, abi.DP, abi.DP, abi.DP,
                                  C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.pm7_stage_core_core.argtypes = [C.POINTER(abi.Molecule), C.c_void_p, abi.DP]
@@ -305,13 +306,15 @@ def core_hamiltonian(z, xyz_bohr, method=0, force_dpath=False):
     return out
 
 
-def fock(z, xyz_bohr, p_tot, p_spin, method=0, force_dpath=False):
+def fock(z, xyz_bohr, p_tot, p_spin, method=0, force_dpath=False, fp32=False):
+    """F = H + J(p_tot) - K(p_spin); fp32=True gives the mixed-precision cycles' FP32 build."""
     m = _Mol(z, xyz_bohr)
     pt = np.ascontiguousarray(p_tot, dtype=np.float64)
     ps = np.ascontiguousarray(p_spin, dtype=np.float64)
     f = np.zeros_like(pt)
-    _check(lib().pm7_stage_fock(C.byref(m.s), params(method), int(force_dpath), pt.ctypes.data_as(abi.DP),
-                                ps.ctypes.data_as(abi.DP), f.ctypes.data_as(abi.DP)))
+    entry = lib().pm7_stage_fock_fp32 if fp32 else lib().pm7_stage_fock
+    _check(entry(C.byref(m.s), params(method), int(force_dpath), pt.ctypes.data_as(abi.DP),
+                 ps.ctypes.data_as(abi.DP), f.ctypes.data_as(abi.DP)))
     return f
 
 

@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 from pm7b200 import api
+from pm7b200 import geometry as G
 
 pytestmark = pytest.mark.gpu
 
@@ -67,3 +68,23 @@ def test_mixed_precision_scf_matches_fp64_oracle():
     assert np.max(np.abs(r["charges"] - o["charges"])) < 1.0e-5
     f = api.run_pm7(z, x)
     assert f["fp32_iterations"] == 0
+
+
+@pytest.mark.parametrize("case", ["water30", "chain_s_cl"])
+def test_fp32_fock_build_against_fp64(case):
+    # the Fock build of the mixed-precision mode's early cycles (density and stored pair
+    # integrals read as float, sums in FP32) against the FP64 build, which matches the oracle
+    # to 1e-10 eV: a converged RHF density of a water cluster and of a chain with S and Cl
+    # (the MNDO/d one-centre block)
+    if case == "water30":
+        z, x = G.water_cluster(30, seed=4)
+    else:
+        z, x = G.substituted_chain(14, np.random.default_rng(5), p_s=0.3, p_cl=0.3)
+    r = api.run_pm7(z, x, want_matrices=1)
+    p = np.asarray(r["density"])
+    f64 = api.fock(z, x, p, 0.5 * p)
+    f32 = api.fock(z, x, p, 0.5 * p, fp32=True)
+    scale = np.max(np.abs(f64))
+    err = np.max(np.abs(f32 - f64))
+    assert err < 2e-6 * scale, (err, scale)
+    assert err > 0.0  # the FP32 kernels ran, not the FP64 ones
