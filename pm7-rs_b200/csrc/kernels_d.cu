@@ -1036,12 +1036,38 @@ __device__ __forceinline__ double pair_d_elem(int n_atoms, const int *__restrict
   return pair_core_energy(P, eu, ev, sqrt(ex * ex + ey * ey + ez * ez));
 }
 
+// The partner atoms v0 .. v0 + 127 of a block (128 threads), dealt to the threads grouped by
+// orbital count (1, 4, 9; the pairs without work last), so that a warp mostly runs one shell
+// structure of the overlap. Each pair writes only its own outputs, so the dealing order does not
+// change any result.
+__device__ __forceinline__ int deal_partner(int n_atoms, const int *__restrict__ z, const DeviceParams &P, int u,
+                                            int v0) {
+  __shared__ int count[4], sorted[128];
+  if (threadIdx.x < 4) count[threadIdx.x] = 0;
+  __syncthreads();
+  const int v = v0 + threadIdx.x;
+  int cls = 3;
+  if (v > u && v < n_atoms) {
+    const int no = P.elements[z[v]].n_orb;
+    cls = no <= 1 ? 0 : (no <= 4 ? 1 : 2);
+  }
+  const int rank = atomicAdd(&count[cls], 1);
+  __syncthreads();
+  int base = 0;
+  for (int c = 0; c < cls; ++c) base += count[c];
+  sorted[base + rank] = v;
+  __syncthreads();
+  return sorted[threadIdx.x];
+}
+
 // All pairs u < v in the MNDO/d frame: beta*S blocks of H and each pair's core-core
 // energy in pair order. Grid (ceil(N/128), N), block 128, blockIdx.y = u.
-__global__ void k_pairs_all_d(int n_atoms, const int *__restrict__ z, const double *__restrict__ xyz,
-                              const int *__restrict__ aoff, int nao, DeviceParams P, double *__restrict__ H,
-                              double *__restrict__ cc_terms) {
-  const int u = blockIdx.y, v = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_pairs_all_d(int n_atoms, const int *__restrict__ z,
+                                                     const double *__restrict__ xyz, const int *__restrict__ aoff,
+                                                     int nao, DeviceParams P, double *__restrict__ H,
+                                                     double *__restrict__ cc_terms) {
+  const int u = blockIdx.y;
+  const int v = deal_partner(n_atoms, z, P, u, blockIdx.x * 128);
   const double ecc = pair_d_elem(n_atoms, z, xyz, aoff, nao, P, H, u, v);
   if (v > u && v < n_atoms) cc_terms[pair_index(n_atoms, u, v)] = ecc;
 }
@@ -1053,7 +1079,7 @@ __global__ void k_b_pairs_all_d(BatchList L, const MolDesc *__restrict__ D, Devi
   const MolDesc &d = D[L.slot[m]];
   const int local = item - L.prefix[m];
   const int u = local / d.cc_nx, bx = local - u * d.cc_nx;
-  const int v = bx * blockDim.x + threadIdx.x;
+  const int v = deal_partner(d.g.n_atoms, d.g.z, P, u, bx * 128);
   const double ecc = pair_d_elem(d.g.n_atoms, d.g.z, d.g.xyz, d.g.aoff, d.g.nao, P, d.H, u, v);
   if (v > u && v < d.g.n_atoms) d.cc_terms[pair_index(d.g.n_atoms, u, v)] = ecc;
 }
