@@ -382,6 +382,7 @@ def run_b200(args, world, rank, local):
     stages = {k: {"ms_total": round(v[0], 3), "calls": v[1], "ms_avg": round(v[0] / max(v[1], 1), 4)}
               for k, v in prof.items()}
     roofline = None
+    i8_ms, i8_calls = prof.get("sp2_square_i8", (0.0, 0))
     sq_ms, sq_calls = prof.get("sp2_square_gemm", (0.0, 0))
     cm_ms, cm_calls = prof.get("commutator_gemm", (0.0, 0))
     gemm_ms = sq_ms + cm_ms
@@ -393,11 +394,36 @@ def run_b200(args, world, rank, local):
         traffic = None
         if sq_traffic is not None and cm_traffic is not None:
             traffic = (sq_calls * sq_traffic + cm_calls * cm_traffic) / launches_g
-        roofline = {"kernel": "k_gemm_sym (SP2 squares) + k_gemm_tn (F.P), FP64 DMMA mma.sync.m16n8k8", "bound": "tensor", "achieved": achieved,
+        label = ("k_gemm_sym (SP2 squares) + k_gemm_tn (F.P)" if sq_calls else "k_gemm_tn (F.P)") + \
+            ", FP64 DMMA mma.sync.m16n8k8"
+        roofline = {"kernel": label, "bound": "tensor", "achieved": achieved,
                     "peak": dgemm, "unit": "TFLOP/s", "frac": (achieved / dgemm) if dgemm else None,
                     "traffic": traffic, "launches": launches_g, "ms_avg": gemm_ms / launches_g,
                     "algorithmic_per_launch": f"{flops / launches_g:.4g} flop (SP2 square nao^3, commutator 2 nao^3)",
                     "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)"}
+    if i8_calls:
+        # the FP64-accuracy squarings on the integer tensor cores: issued int8 work per launch
+        # (36 digit-pair products over the 128 x 64 lower tiles, K padded to 64) against twice
+        # the measured bf16 dense rate (kind::i8 runs at exactly twice kind::f16 per SM), and
+        # the fp64-equivalent rate (nao^3 per symmetric squaring) against the measured DGEMM
+        tm, tn = (nao + 127) // 128, (nao + 63) // 64
+        tiles = sum(min(2 * r + 2, tn) for r in range(tm))
+        kpad = ((nao + 63) // 64) * 64
+        ops = 36.0 * 2.0 * 128 * 64 * kpad * tiles
+        ms_avg = i8_ms / i8_calls
+        achieved_tops = ops / (ms_avg * 1e-3) / 1e12
+        peak_i8 = 2.0 * peaks.get("bf16_tflops", 1590.0)
+        fp64_eq = float(nao) ** 3 / (ms_avg * 1e-3) / 1e12
+        prev = roofline
+        roofline = {"kernel": "k_sp2_step_i8 (SP2 squares, tcgen05.mma kind::i8 on int8 digit planes, TMA, TMEM; "
+                              "fp64 accuracy by the Ozaki scheme)", "bound": "tensor", "achieved": achieved_tops,
+                    "peak": peak_i8, "unit": "TOP/s", "frac": achieved_tops / peak_i8,
+                    "traffic": read_traffic("sp2_square_i8"), "launches": i8_calls, "ms_avg": ms_avg,
+                    "algorithmic_per_launch": f"{ops:.4g} int8 ops issued ({float(nao) ** 3:.4g} fp64-equivalent flop)",
+                    "fp64_equivalent_tflops": fp64_eq, "fp64_equivalent_frac_of_dgemm": (fp64_eq / dgemm) if dgemm else None,
+                    "peak_source": "twice the measured bf16 dense rate in MEASURED_PEAKS.json"}
+        if prev is not None:
+            roofline["commutator_dmma"] = prev
     # pair integrals: the build stage computes every pair's overlap/resonance and core-core
     # terms and the multipole two-electron blocks of the pairs inside 7 Angstrom
     pair_rate = None

@@ -260,6 +260,12 @@ pm7_status pm7_stage_square_tf32(int32_t n, const double *x, double *c_out);
  * Replaces, in those cycles, the product of `commutator_into` (src/scf.rs:1148-1156). */
 pm7_status pm7_stage_product_tf32(int32_t n, const double *a, const double *b, double *c_out);
 
+/* One fused FP64-accuracy SP2 step on the tcgen05 integer tensor cores (int8 digit planes,
+ * Ozaki-scheme emulation of the fp64 product): x_out = x x (square != 0) or 2 x - x x, for a
+ * symmetric n x n x with elements in [-1.98, 1.98]; norms (2 doubles, may be null) receive
+ * tr x_out and |x_out|_F^2 from the step's partials. A stage for accuracy tests. */
+pm7_status pm7_stage_sp2_step_i8(int32_t n, const double *x, int32_t square, double *x_out, double *norms);
+
 /* Failure drill of the bounded device waits (no counterpart in pm7-rs): runs the tcgen05
  * squaring of an n x n zero matrix (1 <= n <= 4096) with its copy producer withholding
  * every copy, so the pipeline's mbarrier waits never complete. Each wait gives up after its

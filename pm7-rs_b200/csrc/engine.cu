@@ -540,6 +540,32 @@ struct Purifier {
   // purifier keeps to Gershgorin.
   DevBuf<double> lz;
   bool tight = true;
+
+  // FP64-accuracy squarings on the integer tensor cores (int8 digit planes, kernels_i8.cu):
+  // two plane sets, read and written alternately with X and X2, and their tensor maps.
+  bool i8 = false;
+  DevBuf<int8_t> dig0, dig1;
+  DevBuf<int> i8err;
+  alignas(64) unsigned char dmap[4][128];
+  void ensure_i8() {
+    if (dig0.p) return;
+    dig0.alloc(sp2_i8_digit_bytes(n), st);
+    dig1.alloc(sp2_i8_digit_bytes(n), st);
+    i8err.alloc(1, st);
+    CUDA_OK(cudaMemsetAsync(i8err.p, 0, sizeof(int), st));
+    if (!make_digit_maps(dig0.p, n, dmap[0], dmap[1]) || !make_digit_maps(dig1.p, n, dmap[2], dmap[3]))
+      throw Failure{PM7_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
+  }
+  // 1: a pipeline wait expired (raised), 2: an iterate element left the digits' range (the
+  // purification is treated as failed); the flag is cleared.
+  int i8_status() {
+    int e = 0;
+    CUDA_OK(cudaMemcpyAsync(&e, i8err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    if (e == 1) throw Failure{PM7_ERR_TIMEOUT, "tcgen05 i8 squaring: a pipeline wait expired"};
+    if (e) CUDA_OK(cudaMemsetAsync(i8err.p, 0, sizeof(int), st));
+    return e;
+  }
   bool project(const double *F, int n_occ, double w, double *P) {
     if (tight && !lz.p) lz.alloc(lanczos_doubles(n), st);
     for (int attempt = 0; attempt < 2; ++attempt) {
@@ -554,16 +580,28 @@ struct Purifier {
       // Fused steps on the ping-pong pair (X, X2): step s reads the iterate from one and
       // writes the next, already updated, to the other; its traces come from the previous
       // step's epilogue (the first from k_sp2_norms).
-      if (!parts.p) parts.alloc(sp2_parts_doubles(n), st);
+      if (!parts.p) parts.alloc(std::max(sp2_parts_doubles(n), 2 * (size_t)sp2_i8_tiles(n) + 8), st);
+      if (i8) {
+        ensure_i8();
+        launch_sp2_digits(st, n, X.p, dig0.p, nullptr, -1, i8err.p);
+      }
+      const char *stage = i8 ? "sp2_square_i8" : "sp2_square_gemm";
       last_iterations = run_chunks(
           [&](int s) {
             if (s == 0) launch_sp2_norms(st, n, X.p, state.p, parts.p);
             launch_sp2_decide(st, (double)n_occ, state.p, parts.p, s, rule);
-            Stage g_(st, "sp2_square_gemm");
-            launch_sp2_step(st, n, s % 2 == 0 ? X.p : X2.p, s % 2 == 0 ? X2.p : X.p, state.p, parts.p, s);
+            Stage g_(st, stage);
+            const double *in = s % 2 == 0 ? X.p : X2.p;
+            double *out = s % 2 == 0 ? X2.p : X.p;
+            if (i8)
+              launch_sp2_step_i8(st, n, dmap[2 * (s % 2)], dmap[2 * (s % 2) + 1], in, out,
+                                 s % 2 == 0 ? dig1.p : dig0.p, state.p, parts.p, s, i8err.p);
+            else
+              launch_sp2_step(st, n, in, out, state.p, parts.p, s);
           },
-          "sp2_square_gemm", hint64);
+          stage, hint64);
       bool ok = pin[kSp2Ok] != 0.0;
+      if (i8 && i8_status() != 0) ok = false;
       // an idempotent X whose trace is not n_occ is a wrong projector (degenerate frontier)
       if (ok && std::fabs(pin[kSp2TrX] - (double)n_occ) > 1.0e-3) ok = false;
       if (ok) {
@@ -577,6 +615,18 @@ struct Purifier {
     return false;
   }
 };
+
+// The fp64 SP2 squarings run on the integer tensor cores (kernels_i8.cu) from kI8MinN orbitals
+// up, on the DMMA GEMM below (the two are level at ~600 orbitals: 0.051 ms per squaring at
+// 600, 0.224 against 0.314 ms at 2,004, 4.2 against 6.9 ms at 6,000); PM7_SP2_GEMM=dmma|i8
+// forces one.
+constexpr int kI8MinN = 768;
+static bool use_i8_sp2(int n) {
+  const char *env = std::getenv("PM7_SP2_GEMM");
+  if (env && std::strcmp(env, "dmma") == 0) return false;
+  if (env && std::strcmp(env, "i8") == 0) return true;
+  return n >= kI8MinN;
+}
 
 // Density solver for the SCF loop: SP2 above kJacobiMax orbitals (tensor-core squarings;
 // 16 against 37 ms per solve at 240 orbitals), the eigendecomposition (Diag) up to it and
@@ -709,6 +759,7 @@ static void run_rhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   Diag eig(ctx, n, Fuse.p, reinterpret_cast<int *>(ctx.pinned + 8192));
   const bool sp2 = use_sp2(n);
   Purifier pur(st, sp2 ? n : 1, reinterpret_cast<double *>(ctx.pinned + 4096));
+  pur.i8 = sp2 && use_i8_sp2(n);
   bool diagonalised = false;  // whether Fuse holds the eigenvectors of the last iteration
   // Mixed precision: fp32 (tcgen05) densities while the DIIS error is large, then fp64
   // refinement cycles; only an fp64 cycle may end the SCF.
@@ -1009,6 +1060,7 @@ static void run_uhf(DeviceContext &ctx, const DeviceParams &P, DeviceMolecule &D
   Diag eig_b(ctx, n, Ub.p, reinterpret_cast<int *>(ctx.pinned + 8192 + 64));
   const bool sp2 = use_sp2(n);
   Purifier pur(st, sp2 ? n : 1, reinterpret_cast<double *>(ctx.pinned + 4096));
+  pur.i8 = sp2 && use_i8_sp2(n);
   bool diag_a = false;  // whether Ua holds the alpha eigenvectors of the last iteration
   DevBuf<double> eps_b;
   eps_b.alloc(n, st);
@@ -1864,6 +1916,52 @@ pm7_status pm7_stage_tf32_wait_drill(int32_t n) {
     CUDA_OK(cudaStreamSynchronize(st));
     CUDA_OK(cudaGetLastError());
     if (e) throw Failure{PM7_ERR_TIMEOUT, "tcgen05 squaring: a pipeline wait expired (drill)"};
+  });
+}
+
+pm7_status pm7_stage_sp2_step_i8(int32_t n, const double *x, int32_t square, double *x_out, double *norms) {
+  return guarded([&] {
+    if (n < 1 || !x || !x_out) throw Failure{PM7_ERR_INVALID_INPUT, "sp2_step_i8 needs n >= 1 and buffers"};
+    DeviceContext &ctx = context_for(0);
+    std::lock_guard<std::mutex> lock(ctx.run_mutex);
+    CUDA_OK(cudaSetDevice(ctx.device));
+    cudaStream_t st = ctx.stream;
+    const size_t nn = (size_t)n * n;
+    const int tiles = sp2_i8_tiles(n);
+    DevBuf<double> X, Y, state, parts;
+    DevBuf<int8_t> dig0, dig1;
+    DevBuf<int> err;
+    upload(X, std::vector<double>(x, x + nn), st);
+    Y.alloc(nn, st);
+    state.alloc(kSp2Len, st);
+    parts.alloc(2 * (size_t)tiles, st);
+    dig0.alloc(sp2_i8_digit_bytes(n), st);
+    dig1.alloc(sp2_i8_digit_bytes(n), st);
+    err.alloc(1, st);
+    CUDA_OK(cudaMemsetAsync(err.p, 0, sizeof(int), st));
+    launch_sp2_reset(st, state.p);
+    const double sq = square ? 1.0 : 0.0;
+    CUDA_OK(cudaMemcpyAsync(state.p + kSp2Square, &sq, sizeof(double), cudaMemcpyHostToDevice, st));
+    launch_sp2_digits(st, n, X.p, dig0.p, nullptr, -1, err.p);
+    alignas(64) unsigned char map_a[128], map_b[128];
+    if (!make_digit_maps(dig0.p, n, map_a, map_b)) throw Failure{PM7_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
+    launch_sp2_step_i8(st, n, map_a, map_b, X.p, Y.p, dig1.p, state.p, parts.p, 0, err.p);
+    std::vector<double> ph(2 * (size_t)tiles);
+    int e = 0;
+    CUDA_OK(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(x_out, Y.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(ph.data(), parts.p, sizeof(double) * ph.size(), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaGetLastError());
+    if (e == 1) throw Failure{PM7_ERR_TIMEOUT, "tcgen05 i8 squaring: a pipeline wait expired"};
+    if (e == 2) throw Failure{PM7_ERR_INVALID_INPUT, "sp2_step_i8: an element outside [-1.98, 1.98]"};
+    if (norms) {
+      norms[0] = norms[1] = 0.0;
+      for (int t = 0; t < tiles; ++t) {
+        norms[0] += ph[2 * t];
+        norms[1] += ph[2 * t + 1];
+      }
+    }
   });
 }
 

@@ -185,6 +185,25 @@ struct Sp2Rule {
 }
 
 namespace pm7 {
+// FP64-accuracy SP2 squarings on the tcgen05 integer tensor cores (kernels_i8.cu): the
+// iterate in fp64 (n x n) and as eight int8 digit planes (sp2_i8_digit_bytes(n) bytes, rows of
+// sp2_i8_ld(n) bytes) whose two tensor maps (128-byte opaque CUtensorMap each) come from
+// make_digit_maps. launch_sp2_step_i8 is the fused step of launch_sp2_step (same state, step
+// and partial protocol) reading x_in and its planes, writing x_out and its planes; `error`:
+// 1 a pipeline wait expired, 2 an element left the digits' range. launch_sp2_digits splits X
+// into planes (step < 0: unconditionally; else only while that step is active).
+int sp2_i8_ld(int n);
+size_t sp2_i8_digit_bytes(int n);
+int sp2_i8_tiles(int n);
+bool make_digit_maps(const int8_t *dig, int n, void *map_a, void *map_b);
+void prepare_i8_kernels();
+void launch_sp2_digits(cudaStream_t st, int n, const double *X, int8_t *dig, const double *state, int step,
+                       int *error);
+void launch_sp2_step_i8(cudaStream_t st, int n, const void *map_a, const void *map_b, const double *x_in,
+                        double *x_out, int8_t *dig_out, double *state, double *parts, int step, int *error);
+}  // namespace pm7
+
+namespace pm7 {
 // FP32-accuracy (3xTF32) symmetric squaring on tcgen05 (kernels_tf32.cu). Matrices are
 // ld x ld fp32, ld a multiple of 32, zero padded beyond n; the maps come from
 // make_square_map (an opaque 128-byte CUtensorMap each).

@@ -22,6 +22,7 @@
 
 #include "common.cuh"
 #include "kernels.hpp"
+#include "tcgen05.cuh"
 
 namespace pm7 {
 namespace {
@@ -30,59 +31,8 @@ constexpr int TM = 128, TN = 128, TK = 32, STAGES = 3;
 constexpr int TILE_BYTES = TM * TK * 4;            // 16 KB: 128 rows x 32 fp32 (128 B per row)
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;        // Ahi, Alo, Bhi, Blo
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;  // + alignment slack + barriers
-constexpr unsigned long long kWaitNs = 1000000000ull;  // a pipeline wait gives up after 1 s
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Bounded wait for phase `parity` of an mbarrier; false when the time limit expired (the
-// CTA's abort flag is then set) or another thread of the CTA already aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
-  const uint32_t addr = smem_u32(bar);
-  unsigned long long t0 = 0;
-  for (uint32_t it = 0; it < (1u << 30); ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if ((it & 15) == 15) {
-      if (*abort_flag) return false;
-      const unsigned long long t = global_ns();
-      if (it == 15) t0 = t;
-      else if (t - t0 > kWaitNs) break;
-    }
-  }
-  *abort_flag = 1;
-  return false;
-}
-
-__device__ __forceinline__ void tma_load_2d(void *smem_dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
-          smem_u32(smem_dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
-      : "memory");
-}
+using namespace tc;
 
 // Shared-memory matrix descriptor: K-major operand, 128-byte swizzle, 8-row groups 1024 B
 // apart (SBO), version 1 (tcgen05), base offset 0 (stage buffers are 1024-byte aligned).
@@ -111,10 +61,6 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b
       "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate));
 }
 
-__device__ __forceinline__ void mma_commit(uint64_t *bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
 
 // One 128x128 tile (bm, bn) of C = A B for symmetric A, B (so B's columns are its rows:
 // both operands K-major row blocks). `smem_raw` is the CTA's dynamic shared memory
@@ -267,28 +213,25 @@ __global__ void __launch_bounds__(128) k_product_tf32x3(const __grid_constant__ 
   product_tile(blockIdx.x / t, blockIdx.x % t, &a_hi, &a_lo, &b_hi, &b_lo, false, n, ld, C, error, smem_raw);
 }
 
+}  // namespace
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
-using EncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                              const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-EncodeFn encode_fn() {
-  static EncodeFn fn = nullptr;
+TensorMapEncodeFn tensor_map_encode_fn() {
+  static TensorMapEncodeFn fn = nullptr;
   static std::once_flag once;
   std::call_once(once, [] {
     void *p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeFn>(p);
+      fn = reinterpret_cast<TensorMapEncodeFn>(p);
   });
   return fn;
 }
 
-}  // namespace
-
 // Tensor map of an ld x ld fp32 row-major matrix with 32 x 128 boxes, 128-byte swizzle.
 bool make_square_map(const float *base, int ld, void *map_out) {
-  EncodeFn fn = encode_fn();
+  TensorMapEncodeFn fn = tensor_map_encode_fn();
   if (!fn || ld % 32 != 0 || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
   const cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)ld};
   const cuuint64_t strides[1] = {(cuuint64_t)ld * 4};

@@ -27,7 +27,7 @@ EXPORTED = [
     "pm7_correction_gradient", "pm7_run_batch_gradient", "pm7_engine_submit_gradient",
     "pm7_dandc_options_default", "pm7_run_dandc", "pm7_dandc_result_free", "pm7_stage_dandc_partition",
     "pm7_dandc_abi_sizes", "pm7_stage_seqsum", "pm7_stage_tf32_wait_drill",
-    "pm7_engine_stats", "pm7_stage_fock_fp32",
+    "pm7_engine_stats", "pm7_stage_fock_fp32", "pm7_stage_sp2_step_i8",
 ]
 
 
@@ -606,6 +606,20 @@ def eigenvalues(matrices, device=0):
         res.append(out[off:off + n].copy())
         off += n
     return res
+
+
+def sp2_step_i8(x, square=True):
+    """One fused FP64-accuracy SP2 step on the tcgen05 integer tensor cores (int8 digit
+    planes): (x x or 2 x - x x, [tr, |.|_F^2] of it from the step's partials)."""
+    L = lib()
+    L.pm7_stage_sp2_step_i8.argtypes = [C.c_int32, abi.DP, C.c_int32, abi.DP, abi.DP]
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n = x.shape[0]
+    out = np.zeros((n, n))
+    norms = np.zeros(2)
+    _check(L.pm7_stage_sp2_step_i8(n, x.ctypes.data_as(abi.DP), int(bool(square)), out.ctypes.data_as(abi.DP),
+                                   norms.ctypes.data_as(abi.DP)))
+    return out, norms
 
 
 def product_tf32(a, b):
