@@ -297,20 +297,36 @@ __global__ void __launch_bounds__(128) k_sp2_step_i8(const __grid_constant__ CUt
 
 // The digit planes (plane p at dig + p plane, rows of ld8 bytes) of an n x n fp64 matrix: the
 // start iterate, and the output of each step (skipped, like the step, once the purification
-// has stopped; step < 0: always).
-__global__ void k_sp2_digits(int n, int ld8, const double *__restrict__ X, int8_t *__restrict__ dig,
-                             const double *__restrict__ state, int step, int *__restrict__ error) {
+// has stopped; step < 0: always). Grid (ceil(n / 1024), n): a thread takes four columns of one
+// row and stores each plane's four digits as one 32-bit word (ld8 is a multiple of 16, so the
+// words stay inside the row's padding).
+__global__ void __launch_bounds__(256) k_sp2_digits(int n, int ld8, const double *__restrict__ X,
+                                                    int8_t *__restrict__ dig, const double *__restrict__ state,
+                                                    int step, int *__restrict__ error) {
   if (step >= 0 && !sp2_active(state, step)) return;
-  const size_t len = (size_t)n * n, plane = (size_t)n * ld8;
-  bool good = true;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x) {
-    const size_t row = e / n, col = e - row * n;
-    int8_t a[kDigits];
-    good = split_digits(X[e], a) && good;
-    int8_t *base = dig + row * ld8 + col;
+  const int row = blockIdx.y, c0 = (blockIdx.x * 256 + threadIdx.x) * 4;
+  if (c0 >= n) return;
+  const size_t plane = (size_t)n * ld8;
+  const double *xr = X + (size_t)row * n;
+  uint32_t word[kDigits];
 #pragma unroll
-    for (int p = 0; p < kDigits; ++p) base[(size_t)p * plane] = a[p];
+  for (int p = 0; p < kDigits; ++p) word[p] = 0u;
+  bool good = true;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    int8_t a[kDigits];
+    if (c0 + q < n) {
+      good = split_digits(xr[c0 + q], a) && good;
+    } else {
+#pragma unroll
+      for (int p = 0; p < kDigits; ++p) a[p] = 0;
+    }
+#pragma unroll
+    for (int p = 0; p < kDigits; ++p) word[p] |= (uint32_t)(uint8_t)a[p] << (8 * q);
   }
+  int8_t *base = dig + (size_t)row * ld8 + c0;
+#pragma unroll
+  for (int p = 0; p < kDigits; ++p) *reinterpret_cast<uint32_t *>(base + (size_t)p * plane) = word[p];
   if (!good) atomicExch(error, 2);
 }
 
@@ -364,7 +380,7 @@ void prepare_i8_kernels() {
 
 void launch_sp2_digits(cudaStream_t st, int n, const double *X, int8_t *dig, const double *state, int step,
                        int *error) {
-  k_sp2_digits<<<1184, 256, 0, st>>>(n, sp2_i8_ld(n), X, dig, state, step, error);
+  k_sp2_digits<<<dim3((n + 1023) / 1024, n), 256, 0, st>>>(n, sp2_i8_ld(n), X, dig, state, step, error);
   note_launch();
 }
 
