@@ -41,6 +41,9 @@ import time
 from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
+# the CPU checker (the OpenMP oracle) runs between GPU measurements in this process: its idle
+# worker threads must sleep rather than spin on the cores the engine's host threads use
+os.environ.setdefault("OMP_WAIT_POLICY", "PASSIVE")
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "pm7-rs_b200"))
 
@@ -511,6 +514,9 @@ def default_extras(args, local):
             "rate_per_s": ln["config"]["rate_per_s"], "capacity_per_s": ln["config"]["capacity_per_s"],
             "plain_fp64_solves_per_s": ln["plain_path"]["value"],
             "served_over_plain": ln["plain_path"]["served_over_plain"],
+            "sustained_solves_per_s": ln["sustained"]["value"],
+            "sustained_over_plain": ln["plain_path"]["sustained_over_plain"],
+            "capacity_over_plain": ln["plain_path"]["capacity_over_plain"],
             "max_dhf_diff_vs_plain_kcal": ln["plain_path"]["max_dhf_diff_kcal"],
             "oracle_check": ln.get("oracle_check"), "failed": ln["config"]["failed"], "clocks": ln["clocks"]}
     for prec in ("fp64", "mixed"):
@@ -644,8 +650,9 @@ def run_stream_bench(args, world, rank, local, oracle_check=False):
         for _ in range(max(1, args.warmup - 1)):
             for k in [eng.submit(z, x, want_matrices=0, precision=prec) for z, x in burst]:
                 eng.poll(k, wait=True)
-        for k in [eng.submit(z, x, want_matrices=0, precision=prec) for z, x in mols]:
-            eng.poll(k, wait=True)
+        for _ in range(2):  # the engine's throughput on a full stream settles on its third pass
+            for k in [eng.submit(z, x, want_matrices=0, precision=prec) for z, x in mols]:
+                eng.poll(k, wait=True)
         t = time.perf_counter()
         tk = [eng.submit(z, x, want_matrices=0, precision=prec) for z, x in mols]
         for k in tk:
@@ -659,6 +666,7 @@ def run_stream_bench(args, world, rank, local, oracle_check=False):
         sampler.start()
         launches0 = api.launch_count()
         tickets = [None] * count
+        submitted = np.zeros(count)
         t0 = time.perf_counter()
         due = t0
         for i, (z, x) in enumerate(mols):
@@ -666,6 +674,7 @@ def run_stream_bench(args, world, rank, local, oracle_check=False):
             now = time.perf_counter()
             if due > now:
                 time.sleep(due - now)
+            submitted[i] = time.perf_counter()
             tickets[i] = eng.submit(z, x, want_matrices=0, precision=prec)
         res = [eng.poll(tk, wait=True)[1] for tk in tickets]
         wall = time.perf_counter() - t0
@@ -685,6 +694,12 @@ def run_stream_bench(args, world, rank, local, oracle_check=False):
     ok = [r for r in res if not isinstance(r, Exception)]
     lat = [r["latency_ms"] for r in ok]
     value = len(ok) * world / wall
+    # sustained rate: completions inside the steady window between the submissions of the
+    # 10th and the 90th percentile request (no ramp-up, no drain), per second of that window
+    finished = np.array([submitted[i] + r["latency_ms"] * 1e-3 for i, r in enumerate(res)
+                         if not isinstance(r, Exception)])
+    w0, w1 = submitted[count // 10], submitted[(9 * count) // 10]
+    sustained = float(np.sum((finished >= w0) & (finished < w1))) / (w1 - w0) * world
     idx = list(range(0, count, max(1, count // 24)))[:24]
     plain, plain_res = _plain_sample(api, mols, idx, local)
     dhf = max(abs(res[i]["heat_of_formation_kcal"] - plain_res[i]["heat_of_formation_kcal"])
@@ -701,7 +716,10 @@ def run_stream_bench(args, world, rank, local, oracle_check=False):
         "latency_ms": _percentiles(lat),
         "e2e": {"value": value, "unit": "solves/s", "note": "submit to finish through pm7_engine, host buffers"},
         "plain_path": {"value": plain, "unit": "solves/s", "sample": f"{len(idx)} molecules of the stream via pm7_run",
-                       "served_over_plain": value / plain, "max_dhf_diff_kcal": dhf},
+                       "served_over_plain": value / plain, "sustained_over_plain": sustained / plain,
+                       "capacity_over_plain": capacity * world / plain, "max_dhf_diff_kcal": dhf},
+        "sustained": {"value": sustained, "unit": "solves/s",
+                      "window": "completions between the submissions of the 10th and 90th percentile requests"},
         "gpu_launches": launches, "clocks": clocks,
         "stages": {k: {"ms_total": round(v[0], 3), "calls": v[1]} for k, v in prof.items()},
         "stages_note": f"one more untimed burst of {len(burst)} requests with stage events",
@@ -788,7 +806,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="water334",
                     choices=["water334", "water1000", "decane", "batch4096", "stream", "dandc640"])
-    ap.add_argument("--stream-count", type=int, default=600)
+    ap.add_argument("--stream-count", type=int, default=1200)
     ap.add_argument("--dandc-carbons", type=int, default=640, help="dandc640: chain length (small cases for profiles)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="batch4096/stream: fp64, or fp32 tcgen05 purification cycles with fp64 refinement")
