@@ -1211,10 +1211,10 @@ class BatchRunner {
   size_t bytes_in_use() const { return bytes_in_use_; }
   long long sp2_fallbacks() const { return sp2_fallbacks_; }
   // Host wall time of each phase of iterate() so far (seconds), for PM7_BATCH_TRACE.
-  static constexpr int kPhases = 7;
+  static constexpr int kPhases = 8;
   static const char *phase_name(int k) {
     static const char *names[kPhases] = {"queue", "mixed_sync", "sp2", "eigensolve", "converge", "retire_end",
-                                         "retire"};
+                                         "retire", "admit"};
     return names[k];
   }
   double phase_seconds(int k) const { return phase_s_[k]; }
@@ -1224,6 +1224,12 @@ class BatchRunner {
   // build phase for all of them); they join the next iteration.
   void admit(std::vector<BatchMol *> &in) {
     if (in.empty()) return;
+    const auto t_admit0 = std::chrono::steady_clock::now();
+    struct AdmitClock {  // host wall of admissions, for PM7_BATCH_TRACE
+      double &acc;
+      std::chrono::steady_clock::time_point t0;
+      ~AdmitClock() { acc += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+    } admit_clock{phase_s_[kPhases - 1], t_admit0};
     CUDA_OK(cudaSetDevice(ctx_.device));
     const int n = (int)in.size();
     for (BatchMol *b : in) {
