@@ -11,18 +11,17 @@
 // product with fixed-point splits. The error of one squaring is ~1e-17 n in the largest
 // element, about that of an fp64 GEMM.
 //
-// One CTA per 128 x 64 tile of the lower triangle (the upper part mirrored). Warp 0 lane 0
-// feeds a 2-stage ring with two 3-D TMA loads per stage (the eight planes of the A row block
-// and of the B row block, 64 bytes of K each, 64-byte swizzle, no multicast); warp 1 lane 0
-// issues the 2 x 36 digit-pair MMAs of each stage (M = 128, N = 64, K = 32) into eight 64-column
-// int32 accumulators in TMEM (512 columns, G_g at column 64 g); after the last stage all four
-// warps combine the accumulators in fp64 (Horner over g), stage the tile in shared memory and
-// apply the fused SP2 step: X_{k+1} = X_k^2 or 2 X_k - X_k^2 by the step's decision, written
-// in fp64 with its mirror (coalesced), and the tile's share of tr X_{k+1} and |X_{k+1}|_F^2
-// for the next decision. A separate elementwise kernel then splits X_{k+1} into its digit
-// planes (integer arithmetic, every SM busy), which keeps that work out of the epilogue: with
-// all 512 TMEM columns in use a CTA's epilogue cannot overlap another tile's MMAs. Every
-// mbarrier wait has a time limit.
+// Tiles of 128 x 64 over the lower triangle (the upper part mirrored), walked by a persistent
+// CTA per SM with specialised warps. A producer lane feeds a 3-stage ring with two 3-D TMA loads
+// per stage (the eight planes of the A row block and of the B row block, 32 bytes of K each,
+// 32-byte swizzle, no multicast); an MMA lane issues the 36 digit-pair MMAs of each stage
+// (M = 128, N = 64, K = 32) into eight 64-column int32 accumulators in TMEM (all 512 columns,
+// G_g at column 64 g); four epilogue warps combine the accumulators in fp64 (Horner over g)
+// into a staging tile, release TMEM for the CTA's next tile, and apply the fused SP2 step while
+// that tile's MMAs run: X_{k+1} = X_k^2 or 2 X_k - X_k^2 by the step's decision, written in
+// fp64 with its mirror (coalesced), and the tile's share of tr X_{k+1} and |X_{k+1}|_F^2 for
+// the next decision. A separate elementwise kernel then splits X_{k+1} into its digit planes
+// (integer arithmetic, every SM busy). Every mbarrier wait has a time limit.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -42,15 +41,17 @@ constexpr int IM = 128, IN = 64;         // tile rows, columns
 constexpr int kTmemCols = kDigits * IN;  // eight 64-column accumulators
 constexpr int LDT = IN + 1;              // staging row stride (doubles)
 
-// The stage geometry for KS bytes of K per stage (32: 32-byte swizzle, 4 stages of 48 KB;
-// 64: 64-byte swizzle, 2 stages of 96 KB).
+// The stage geometry for KS bytes of K per stage (32: 32-byte swizzle, 3 stages of 48 KB), and
+// the CTA's shared memory: the stages, the epilogue's fp64 staging tile (its own, so that the
+// next tile's loads proceed during the epilogue), the partials, the barriers and the alignment
+// slack.
 template <int KS>
 struct I8Stage {
-  static constexpr int STAGES = KS == 32 ? 4 : 2;
+  static constexpr int STAGES = 3;
   static constexpr int A_PLANE = IM * KS, B_PLANE = IN * KS;
   static constexpr int BYTES = kDigits * (A_PLANE + B_PLANE);
-  static constexpr int SMEM = STAGES * BYTES + 1024 + 256;  // + alignment slack + barriers
-  static_assert(IM * LDT * 8 + 64 <= STAGES * BYTES, "epilogue staging fits in the stage buffers");
+  static constexpr int SMEM = STAGES * BYTES + IM * LDT * 8 + 64 + (2 * STAGES + 2) * 8 + 16 + 1024;
+  static_assert(SMEM <= 227 * 1024, "one CTA per SM within the shared-memory limit");
 };
 
 // Shared-memory matrix descriptor: K-major operand with KS-byte rows and the matching swizzle
@@ -123,32 +124,39 @@ __device__ __forceinline__ void i8_tile(int t, int n, int &bm, int &bn) {
   bn = t;
 }
 
-// One fused SP2 step (see the file header) into x_out (fp64; its digit planes follow from
-// k_sp2_digits); `map_a` / `map_b` are the input digit planes' 3-D tensor maps with 128- and
-// 64-row boxes. The step does nothing once an earlier step has stopped the purification.
+// Persistent fused SP2 steps (see the file header) into x_out (fp64; its digit planes follow
+// from k_sp2_digits). One CTA per SM walks the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
+// with specialised warps: warp 4 lane 0 feeds the TMA ring (running ahead into the next tile),
+// warp 5 lane 0 issues the MMAs and owns the TMEM allocation, warps 0-3 (TMEM lane quarters
+// 0-3) are the epilogue. The eight accumulators fill the 512 TMEM columns, so the epilogue first
+// drains them into the fp64 staging tile and releases TMEM (tmem_empty), and only then applies
+// the SP2 update and stores, while the MMAs of the CTA's next tile already run. `map_a` /
+// `map_b` are the input digit planes' 3-D tensor maps with 128- and 64-row boxes. The step does
+// nothing once an earlier step has stopped the purification.
 template <int KS>
-__global__ void __launch_bounds__(128) k_sp2_step_i8(const __grid_constant__ CUtensorMap map_a,
-                                                     const __grid_constant__ CUtensorMap map_b, int n,
-                                                     const double *__restrict__ x_in, double *__restrict__ x_out,
-                                                     double *__restrict__ state, int step,
-                                                     double *__restrict__ parts, int *__restrict__ error) {
+__global__ void __launch_bounds__(192, 1) k_sp2_step_i8(const __grid_constant__ CUtensorMap map_a,
+                                                        const __grid_constant__ CUtensorMap map_b, int n,
+                                                        const double *__restrict__ x_in, double *__restrict__ x_out,
+                                                        double *__restrict__ state, int step,
+                                                        double *__restrict__ parts, int *__restrict__ error) {
   using G = I8Stage<KS>;
   constexpr int ISTAGES = G::STAGES, I_STAGE = G::BYTES, A_PLANE = G::A_PLANE, B_PLANE = G::B_PLANE;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   if (!sp2_active(state, step)) return;  // the whole CTA, before any barrier or TMEM set-up
-  int bm, bn;
-  i8_tile(blockIdx.x, n, bm, bn);
+  const int tiles = i8_tile_count(n);
   const bool square = state[kSp2Square] != 0.0;
-  if (blockIdx.x == 0 && threadIdx.x == 0) state[kSp2Parts] = (double)gridDim.x;
+  if (blockIdx.x == 0 && threadIdx.x == 0) state[kSp2Parts] = (double)tiles;
 
   unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem + ISTAGES * I_STAGE);
+  double *T = reinterpret_cast<double *>(smem + ISTAGES * I_STAGE);  // epilogue staging, IM x LDT
+  double *red = T + IM * LDT;
+  uint64_t *full = reinterpret_cast<uint64_t *>(red + 8);
   uint64_t *empty = full + ISTAGES;
-  uint64_t *done = empty + ISTAGES;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+  uint64_t *tmem_full = empty + ISTAGES;
+  uint64_t *tmem_empty = tmem_full + 1;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tmem_empty + 1);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
-  const int m0 = bm * IM, n0 = bn * IN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ktiles = (n + KS - 1) / KS;
 
@@ -157,11 +165,12 @@ __global__ void __launch_bounds__(128) k_sp2_step_i8(const __grid_constant__ CUt
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(done, 1);
+    mbar_init(tmem_full, 1);
+    mbar_init(tmem_empty, 4);  // one arrival per epilogue warp
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == 5) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -171,128 +180,156 @@ __global__ void __launch_bounds__(128) k_sp2_step_i8(const __grid_constant__ CUt
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == 0 && lane == 0) {
-    // producer: TMA ring, all eight planes of both row blocks per stage
-    for (int kt = 0; kt < ktiles; ++kt) {
-      const int s = kt % ISTAGES;
-      if (kt >= ISTAGES && !mbar_wait(&empty[s], (uint32_t)((kt / ISTAGES - 1) & 1), abort_flag)) break;
-      unsigned char *st = smem + s * I_STAGE;
-      mbar_expect_tx(&full[s], I_STAGE);
-      tma_load_3d(st, &map_a, &full[s], kt * KS, m0, 0);
-      tma_load_3d(st + kDigits * A_PLANE, &map_b, &full[s], kt * KS, n0, 0);
-    }
-  } else if (warp == 1 && lane == 0) {
-    // MMA issuer: digit pairs (i, j), i + j <= 7, into accumulator i + j
-    bool ok = true;
-    for (int kt = 0; kt < ktiles && ok; ++kt) {
-      const int s = kt % ISTAGES;
-      if (!mbar_wait(&full[s], (uint32_t)((kt / ISTAGES) & 1), abort_flag)) {
-        ok = false;
-        break;
+  if (warp == 4) {
+    if (lane == 0) {  // producer: the TMA ring over all of this CTA's tiles
+      int g = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+        int bm, bn;
+        i8_tile(t, n, bm, bn);
+        for (int kt = 0; kt < ktiles; ++kt, ++g) {
+          const int s = g % ISTAGES;
+          if (g >= ISTAGES && !mbar_wait(&empty[s], (uint32_t)((g / ISTAGES - 1) & 1), abort_flag)) {
+            ok = false;
+            break;
+          }
+          unsigned char *st = smem + s * I_STAGE;
+          mbar_expect_tx(&full[s], I_STAGE);
+          tma_load_3d(st, &map_a, &full[s], kt * KS, bm * IM, 0);
+          tma_load_3d(st + kDigits * A_PLANE, &map_b, &full[s], kt * KS, bn * IN, 0);
+        }
       }
+    }
+  } else if (warp == 5) {
+    if (lane == 0) {  // MMA issuer: digit pairs (i, j), i + j <= 7, into accumulator i + j
+      int g = 0, u = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++u) {
+        // the epilogue has drained the previous tile's accumulators
+        if (u > 0 && !mbar_wait(tmem_empty, (uint32_t)((u - 1) & 1), abort_flag)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        for (int kt = 0; kt < ktiles; ++kt, ++g) {
+          const int s = g % ISTAGES;
+          if (!mbar_wait(&full[s], (uint32_t)((g / ISTAGES) & 1), abort_flag)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          unsigned char *st = smem + s * I_STAGE;
+          // plane and K offsets go into the descriptors' start-address field (16-byte units;
+          // the stage lies below 256 KB, so the 14-bit field does not carry)
+          const uint64_t da = desc_swz<KS>(st), db = desc_swz<KS>(st + kDigits * A_PLANE);
+#pragma unroll
+          for (int ks = 0; ks < KS / 32; ++ks) {  // K = 32 bytes per MMA: start address + 32 ks bytes
+            const uint64_t koff = (uint64_t)(2 * ks);
+#pragma unroll
+            for (int i = 0; i < kDigits; ++i) {
+              const uint64_t a = da + (uint64_t)((i * A_PLANE) >> 4) + koff;
+#pragma unroll
+              for (int j = 0; j + i < kDigits; ++j)
+                mma_i8(tmem + (uint32_t)((i + j) * IN), a, db + (uint64_t)((j * B_PLANE) >> 4) + koff,
+                       (kt > 0 || ks > 0 || i > 0) ? 1u : 0u);
+            }
+          }
+          mma_commit(&empty[s]);  // the stage is free once these MMAs have read it
+        }
+        if (ok) mma_commit(tmem_full);  // the tile's accumulators are final once its MMAs completed
+      }
+      if (!ok) *abort_flag = 1;
+    }
+  } else {
+    // epilogue, warps 0-3: warp w reads TMEM lanes 32 w .. 32 w + 31 = tile rows
+    int u = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++u) {
+      int bm, bn;
+      i8_tile(t, n, bm, bn);
+      const int m0 = bm * IM, n0 = bn * IN;
+      const bool ok = mbar_wait(tmem_full, (uint32_t)(u & 1), abort_flag);
+      asm volatile("bar.sync 1, 128;" ::: "memory");  // every epilogue thread has its verdict
+      if (!ok || *abort_flag) break;
       asm volatile("tcgen05.fence::after_thread_sync;");
-      unsigned char *st = smem + s * I_STAGE;
-      // plane and K offsets go into the descriptors' start-address field (16-byte units; the
-      // stage lies below 256 KB, so the 14-bit field does not carry)
-      const uint64_t da = desc_swz<KS>(st), db = desc_swz<KS>(st + kDigits * A_PLANE);
+      // accumulators -> X_k^2 tile in fp64 (Horner over g), thread = tile row
+#pragma unroll 1
+      for (int h = 0; h < IN / 32; ++h) {
+        double acc[32];
+        uint32_t r[32];
+        tmem_ld32(tmem, warp, (kDigits - 1) * IN + 32 * h, r);
 #pragma unroll
-      for (int ks = 0; ks < KS / 32; ++ks) {  // K = 32 bytes per MMA: start address + 32 ks bytes
-        const uint64_t koff = (uint64_t)(2 * ks);
+        for (int q = 0; q < 32; ++q) acc[q] = (double)(int)r[q];
+#pragma unroll 1
+        for (int g = kDigits - 2; g >= 0; --g) {
+          tmem_ld32(tmem, warp, g * IN + 32 * h, r);
 #pragma unroll
-        for (int i = 0; i < kDigits; ++i) {
-          const uint64_t a = da + (uint64_t)((i * A_PLANE) >> 4) + koff;
+          for (int q = 0; q < 32; ++q) acc[q] = (double)(int)r[q] + acc[q] * 0.0078125;  // 2^-7
+        }
 #pragma unroll
-          for (int j = 0; j + i < kDigits; ++j)
-            mma_i8(tmem + (uint32_t)((i + j) * IN), a, db + (uint64_t)((j * B_PLANE) >> 4) + koff,
-                   (kt > 0 || ks > 0 || i > 0) ? 1u : 0u);
+        for (int q = 0; q < 32; ++q) T[(warp * 32 + lane) * LDT + 32 * h + q] = acc[q] * 0.000244140625;  // 2^-12
+      }
+      // TMEM is free for the next tile's MMAs
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(tmem_empty)) : "memory");
+      asm volatile("bar.sync 1, 128;" ::: "memory");  // the staging tile is complete
+      // the tile's lower-triangle elements (row >= column), thread = column c of a 64-row half;
+      // X_k read 8 rows at a time; the new value goes back into the staging for the mirror
+      double tr = 0.0, fro = 0.0;
+      const int c = threadIdx.x & (IN - 1), i_lo = (threadIdx.x / IN) * (IM / 2), gc = n0 + c;
+      for (int i0 = i_lo; i0 < i_lo + IM / 2; i0 += 8) {
+        double xo[8];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+          const int gr = m0 + i0 + v;
+          const bool live = !square && gr < n && gc < n && gr >= gc;
+          xo[v] = live ? __ldg(x_in + (size_t)gr * n + gc) : 0.0;
+        }
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+          const int i = i0 + v, gr = m0 + i;
+          if (gr >= n || gc >= n || gr < gc) continue;
+          const double y = T[i * LDT + c];
+          const double x = square ? y : 2.0 * xo[v] - y;
+          T[i * LDT + c] = x;
+          x_out[(size_t)gr * n + gc] = x;
+          if (gr == gc) {
+            tr += x;
+            fro += x * x;
+          } else {
+            fro += 2.0 * x * x;
+          }
         }
       }
-      mma_commit(&empty[s]);  // the stage is free once these MMAs have read it
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+      // the mirror (column block n0 .. n0 + 63 as rows), thread = column m0 + threadIdx.x
+      const int mc = m0 + threadIdx.x;
+      for (int j = 0; j < IN; ++j) {
+        const int gr = n0 + j;
+        if (gr >= n || mc >= n || mc <= gr) continue;
+        x_out[(size_t)gr * n + mc] = T[threadIdx.x * LDT + j];
+      }
+      // the tile's partials, summed in a fixed order
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        tr += __shfl_down_sync(0xffffffffu, tr, o);
+        fro += __shfl_down_sync(0xffffffffu, fro, o);
+      }
+      if (lane == 0) {
+        red[2 * warp] = tr;
+        red[2 * warp + 1] = fro;
+      }
+      asm volatile("bar.sync 1, 128;" ::: "memory");  // partials written, staging reads done
+      if (threadIdx.x == 0) {
+        parts[2 * t] = (red[0] + red[2]) + (red[4] + red[6]);
+        parts[2 * t + 1] = (red[1] + red[3]) + (red[5] + red[7]);
+      }
     }
-    if (ok) mma_commit(done);  // the accumulators are final once every MMA completed
-    else *abort_flag = 1;
   }
-  __syncwarp();
-  const bool ok = __syncthreads_and(mbar_wait(done, 0u, abort_flag) ? 1 : 0) != 0;
-  asm volatile("tcgen05.fence::after_thread_sync;");
-  if (ok) {
-    // accumulators -> X_k^2 tile in fp64 (thread = tile row), staged in the free stage buffers
-    double *T = reinterpret_cast<double *>(smem);
-    double *red = T + IM * LDT;
-#pragma unroll 1
-    for (int h = 0; h < IN / 32; ++h) {
-      double acc[32];
-      uint32_t r[32];
-      tmem_ld32(tmem, warp, (kDigits - 1) * IN + 32 * h, r);
-#pragma unroll
-      for (int q = 0; q < 32; ++q) acc[q] = (double)(int)r[q];
-#pragma unroll 1
-      for (int g = kDigits - 2; g >= 0; --g) {
-        tmem_ld32(tmem, warp, g * IN + 32 * h, r);
-#pragma unroll
-        for (int q = 0; q < 32; ++q) acc[q] = (double)(int)r[q] + acc[q] * 0.0078125;  // 2^-7
-      }
-#pragma unroll
-      for (int q = 0; q < 32; ++q) T[(warp * 32 + lane) * LDT + 32 * h + q] = acc[q] * 0.000244140625;  // 2^-12
-    }
-    __syncthreads();
-    // the tile's lower-triangle elements (row >= column), thread = column c of a 64-row half;
-    // X_k read 8 rows at a time; the new value goes back into the staging for the mirror
-    double tr = 0.0, fro = 0.0;
-    const int c = threadIdx.x & (IN - 1), i_lo = (threadIdx.x / IN) * (IM / 2), gc = n0 + c;
-    for (int i0 = i_lo; i0 < i_lo + IM / 2; i0 += 8) {
-      double xo[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int gr = m0 + i0 + u;
-        const bool live = !square && gr < n && gc < n && gr >= gc;
-        xo[u] = live ? __ldg(x_in + (size_t)gr * n + gc) : 0.0;
-      }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int i = i0 + u, gr = m0 + i;
-        if (gr >= n || gc >= n || gr < gc) continue;
-        const double v = T[i * LDT + c];
-        const double x = square ? v : 2.0 * xo[u] - v;
-        T[i * LDT + c] = x;
-        x_out[(size_t)gr * n + gc] = x;
-        if (gr == gc) {
-          tr += x;
-          fro += x * x;
-        } else {
-          fro += 2.0 * x * x;
-        }
-      }
-    }
-    __syncthreads();
-    // the mirror (column block n0 .. n0 + 63 as rows), thread = column m0 + t
-    const int t = threadIdx.x, mc = m0 + t;
-    for (int j = 0; j < IN; ++j) {
-      const int gr = n0 + j;
-      if (gr >= n || mc >= n || mc <= gr) continue;
-      x_out[(size_t)gr * n + mc] = T[t * LDT + j];
-    }
-    // the tile's partials, summed in a fixed order
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      tr += __shfl_down_sync(0xffffffffu, tr, o);
-      fro += __shfl_down_sync(0xffffffffu, fro, o);
-    }
-    if (lane == 0) {
-      red[2 * warp] = tr;
-      red[2 * warp + 1] = fro;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      parts[2 * blockIdx.x] = (red[0] + red[2]) + (red[4] + red[6]);
-      parts[2 * blockIdx.x + 1] = (red[1] + red[3]) + (red[5] + red[7]);
-    }
-  } else if (threadIdx.x == 0) {
-    atomicExch(error, 1);
-  }
+  if (threadIdx.x == 0 && *abort_flag) atomicExch(error, 1);
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+  if (warp == 5) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 
 // The digit planes (plane p at dig + p plane, rows of ld8 bytes) of an n x n fp64 matrix: the
@@ -332,10 +369,20 @@ __global__ void __launch_bounds__(256) k_sp2_digits(int n, int ld8, const double
 
 }  // namespace
 
-// K bytes per pipeline stage: 64 (two 96 KB stages, 64-byte swizzle) measured 3% faster than
-// 32 (four 48 KB stages, 32-byte swizzle) at orders 2,004 and 6,000.
-constexpr int kKStage = 64;
+// K bytes per pipeline stage (32-byte swizzle): with the epilogue's own staging tile, three
+// 48 KB stages fit beside it.
+constexpr int kKStage = 32;
 static int i8_kstage() { return kKStage; }
+
+// CTAs of the persistent step: one per SM (or per tile, when there are fewer tiles).
+static int i8_grid(int tiles) {
+  static int sms[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int &c = sms[dev & 63];
+  if (c == 0 && cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) c = 148;
+  return tiles < c ? tiles : c;
+}
 
 int sp2_i8_ld(int n) { return ((n + 15) / 16) * 16; }
 size_t sp2_i8_digit_bytes(int n) { return (size_t)kDigits * n * sp2_i8_ld(n); }
@@ -373,8 +420,7 @@ void prepare_i8_kernels() {
   cudaGetDevice(&dev);
   std::lock_guard<std::mutex> lock(mu);
   if (dev < 0 || dev >= 64 || done[dev]) return;
-  cudaFuncSetAttribute(k_sp2_step_i8<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, I8Stage<32>::SMEM);
-  cudaFuncSetAttribute(k_sp2_step_i8<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, I8Stage<64>::SMEM);
+  cudaFuncSetAttribute(k_sp2_step_i8<kKStage>, cudaFuncAttributeMaxDynamicSharedMemorySize, I8Stage<kKStage>::SMEM);
   done[dev] = true;
 }
 
@@ -389,12 +435,8 @@ void launch_sp2_step_i8(cudaStream_t st, int n, const void *map_a, const void *m
   prepare_i8_kernels();
   const CUtensorMap &ma = *reinterpret_cast<const CUtensorMap *>(map_a);
   const CUtensorMap &mb = *reinterpret_cast<const CUtensorMap *>(map_b);
-  if (i8_kstage() == 64)
-    k_sp2_step_i8<64><<<i8_tile_count(n), 128, I8Stage<64>::SMEM, st>>>(ma, mb, n, x_in, x_out, state, step,
-                                                                         parts, error);
-  else
-    k_sp2_step_i8<32><<<i8_tile_count(n), 128, I8Stage<32>::SMEM, st>>>(ma, mb, n, x_in, x_out, state, step,
-                                                                         parts, error);
+  k_sp2_step_i8<kKStage><<<i8_grid(i8_tile_count(n)), 192, I8Stage<kKStage>::SMEM, st>>>(
+      ma, mb, n, x_in, x_out, state, step, parts, error);
   note_launch();
   launch_sp2_digits(st, n, x_out, dig_out, state, step, error);
 }
