@@ -406,12 +406,12 @@ def run_b200(args, world, rank, local):
                     "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)"}
     if i8_calls:
         # the FP64-accuracy squarings on the integer tensor cores: issued int8 work per launch
-        # (36 digit-pair products over the 128 x 64 lower tiles, K padded to 64) against twice
+        # (36 digit-pair products over the 128 x 64 lower tiles, K padded to 32) against twice
         # the measured bf16 dense rate (kind::i8 runs at exactly twice kind::f16 per SM), and
         # the fp64-equivalent rate (nao^3 per symmetric squaring) against the measured DGEMM
         tm, tn = (nao + 127) // 128, (nao + 63) // 64
         tiles = sum(min(2 * r + 2, tn) for r in range(tm))
-        kpad = ((nao + 63) // 64) * 64
+        kpad = ((nao + 31) // 32) * 32
         ops = 36.0 * 2.0 * 128 * 64 * kpad * tiles
         ms_avg = i8_ms / i8_calls
         achieved_tops = ops / (ms_avg * 1e-3) / 1e12
