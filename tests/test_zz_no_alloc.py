@@ -53,6 +53,17 @@ def test_noalloc_matches_the_allocating_entry_point_twice_in_a_row():
     np.testing.assert_allclose(_call_noalloc(z, xyz), api.corrections(z, xyz), rtol=1e-11, atol=1e-11)
 
 
+@pytest.mark.parametrize("method,smooth", [(0, True), (3, False), (4, False), (4, True)])
+def test_noalloc_covers_every_correction_branch(method, smooth):
+    # the smooth C6 dispersion, PM7-minus and the PM7-HH hydrogen-bond terms share the same
+    # static scratch: each branch against the allocating entry point, twice in a row
+    for z, xyz in (G.water_cluster(24, seed=5), G.alkane(7, seed=2)):
+        want = api.corrections(z, xyz, method=method, smooth=smooth)
+        for _ in range(2):
+            got = _call_noalloc(z, xyz, method=method, smooth=smooth)
+            np.testing.assert_allclose(got, want, rtol=1e-11, atol=1e-11)
+
+
 def test_noalloc_rejects_sizes_beyond_its_static_scratch():
     f, lib = _entry()
     limit = lib.pm7_corrections_noalloc_max_atoms()
