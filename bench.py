@@ -41,9 +41,6 @@ import time
 from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
-# the CPU checker (the OpenMP oracle) runs between GPU measurements in this process: its idle
-# worker threads must sleep rather than spin on the cores the engine's host threads use
-os.environ.setdefault("OMP_WAIT_POLICY", "PASSIVE")
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "pm7-rs_b200"))
 
@@ -821,6 +818,10 @@ def main():
         # CPU only: rank 0 runs, the other ranks exit without joining a process group
         run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
         return
+    # this arm runs the CPU checker (the OpenMP oracle) between GPU measurements: its idle worker
+    # threads must sleep rather than spin on the cores the engine's host threads use (set before
+    # the first OpenMP library loads; the reference arm keeps the default policy)
+    os.environ.setdefault("OMP_WAIT_POLICY", "PASSIVE")
     world, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":
