@@ -372,7 +372,6 @@ __global__ void __launch_bounds__(256) k_sp2_digits(int n, int ld8, const double
 // K bytes per pipeline stage (32-byte swizzle): with the epilogue's own staging tile, three
 // 48 KB stages fit beside it.
 constexpr int kKStage = 32;
-static int i8_kstage() { return kKStage; }
 
 // CTAs of the persistent step: one per SM (or per tile, when there are fewer tiles).
 static int i8_grid(int tiles) {
@@ -398,7 +397,7 @@ bool make_digit_maps(const int8_t *dig, int n, void *map_a, void *map_b) {
   const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)kDigits};
   const cuuint64_t strides[2] = {(cuuint64_t)ld8, (cuuint64_t)ld8 * n};
   const cuuint32_t estr[3] = {1, 1, 1};
-  const cuuint32_t ks = (cuuint32_t)i8_kstage();
+  const cuuint32_t ks = (cuuint32_t)kKStage;
   const cuuint32_t box_a[3] = {ks, IM, kDigits}, box_b[3] = {ks, IN, kDigits};
   void *maps[2] = {map_a, map_b};
   const cuuint32_t *boxes[2] = {box_a, box_b};
