@@ -375,11 +375,17 @@ constexpr int kKStage = 32;
 
 // CTAs of the persistent step: one per SM (or per tile, when there are fewer tiles).
 static int i8_grid(int tiles) {
+  static std::mutex mu;
   static int sms[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
-  int &c = sms[dev & 63];
-  if (c == 0 && cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) c = 148;
+  int c;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    int &slot = sms[dev & 63];
+    if (slot == 0 && cudaDeviceGetAttribute(&slot, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) slot = 148;
+    c = slot;
+  }
   return tiles < c ? tiles : c;
 }
 
